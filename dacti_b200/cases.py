@@ -1,0 +1,121 @@
+"""The benchmark and parity configurations as programmatic cases.
+
+DACTI's TOML initial conditions only express uniform and single-jump states
+(config/config.cpp:194-243), so the quadrant, shock-drop and random-batch cases are written here
+as ``x2p`` functions over cell centres, the way ``Config::ic.x2p`` is consumed by
+``Scene::init_domain`` (scene/scene.cpp:413-414). Coordinates are those of the reference: the root
+box is centred at the origin with side ``max(active_size)``.
+"""
+from __future__ import annotations
+
+import math
+from typing import Optional
+
+import numpy as np
+
+from .casefile import Case, SolverParams
+from .models import BcType, ModelId, ModelShape
+from .scene import BoundarySpec, SceneSpec, SphereObject, build_tree
+
+ZG = BoundarySpec(BcType.ZERO_GRADIENT)
+
+
+def _zg_box(D: int):
+    return [(ZG, ZG) for _ in range(D)]
+
+
+def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_cfl: float = 0.5) -> Case:
+    """Config 1: 2D Euler Lax-Liu configuration 3 on the unit square, quadrants split at x=y=0.
+
+    States (rho, u, v, p): TR (1.5,0,0,1.5), TL (0.5323,1.206,0,0.3), BL (0.138,1.206,1.206,0.029),
+    BR (0.5323,0,1.206,0.3); outflow (zero-gradient) boundaries; density-weighted Laplacian
+    indicator. The pair of thresholds (0.02, 0.05) is one for which the reference completes the run
+    to t = 0.3 (tighter pairs make the reference itself produce NaN near t = 0.29).
+    """
+    shape = ModelShape(ModelId.EULER, 2)
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        x, y = c[:, 0], c[:, 1]
+        out = np.empty((c.shape[0], 4))
+        tr = (x > 0) & (y > 0)
+        tl = (x <= 0) & (y > 0)
+        bl = (x <= 0) & (y <= 0)
+        br = (x > 0) & (y <= 0)
+        out[tr] = (1.5, 0.0, 0.0, 1.5)
+        out[tl] = (0.5323, 1.206, 0.0, 0.3)
+        out[bl] = (0.138, 1.206, 1.206, 0.029)
+        out[br] = (0.5323, 0.0, 1.206, 0.3)
+        return out
+
+    spec = SceneSpec(shape, (1.0, 1.0), base_level, base_level + levels, x2p, _zg_box(2))
+    prm = SolverParams(
+        side_length=1.0, active_size=(1.0, 1.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
+        weights=(1.0, 0.0, 0.0, 0.0),
+    )
+    return Case(build_tree(spec), prm)
+
+
+def normal_shock(rho1: float, p1: float, mach: float, gamma: float = 1.4, P0: float = 0.0):
+    """Post-shock (rho, u, p) behind a normal shock moving into gas at rest.
+
+    Same relations as config::compute_normal_shock (config/util.hpp:135-150).
+    """
+    c1 = math.sqrt(gamma * (p1 + P0) / rho1)
+    r_ratio = 1.0 - 2.0 / (gamma + 1) * (1 - 1 / (mach * mach))
+    r2 = rho1 / r_ratio
+    u2 = 2.0 / (gamma + 1) * (mach - 1 / mach) * c1
+    p2 = p1 * (((2 * P0 / p1 + 1) * (1 - r_ratio) * gamma + 1 + r_ratio) / ((r_ratio - 1) * gamma + 1 + r_ratio))
+    return r2, u2, p2
+
+
+def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: float = 8e-3, aspect: int = 2,
+               drop_radius: float = 0.5e-3, shock_x: float = -1.0e-3, mach: float = 1.5,
+               thresholds=(0.02, 0.05), max_cfl: float = 0.5, weights: Optional[tuple] = None) -> Case:
+    """Config 2: five-equation air-water shock-drop.
+
+    Domain ``length`` x ``length/aspect`` (x ``length/aspect``) with a ``2^base_level`` cell root
+    grid along x, ``levels`` refinement levels; water drop (stiffened gas gamma=4.4, pi_inf=6e8 Pa,
+    rho=1000) of ``drop_radius`` at the origin in air (gamma=1.4, rho=1.2, p=1e5); a Mach ``mach``
+    planar shock at x = ``shock_x`` moving in +x with the Rankine-Hugoniot post-shock state behind
+    it; volume fraction smeared with a tanh over the finest cell size. The inflow face carries the
+    post-shock state; all other faces are zero-gradient. Surface tension and viscosity are zero.
+    """
+    shape = ModelShape(ModelId.MULTI, dims)
+    E = shape.E
+    rho_w, rho_a, p0 = 1000.0, 1.2, 1.0e5
+    r2, u2, p2 = normal_shock(rho_a, p0, mach)
+    active = [length] + [length / aspect] * (dims - 1)
+
+    def state(rho_air: float, u: float, p: float) -> np.ndarray:
+        s = np.zeros(E)
+        s[0] = 0.0          # alpha1 rho1 (water)
+        s[1] = rho_air      # alpha2 rho2 (air)
+        s[2] = u
+        s[shape.ip] = p
+        s[shape.ia] = 0.0
+        return s
+
+    post = state(r2, u2, p2)
+    pre = state(rho_a, 0.0, p0)
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        out = np.where((c[:, 0] > shock_x)[:, None], pre[None, :], post[None, :])
+        return out.copy()
+
+    inflow = BoundarySpec(BcType.INFLOW, list(post), None, 0.0)
+    dbc = [(inflow, ZG)] + [(ZG, ZG) for _ in range(dims - 1)]
+    spec = SceneSpec(
+        shape, active, base_level, base_level + levels, x2p, dbc,
+        jump=(0, shock_x),
+        objects=[SphereObject((0.0, 0.0, 0.0), drop_radius, "droplet")],
+        diffuse_ic=True, rho_ref=(rho_w, rho_a),
+    )
+    if weights is None:
+        weights = (1e-3, 1.0) + (0.0,) * dims + (3e-6, 1.0)
+    prm = SolverParams(
+        side_length=length, active_size=active, periodic=[False] * dims, max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level, weights=weights,
+        gamma1=4.4, gamma2=1.4, P1=6.0e8, P2=0.0,
+    )
+    return Case(build_tree(spec), prm)

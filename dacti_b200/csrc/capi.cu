@@ -1,0 +1,86 @@
+// extern "C" entry points of include/dacti_gpu.h.
+#include "solver.cuh"
+
+#include <string>
+
+struct dg_solver {
+	dg::SolverBase *impl;
+};
+
+namespace {
+thread_local std::string g_create_error;
+
+template<typename Fn>
+int guarded(dg_solver *s, Fn &&fn) {
+	try {
+		fn();
+		return DG_OK;
+	} catch (const dg::dg_error &e) {
+		if (s && s->impl) s->impl->last_error = e.what();
+		else g_create_error = e.what();
+		return e.code;
+	} catch (const std::exception &e) {
+		if (s && s->impl) s->impl->last_error = e.what();
+		else g_create_error = e.what();
+		return DG_ERR_ARG;
+	}
+}
+}  // namespace
+
+extern "C" {
+
+int dg_create(const dg_case *c, dg_solver **out) {
+	if (!c || !out) return DG_ERR_ARG;
+	*out = nullptr;
+	return guarded(nullptr, [&] {
+		dg::SolverBase *impl = nullptr;
+		switch (c->model) {
+			case DG_EULER: impl = dg::make_solver_euler(*c); break;
+			case DG_NAVIER_STOKES: impl = dg::make_solver_ns(*c); break;
+			case DG_MULTI: impl = dg::make_solver_multi(*c); break;
+			default: throw dg::dg_error(DG_ERR_ARG, "unknown model id");
+		}
+		*out = new dg_solver{impl};
+	});
+}
+
+int dg_set_stream(dg_solver *s, void *stream) {
+	if (!s) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_stream((cudaStream_t) stream); });
+}
+
+int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) {
+	if (!s || !force_break || !global_dt) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->step(signal, force_break, global_dt, fn, user); });
+}
+
+int dg_cell_count(dg_solver *s, long long *n) {
+	if (!s || !n) return DG_ERR_ARG;
+	return guarded(s, [&] { *n = s->impl->cell_count(); });
+}
+
+int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out) {
+	if (!s || !levels || !data) return DG_ERR_ARG;
+	return guarded(s, [&] {
+		long long n = s->impl->read_cells(levels, data, max_cells);
+		if (n_out) *n_out = n;
+	});
+}
+
+int dg_get_stats(dg_solver *s, dg_stats *out) {
+	if (!s || !out) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->stats(out); });
+}
+
+const char *dg_last_error(dg_solver *s) {
+	if (!s) return g_create_error.c_str();
+	return s->impl->last_error.c_str();
+}
+
+void dg_destroy(dg_solver *s) {
+	if (!s) return;
+	delete s->impl;
+	delete s;
+}
+
+}  // extern "C"

@@ -1,0 +1,544 @@
+// Host side of the solver: node-pool management, the Integrator constructor sequence and the ACTI
+// level scheduler of Integrator::integrate, issuing the stage kernels of stages.cuh.
+#pragma once
+
+#include "../../include/dacti_gpu.h"
+#include "stages.cuh"
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace dg {
+
+struct dg_error : std::runtime_error {
+	int code;
+	dg_error(int c, const std::string &m) :
+	    std::runtime_error(m), code(c) {}
+};
+
+#define DG_CUDA(x)                                                                                     \
+	do {                                                                                               \
+		cudaError_t e_ = (x);                                                                          \
+		if (e_ != cudaSuccess)                                                                         \
+			throw ::dg::dg_error(DG_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_));         \
+	} while (0)
+
+class SolverBase {
+public:
+	virtual ~SolverBase() = default;
+	virtual void step(int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) = 0;
+	virtual long long cell_count() = 0;
+	virtual long long read_cells(int *levels, double *data, long long max_cells) = 0;
+	virtual void stats(dg_stats *out) = 0;
+	virtual void set_stream(cudaStream_t s) = 0;
+	std::string last_error;
+};
+
+inline int grid_for(long long n, int max_blocks = 148 * 16) {
+	long long b = (n + BLOCK - 1) / BLOCK;
+	if (b < 1) b = 1;
+	if (b > max_blocks) b = max_blocks;
+	return (int) b;
+}
+
+template<class M>
+class Solver : public SolverBase {
+	static constexpr int D = M::D, E = M::E, NC = 1 << D, NF = 2 * D;
+
+	cudaStream_t st_ = 0;
+	Consts C_{};
+	BcTable B_{};
+	Pool P_{};
+	Lists Ls_{};
+	Counters *d_cnt_ = nullptr;
+	Counters *h_cnt_ = nullptr;  // pinned
+	void *pool_mem_  = nullptr;
+	void *list_mem_  = nullptr;
+	void *bc_mem_    = nullptr;
+	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
+	double *d_read_    = nullptr;
+	int32_t *d_readlv_ = nullptr;
+	long long read_cap_ = 0;
+	int limiter_ = 0;
+
+	// scheduler state (integrator/integrator.hpp:46-58)
+	int acti_counter_[MAX_ACTI] = {};
+	double acti_time_[MAX_ACTI] = {};
+	int max_acti_ = 0;
+	double global_dt_ = -INFINITY;
+	long long n_substeps_ = 0, n_global_ = 0, updates_ = 0, n_gc_ = 0;
+	long long n_split_total_ = 0, n_unsplit_total_ = 0;
+	int stamp_ = 0;
+
+public:
+	explicit Solver(const dg_case &c) {
+		limiter_ = c.limiter;
+		setup_consts(c);
+		upload_bcs(c);
+		int cap = c.n_nodes + c.n_nodes / 2 + 1024;
+		alloc_pool(cap);
+		alloc_lists(cap);
+		DG_CUDA(cudaMalloc(&d_cnt_, sizeof(Counters)));
+		DG_CUDA(cudaMallocHost(&h_cnt_, sizeof(Counters)));
+		DG_CUDA(cudaMemset(d_cnt_, 0, sizeof(Counters)));
+		upload_tree(c);
+		construct();
+	}
+
+	~Solver() override {
+		cudaStreamSynchronize(st_);
+		cudaFree(pool_mem_);
+		cudaFree(list_mem_);
+		cudaFree(bc_mem_);
+		cudaFree(d_cnt_);
+		cudaFreeHost(h_cnt_);
+		cudaFree(d_leaves_);
+		cudaFree(d_read_);
+		cudaFree(d_readlv_);
+	}
+
+	void set_stream(cudaStream_t s) override { st_ = s; }
+
+	// ---------------------------------------------------------------------------------------
+	void setup_consts(const dg_case &c) {
+		const double *pr = c.params;
+		C_.side = pr[DG_P_SIDE];
+		for (int d = 0; d < 3; ++d) {
+			C_.active[d]   = pr[DG_P_ACTIVE0 + d];
+			C_.periodic[d] = pr[DG_P_PERIODIC0 + d] != 0.0;
+		}
+		C_.max_cfl              = pr[DG_P_MAX_CFL];
+		C_.min_err              = pr[DG_P_MIN_ERR];
+		C_.max_err              = pr[DG_P_MAX_ERR];
+		C_.max_refinement_level = (int) pr[DG_P_MAX_LEVEL];
+		max_dt_cfg_             = pr[DG_P_MAX_DT];
+		for (int q = 0; q < E; ++q) C_.weights[q] = c.weights[q];
+		ModelConsts &m = C_.m;
+		m.ns_mu = pr[DG_P_NS_MU];
+		m.ns_lambda = pr[DG_P_NS_LAMBDA];
+		m.gamma1 = pr[DG_P_GAMMA1];
+		m.gamma2 = pr[DG_P_GAMMA2];
+		m.P1 = pr[DG_P_P1];
+		m.P2 = pr[DG_P_P2];
+		m.cp1 = pr[DG_P_CP1];
+		m.cp2 = pr[DG_P_CP2];
+		m.cv1 = pr[DG_P_CV1];
+		m.cv2 = pr[DG_P_CV2];
+		m.mu1 = pr[DG_P_MU1];
+		m.mu2 = pr[DG_P_MU2];
+		m.lambda1 = pr[DG_P_LAMBDA1];
+		m.lambda2 = pr[DG_P_LAMBDA2];
+		m.sigma = pr[DG_P_SIGMA];
+		if (c.n_zones > MAX_ZONES) throw dg_error(DG_ERR_ARG, "too many refinement zones");
+		C_.n_zones = c.n_zones;
+		for (int z = 0; z < c.n_zones; ++z) {
+			for (int d = 0; d < 3; ++d) {
+				C_.zx0[z][d] = c.zones[7 * z + d];
+				C_.zx1[z][d] = c.zones[7 * z + 3 + d];
+			}
+			C_.zlevel[z] = (int) c.zones[7 * z + 6];
+		}
+		// Per-level size (exact halving from the root, integrator/domain.hpp:207), and volume/area
+		// evaluated with the same std::pow calls as Cell::volume / CellFace::area
+		// (integrator/cell.hpp:575-577, 622-624).
+		double s = C_.side;
+		for (int l = 0; l < MAX_TREE; ++l) {
+			C_.size[l] = s;
+			C_.vol[l]  = std::pow(s, D);
+			C_.area[l] = std::pow(s, D - 1);
+			for (int d = 0; d < 3; ++d) {
+				if (d >= D) {
+					C_.a0[l][d] = 0;
+					C_.na[l][d] = 1;
+					continue;
+				}
+				// active box [-A/2, A/2] in cells of level l of the root box [-S/2, S/2]
+				double cells = C_.active[d] / s;
+				double off   = 0.5 * (C_.side - C_.active[d]) / s;
+				long long nc = std::llround(cells), oc = std::llround(off);
+				C_.na[l][d]  = (int) nc;
+				C_.a0[l][d]  = (int) oc;
+				if (l >= (int) pr[DG_P_MIN_LEVEL] && (std::fabs(cells - nc) > 1e-9 || std::fabs(off - oc) > 1e-9))
+					throw dg_error(DG_ERR_UNSUPPORTED, "active box not aligned with the cell grid at the base level");
+			}
+			s = 0.5 * s;
+		}
+	}
+
+	void upload_bcs(const dg_case &c) {
+		int n        = c.n_bc > 0 ? c.n_bc : 1;
+		size_t bytes = sizeof(int) * n + sizeof(double) * n * (E + D + 1) + 1024;
+		DG_CUDA(cudaMalloc(&bc_mem_, bytes));
+		char *b   = (char *) bc_mem_;
+		int *type = (int *) b;
+		b += ((sizeof(int) * n + 255) / 256) * 256;
+		double *pin = (double *) b;
+		double *nrm = pin + (size_t) n * E;
+		double *fad = nrm + (size_t) n * D;
+		if (c.n_bc > 0) {
+			DG_CUDA(cudaMemcpy(type, c.bc_type, sizeof(int) * c.n_bc, cudaMemcpyHostToDevice));
+			DG_CUDA(cudaMemcpy(pin, c.bc_p_in, sizeof(double) * c.n_bc * E, cudaMemcpyHostToDevice));
+			DG_CUDA(cudaMemcpy(nrm, c.bc_normal, sizeof(double) * c.n_bc * D, cudaMemcpyHostToDevice));
+			DG_CUDA(cudaMemcpy(fad, c.bc_fade_in, sizeof(double) * c.n_bc, cudaMemcpyHostToDevice));
+		}
+		B_ = BcTable{c.n_bc, type, pin, nrm, fad};
+	}
+
+	// ---------------------------------------------------------------------------------------
+	// Node pool: every field is an array of `cap` entries per component.
+	struct Field {
+		void **ptr;
+		size_t elem;
+		int comps;
+	};
+
+	std::vector<Field> fields(Pool &P) {
+		return {
+		    {(void **) &P.parent, 4, 1}, {(void **) &P.child, 4, NC}, {(void **) &P.level, 1, 1},
+		    {(void **) &P.acti, 1, 1}, {(void **) &P.clu, 1, 1}, {(void **) &P.flags, 4, 1},
+		    {(void **) &P.coord, 4, D}, {(void **) &P.nbr, 4, NF}, {(void **) &P.bc, 2, NF},
+		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
+		    {(void **) &P.p, 8, E}, {(void **) &P.rhs, 8, E}, {(void **) &P.slope, 8, D * E},
+		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
+		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
+		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.op, 1, 1},
+		    {(void **) &P.tmp, 8, 1},
+		};
+	}
+
+	static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+	void *carve_pool(Pool &P, int cap) {
+		P.cap        = cap;
+		auto fs      = fields(P);
+		size_t total = 0;
+		for (auto &f: fs) total += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
+		void *mem = nullptr;
+		DG_CUDA(cudaMalloc(&mem, total));
+		DG_CUDA(cudaMemsetAsync(mem, 0, total, st_));
+		char *b = (char *) mem;
+		for (auto &f: fs) {
+			*f.ptr = b;
+			b += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
+		}
+		return mem;
+	}
+
+	void alloc_pool(int cap) { pool_mem_ = carve_pool(P_, cap); }
+
+	void grow_pool(int new_cap) {
+		Pool NP{};
+		void *mem = carve_pool(NP, new_cap);
+		auto fo = fields(P_), fn = fields(NP);
+		for (size_t k = 0; k < fo.size(); ++k) {
+			if (fo[k].comps <= 0) continue;
+			DG_CUDA(cudaMemcpy2DAsync(*fn[k].ptr, fn[k].elem * (size_t) new_cap, *fo[k].ptr,
+			                          fo[k].elem * (size_t) P_.cap, fo[k].elem * (size_t) P_.cap, fo[k].comps,
+			                          cudaMemcpyDeviceToDevice, st_));
+		}
+		DG_CUDA(cudaStreamSynchronize(st_));
+		cudaFree(pool_mem_);
+		pool_mem_ = mem;
+		P_        = NP;
+		// lists grow with the pool
+		Lists old = Ls_;
+		void *old_mem = list_mem_;
+		int old_cap   = list_cap_;
+		alloc_lists(new_cap);
+		for (int l = 0; l < MAX_ACTI; ++l) {
+			DG_CUDA(cudaMemcpyAsync(Ls_.clu[l], old.clu[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
+			DG_CUDA(cudaMemcpyAsync(Ls_.buf[l], old.buf[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
+		}
+		DG_CUDA(cudaStreamSynchronize(st_));
+		cudaFree(old_mem);
+	}
+
+	int list_cap_ = 0;
+	void alloc_lists(int cap) {
+		const int nlists = 2 * MAX_ACTI + 6;
+		size_t one       = align_up(sizeof(int32_t) * (size_t) cap);
+		DG_CUDA(cudaMalloc(&list_mem_, one * nlists));
+		char *b = (char *) list_mem_;
+		for (int l = 0; l < MAX_ACTI; ++l) {
+			Ls_.clu[l] = (int32_t *) b;
+			b += one;
+			Ls_.buf[l] = (int32_t *) b;
+			b += one;
+		}
+		Ls_.tmp     = (int32_t *) b;
+		b += one;
+		Ls_.recv    = (int32_t *) b;
+		b += one;
+		Ls_.split   = (int32_t *) b;
+		b += one;
+		Ls_.unsplit = (int32_t *) b;
+		b += one;
+		Ls_.fresh   = (int32_t *) b;
+		b += one;
+		Ls_.upd     = (int32_t *) b;
+		list_cap_   = cap;
+	}
+
+	// ---------------------------------------------------------------------------------------
+	template<typename T>
+	void upload_soa(T *dst, const T *src_rowmajor, int n, int comps) {
+		std::vector<T> tmp((size_t) n * comps);
+		for (int i = 0; i < n; ++i)
+			for (int c = 0; c < comps; ++c) tmp[(size_t) c * n + i] = src_rowmajor[(size_t) i * comps + c];
+		for (int c = 0; c < comps; ++c)
+			DG_CUDA(cudaMemcpy(dst + (size_t) c * P_.cap, tmp.data() + (size_t) c * n, sizeof(T) * n, cudaMemcpyHostToDevice));
+	}
+
+	std::vector<int32_t> active_leaves_;
+
+	void upload_tree(const dg_case &c) {
+		const int n = c.n_nodes;
+		DG_CUDA(cudaStreamSynchronize(st_));
+		std::vector<int8_t> lv(n), ac(n, -1), cl(n, CLU_NONE);
+		std::vector<int32_t> coord((size_t) n * D, 0);
+		std::vector<int16_t> bc((size_t) n * NF);
+		for (int i = 0; i < n; ++i) {
+			lv[i] = (int8_t) c.level[i];
+			for (int f = 0; f < NF; ++f) bc[(size_t) i * NF + f] = (int16_t) c.bc[(size_t) i * NF + f];
+		}
+		// integer coordinates, parents before children
+		std::vector<int> order;
+		order.reserve(n);
+		if (n > 1) order.push_back(1);
+		for (size_t h = 0; h < order.size(); ++h) {
+			int x = order[h];
+			if (c.flags[x] & DG_F_LEAF) continue;
+			for (int k = 0; k < NC; ++k) {
+				int ch = c.children[(size_t) x * NC + k];
+				if (ch <= 0) continue;
+				for (int d = 0; d < D; ++d) coord[(size_t) ch * D + d] = 2 * coord[(size_t) x * D + d] + ((k >> d) & 1);
+				order.push_back(ch);
+			}
+		}
+		upload_soa(P_.parent, c.parent, n, 1);
+		upload_soa(P_.child, c.children, n, NC);
+		upload_soa(P_.level, lv.data(), n, 1);
+		upload_soa(P_.acti, ac.data(), n, 1);
+		upload_soa(P_.clu, cl.data(), n, 1);
+		upload_soa(P_.flags, (const uint32_t *) c.flags, n, 1);
+		upload_soa(P_.coord, coord.data(), n, D);
+		upload_soa(P_.bc, bc.data(), n, NF);
+		upload_soa(P_.center, c.center, n, D);
+		upload_soa(P_.p, c.p, n, E);
+		active_leaves_.clear();
+		for (int i = 1; i < n; ++i)
+			if ((c.flags[i] & DG_F_LEAF) && (c.flags[i] & DG_F_ACTIVE)) active_leaves_.push_back(i);
+		h_cnt_->top = n;
+		DG_CUDA(cudaMemcpy(&d_cnt_->top, &n, sizeof(int), cudaMemcpyHostToDevice));
+	}
+
+	// Integrator constructor body (integrator/integrator.hpp:100-160).
+	void construct() {
+		const int n = (int) active_leaves_.size();
+		DG_CUDA(cudaMalloc(&d_leaves_, sizeof(int32_t) * (n > 0 ? n : 1)));
+		DG_CUDA(cudaMemcpy(d_leaves_, active_leaves_.data(), sizeof(int32_t) * n, cudaMemcpyHostToDevice));
+		const int g = grid_for(n);
+		k_init_cells<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, d_cnt_);
+		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
+		k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, d_leaves_, n, limiter_, d_cnt_);
+		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n);
+		DG_CUDA(cudaGetLastError());
+		sync_counters();
+		global_dt_ = std::fmax(-INFINITY, h_cnt_->dmax);
+		global_dt_ = std::min(0.9 * global_dt_, max_dt_cfg());
+		k_assign<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, global_dt_, Ls_, d_cnt_);
+		DG_CUDA(cudaGetLastError());
+		sync_counters();
+		check_status();
+		max_acti_ = 0;
+		for (int l = 0; l < MAX_ACTI; ++l)
+			if (h_cnt_->clu[l] > 0) max_acti_ = std::max(max_acti_, l);
+	}
+
+	double max_dt_cfg_ = 1.0;
+	double max_dt_cfg() const { return max_dt_cfg_; }
+
+public:
+	void set_max_dt(double v) { max_dt_cfg_ = v; }
+
+private:
+	void multiphase_aux(const int32_t *list, int n) {
+		// α smoothing, normals and curvature are added with the multiphase stages.
+		(void) list;
+		(void) n;
+		throw dg_error(DG_ERR_UNSUPPORTED, "multiphase auxiliary stages are not built yet");
+	}
+
+	void sync_counters() {
+		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters), cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaStreamSynchronize(st_));
+	}
+
+	void check_status() {
+		uint32_t s = h_cnt_->status & ~ST_NAN;
+		if (s & ST_CAPACITY) throw dg_error(DG_ERR_CAPACITY, "device list or pool capacity exceeded");
+		if (s & ST_DEPTH) throw dg_error(DG_ERR_DEPTH, "tree level jump deeper than supported");
+		if (s & ST_MISSING_BC) throw dg_error(DG_ERR_MISSING_BC, "face without neighbour or boundary condition");
+		if (s & ST_SPLIT_UNSPLIT) throw dg_error(DG_ERR_UNSUPPORTED, "cell both split and coarsened in one substep");
+	}
+
+	// One ACTI-level substep: impl/integrate.hpp:277-299 minus the host bookkeeping.
+	void substep(int L) {
+		const int n      = h_cnt_->clu[L];
+		const double dtL = global_dt_ / (double) (1 << L);
+		// room for every cell of the cluster to split
+		const long long need = (long long) h_cnt_->top + (long long) NC * n + 16;
+		if (need > P_.cap) grow_pool((int) std::min<long long>(std::max<long long>(need, (long long) P_.cap * 3 / 2), 2000000000LL));
+		const int stamp_recv = ++stamp_;
+		const int stamp_upd  = ++stamp_;
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_recv, 0, sizeof(int) * 7, st_));
+		const int g        = grid_for(n);
+		int32_t *list      = Ls_.clu[L];
+		const int counterL = acti_counter_[L];
+
+		k_flux<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL, stamp_recv, 1, Ls_.recv, d_cnt_);
+		k_flux<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0, L, dtL,
+		                                                          stamp_recv, 0, Ls_.recv, d_cnt_);
+		k_update<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
+		k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		if constexpr (M::MULTI) multiphase_aux(list, n);
+		k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
+		k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_);
+		k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, d_cnt_);
+		k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, d_cnt_);
+		const int gf = grid_for((long long) n * (NC + 1));
+		k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
+		k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, 0, Ls_.upd, d_cnt_);
+		k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_);
+		k_reassign<M><<<gf, BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, &d_cnt_->n_new, 0, L, dtL, counterL, Ls_, d_cnt_);
+		std::swap(Ls_.clu[L], Ls_.tmp);
+		k_set_count<<<1, 1, 0, st_>>>(&d_cnt_->clu[L], &d_cnt_->n_tmp);
+		DG_CUDA(cudaGetLastError());
+	}
+
+	void flush(int L) {
+		if (h_cnt_->buf[L] == 0) return;
+		k_flush<<<grid_for(h_cnt_->buf[L]), BLOCK, 0, st_>>>(P_, Ls_.buf[L], &d_cnt_->buf[L], Ls_.clu[L], &d_cnt_->clu[L], L,
+		                                                   d_cnt_);
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->buf[L], 0, sizeof(int), st_));
+		DG_CUDA(cudaGetLastError());
+	}
+
+public:
+	// Integrator::integrate (impl/integrate.hpp:12-87)
+	void step(int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) override {
+		C_.signal   = signal;
+		*force_break = 0;
+		const int top_seq = 1 << (MAX_ACTI - 1);
+		int seq           = 0;
+		while (true) {
+			int finest = max_acti_;
+			for (int l = MAX_ACTI - 1; l > finest; --l)
+				if (h_cnt_->clu[l] > 0) {
+					finest = l;
+					break;
+				}
+			const int stride = 1 << (MAX_ACTI - 1 - finest);
+			seq              = (seq / stride + 1) * stride;
+			if (seq > top_seq) break;
+			for (int l = 0; l < MAX_ACTI; ++l) {
+				if (seq % (1 << l) != 0) continue;
+				const int L = MAX_ACTI - l - 1;
+				if (h_cnt_->clu[L] > 0 && L > max_acti_) {
+					max_acti_     = L;
+					acti_time_[L] = acti_time_[L - 1];
+				}
+				if (L > max_acti_) continue;
+				substep(L);
+				acti_counter_[L] = (acti_counter_[L] + 1) % 2;
+				const double dtL = global_dt_ / (double) (1 << L);
+				acti_time_[L] += dtL;
+				flush(L);
+				sync_counters();
+				check_status();
+				n_split_total_ += h_cnt_->n_split;
+				n_unsplit_total_ += h_cnt_->n_unsplit;
+				n_substeps_++;
+				updates_ += h_cnt_->clu[L];
+				if (h_cnt_->status & ST_NAN) {
+					*force_break = 1;
+					*global_dt   = global_dt_;
+					return;
+				}
+				if (fn) fn(user, L, acti_time_[L], (int) n_substeps_, dtL, h_cnt_->clu[L]);
+			}
+		}
+		long long n_in = 0;
+		for (int l = 0; l < MAX_ACTI; ++l) n_in += h_cnt_->clu[l];
+		n_global_++;
+		if ((double) n_in / (double) (h_cnt_->top - 1) < 0.2) gc();
+		*global_dt = global_dt_;
+	}
+
+private:
+	void gc() { throw dg_error(DG_ERR_UNSUPPORTED, "garbage collection (Domain::gc) is not built yet"); }
+
+public:
+	long long cell_count() override {
+		long long n = 0;
+		for (int l = 0; l < MAX_ACTI; ++l) n += h_cnt_->clu[l] + h_cnt_->buf[l];
+		return n;
+	}
+
+	long long read_cells(int *levels, double *data, long long max_cells) override {
+		constexpr int W = D + 1 + 2 * E + 3;
+		long long n = cell_count();
+		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
+		if (n > read_cap_) {
+			cudaFree(d_read_);
+			cudaFree(d_readlv_);
+			DG_CUDA(cudaMalloc(&d_read_, sizeof(double) * W * n));
+			DG_CUDA(cudaMalloc(&d_readlv_, sizeof(int32_t) * 2 * n));
+			read_cap_ = n;
+		}
+		long long base = 0;
+		for (int pass = 0; pass < 2; ++pass) {
+			for (int l = 0; l < MAX_ACTI; ++l) {
+				int cnt = pass == 0 ? h_cnt_->clu[l] : h_cnt_->buf[l];
+				if (cnt == 0) continue;
+				const int32_t *list = pass == 0 ? Ls_.clu[l] : Ls_.buf[l];
+				k_gather_cells<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, (int) base, d_read_, d_readlv_);
+				base += cnt;
+			}
+		}
+		DG_CUDA(cudaGetLastError());
+		DG_CUDA(cudaMemcpyAsync(data, d_read_, sizeof(double) * W * n, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaMemcpyAsync(levels, d_readlv_, sizeof(int32_t) * 2 * n, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaStreamSynchronize(st_));
+		return n;
+	}
+
+	void stats(dg_stats *o) override {
+		std::memset(o, 0, sizeof(*o));
+		for (int l = 0; l < MAX_ACTI; ++l) {
+			o->n_clusters[l]   = h_cnt_->clu[l];
+			o->n_buffers[l]    = h_cnt_->buf[l];
+			o->acti_time[l]    = acti_time_[l];
+			o->acti_counter[l] = acti_counter_[l];
+		}
+		o->tree_size      = h_cnt_->top;
+		o->n_splits       = n_split_total_;
+		o->n_unsplits     = n_unsplit_total_;
+		o->n_gc           = n_gc_;
+		o->n_substeps     = n_substeps_;
+		o->n_global_steps = n_global_;
+		o->cell_updates   = updates_;
+		o->max_acti_level = max_acti_;
+		o->global_dt      = global_dt_;
+	}
+};
+
+SolverBase *make_solver_euler(const dg_case &c);
+SolverBase *make_solver_ns(const dg_case &c);
+SolverBase *make_solver_multi(const dg_case &c);
+
+}  // namespace dg

@@ -1,0 +1,10 @@
+// Instantiation of the solver for the Euler model in 2D and 3D.
+#include "solver.cuh"
+
+namespace dg {
+SolverBase *make_solver_euler(const dg_case &c) {
+	if (c.dims == 2) return new Solver<Euler<2>>(c);
+	if (c.dims == 3) return new Solver<Euler<3>>(c);
+	throw dg_error(DG_ERR_ARG, "dims must be 2 or 3");
+}
+}  // namespace dg

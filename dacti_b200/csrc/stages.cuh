@@ -1,0 +1,870 @@
+// Stage kernels of one ACTI-level substep (impl/integrate.hpp:26-67), one thread per cell.
+//
+// Flux accumulation is gather based and free of floating-point atomics: every cell of the running
+// cluster sums, in a fixed face order, the fluxes it owns plus the fluxes its same-cluster
+// neighbours own across shared faces (re-evaluating them with identical inputs gives identical
+// values); cells of slower time levels that receive fluxes (the coarse side of the LTS coupling,
+// impl/flux.hpp:82-91) are collected into a receiver list and gather the same way in a second pass.
+// The result is independent of list order and of scheduling, so runs are bitwise reproducible.
+#pragma once
+
+#include "tree.cuh"
+
+namespace dg {
+
+constexpr int BLOCK = 256;
+
+__device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
+__device__ __forceinline__ int gstride() { return gridDim.x * blockDim.x; }
+
+__device__ __forceinline__ void append(int32_t *list, int *count, int value, int cap, uint32_t *status) {
+	int pos = atomicAdd(count, 1);
+	if (pos < cap) list[pos] = value;
+	else set_status(status, ST_CAPACITY);
+}
+
+// --------------------------------------------------------------------------------------------
+// Interior face flux: Model::flux(left, right, face) with the face of the owning cell
+// (impl/flux.hpp:32-39, 80-91; model/euler.hpp:156-200, navier_stokes.hpp:387-408,
+// multi.hpp:249-302). `dir_o` is the owner's direction towards `other`; for dir_o == 0 the owner is
+// the right state and the face keeps the owner's centre (the reference relabels face.dir = 1).
+// `shift` moves the non-owner's centre by the active size across a periodic wrap.
+// --------------------------------------------------------------------------------------------
+template<class M>
+__device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
+                                           double dtL, double *F) {
+	constexpr int E = M::E, D = M::D;
+	const int cap   = P.cap;
+	const int lo    = P.level[owner];
+	const double so = C.size[lo];
+	const double co = at(P.center, cap, dim, owner);
+	const double fc = co + so * (dir_o - 0.5);
+	const double t0 = P.t[owner];
+	const double t1 = t0 + dtL;
+	const double area = C.area[lo];
+
+	double cx = at(P.center, cap, dim, other);
+	if (C.periodic[dim]) {
+		if (dir_o == 1) {
+			if (co + so > 0.5 * C.active[dim]) cx += C.active[dim];
+		} else {
+			if (co - so < -0.5 * C.active[dim]) cx -= C.active[dim];
+		}
+	}
+	const int iL = dir_o == 1 ? owner : other;
+	const int iR = dir_o == 1 ? other : owner;
+	const double cL = dir_o == 1 ? co : cx;
+	const double cR = dir_o == 1 ? cx : co;
+
+	const double tm   = 0.5 * (t1 + t0);
+	const double dt_n = tm - P.t[iL];
+	const double dt_p = tm - P.t[iR];
+	double pn[E], pp[E];
+	for (int q = 0; q < E; ++q) {
+		double v = at(P.p, cap, q, iL) + at(P.slope, cap, dim * E + q, iL) * (fc - cL);
+		pn[q]    = v - at(P.rhs, cap, q, iL) * dt_n;
+		double w = at(P.p, cap, q, iR) + at(P.slope, cap, dim * E + q, iR) * (fc - cR);
+		pp[q]    = w - at(P.rhs, cap, q, iR) * dt_p;
+	}
+	double ka = 0.0;
+	if constexpr (M::MULTI) ka = 0.5 * (at(P.k, cap, M::KAPPA, iL) + at(P.k, cap, M::KAPPA, iR));
+	double pm[E];
+	middle_state<M>(C.m, pn, pp, ka, dim, pm);
+	phys_flux<M>(C.m, pm, 0.0, dim, false, F);
+	const double dtf = t1 - t0;
+
+	if constexpr (M::MULTI) {
+		constexpr int IA = M::IA, IU = M::IU, IP = M::IP;
+		const double a = pm[IA];
+		if (a > 1e-5 && a < 1 - 1e-5) {
+			double n  = 0.5 * (at(P.k, cap, M::IKN + dim, iL) + at(P.k, cap, M::IKN + dim, iR));
+			double uc = MULTI_UC * fabs(pm[IU + dim]) * n;
+			double ke = 0.0;
+			for (int i = 0; i < D; ++i) {
+				F[IU + i] += uc * ((1 - a) * pm[0] - a * pm[1]) * pm[IU + i];
+				ke += 0.5 * pm[IU + i] * pm[IU + i];
+			}
+			F[0] += uc * (1 - a) * pm[0];
+			F[1] += uc * (-a) * pm[1];
+			const ModelConsts &m = C.m;
+			F[IP] += uc * ((1 - a) * pm[0] - a * pm[1]) * ke +
+			         uc * (1 - a) * a *
+			             (pm[IP] * (1 / (m.gamma1 - 1) - 1 / (m.gamma2 - 1)) + m.gamma1 * m.P1 / (m.gamma1 - 1) -
+			              m.gamma2 * m.P2 / (m.gamma2 - 1));
+			F[IA] += uc * (1 - a) * a;
+		}
+	}
+	if constexpr (M::VISC) {
+		constexpr int G = M::G;
+		double du[D * G], vel[D], fv[D + 1];
+		for (int i = 0; i < D; ++i)
+			for (int g = 0; g < G; ++g) du[i * G + g] = 0.5 * (at(P.grad, cap, i * G + g, iL) + at(P.grad, cap, i * G + g, iR));
+		for (int i = 0; i < D; ++i) vel[i] = 0.5 * (at(P.p, cap, M::IU + i, iL) + at(P.p, cap, M::IU + i, iR));
+		if constexpr (M::MULTI) {
+			// multi.hpp:287-301: viscous and heat terms enter before the area * dt scaling
+			visc_flux<D>(du, G, vel, visc_mu<M>(C.m, pm), dim, fv);
+			for (int i = 0; i <= D; ++i) F[M::IU + i] -= fv[i];
+			F[M::IU + D] -= du[dim * G + M::DT] * visc_lambda<M>(C.m, pm);
+			for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
+		} else {
+			// navier_stokes.hpp:387-408: convective part scaled first, then scaled viscous/heat terms
+			for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
+			visc_flux<D>(du, G, vel, C.m.ns_mu, dim, fv);
+			for (int i = 0; i <= D; ++i) F[M::IU + i] -= fv[i] * area * dtf;
+			double fh = C.m.ns_lambda * du[dim * G + M::DT] * area * dtf;
+			F[M::IU + D] -= fh;
+		}
+	} else {
+		for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
+	}
+}
+
+// Boundary::boundary_flux (integrator/boundary.hpp:130-160), from the cell-centre state.
+template<class M>
+__device__ __noinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
+                                           int dir, double dtL, double *F) {
+	constexpr int E = M::E, D = M::D;
+	const int cap = P.cap;
+	double pc[E], pb[E];
+	load_p<M>(P, i, pc);
+	const double t0 = P.t[i];
+	const double t1 = t0 + dtL;
+	boundary_value<M>(C.m, B, b, pc, t0, pb);
+	const int type = B.type[b];
+	if (type == BC_FREESLIP) {
+		phys_flux<M>(C.m, pc, pb[M::IU + dim], dim, true, F);
+	} else if (type == BC_NOSLIP) {
+		for (int q = 0; q < M::F; ++q) F[q] = 0.0;
+		F[M::IU + dim] = pb[M::IP];
+	} else {
+		double pm[E];
+		middle_state<M>(C.m, pb, pc, 0.0, dim, pm);
+		phys_flux<M>(C.m, pm, 0.0, dim, false, F);
+	}
+	if constexpr (M::VISC) {
+		constexpr int G = M::G;
+		double g[D * G], z[D], fv[D + 1];
+		for (int c = 0; c < D * G; ++c) g[c] = at(P.grad, cap, c, i);
+		for (int d = 0; d < D; ++d) z[d] = 0.0;
+		visc_flux<D>(g, G, z, visc_mu<M>(C.m, pc), dim, fv);
+		for (int k = 0; k <= D; ++k) F[M::IU + k] -= fv[k];
+	}
+	const double area = C.area[P.level[i]];
+	const double dirn = (double) (2 * dir - 1);
+	for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * (t1 - t0) * dirn;
+}
+
+template<int NFL>
+__device__ __forceinline__ void acc_add(double *acc, const double *F, bool plus) {
+	if (plus)
+		for (int q = 0; q < NFL; ++q) acc[q] += F[q];
+	else
+		for (int q = 0; q < NFL; ++q) acc[q] -= F[q];
+}
+
+// Adds to `acc` the fluxes owned by running-cluster cells across face (dim, dir) of cell i whose
+// neighbour slot is nb (a non-owning side's view of impl/flux.hpp:58-59).
+template<class M>
+__device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t *status, int i, int nb, int dim,
+                                       int dir, int L, double dtL, double *acc) {
+	const int cap = P.cap;
+	const int li = P.level[i], ai = P.acti[i];
+	const int dn = 1 - dir;  // owner's direction towards i
+	double F[M::F];
+	if (P.flags[nb] & F_LEAF) {
+		if (P.level[nb] == li && P.clu[nb] == L) {
+			const int an = P.acti[nb];
+			if (ai <= an && (dn == 1 || ai < an)) {
+				interior_flux<M>(P, C, nb, i, dim, dn, dtL, F);
+				acc_add<M::F>(acc, F, dn == 1);
+			}
+		}
+		return;
+	}
+	// finer cells across the face: the children (or grandchildren) of nb on its side facing i
+	for (int c = 0; c < (1 << M::D); ++c) {
+		if (((c >> dim) & 1) != dn) continue;
+		const int ch = P.child[(size_t) c * cap + nb];
+		if (P.flags[ch] & F_LEAF) {
+			if (P.clu[ch] == L && ai <= P.acti[ch]) {
+				interior_flux<M>(P, C, ch, i, dim, dn, dtL, F);
+				acc_add<M::F>(acc, F, dn == 1);
+			}
+			continue;
+		}
+		for (int g = 0; g < (1 << M::D); ++g) {
+			if (((g >> dim) & 1) != dn) continue;
+			const int gc = P.child[(size_t) g * cap + ch];
+			if (!(P.flags[gc] & F_LEAF)) {
+				set_status(status, ST_DEPTH);
+				continue;
+			}
+			if (P.clu[gc] == L && ai <= P.acti[gc]) {
+				interior_flux<M>(P, C, gc, i, dim, dn, dtL, F);
+				acc_add<M::F>(acc, F, dn == 1);
+			}
+		}
+	}
+}
+
+// flux_update (impl/flux.hpp:11-97). cluster_mode: cells of cluster L (own faces + same-cluster
+// owners, marking receivers); otherwise: receivers (fluxes owned by cluster-L neighbours only).
+template<class M>
+__global__ void k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr, int n_host, int L,
+                       double dtL, int stamp, int cluster_mode, int32_t *recv, Counters *cnt) {
+	const int n   = n_ptr ? *n_ptr : n_host;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i  = list[tid];
+		const int li = P.level[i], ai = P.acti[i];
+		double acc[M::F];
+		for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
+		double F[M::F];
+		for (int dim = 0; dim < M::D; ++dim) {
+			for (int dir = 0; dir < 2; ++dir) {
+				const int f  = 2 * dim + dir;
+				const int nb = P.nbr[(size_t) f * cap + i];
+				if (nb == 0) {
+					if (cluster_mode) {
+						const int b = P.bc[(size_t) f * cap + i];
+						if (b < 0) {
+							set_status(&cnt->status, ST_MISSING_BC);
+							continue;
+						}
+						boundary_flux<M>(P, C, B, i, b, dim, dir, dtL, F);
+						acc_add<M::F>(acc, F, false);
+					}
+					continue;
+				}
+				if (cluster_mode) {
+					const uint32_t fn = P.flags[nb];
+					const int ln = P.level[nb], an = P.acti[nb];
+					const bool owned = (fn & F_LEAF) && an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)));
+					if (owned) {
+						interior_flux<M>(P, C, i, nb, dim, dir, dtL, F);
+						acc_add<M::F>(acc, F, dir == 0);
+						if (P.clu[nb] != L) {
+							if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
+						}
+						continue;
+					}
+				}
+				gather_owned_by_others<M>(P, C, &cnt->status, i, nb, dim, dir, L, dtL, acc);
+			}
+		}
+		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] += acc[q];
+	}
+}
+
+// cell_update (impl/cell_update.hpp:10-90)
+template<class M>
+__global__ void k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, Counters *cnt) {
+	constexpr int E = M::E;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double pold[E], u[E], du[M::F], p[E];
+		load_p<M>(P, i, pold);
+		for (int q = 0; q < E; ++q) u[q] = at(P.u, cap, q, i);
+		double gold[M::G > 0 ? M::G : 1];
+		grad_input<M>(C.m, pold, gold);
+		const double V = C.vol[P.level[i]];
+		for (int q = 0; q < M::F; ++q) du[q] = at(P.flux, cap, q, i) / V;
+		for (int q = 0; q < E; ++q) u[q] += du[q];
+		if constexpr (M::MULTI) {
+			if (!C.signal) {
+				if (u[M::IA] > 0.001)
+					for (int k = M::IU; k < M::IU + M::D; ++k) u[k] = 0.0;
+			}
+			// source (model/multi.hpp:186-203) from the pre-update state
+			const double kap = at(P.k, cap, M::KAPPA, i);
+			const double sg  = C.m.sigma;
+			double s[E];
+			for (int q = 0; q < E; ++q) s[q] = 0.0;
+			for (int d = 0; d < M::D; ++d) s[M::IU + d] = -sg * kap * du[M::IA + 2 + d];
+			s[M::IP] = sg * kap * (-du[M::IA] + pold[M::IA] * du[M::IA + 1]);
+			s[M::IA] = -pold[M::IA] * du[M::IA + 1];
+			for (int q = 0; q < E; ++q) u[q] = u[q] + s[q];
+		}
+		prim_from_cons<M>(C.m, u, p);
+		if (isnan(p[M::IP]) || isnan(p[0])) set_status(&cnt->status, ST_NAN);
+		if constexpr (M::MULTI) {
+			p[0] = smax(p[0], 1e-3);
+			p[1] = smax(p[1], 1e-6);
+		} else {
+			p[0] = smax(p[0], 1e-3);
+		}
+		p[M::IP] = smax(p[M::IP], 1e-3);
+		cons_from_prim<M>(C.m, p, u);
+		if constexpr (M::G > 0) {
+			double gnew[M::G];
+			grad_input<M>(C.m, p, gnew);
+			for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = (gnew[g] - gold[g]) / dtL;
+		}
+		if constexpr (M::MULTI) {
+			P.k[(size_t) 0 * cap + i]        = C.m.mu1 * p[M::IA] + C.m.mu2 * (1 - p[M::IA]);
+			P.k[(size_t) M::ALPHAS * cap + i] = p[M::IA];
+		}
+		for (int q = 0; q < E; ++q) {
+			P.u[(size_t) q * cap + i] = u[q];
+			P.p[(size_t) q * cap + i] = p[q];
+		}
+		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
+		P.t[i] = P.t[i] + dtL;
+	}
+}
+
+// State of the neighbour across face (dim, dir) as compute_slope sees it (impl/slopes.hpp:208-246):
+// a ghost at distance h for boundaries, the recursive child mean for finer neighbours.
+template<class M>
+__device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int i, int dim, int dir,
+                           const double *pc, double *pv, double &x, double &tv) {
+	const int cap = P.cap;
+	const int nb  = P.nbr[(size_t) (2 * dim + dir) * cap + i];
+	const double h = C.size[P.level[i]];
+	if (nb == 0) {
+		const int b = P.bc[(size_t) (2 * dim + dir) * cap + i];
+		if (b < 0) {
+			set_status(status, ST_MISSING_BC);
+			for (int q = 0; q < M::E; ++q) pv[q] = pc[q];
+		} else {
+			boundary_value<M>(C.m, B, b, pc, P.t[i], pv);
+		}
+		x  = dir == 0 ? -h : h;
+		tv = P.t[i];
+		return;
+	}
+	if (!(P.flags[nb] & F_LEAF)) {
+		interp_p<M, INTERP_DEPTH>(P, status, nb, pv);
+		tv = interp_scalar<M::D, INTERP_DEPTH>(P, status, nb, P.t);
+	} else {
+		load_p<M>(P, nb, pv);
+		tv = P.t[nb];
+	}
+	const double hn = C.size[P.level[nb]];
+	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
+}
+
+// compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients and the Hancock rhs.
+template<class M>
+__device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim, int i) {
+	constexpr int E = M::E, D = M::D;
+	const int cap = P.cap;
+	double pc[E];
+	load_p<M>(P, i, pc);
+	double slope[D * E];
+	for (int dim = 0; dim < D; ++dim) {
+		double pn[E], pp[E], xn, xp, tn, tp;
+		const double xc = 0.0;
+		slope_side<M>(P, C, B, status, i, dim, 0, pc, pn, xn, tn);
+		slope_side<M>(P, C, B, status, i, dim, 1, pc, pp, xp, tp);
+		for (int q = 0; q < E; ++q) {
+			double sn = (pc[q] - pn[q]) / (xc - xn);
+			double sp = (pp[q] - pc[q]) / (xp - xc);
+			slope[dim * E + q] = limit(lim, sn, sp);
+		}
+		if constexpr (M::G > 0) {
+			double gp[M::G], gn[M::G];
+			grad_input<M>(C.m, pp, gp);
+			grad_input<M>(C.m, pn, gn);
+			for (int g = 0; g < M::G; ++g) {
+				double ts = at(P.tslope, cap, g, i);
+				P.grad[(size_t) (dim * M::G + g) * cap + i] = (gp[g] - gn[g] - ts * (tp - tn)) / (xp - xn);
+			}
+		}
+	}
+	for (int c = 0; c < D * E; ++c) P.slope[(size_t) c * cap + i] = slope[c];
+	double rhs[E];
+	double kap = 0.0;
+	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
+	compute_rhs<M>(C.m, pc, slope, kap, rhs);
+	for (int q = 0; q < E; ++q) P.rhs[(size_t) q * cap + i] = rhs[q];
+}
+
+template<class M>
+__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
+	for (int tid = gtid(); tid < n; tid += gstride()) compute_slope<M>(P, C, B, &cnt->status, lim, list[tid]);
+}
+
+// Recompute the Hancock rhs from the stored slope (used for split parents, whose curvature may
+// have changed since the slope stage; impl/adaptive_refinement.hpp:169).
+template<class M>
+__device__ void recompute_rhs(const Pool &P, const Consts &C, int i) {
+	constexpr int E = M::E, D = M::D;
+	const int cap = P.cap;
+	double pc[E], slope[D * E], rhs[E];
+	load_p<M>(P, i, pc);
+	for (int c = 0; c < D * E; ++c) slope[c] = at(P.slope, cap, c, i);
+	double kap = 0.0;
+	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
+	compute_rhs<M>(C.m, pc, slope, kap, rhs);
+	for (int q = 0; q < E; ++q) P.rhs[(size_t) q * cap + i] = rhs[q];
+}
+
+// Scene::can_split (scene/scene.hpp:50-61) with identity-transform refinement zones.
+template<int D>
+__device__ bool can_split_at(const Pool &P, const Consts &C, int i) {
+	const int l = P.level[i];
+	if (l < C.max_refinement_level) return true;
+	for (int z = 0; z < C.n_zones; ++z) {
+		if (l < C.zlevel[z]) {
+			bool in = true;
+			for (int d = 0; d < 3; ++d) {
+				double x = d < D ? at(P.center, P.cap, d, i) : 0.0;
+				in = in && (x < C.zx1[z][d]) && (x > C.zx0[z][d]);
+			}
+			if (in) return true;
+		}
+	}
+	return false;
+}
+
+// Error estimation and split/unsplit detection (impl/adaptive_refinement.hpp:16-149) with the
+// weighted_laplacian estimator (integrator/error_estimators.hpp:19-37).
+template<class M>
+__global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list,
+                           Counters *cnt) {
+	constexpr int E = M::E, D = M::D;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i  = list[tid];
+		const int li = P.level[i];
+		const double h = C.size[li];
+		double pc[E];
+		load_p<M>(P, i, pc);
+		double error = 0.0;
+		for (int dim = 0; dim < D; ++dim) {
+			double d2[E];
+			for (int q = 0; q < E; ++q) d2[q] = pc[q] * -2.0;
+			bool missing = false;
+			for (int dir = 0; dir < 2; ++dir) {
+				const int nb = P.nbr[(size_t) (2 * dim + dir) * cap + i];
+				if (nb == 0) {
+					missing = true;
+					break;
+				}
+				double v[E];
+				if (!(P.flags[nb] & F_LEAF)) {
+					interp_p<M, INTERP_DEPTH>(P, &cnt->status, nb, v);
+				} else if (P.level[nb] < li) {
+					double x[D];
+					for (int d = 0; d < D; ++d) x[d] = at(P.center, cap, d, i) + (d == dim ? h * (2 * dir - 1.0) : 0.0 * h);
+					if (C.periodic[dim] && dir == 0 && x[dim] < -0.5 * C.active[dim]) x[dim] += C.active[dim];
+					if (C.periodic[dim] && dir == 1 && x[dim] > 0.5 * C.active[dim]) x[dim] -= C.active[dim];
+					load_p<M>(P, nb, v);
+					for (int d = 0; d < D; ++d) {
+						const double off = x[d] - at(P.center, cap, d, nb);
+						for (int q = 0; q < E; ++q) v[q] = v[q] + at(P.slope, cap, d * E + q, nb) * off;
+					}
+				} else {
+					load_p<M>(P, nb, v);
+				}
+				for (int q = 0; q < E; ++q) d2[q] = d2[q] + v[q];
+			}
+			if (missing)
+				for (int q = 0; q < E; ++q) d2[q] = 0.0;
+			double sq = 0.0;
+			for (int q = 0; q < E; ++q) {
+				const double w = d2[q] * C.weights[q];
+				sq += w * w;
+			}
+			error += sq;
+		}
+		error = sqrt(error);
+		P.err[i] = error;
+
+		uint32_t fl = P.flags[i];
+		if (fl & F_CAN_SPLIT) {
+			if (!can_split_at<D>(P, C, i)) {
+				fl &= ~F_CAN_SPLIT;
+				P.flags[i] = fl;
+			}
+		}
+		uint8_t op = OP_NONE;
+		const bool want_split = (error > C.max_err && (fl & F_CAN_SPLIT)) || (fl & F_SHOULD_SPLIT);
+		if (want_split) {
+			bool ready = true;
+			for (int f = 0; f < 2 * D; ++f) {
+				const int nb = P.nbr[(size_t) f * cap + i];
+				if (nb != 0 && P.level[nb] < li - 1) ready = false;
+			}
+			if (ready) op |= OP_SPLIT;
+		}
+		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1) {
+			bool ok = true;
+			for (int f = 0; f < 2 * D; ++f) {
+				const int nb = P.nbr[(size_t) f * cap + i];
+				if (nb != 0 && (!(P.flags[nb] & F_LEAF) || P.acti[nb] > L)) ok = false;
+			}
+			if (ok) op |= OP_UCAND;
+		}
+		P.op[i] = op;
+		if (op & OP_SPLIT) append(split_list, &cnt->n_split, i, cap, &cnt->status);
+	}
+}
+
+// A parent coarsens when all its children are coarsening candidates of this cluster
+// (impl/adaptive_refinement.hpp:198-209); the first child decides.
+template<class M>
+__global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int32_t *unsplit_list, Counters *cnt) {
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		if (!(P.op[i] & OP_UCAND)) continue;
+		const int par = P.parent[i];
+		if (P.child[par] != i) continue;
+		bool all = true;
+		for (int c = 0; c < (1 << M::D); ++c) {
+			const int ch = P.child[(size_t) c * cap + par];
+			const uint8_t o = P.op[ch];
+			if (P.clu[ch] != L || !(o & OP_UCAND)) all = false;
+			if (P.clu[ch] == L && (o & OP_SPLIT) && (o & OP_UCAND)) {
+				set_status(&cnt->status, ST_SPLIT_UNSPLIT);
+				all = false;
+			}
+		}
+		if (all) append(unsplit_list, &cnt->n_unsplit, par, cap, &cnt->status);
+	}
+}
+
+// Domain::split (integrator/domain.hpp:192-247) plus the child set-up of
+// impl/adaptive_refinement.hpp:167-195. Children take the parent's primitive state extrapolated
+// with its slope, reuse the parent's old child slots when it has any, start with a zero Hancock
+// rhs, and join the running cluster.
+template<class M>
+__global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
+                        Counters *cnt) {
+	constexpr int E = M::E, D = M::D, NC = 1 << D;
+	const int n   = *n_ptr;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int par = split_list[tid];
+		if constexpr (M::MULTI) recompute_rhs<M>(P, C, par);
+		const int lp   = P.level[par];
+		const double q = 0.25 * C.size[lp];
+		int slots[NC];
+		bool reuse = P.child[par] != 0;
+		if (reuse) {
+			for (int c = 0; c < NC; ++c) slots[c] = P.child[(size_t) c * cap + par];
+		} else {
+			const int first = atomicAdd(&cnt->top, NC);
+			if (first + NC > cap) {
+				set_status(&cnt->status, ST_CAPACITY);
+				continue;
+			}
+			for (int c = 0; c < NC; ++c) {
+				slots[c]                             = first + c;
+				P.child[(size_t) c * cap + par] = first + c;
+			}
+		}
+		double pp[E], pc[D];
+		load_p<M>(P, par, pp);
+		for (int d = 0; d < D; ++d) pc[d] = at(P.center, cap, d, par);
+		for (int c = 0; c < NC; ++c) {
+			const int s = slots[c];
+			P.parent[s] = par;
+			P.level[s]  = (int8_t) (lp + 1);
+			P.acti[s]   = (int8_t) L;
+			P.clu[s]    = (int8_t) L;
+			P.flags[s]  = F_LEAF | F_ACTIVE | F_CAN_SPLIT | F_CAN_UNSPLIT;
+			double cc[D];
+			for (int d = 0; d < D; ++d) {
+				const double qd = (c >> d) & 1 ? 1.0 : -1.0;
+				cc[d] = pc[d] + q * qd;
+				P.center[(size_t) d * cap + s] = cc[d];
+				P.coord[(size_t) d * cap + s]  = 2 * P.coord[(size_t) d * cap + par] + ((c >> d) & 1);
+			}
+			P.t[s] = P.t[par];
+			double p[E], u[E];
+			for (int k = 0; k < E; ++k) p[k] = pp[k];
+			for (int d = 0; d < D; ++d) {
+				const double off = cc[d] - pc[d];
+				for (int k = 0; k < E; ++k) p[k] = p[k] + at(P.slope, cap, d * E + k, par) * off;
+			}
+			cons_from_prim<M>(C.m, p, u);
+			for (int k = 0; k < E; ++k) {
+				P.p[(size_t) k * cap + s]   = p[k];
+				P.u[(size_t) k * cap + s]   = u[k];
+				P.rhs[(size_t) k * cap + s] = 0.0;
+			}
+			for (int k = 0; k < D * E; ++k) P.slope[(size_t) k * cap + s] = at(P.slope, cap, k, par);
+			for (int k = 0; k < M::P; ++k) P.k[(size_t) k * cap + s] = at(P.k, cap, k, par);
+			for (int k = 0; k < M::G; ++k) P.tslope[(size_t) k * cap + s] = at(P.tslope, cap, k, par);
+			for (int k = 0; k < D * M::G; ++k) P.grad[(size_t) k * cap + s] = at(P.grad, cap, k, par);
+			for (int k = 0; k < M::F; ++k) P.flux[(size_t) k * cap + s] = 0.0;
+			P.err[s] = -1.0;
+			for (int dim = 0; dim < D; ++dim) {
+				for (int dir = 0; dir < 2; ++dir) {
+					const int f = 2 * dim + dir;
+					P.nbr[(size_t) f * cap + s] = 0;
+					P.bc[(size_t) f * cap + s]  = ((c & (1 << dim)) == (dir << dim)) ? P.bc[(size_t) f * cap + par] : (int16_t) -1;
+				}
+			}
+			if (!reuse)
+				for (int k = 0; k < NC; ++k) P.child[(size_t) k * cap + s] = 0;
+			append(fresh, &cnt->n_new, s, cap, &cnt->status);
+		}
+		P.flags[par] &= ~(F_LEAF | F_SHOULD_SPLIT);
+	}
+}
+
+// Domain::unsplit with interpolated_cell (integrator/domain.hpp:150-180, 296-325): the parent takes
+// the children's mean t, u, k, t_slope and gradient (the gradient sum starts from the parent's own
+// stale gradient, as interpolated_cell does not reset it) and keeps its old slope and rhs.
+template<class M>
+__global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh,
+                          Counters *cnt) {
+	constexpr int E = M::E, D = M::D, NC = 1 << D, G = M::G;
+	const int n   = *n_ptr;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int par = unsplit_list[tid];
+		double t = 0.0, u[E], kk[M::P > 0 ? M::P : 1], ts[G > 0 ? G : 1], gr[D * G > 0 ? D * G : 1];
+		for (int q = 0; q < E; ++q) u[q] = 0.0;
+		for (int q = 0; q < M::P; ++q) kk[q] = 0.0;
+		for (int q = 0; q < G; ++q) ts[q] = 0.0;
+		for (int q = 0; q < D * G; ++q) gr[q] = at(P.grad, cap, q, par);
+		double error = 0.0;
+		for (int c = 0; c < NC; ++c) {
+			const int ch = P.child[(size_t) c * cap + par];
+			t += P.t[ch];
+			for (int q = 0; q < E; ++q) u[q] = u[q] + at(P.u, cap, q, ch);
+			for (int q = 0; q < M::P; ++q) kk[q] = kk[q] + at(P.k, cap, q, ch);
+			for (int q = 0; q < D * G; ++q) gr[q] = gr[q] + at(P.grad, cap, q, ch);
+			for (int q = 0; q < G; ++q) ts[q] = ts[q] + at(P.tslope, cap, q, ch);
+		}
+		for (int c = 0; c < NC; ++c) {
+			const int ch = P.child[(size_t) c * cap + par];
+			error += P.err[ch];
+			P.flags[ch] |= F_GARBAGE | F_LEAF;
+		}
+		t = t / (double) NC;
+		for (int q = 0; q < G; ++q) ts[q] = ts[q] / (double) NC;
+		for (int q = 0; q < E; ++q) u[q] = u[q] / (double) NC;
+		double p[E];
+		prim_from_cons<M>(C.m, u, p);
+		for (int q = 0; q < M::P; ++q) kk[q] = kk[q] / (double) NC;
+		for (int q = 0; q < D * G; ++q) gr[q] = gr[q] / (double) NC;
+		P.t[par] = t;
+		for (int q = 0; q < E; ++q) {
+			P.u[(size_t) q * cap + par] = u[q];
+			P.p[(size_t) q * cap + par] = p[q];
+		}
+		for (int q = 0; q < M::P; ++q) P.k[(size_t) q * cap + par] = kk[q];
+		for (int q = 0; q < G; ++q) P.tslope[(size_t) q * cap + par] = ts[q];
+		for (int q = 0; q < D * G; ++q) P.grad[(size_t) q * cap + par] = gr[q];
+		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + par] = 0.0;
+		for (int f = 0; f < 2 * D; ++f) P.nbr[(size_t) f * cap + par] = 0;
+		P.err[par]   = error;
+		P.flags[par] = (P.flags[par] | F_LEAF | F_ACTIVE | F_CAN_SPLIT) & ~F_GARBAGE;
+		P.acti[par]  = (int8_t) L;
+		P.clu[par]   = (int8_t) L;
+		append(fresh, &cnt->n_new, par, cap, &cnt->status);
+	}
+}
+
+// Domain::update_neighbors for one active leaf (integrator/domain.hpp:249-293): faces without a
+// boundary get the node found at the same level (or the coarser leaf); a neighbour more than one
+// level coarser is flagged should_split.
+template<class M>
+__device__ void update_neighbors_leaf(const Pool &P, const Consts &C, int i) {
+	const int cap = P.cap;
+	const int li  = P.level[i];
+	for (int dim = 0; dim < M::D; ++dim) {
+		for (int dir = 0; dir < 2; ++dir) {
+			const int f = 2 * dim + dir;
+			if (P.bc[(size_t) f * cap + i] >= 0) continue;
+			const int nb = find_neighbor<M::D>(P, C, i, dim, dir);
+			if (nb == 0 || !(P.flags[nb] & F_ACTIVE)) continue;
+			P.nbr[(size_t) f * cap + i] = nb;
+			if (P.level[nb] < li - 1) atomicOr(&P.flags[nb], (uint32_t) F_SHOULD_SPLIT);
+		}
+	}
+}
+
+// update_neighbors applied to a node: leaves directly, non-leaves through all their descendants.
+template<class M>
+__device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_t *status, int root) {
+	constexpr int NC = 1 << M::D;
+	int stack[64];
+	int sp = 0;
+	stack[sp++] = root;
+	while (sp > 0) {
+		const int x = stack[--sp];
+		const uint32_t fl = P.flags[x];
+		if (fl & F_LEAF) {
+			if (fl & F_ACTIVE) update_neighbors_leaf<M>(P, C, x);
+			continue;
+		}
+		for (int c = NC - 1; c >= 0; --c) {
+			if (sp >= 64) {
+				set_status(status, ST_DEPTH);
+				break;
+			}
+			stack[sp++] = P.child[(size_t) c * P.cap + x];
+		}
+	}
+}
+
+// Neighbour repair, first pass (impl/adaptive_refinement.hpp:236-249): new children and coarsened
+// parents, then queue their neighbours for the second pass.
+template<class M>
+__global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *fresh, int stamp, int32_t *upd,
+                            Counters *cnt) {
+	const int n   = *n_ptr;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = fresh[tid];
+		update_neighbors_subtree<M>(P, C, &cnt->status, i);
+		for (int f = 0; f < 2 * M::D; ++f) {
+			const int nb = P.nbr[(size_t) f * cap + i];
+			if (nb != 0 && ((P.flags[nb] & F_ACTIVE) || !(P.flags[nb] & F_LEAF))) {
+				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(upd, &cnt->n_upd, nb, cap, &cnt->status);
+			}
+		}
+	}
+}
+
+template<class M>
+__global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, int n_host, const int32_t *list, Counters *cnt) {
+	const int n = n_ptr ? *n_ptr : n_host;
+	for (int tid = gtid(); tid < n; tid += gstride()) update_neighbors_subtree<M>(P, C, &cnt->status, list[tid]);
+}
+
+// ACTI reassignment (impl/adaptive_refinement.hpp:264-322): per-cell CFL decides whether a cell
+// stays, drops one time level (into the buffer of L-1, only when level L is synchronised with L-1)
+// or rises by floor(log2(cfl/max_cfl))+1 levels.
+template<class M>
+__global__ void k_reassign(Pool P, Consts C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL,
+                           int counter_L, Lists Ls, Counters *cnt) {
+	const int n   = n_ptr ? *n_ptr : n_host;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double p[M::E];
+		load_p<M>(P, i, p);
+		const double mdt = max_delta_time<M>(C.m, p, C.size[P.level[i]]);
+		P.maxdt[i]       = mdt;
+		double cfl       = dtL / mdt;
+		const uint32_t fl = P.flags[i];
+		if (!(fl & F_LEAF) || (fl & F_GARBAGE)) {
+			P.cfl[i] = cfl;
+			P.clu[i] = CLU_NONE;
+			continue;
+		}
+		if (cfl < 0.5 * C.max_cfl && counter_L == 1 && L > 0) {
+			append(Ls.buf[L - 1], &cnt->buf[L - 1], i, cap, &cnt->status);
+			cfl *= 2;
+			P.clu[i] = (int8_t) (BUF_BASE + L - 1);
+		} else if (cfl > C.max_cfl && L < MAX_ACTI - 1) {
+			const int raise = (int) log2(cfl / C.max_cfl) + 1;
+			if (L + raise < MAX_ACTI) {
+				append(Ls.clu[L + raise], &cnt->clu[L + raise], i, cap, &cnt->status);
+				P.acti[i] = (int8_t) (L + raise);
+				cfl /= (double) (1 << raise);
+				P.clu[i] = (int8_t) (L + raise);
+			} else {
+				P.clu[i] = CLU_NONE;
+			}
+		} else {
+			append(Ls.tmp, &cnt->n_tmp, i, cap, &cnt->status);
+			P.clu[i] = (int8_t) L;
+		}
+		P.cfl[i] = cfl;
+	}
+}
+
+// flush_acti_buffer (impl/acti_utils.hpp:365-372)
+static __global__ void k_flush(Pool P, const int32_t *buf, const int *n_ptr, int32_t *clu_list, int *clu_count, int L,
+                        Counters *cnt) {
+	const int n = *n_ptr;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = buf[tid];
+		append(clu_list, clu_count, i, P.cap, &cnt->status);
+		P.acti[i] = (int8_t) L;
+		P.clu[i]  = (int8_t) L;
+	}
+}
+
+static __global__ void k_set_count(int *dst, const int *src) { *dst = *src; }
+
+// --------------------------------------------------------------------------------------------
+// Initialisation (integrator/integrator.hpp:100-160)
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ void atomic_max_pos_double(double *addr, double v) {
+	// non-negative doubles order like their bit patterns as signed 64-bit integers
+	atomicMax(reinterpret_cast<long long *>(addr), __double_as_longlong(v));
+}
+
+template<class M>
+__global__ void k_init_cells(Pool P, Consts C, const int32_t *list, int n, Counters *cnt) {
+	constexpr int E = M::E;
+	const int cap = P.cap;
+	double local_max = -INFINITY;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double p[E], u[E];
+		load_p<M>(P, i, p);
+		cons_from_prim<M>(C.m, p, u);
+		for (int q = 0; q < E; ++q) P.u[(size_t) q * cap + i] = u[q];
+		if constexpr (M::MULTI) {
+			P.k[(size_t) 0 * cap + i]         = C.m.mu1 * p[M::IA] + C.m.mu2 * (1 - p[M::IA]);
+			P.k[(size_t) M::ALPHAS * cap + i] = p[M::IA];
+		}
+		for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = 0.0;
+		const double mdt = max_delta_time<M>(C.m, p, C.size[P.level[i]]);
+		P.maxdt[i] = mdt;
+		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
+		local_max = smax(local_max, mdt);
+	}
+	// warp-shuffle max, then one atomic per warp
+	for (int off = 16; off > 0; off >>= 1) local_max = smax(local_max, __shfl_xor_sync(0xffffffffu, local_max, off));
+	if ((threadIdx.x & 31) == 0 && local_max > 0) atomic_max_pos_double(&cnt->dmax, local_max);
+}
+
+template<class M>
+__global__ void k_nbr_init(Pool P, Consts C, const int32_t *list, int n) {
+	for (int tid = gtid(); tid < n; tid += gstride()) update_neighbors_leaf<M>(P, C, list[tid]);
+}
+
+// assign_to_acti_clusters (impl/acti_utils.hpp:11-24)
+template<class M>
+__global__ void k_assign(Pool P, Consts C, const int32_t *list, int n, double global_dt, Lists Ls, Counters *cnt) {
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		const uint32_t fl = P.flags[i];
+		if (!(fl & F_ACTIVE) || !(fl & F_LEAF)) continue;
+		double cfl = global_dt / P.maxdt[i];
+		int lvl    = (int) log2(cfl / C.max_cfl);
+		lvl        = lvl < 0 ? 0 : (lvl > MAX_ACTI - 1 ? MAX_ACTI - 1 : lvl);
+		cfl /= (double) (1 << lvl);
+		P.cfl[i]  = cfl;
+		P.acti[i] = (int8_t) lvl;
+		P.clu[i]  = (int8_t) lvl;
+		append(Ls.clu[lvl], &cnt->clu[lvl], i, P.cap, &cnt->status);
+	}
+}
+
+// Gather of active-cell records for the read-back API.
+template<class M>
+__global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, double *out, int32_t *lv) {
+	constexpr int E = M::E, D = M::D, W = D + 1 + 2 * E + 3;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		const int r = base + tid;
+		lv[2 * r]     = P.level[i];
+		lv[2 * r + 1] = P.acti[i];
+		double *o     = out + (size_t) r * W;
+		int k         = 0;
+		for (int d = 0; d < D; ++d) o[k++] = at(P.center, cap, d, i);
+		o[k++] = P.t[i];
+		for (int q = 0; q < E; ++q) o[k++] = at(P.u, cap, q, i);
+		for (int q = 0; q < E; ++q) o[k++] = at(P.p, cap, q, i);
+		o[k++] = P.err[i];
+		o[k++] = P.maxdt[i];
+		o[k++] = P.cfl[i];
+	}
+}
+
+}  // namespace dg

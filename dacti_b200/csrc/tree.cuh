@@ -1,0 +1,172 @@
+// Node-pool access helpers: neighbour search, recursive child averages, boundary ghost states.
+#pragma once
+
+#include "model.cuh"
+
+namespace dg {
+
+__device__ __forceinline__ double at(const double *a, int cap, int c, int i) { return a[(size_t) c * cap + i]; }
+__device__ __forceinline__ bool is_leaf(const Pool &P, int i) { return P.flags[i] & F_LEAF; }
+__device__ __forceinline__ bool is_active(const Pool &P, int i) { return P.flags[i] & F_ACTIVE; }
+
+template<class M>
+__device__ __forceinline__ void load_p(const Pool &P, int i, double *p) {
+	for (int q = 0; q < M::E; ++q) p[q] = at(P.p, P.cap, q, i);
+}
+
+__device__ __forceinline__ void set_status(uint32_t *status, uint32_t bit) { atomicOr(status, bit); }
+
+// Domain::find(location, node.tree_level) for the face (dim, dir) of node i, as used by
+// update_neighbors (integrator/domain.hpp:65-82, 249-293, 407-417). The location is the centre of
+// the same-level neighbour; in integer cell coordinates the root-down descent becomes: step up to
+// the common ancestor, then down towards the target until a leaf or the node's level. Returns 0 when
+// the location lies outside the active box of a non-periodic dimension.
+template<int D>
+__device__ int find_neighbor(const Pool &P, const Consts &C, int i, int dim, int dir) {
+	const int cap = P.cap;
+	const int l   = P.level[i];
+	int tc[3];
+	for (int d = 0; d < D; ++d) tc[d] = P.coord[(size_t) d * cap + i];
+	tc[dim] += 2 * dir - 1;
+	const int lo = C.a0[l][dim], hi = C.a0[l][dim] + C.na[l][dim];
+	if (tc[dim] < lo || tc[dim] >= hi) {
+		if (!C.periodic[dim]) return 0;
+		tc[dim] += (tc[dim] < lo) ? C.na[l][dim] : -C.na[l][dim];
+	}
+	const int own = P.coord[(size_t) dim * cap + i];
+	int a = i, m = l;
+	// ascend while the ancestor at level m does not contain the target along `dim`
+	for (int guard = 0; guard < MAX_TREE && m > 0 && ((tc[dim] >> (l - m)) != (own >> (l - m))); ++guard) {
+		a = P.parent[a];
+		--m;
+	}
+	// descend towards the target
+	for (int guard = 0; guard < MAX_TREE && !(P.flags[a] & F_LEAF) && m < l; ++guard) {
+		int ci = 0;
+		for (int d = 0; d < D; ++d) ci |= ((tc[d] >> (l - m - 1)) & 1) << d;
+		a = P.child[(size_t) ci * cap + a];
+		++m;
+	}
+	return a;
+}
+
+// Domain::interpolate_p / interpolate_t / interpolate_k (integrator/domain.hpp:84-148): the value of
+// a leaf, or the mean over the active children of a non-leaf, recursively.
+template<class M, int DEPTH>
+__device__ void interp_p(const Pool &P, uint32_t *status, int n, double *out) {
+	if (P.flags[n] & F_LEAF) {
+		load_p<M>(P, n, out);
+		return;
+	}
+	if constexpr (DEPTH == 0) {
+		set_status(status, ST_DEPTH);
+		for (int q = 0; q < M::E; ++q) out[q] = 0.0;
+	} else {
+		double f[M::E];
+		for (int q = 0; q < M::E; ++q) f[q] = 0.0;
+		int cnt = 0;
+		for (int c = 0; c < (1 << M::D); ++c) {
+			int ch = P.child[(size_t) c * P.cap + n];
+			if (P.flags[ch] & F_ACTIVE) {
+				double tmp[M::E];
+				interp_p<M, DEPTH - 1>(P, status, ch, tmp);
+				for (int q = 0; q < M::E; ++q) f[q] = f[q] + tmp[q];
+				cnt++;
+			}
+		}
+		for (int q = 0; q < M::E; ++q) out[q] = f[q] / (double) cnt;
+	}
+}
+
+// Scalar field average (t, k[i] or p[i]); `arr` is the SoA base of that component.
+template<int D, int DEPTH>
+__device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const double *arr) {
+	if (P.flags[n] & F_LEAF) return arr[n];
+	if constexpr (DEPTH == 0) {
+		set_status(status, ST_DEPTH);
+		return 0.0;
+	} else {
+		double f = 0.0;
+		int cnt  = 0;
+		for (int c = 0; c < (1 << D); ++c) {
+			int ch = P.child[(size_t) c * P.cap + n];
+			if (P.flags[ch] & F_ACTIVE) {
+				f += interp_scalar<D, DEPTH - 1>(P, status, ch, arr);
+				cnt++;
+			}
+		}
+		return f / (double) cnt;
+	}
+}
+
+constexpr int INTERP_DEPTH = 4;
+
+// Boundary::boundary_value (integrator/boundary.hpp:75-123): ghost primitive state of a face.
+template<class M>
+__device__ void boundary_value(const ModelConsts &m, const BcTable &B, int b, const double *pc, double tc,
+                               double *pb) {
+	const int type = B.type[b];
+	if (type == BC_FREESLIP) {
+		const double *n = B.normal + (size_t) b * M::D;
+		for (int q = 0; q < M::E; ++q) pb[q] = pc[q];
+		double dot = 0.0;
+		for (int i = 0; i < M::D; ++i) dot += pc[M::IU + i] * n[i];
+		for (int i = 0; i < M::D; ++i) pb[M::IU + i] = pc[M::IU + i] - n[i] * dot;
+		return;
+	}
+	if (type == BC_NOSLIP) {
+		for (int q = 0; q < M::E; ++q) pb[q] = pc[q];
+		for (int i = 0; i < M::D; ++i) pb[M::IU + i] *= -1.0;
+		return;
+	}
+	if (type == BC_INFLOW || type == BC_INFLOW_R) {
+		const double *pin = B.p_in + (size_t) b * M::E;
+		for (int q = 0; q < M::E; ++q) pb[q] = pin[q];
+		if (!supersonic<M>(m, pc)) pb[M::IP] = pc[M::IP];
+		double fade = B.fade_in[b];
+		if (fade > 0.0) {
+			double vm = smin(tc / fade, 1.0);
+			for (int i = 0; i < M::D; ++i) pb[M::IU + i] *= vm;
+		}
+		return;
+	}
+	if (type == BC_DIRICHLET) {
+		const double *pin = B.p_in + (size_t) b * M::E;
+		for (int q = 0; q < M::E; ++q) pb[q] = pin[q];
+		return;
+	}
+	// outflow, zeroGradient (and the unused neumann)
+	for (int q = 0; q < M::E; ++q) pb[q] = pc[q];
+}
+
+// Slope limiters (integrator/slope_limiters.hpp:7-57).
+enum : int { LIM_MINMOD = 0, LIM_UNLIMITED, LIM_VAN_LEER, LIM_SUPERBEE, LIM_VON_ALBA_2, LIM_KOREN, LIM_FIRST_ORDER };
+
+__device__ __forceinline__ double limit(int lim, double s1, double s2) {
+	switch (lim) {
+		case LIM_MINMOD:
+			if (s1 * s2 <= 0.0) return 0.0;
+			else if (fabs(s1) < fabs(s2)) return s1;
+			else return s2;
+		case LIM_UNLIMITED: return 0.5 * (s1 + s2);
+		case LIM_VAN_LEER: {
+			double r = s1 / s2;
+			return (r + fabs(r)) / (1 + fabs(r)) * s2;
+		}
+		case LIM_SUPERBEE: {
+			double r = s1 / s2;
+			return smax(smax(0.0, smin(2.0 * r, 1.0)), smin(r, 2.0)) * s2;
+		}
+		case LIM_VON_ALBA_2: {
+			double r = s1 / s2;
+			return 2.0 * r / (r * r + 1) * s2;
+		}
+		case LIM_KOREN: {
+			double r = (s1 + 1e-9) / (s2 + 1e-9);
+			return smax(0.0, smin(2.0 * r, smin((1.0 + 2.0 * r) / 3.0, 2.))) * s2;
+		}
+		default: return 0.0;
+	}
+}
+
+}  // namespace dg

@@ -1,0 +1,205 @@
+"""Python binding of the C ABI (include/dacti_gpu.h), shaped like DACTI's Integrator.
+
+``Solver(case)`` runs the Integrator constructor (integrator/integrator.hpp:72-163) on the device,
+``integrate()`` advances one global step like Integrator::integrate (impl/integrate.hpp:12-87),
+``n_active_cells()`` and ``active_cells()`` mirror n_active_cells / for_each_active_cell
+(integrator/integrator.hpp:172-202). There is no CPU fallback: without the compiled library or a
+CUDA device, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Callable, Optional
+
+import numpy as np
+
+from .casefile import Case, Snapshot
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libdacti_gpu.so")
+
+DG_OK = 0
+STATUS_NAMES = {
+    -1: "DG_ERR_ARG", -2: "DG_ERR_CUDA", -3: "DG_ERR_CAPACITY", -4: "DG_ERR_DEPTH", -5: "DG_ERR_MISSING_BC",
+    -6: "DG_ERR_UNSUPPORTED",
+}
+
+LIMITERS = {"minmod": 0, "unlimited": 1, "van_leer": 2, "superbee": 3, "von_alba_2": 4, "koren": 5,
+            "first_order": 6}
+
+
+class DgCase(ctypes.Structure):
+    _fields_ = [
+        ("model", ctypes.c_int), ("dims", ctypes.c_int), ("n_nodes", ctypes.c_int), ("n_bc", ctypes.c_int),
+        ("n_zones", ctypes.c_int), ("limiter", ctypes.c_int),
+        ("params", ctypes.POINTER(ctypes.c_double)), ("weights", ctypes.POINTER(ctypes.c_double)),
+        ("zones", ctypes.POINTER(ctypes.c_double)), ("bc_type", ctypes.POINTER(ctypes.c_int)),
+        ("bc_p_in", ctypes.POINTER(ctypes.c_double)), ("bc_normal", ctypes.POINTER(ctypes.c_double)),
+        ("bc_fade_in", ctypes.POINTER(ctypes.c_double)), ("parent", ctypes.POINTER(ctypes.c_int)),
+        ("children", ctypes.POINTER(ctypes.c_int)), ("level", ctypes.POINTER(ctypes.c_int)),
+        ("flags", ctypes.POINTER(ctypes.c_uint)), ("bc", ctypes.POINTER(ctypes.c_int)),
+        ("center", ctypes.POINTER(ctypes.c_double)), ("p", ctypes.POINTER(ctypes.c_double)),
+    ]
+
+
+class DgStats(ctypes.Structure):
+    _fields_ = [
+        ("n_clusters", ctypes.c_longlong * 16), ("n_buffers", ctypes.c_longlong * 16),
+        ("tree_size", ctypes.c_longlong), ("n_splits", ctypes.c_longlong), ("n_unsplits", ctypes.c_longlong),
+        ("n_gc", ctypes.c_longlong), ("n_substeps", ctypes.c_longlong), ("n_global_steps", ctypes.c_longlong),
+        ("cell_updates", ctypes.c_longlong), ("max_acti_level", ctypes.c_int), ("global_dt", ctypes.c_double),
+        ("acti_time", ctypes.c_double * 16), ("acti_counter", ctypes.c_int * 16),
+    ]
+
+
+SUBSTEP_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                              ctypes.c_longlong)
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Loads the compiled library; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m dacti_b200.build`")
+    lib = ctypes.CDLL(path)
+    vp = ctypes.c_void_p
+    lib.dg_create.argtypes = [ctypes.POINTER(DgCase), ctypes.POINTER(vp)]
+    lib.dg_set_stream.argtypes = [vp, vp]
+    lib.dg_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                            SUBSTEP_FN, vp]
+    lib.dg_cell_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.dg_read_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                  ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
+    lib.dg_last_error.argtypes = [vp]
+    lib.dg_last_error.restype = ctypes.c_char_p
+    lib.dg_destroy.argtypes = [vp]
+    lib.dg_destroy.restype = None
+    _lib = lib
+    return lib
+
+
+EXPORTED_SYMBOLS = ("dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells", "dg_get_stats",
+                    "dg_last_error", "dg_destroy")
+
+
+class DgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+def _ptr(a: np.ndarray, ctype):
+    return a.ctypes.data_as(ctypes.POINTER(ctype))
+
+
+class Solver:
+    def __init__(self, case: Case, limiter: str = "minmod"):
+        self._lib = load_library()
+        t, prm = case.tree, case.params
+        sh = t.shape
+        self.shape = sh
+        self.side_length = prm.side_length
+        E, D = sh.E, sh.dims
+        nb = max(len(t.bcs), 1)
+        keep = dict(
+            params=prm.param_vector(),
+            weights=np.ascontiguousarray(prm.weights, np.float64).reshape(E),
+            zones=np.array([[*(list(z.x0) + [0.0] * 3)[:3], *(list(z.x1) + [0.0] * 3)[:3], float(z.level)]
+                            for z in prm.zones] or [[0.0] * 7], np.float64),
+            bc_type=np.array([int(b.type) for b in t.bcs] or [0], np.int32),
+            bc_p_in=np.array([list(b.p_in) for b in t.bcs] or [[0.0] * E], np.float64).reshape(nb, E),
+            bc_normal=np.array([list(b.normal) for b in t.bcs] or [[0.0] * D], np.float64).reshape(nb, D),
+            bc_fade_in=np.array([b.fade_in for b in t.bcs] or [0.0], np.float64),
+            parent=np.ascontiguousarray(t.parent, np.int32),
+            children=np.ascontiguousarray(t.children, np.int32),
+            level=np.ascontiguousarray(t.level, np.int32),
+            flags=np.ascontiguousarray(t.flags, np.uint32),
+            bc=np.ascontiguousarray(t.bc, np.int32),
+            center=np.ascontiguousarray(t.center, np.float64),
+            p=np.ascontiguousarray(t.p, np.float64),
+        )
+        c = DgCase()
+        c.model, c.dims, c.n_nodes = int(sh.model), D, t.n_nodes
+        c.n_bc, c.n_zones, c.limiter = len(t.bcs), len(prm.zones), LIMITERS[limiter]
+        dbl, it = ctypes.c_double, ctypes.c_int
+        c.params, c.weights, c.zones = _ptr(keep["params"], dbl), _ptr(keep["weights"], dbl), _ptr(keep["zones"], dbl)
+        c.bc_type, c.bc_p_in = _ptr(keep["bc_type"], it), _ptr(keep["bc_p_in"], dbl)
+        c.bc_normal, c.bc_fade_in = _ptr(keep["bc_normal"], dbl), _ptr(keep["bc_fade_in"], dbl)
+        c.parent, c.children, c.level = _ptr(keep["parent"], it), _ptr(keep["children"], it), _ptr(keep["level"], it)
+        c.flags, c.bc = _ptr(keep["flags"], ctypes.c_uint), _ptr(keep["bc"], it)
+        c.center, c.p = _ptr(keep["center"], dbl), _ptr(keep["p"], dbl)
+        h = ctypes.c_void_p()
+        rc = self._lib.dg_create(ctypes.byref(c), ctypes.byref(h))
+        if rc != DG_OK:
+            raise DgError(rc, self._lib.dg_last_error(None).decode())
+        self._h = h
+        self.global_dt = self.stats().global_dt
+        self.time = 0.0
+
+    # -- reference Integrator surface ---------------------------------------------------------
+    def integrate(self, substep_hook: Optional[Callable] = None, signal: bool = True) -> tuple:
+        """One global step. Returns (global_dt, force_break)."""
+        fb = ctypes.c_int(0)
+        gdt = ctypes.c_double(0.0)
+        if substep_hook is not None:
+            def tramp(_u, level, at, ns, dtl, csize):
+                substep_hook(self, level, at, ns, dtl, csize)
+            cb = SUBSTEP_FN(tramp)
+        else:
+            cb = SUBSTEP_FN()
+        self._check(self._lib.dg_step(self._h, 1 if signal else 0, ctypes.byref(fb), ctypes.byref(gdt), cb, None))
+        self.global_dt = gdt.value
+        return gdt.value, bool(fb.value)
+
+    def n_active_cells(self) -> int:
+        n = ctypes.c_longlong()
+        self._check(self._lib.dg_cell_count(self._h, ctypes.byref(n)))
+        return int(n.value)
+
+    def active_cells(self) -> Snapshot:
+        sh = self.shape
+        D, E = sh.dims, sh.E
+        W = D + 1 + 2 * E + 3
+        n = self.n_active_cells()
+        lv = np.zeros((max(n, 1), 2), np.int32)
+        data = np.zeros((max(n, 1), W), np.float64)
+        got = ctypes.c_longlong()
+        self._check(self._lib.dg_read_cells(self._h, _ptr(lv, ctypes.c_int), _ptr(data, ctypes.c_double), n,
+                                            ctypes.byref(got)))
+        st = self.stats()
+        n_in = int(sum(st.n_clusters))
+        return Snapshot(
+            D, E, int(st.n_global_steps), int(st.n_substeps), int(st.tree_size), n_in, self.time, st.global_dt,
+            float(st.cell_updates), lv[:n, 0].copy(), lv[:n, 1].copy(), data[:n, :D].copy(), data[:n, D].copy(),
+            data[:n, D + 1:D + 1 + E].copy(), data[:n, D + 1 + E:D + 1 + 2 * E].copy(), data[:n, D + 1 + 2 * E].copy(),
+            data[:n, D + 2 + 2 * E].copy(), data[:n, D + 3 + 2 * E].copy(),
+        )
+
+    def stats(self) -> DgStats:
+        s = DgStats()
+        self._check(self._lib.dg_get_stats(self._h, ctypes.byref(s)))
+        return s
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self._lib.dg_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dg_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != DG_OK:
+            raise DgError(rc, self._lib.dg_last_error(self._h).decode())

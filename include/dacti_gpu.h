@@ -1,0 +1,124 @@
+/*
+ * dacti_gpu.h — C ABI of the B200 octree finite-volume step.
+ *
+ * Drop-in replacement for the solver step of DACTI's header-only
+ * dacti::integrator::Integrator<Model, Limiter, ErrorEstimator>
+ * (src/lib/integrator/integrator.hpp:14-225). The reference has no FFI layer; these entry points
+ * are what its class template does, flattened to plain pointers and sizes so that any host (the C++
+ * adapter include/dacti_gpu/integrator.hpp, ctypes, cgo, JNI) can bind them. All functions return a
+ * dg_status; nothing throws across the ABI.
+ */
+#ifndef DACTI_GPU_H
+#define DACTI_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct dg_solver dg_solver;
+
+/* status codes */
+enum {
+	DG_OK              = 0,
+	DG_ERR_ARG         = -1, /* invalid argument or unsupported model/dimension */
+	DG_ERR_CUDA        = -2, /* CUDA runtime error (dg_last_error has the text) */
+	DG_ERR_CAPACITY    = -3, /* node pool or list capacity exceeded on the device */
+	DG_ERR_DEPTH       = -4, /* tree deeper than the neighbourhood walkers support */
+	DG_ERR_MISSING_BC  = -5, /* a face with neither neighbour nor boundary condition */
+	DG_ERR_UNSUPPORTED = -6  /* feature of the reference not supported by this build */
+};
+
+/* model ids (dacti::model::euler / navier_stokes / multi) */
+enum { DG_EULER = 0, DG_NAVIER_STOKES = 1, DG_MULTI = 2 };
+
+/* limiter ids (dacti::integrator::slope, integrator/slope_limiters.hpp:7-57) */
+enum { DG_MINMOD = 0, DG_UNLIMITED, DG_VAN_LEER, DG_SUPERBEE, DG_VON_ALBA_2, DG_KOREN, DG_FIRST_ORDER };
+
+/* layout of dg_case.params (Config fields read by integrator/integrator.hpp:80-86 and model constants) */
+enum {
+	DG_P_SIDE = 0, DG_P_ACTIVE0 = 1, DG_P_PERIODIC0 = 4, DG_P_MAX_CFL = 7, DG_P_MAX_DT = 8, DG_P_MIN_ERR = 9,
+	DG_P_MAX_ERR = 10, DG_P_MAX_LEVEL = 11, DG_P_MIN_LEVEL = 12, DG_P_GAMMA = 13, DG_P_NS_MU = 14,
+	DG_P_NS_LAMBDA = 15, DG_P_GAMMA1 = 16, DG_P_GAMMA2 = 17, DG_P_P1 = 18, DG_P_P2 = 19, DG_P_CP1 = 20,
+	DG_P_CP2 = 21, DG_P_CV1 = 22, DG_P_CV2 = 23, DG_P_MU1 = 24, DG_P_MU2 = 25, DG_P_LAMBDA1 = 26,
+	DG_P_LAMBDA2 = 27, DG_P_SIGMA = 28, DG_N_PARAMS = 32
+};
+
+/* node flag bits of dg_case.flags (integrator/node.hpp:60-66) */
+enum {
+	DG_F_LEAF = 1, DG_F_ACTIVE = 2, DG_F_GARBAGE = 4, DG_F_CAN_SPLIT = 8, DG_F_CAN_UNSPLIT = 16,
+	DG_F_SHOULD_SPLIT = 32, DG_F_IS_BOUNDARY = 64
+};
+
+/*
+ * The initial tree as Scene::init_domain leaves it (scene/scene.cpp:369-431): every node slot,
+ * slot 0 the null node and slot 1 the root. Arrays are row-major per node:
+ * children[n][2^D], bc[n][2D] (index into the boundary table or -1), center[n][D], p[n][E].
+ */
+typedef struct dg_case {
+	int model, dims;
+	int n_nodes, n_bc, n_zones;
+	int limiter;
+	const double *params;     /* DG_N_PARAMS */
+	const double *weights;    /* E: weighted_laplacian weights (integrator/error_estimators.hpp:336) */
+	const double *zones;      /* n_zones x {x0[3], x1[3], max_level} refinement zones */
+	const int *bc_type;       /* n_bc Boundary::Type values (integrator/boundary.hpp:23-32) */
+	const double *bc_p_in;    /* n_bc x E */
+	const double *bc_normal;  /* n_bc x D */
+	const double *bc_fade_in; /* n_bc */
+	const int *parent;
+	const int *children;
+	const int *level;
+	const unsigned *flags;
+	const int *bc;
+	const double *center;
+	const double *p;
+} dg_case;
+
+/* Called after every level substep, like the substep_hook of Integrator::integrate
+ * (impl/integrate.hpp:64): (user, level, level time, substep count, level dt, cluster size). */
+typedef void (*dg_substep_fn)(void *user, int level, double acti_time, int n_substeps, double dt_level,
+                              long long cluster_size);
+
+typedef struct dg_stats {
+	long long n_clusters[16];   /* cells per ACTI cluster */
+	long long n_buffers[16];    /* cells waiting in ACTI buffers */
+	long long tree_size;        /* node slots incl. the null slot (Domain::tree.size()) */
+	long long n_splits, n_unsplits, n_gc;
+	long long n_substeps, n_global_steps;
+	long long cell_updates;     /* sum of cluster sizes over executed substeps */
+	int max_acti_level;
+	double global_dt;
+	double acti_time[16];
+	int acti_counter[16];
+} dg_stats;
+
+/* Integrator constructor (integrator/integrator.hpp:72-163) on a flattened initial tree. */
+int dg_create(const dg_case *c, dg_solver **out);
+
+/* Optional CUDA stream (cudaStream_t) on which all work of this solver is issued. */
+int dg_set_stream(dg_solver *s, void *cuda_stream);
+
+/* Integrator::integrate (impl/integrate.hpp:12-87): one global step over all ACTI levels.
+ * force_break is set when a cell update produced NaN (the step stops at that substep). */
+int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user);
+
+/* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */
+int dg_cell_count(dg_solver *s, long long *n);
+
+/* for_each_active_cell (integrator/integrator.hpp:172-191): clusters 0..15 then buffers 0..15.
+ * levels[n][2] = {tree_level, acti_level}; data[n][D + 1 + 2E + 3] =
+ * {center[D], t, u[E], p[E], error, max_dt, cfl}. */
+int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
+
+int dg_get_stats(dg_solver *s, dg_stats *out);
+
+/* Text of the last error on this solver (or of the last failed dg_create when s is NULL). */
+const char *dg_last_error(dg_solver *s);
+
+void dg_destroy(dg_solver *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DACTI_GPU_H */

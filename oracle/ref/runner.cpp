@@ -1,0 +1,233 @@
+// Oracle (test infrastructure, not the product): drives DACTI's own, unmodified
+// Integrator<Model, minmod, weighted_laplacian> (src/lib/integrator/integrator.hpp) on a flat case
+// file, the way default_driver::run does (driver/default_driver.hpp:197-213), and writes binary
+// snapshots of every active cell at the requested global steps.
+//
+// Usage: dacti_ref_runner <case.bin> <out_prefix> <n_global_steps> [--check s1,s2,..]
+//                         [--t-end T] [--neighbor-audit] [--quiet]
+// Prints one JSON line with timing (wall time of integrate() calls only), substep and
+// leaf-update counts. Leaf cell-updates are counted in the substep hook as the level's cluster
+// size, as impl/integrate.hpp:57-64 exposes it.
+#include "case_io.hpp"
+
+#include "integrator/error_estimators.hpp"
+#include "integrator/integrator.hpp"
+#include "integrator/slope_limiters.hpp"
+#include "model/euler.hpp"
+#include "model/multi.hpp"
+#include "model/navier_stokes.hpp"
+#include "scene/scene.hpp"
+
+#include <chrono>
+#include <cstdio>
+#include <set>
+#include <sstream>
+
+using namespace dacti;
+
+namespace {
+
+	struct Options {
+		std::string case_path, out_prefix;
+		int n_steps = 1;
+		double t_end = -1.0;
+		std::set<int> checks;
+		bool neighbor_audit = false;
+		bool quiet = false;
+	};
+
+	template<typename Model>
+	void set_model_constants(const oracle::CaseData &c) {
+		using namespace oracle;
+		if constexpr (Model::Multiphase) {
+			Model::gamma1  = c.params[P_GAMMA1];
+			Model::gamma2  = c.params[P_GAMMA2];
+			Model::P1      = c.params[P_P1];
+			Model::P2      = c.params[P_P2];
+			Model::cp1     = c.params[P_CP1];
+			Model::cp2     = c.params[P_CP2];
+			Model::cv1     = c.params[P_CV1];
+			Model::cv2     = c.params[P_CV2];
+			Model::mu1     = c.params[P_MU1];
+			Model::mu2     = c.params[P_MU2];
+			Model::lambda1 = c.params[P_LAMBDA1];
+			Model::lambda2 = c.params[P_LAMBDA2];
+			Model::sigma   = c.params[P_SIGMA];
+		} else if constexpr (Model::Viscosity) {
+			Model::mu_     = c.params[P_NS_MU];
+			Model::lambda_ = c.params[P_NS_LAMBDA];
+		}
+	}
+
+	// Counts active leaves whose stored neighbour index differs from a fresh Domain::find, i.e.
+	// pointers that update_neighbors (integrator/domain.hpp:249-293) would change if called now.
+	template<typename Integ>
+	long audit_neighbors(Integ &in) {
+		using vecn_t = typename Integ::vecn_t_pub;
+		long bad     = 0;
+		auto &dom    = in.domain;
+		for (size_t i = 1; i < dom.tree.size(); ++i) {
+			auto &node = dom.tree[i];
+			if (!node.is_leaf || !node.is_active || node.is_garbage) continue;
+			for (int dim = 0; dim < (int) Integ::NumDims; dim++) {
+				for (int dir = 0; dir < 2; dir++) {
+					if (node.boundaries.get(dim, dir).has_value()) continue;
+					vecn_t loc = node.cell.center + vecn_t::unit(dim) * node.cell.size * (2 * dir - 1.0);
+					size_t nb  = dom.find(loc, node.tree_level);
+					if (!nb || !dom.tree[nb].is_active) continue;
+					if (nb != node.neighbors.get(dim, dir)) bad++;
+				}
+			}
+		}
+		return bad;
+	}
+
+	template<typename Model>
+	struct Runner : public integrator::Integrator<Model, integrator::slope::minmod, integrator::error::weighted_laplacian<Model::NumEqns>> {
+		using Base     = integrator::Integrator<Model, integrator::slope::minmod, integrator::error::weighted_laplacian<Model::NumEqns>>;
+		using vecn_t_pub = linalg::vec<scalar_t, Model::NumDims>;
+		using Base::Base;
+	};
+
+	template<typename Model>
+	void write_snapshot(Runner<Model> &in, const std::string &path, int step, double time, double updates) {
+		constexpr int D = Model::NumDims;
+		constexpr int E = Model::NumEqns;
+		oracle::SnapWriter w(path);
+		size_t n_clusters = 0;
+		for (int l = 0; l < Runner<Model>::MAX_LEVEL; l++) n_clusters += in.acti_clusters[l].size();
+		int32_t hdr[8] = {D, E, (int32_t) in.n_active_cells(), (int32_t) n_clusters, step, in.n_substeps, (int32_t) in.domain.tree.size(), 0};
+		w.put("DGSNAP01", 8);
+		w.put(hdr, 8);
+		double hd[3] = {time, in.global_dt, updates};
+		w.put(hd, 3);
+		in.for_each_active_cell([&](int, auto &node) {
+			int32_t lv[2] = {node.tree_level, node.acti_level};
+			w.put(lv, 2);
+			double buf[D + 1 + 2 * E + 3];
+			int k = 0;
+			for (int d = 0; d < D; d++) buf[k++] = node.cell.center[d];
+			buf[k++] = node.cell.t;
+			for (int q = 0; q < E; q++) buf[k++] = node.cell.u[q];
+			for (int q = 0; q < E; q++) buf[k++] = node.cell.p[q];
+			buf[k++] = node.error;
+			buf[k++] = node.max_dt;
+			buf[k++] = node.cfl;
+			w.put(buf, k);
+		});
+	}
+
+	template<typename Model>
+	int run(const oracle::CaseData &c, const Options &o) {
+		using namespace oracle;
+		constexpr int D = Model::NumDims;
+		constexpr int E = Model::NumEqns;
+		set_model_constants<Model>(c);
+
+		auto cfg         = std::make_shared<config::Config<Model>>();
+		cfg->case_data   = &c;
+		cfg->side_length = c.params[P_SIDE];
+		for (int d = 0; d < D; d++) {
+			cfg->active_size[d] = c.params[P_ACTIVE0 + d];
+			cfg->IsPeriodic[d]  = c.params[P_PERIODIC0 + d] != 0.0;
+		}
+		cfg->max_cfl              = c.params[P_MAX_CFL];
+		cfg->max_dt               = c.params[P_MAX_DT];
+		cfg->error_threshold      = vec2_t{c.params[P_MIN_ERR], c.params[P_MAX_ERR]};
+		cfg->max_refinement_level = (int) c.params[P_MAX_LEVEL];
+		cfg->min_refinement_level = (int) c.params[P_MIN_LEVEL];
+		typename Model::prim_t w;
+		for (int q = 0; q < E; q++) w[q] = c.weights[q];
+		cfg->error_weights = w;
+		for (auto &z: c.zones) {
+			typename config::Config<Model>::RefineZone rz;
+			rz.x0               = vec3_t{z.x0[0], z.x0[1], z.x0[2]};
+			rz.x1               = vec3_t{z.x1[0], z.x1[1], z.x1[2]};
+			rz.refinement_level = (size_t) z.level;
+			cfg->refine_zones.push_back(rz);
+		}
+
+		scene::Scene<Model> scene(cfg);
+		using clk = std::chrono::steady_clock;
+		auto t0   = clk::now();
+		Runner<Model> in{integrator::slope::minmod{}, integrator::error::weighted_laplacian<E>{w}, scene, cfg};
+		double init_s = std::chrono::duration<double>(clk::now() - t0).count();
+
+		double time = 0.0, updates = 0.0, integ_s = 0.0;
+		long substeps = 0, gc_events = 0, audit_bad = 0;
+		int steps_done   = 0;
+		bool force_break = false;
+		if (o.checks.count(0)) write_snapshot(in, o.out_prefix + "_0.snap", 0, time, updates);
+
+		for (int step = 1; step <= o.n_steps; ++step) {
+			if (o.t_end > 0 && time >= o.t_end) break;
+			double step_updates = 0.0;
+			bool will_gc        = false;
+			auto hook           = [&](auto &itg, int level, scalar_t, int, scalar_t) {
+                step_updates += (double) itg.acti_clusters[level].size();
+                substeps++;
+                if (level == 0) {
+                    size_t n = 0;
+                    for (int l = 0; l < Runner<Model>::MAX_LEVEL; l++) n += itg.acti_clusters[l].size();
+                    will_gc = (double) n / (double) (itg.domain.tree.size() - 1) < 0.2;
+                }
+			};
+			auto a = clk::now();
+			in.integrate(hook, true, force_break);
+			integ_s += std::chrono::duration<double>(clk::now() - a).count();
+			time += in.global_dt;
+			updates += step_updates;
+			steps_done = step;
+			if (will_gc) gc_events++;
+			if (o.neighbor_audit) audit_bad += audit_neighbors(in);
+			if (o.checks.count(step)) write_snapshot(in, o.out_prefix + "_" + std::to_string(step) + ".snap", step, time, updates);
+			if (force_break) break;
+		}
+
+		std::printf("{\"steps\": %d, \"time\": %.17g, \"global_dt\": %.17g, \"substeps\": %ld, \"updates\": %.0f, "
+		            "\"integrate_s\": %.6f, \"init_s\": %.6f, \"updates_per_s\": %.6g, \"n_active\": %zu, "
+		            "\"tree_size\": %zu, \"gc_events\": %ld, \"force_break\": %s, \"neighbor_audit_mismatch\": %ld, "
+		            "\"threads\": %d}\n",
+		            steps_done, time, in.global_dt, substeps, updates, integ_s, init_s,
+		            integ_s > 0 ? updates / integ_s : 0.0, in.n_active_cells(), in.domain.tree.size(), gc_events,
+		            force_break ? "true" : "false", audit_bad, omp_get_max_threads());
+		return force_break ? 3 : 0;
+	}
+
+}    // namespace
+
+int main(int argc, char **argv) {
+	if (argc < 4) {
+		std::fprintf(stderr, "usage: %s <case.bin> <out_prefix> <n_global_steps> [--check a,b] [--t-end T] [--neighbor-audit]\n", argv[0]);
+		return 2;
+	}
+	Options o;
+	o.case_path  = argv[1];
+	o.out_prefix = argv[2];
+	o.n_steps    = std::atoi(argv[3]);
+	for (int i = 4; i < argc; ++i) {
+		std::string a = argv[i];
+		if (a == "--check" && i + 1 < argc) {
+			std::stringstream ss(argv[++i]);
+			std::string tok;
+			while (std::getline(ss, tok, ',')) o.checks.insert(std::atoi(tok.c_str()));
+		} else if (a == "--t-end" && i + 1 < argc) {
+			o.t_end = std::atof(argv[++i]);
+		} else if (a == "--neighbor-audit") {
+			o.neighbor_audit = true;
+		} else if (a == "--quiet") {
+			o.quiet = true;
+		}
+	}
+	spdlog::set_level(spdlog::level::warn);
+	oracle::CaseData c = oracle::read_case(o.case_path);
+	switch (c.model * 10 + c.dims) {
+		case 2: return run<model::euler<2>>(c, o);
+		case 3: return run<model::euler<3>>(c, o);
+		case 12: return run<model::navier_stokes<2>>(c, o);
+		case 13: return run<model::navier_stokes<3>>(c, o);
+		case 22: return run<model::multi<2>>(c, o);
+		case 23: return run<model::multi<3>>(c, o);
+		default: std::fprintf(stderr, "unsupported model/dims %d/%d\n", c.model, c.dims); return 2;
+	}
+}
