@@ -24,15 +24,19 @@ def _zg_box(D: int):
     return [(ZG, ZG) for _ in range(D)]
 
 
-def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_cfl: float = 0.5) -> Case:
+def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
+             model: ModelId = ModelId.EULER, mu: float = 0.0, prandtl: Optional[float] = None) -> Case:
     """Config 1: 2D Euler Lax-Liu configuration 3 on the unit square, quadrants split at x=y=0.
 
     States (rho, u, v, p): TR (1.5,0,0,1.5), TL (0.5323,1.206,0,0.3), BL (0.138,1.206,1.206,0.029),
     BR (0.5323,0,1.206,0.3); outflow (zero-gradient) boundaries; density-weighted Laplacian
     indicator. The pair of thresholds (0.02, 0.05) is one for which the reference completes the run
     to t = 0.3 (tighter pairs make the reference itself produce NaN near t = 0.29).
+
+    With ``model=ModelId.NAVIER_STOKES`` the same problem runs with constant viscosity ``mu`` and
+    conductivity ``mu * cp / prandtl`` (model/navier_stokes.hpp:454-459).
     """
-    shape = ModelShape(ModelId.EULER, 2)
+    shape = ModelShape(model, 2)
 
     def x2p(c: np.ndarray) -> np.ndarray:
         x, y = c[:, 0], c[:, 1]
@@ -52,6 +56,7 @@ def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_
         side_length=1.0, active_size=(1.0, 1.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
         weights=(1.0, 0.0, 0.0, 0.0),
+        ns_mu=mu, ns_lambda=(mu * 1005.0 / prandtl) if prandtl else 0.0,
     )
     return Case(build_tree(spec), prm)
 

@@ -5,6 +5,8 @@
 #include "../../include/dacti_gpu.h"
 #include "stages.cuh"
 
+#include <cub/cub.cuh>
+
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -366,11 +368,20 @@ public:
 	void set_max_dt(double v) { max_dt_cfg_ = v; }
 
 private:
+	// smooth_alpha x3, normal_update, curvature_update, smooth_curvature over one cell list
+	// (impl/integrate.hpp:284-289, integrator/integrator.hpp:134-143).
 	void multiphase_aux(const int32_t *list, int n) {
-		// α smoothing, normals and curvature are added with the multiphase stages.
-		(void) list;
-		(void) n;
-		throw dg_error(DG_ERR_UNSUPPORTED, "multiphase auxiliary stages are not built yet");
+		if constexpr (M::MULTI) {
+			const int g = grid_for(n);
+			for (int it = 0; it < 3; ++it) {
+				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
+				k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS);
+			}
+			k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
+			k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
+			k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
+			k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA);
+		}
 	}
 
 	void sync_counters() {
@@ -480,7 +491,56 @@ public:
 	}
 
 private:
-	void gc() { throw dg_error(DG_ERR_UNSUPPORTED, "garbage collection (Domain::gc) is not built yet"); }
+	// Integrator::gc (impl/acti_utils.hpp:59-74): compact the node slots, then reassign every active
+	// leaf to an ACTI level from its stored max_dt, resetting the hysteresis.
+	void gc() {
+		const int top = h_cnt_->top;
+		for (int l = 0; l < MAX_ACTI; ++l)
+			if (h_cnt_->buf[l] != 0) throw dg_error(DG_ERR_UNSUPPORTED, "garbage collection with non-empty ACTI buffers");
+		int32_t *keep = nullptr, *newidx = nullptr;
+		DG_CUDA(cudaMalloc(&keep, sizeof(int32_t) * (top + 1)));
+		DG_CUDA(cudaMalloc(&newidx, sizeof(int32_t) * (top + 1)));
+		const int g = grid_for(top);
+		k_gc_keep<<<g, BLOCK, 0, st_>>>(P_, top, keep);
+		size_t tmp_bytes = 0;
+		DG_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, keep, newidx, top + 1, st_));
+		void *tmp = nullptr;
+		DG_CUDA(cudaMalloc(&tmp, tmp_bytes));
+		DG_CUDA(cudaMemsetAsync(keep + top, 0, sizeof(int32_t), st_));
+		DG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, keep, newidx, top + 1, st_));
+		int new_top = 0;
+		DG_CUDA(cudaMemcpyAsync(&new_top, newidx + top, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		Pool NP{};
+		void *mem = carve_pool(NP, P_.cap);
+		auto fo = fields(P_), fn = fields(NP);
+		for (size_t k = 0; k < fo.size(); ++k) {
+			if (fo[k].comps <= 0) continue;
+			k_gc_move<<<g, BLOCK, 0, st_>>>((const char *) *fo[k].ptr, (char *) *fn[k].ptr, (int) fo[k].elem, fo[k].comps,
+			                                 P_.cap, top, keep, newidx);
+		}
+		DG_CUDA(cudaStreamSynchronize(st_));
+		k_gc_remap<D><<<grid_for(new_top), BLOCK, 0, st_>>>(NP, new_top, keep, newidx);
+		cudaFree(pool_mem_);
+		pool_mem_ = mem;
+		P_        = NP;
+		// full ACTI reassignment
+		Counters z{};
+		z.top    = new_top;
+		z.status = 0;
+		DG_CUDA(cudaMemcpyAsync(d_cnt_, &z, sizeof(Counters), cudaMemcpyHostToDevice, st_));
+		k_collect_active_leaves<<<grid_for(new_top), BLOCK, 0, st_>>>(P_, new_top, Ls_.fresh, &d_cnt_->n_new);
+		DG_CUDA(cudaStreamSynchronize(st_));
+		int n_leaves = 0;
+		DG_CUDA(cudaMemcpy(&n_leaves, &d_cnt_->n_new, sizeof(int), cudaMemcpyDeviceToHost));
+		k_assign<M><<<grid_for(n_leaves), BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, n_leaves, global_dt_, Ls_, d_cnt_);
+		DG_CUDA(cudaGetLastError());
+		sync_counters();
+		check_status();
+		cudaFree(tmp);
+		cudaFree(keep);
+		cudaFree(newidx);
+		n_gc_++;
+	}
 
 public:
 	long long cell_count() override {

@@ -868,3 +868,193 @@ __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, dou
 }
 
 }  // namespace dg
+
+namespace dg {
+
+// --------------------------------------------------------------------------------------------
+// Multiphase auxiliary stages (impl/smooth.hpp, impl/normal_curvature.hpp)
+// --------------------------------------------------------------------------------------------
+
+// Value of a parameter component on the far side of face (dim, dir): the boundary ghost's volume
+// fraction, the recursive child mean of k[comp] for finer neighbours, else the neighbour's k[comp].
+// `x` receives the centre distance used by compute_normal/compute_curvature (half a cell at a
+// boundary, impl/normal_curvature.hpp:161-183).
+template<class M>
+__device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int i, int dim, int dir,
+                         int comp, bool zero_at_boundary, double &x) {
+	const int cap  = P.cap;
+	const int nb   = P.nbr[(size_t) (2 * dim + dir) * cap + i];
+	const double h = C.size[P.level[i]];
+	if (nb == 0) {
+		x = dir == 0 ? -0.5 * h : 0.5 * h;
+		if (zero_at_boundary) return 0.0;
+		const int b = P.bc[(size_t) (2 * dim + dir) * cap + i];
+		double pc[M::E], pb[M::E];
+		load_p<M>(P, i, pc);
+		if (b < 0) {
+			set_status(status, ST_MISSING_BC);
+			return pc[M::IA];
+		}
+		boundary_value<M>(C.m, B, b, pc, P.t[i], pb);
+		return pb[M::IA];
+	}
+	const double hn = C.size[P.level[nb]];
+	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
+	if (!(P.flags[nb] & F_LEAF)) return interp_scalar<M::D, INTERP_DEPTH>(P, status, nb, P.k + (size_t) comp * cap);
+	return at(P.k, cap, comp, nb);
+}
+
+// smooth_alpha, one Jacobi sweep into P.tmp (impl/smooth.hpp:10-51)
+template<class M>
+__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i     = list[tid];
+		const double ac = at(P.k, cap, M::ALPHAS, i);
+		double s        = 0.0;
+		for (int dim = 0; dim < M::D; ++dim) {
+			double x;
+			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x);
+			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x);
+			s += 0.5 * (an + ap) + ac;
+		}
+		P.tmp[i] = s / (double) (2 * M::D);
+	}
+}
+
+static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp) {
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		P.k[(size_t) comp * P.cap + i] = P.tmp[i];
+	}
+}
+
+// compute_normal (impl/normal_curvature.hpp:7-55)
+template<class M>
+__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	constexpr int D = M::D;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double nrm[D];
+		for (int dim = 0; dim < D; ++dim) {
+			double xn, xp;
+			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, xn);
+			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, xp);
+			nrm[dim] = (ap - an) / (xp - xn);
+		}
+		double sq = 0.0;
+		for (int d = 0; d < D; ++d) sq += nrm[d] * nrm[d];
+		const double len = sqrt(sq);
+		for (int d = 0; d < D; ++d) nrm[d] = (len < 1e-10) ? 0.0 : nrm[d] / len;
+		for (int d = 0; d < D; ++d) P.k[(size_t) (M::IKN + d) * cap + i] = nrm[d];
+	}
+}
+
+// compute_curvature (impl/normal_curvature.hpp:59-102)
+template<class M>
+__global__ void k_curvature(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i  = list[tid];
+		double kappa = 0.0;
+		for (int dim = 0; dim < M::D; ++dim) {
+			double xn, xp;
+			const double nn = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::IKN + dim, true, xn);
+			const double np = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::IKN + dim, true, xp);
+			kappa -= (np - nn) / (xp - xn);
+		}
+		P.k[(size_t) M::KAPPA * cap + i] = kappa;
+	}
+}
+
+// smooth_curvature, one weighted sweep into P.tmp (impl/smooth.hpp:63-133)
+template<class M>
+__global__ void k_smooth_kappa(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i     = list[tid];
+		const double kc = at(P.k, cap, M::KAPPA, i);
+		const double as = at(P.k, cap, M::ALPHAS, i);
+		const double xc = as * (1 - as);
+		const double wc = xc * xc;
+		double ks = 0.0, w = 0.0;
+		for (int dim = 0; dim < M::D; ++dim) {
+			double kv[2], av[2];
+			for (int dir = 0; dir < 2; ++dir) {
+				const int nb = P.nbr[(size_t) (2 * dim + dir) * cap + i];
+				if (nb == 0) {
+					kv[dir] = 0.0;
+					const int b = P.bc[(size_t) (2 * dim + dir) * cap + i];
+					double pc[M::E], pb[M::E];
+					load_p<M>(P, i, pc);
+					if (b < 0) {
+						set_status(&cnt->status, ST_MISSING_BC);
+						av[dir] = pc[M::IA];
+					} else {
+						boundary_value<M>(C.m, B, b, pc, P.t[i], pb);
+						av[dir] = pb[M::IA];
+					}
+				} else if (!(P.flags[nb] & F_LEAF)) {
+					kv[dir] = interp_scalar<M::D, INTERP_DEPTH>(P, &cnt->status, nb, P.k + (size_t) M::KAPPA * cap);
+					av[dir] = interp_scalar<M::D, INTERP_DEPTH>(P, &cnt->status, nb, P.p + (size_t) M::IA * cap);
+				} else {
+					kv[dir] = at(P.k, cap, M::KAPPA, nb);
+					av[dir] = at(P.p, cap, M::IA, nb);
+				}
+			}
+			const double xn = av[0] * (1 - av[0]), xp = av[1] * (1 - av[1]);
+			const double wn = xn * xn, wp = xp * xp;
+			ks += 0.5 * (wn * kv[0] + wp * kv[1]) + kc * wc;
+			w += 0.5 * (wn + wp) + wc;
+		}
+		P.tmp[i] = (w > 1e-6) ? ks / w : 0.0;
+	}
+}
+
+// --------------------------------------------------------------------------------------------
+// Garbage collection (integrator/domain.hpp:327-356): order-preserving compaction of the non-garbage
+// slots with every link remapped (links to removed slots become 0).
+// --------------------------------------------------------------------------------------------
+static __global__ void k_gc_keep(Pool P, int top, int32_t *keep) {
+	for (int i = gtid(); i < top; i += gstride()) keep[i] = (i == 0 || !(P.flags[i] & F_GARBAGE)) ? 1 : 0;
+}
+
+// Moves component c of every kept slot of `src` to its new index in `dst` (elem bytes per entry).
+static __global__ void k_gc_move(const char *src, char *dst, int elem, int comps, int cap, int top, const int32_t *keep,
+                          const int32_t *newidx) {
+	for (int i = gtid(); i < top; i += gstride()) {
+		if (!keep[i]) continue;
+		const int j = newidx[i];
+		for (int c = 0; c < comps; ++c) {
+			const size_t so = ((size_t) c * cap + i) * elem, dof = ((size_t) c * cap + j) * elem;
+			for (int b = 0; b < elem; ++b) dst[dof + b] = src[so + b];
+		}
+	}
+}
+
+template<int D>
+__global__ void k_gc_remap(Pool P, int new_top, const int32_t *keep, const int32_t *newidx) {
+	constexpr int NC = 1 << D, NF = 2 * D;
+	const int cap = P.cap;
+	for (int j = gtid(); j < new_top; j += gstride()) {
+		auto mapv = [&](int32_t old) { return (old > 0 && keep[old]) ? newidx[old] : 0; };
+		P.parent[j] = mapv(P.parent[j]);
+		for (int c = 0; c < NC; ++c) P.child[(size_t) c * cap + j] = mapv(P.child[(size_t) c * cap + j]);
+		for (int f = 0; f < NF; ++f) P.nbr[(size_t) f * cap + j] = mapv(P.nbr[(size_t) f * cap + j]);
+		P.clu[j] = CLU_NONE;
+	}
+}
+
+static __global__ void k_collect_active_leaves(Pool P, int top, int32_t *out, int *count) {
+	for (int i = gtid(); i < top; i += gstride()) {
+		if (i == 0) continue;
+		const uint32_t f = P.flags[i];
+		if ((f & F_LEAF) && (f & F_ACTIVE) && !(f & F_GARBAGE)) {
+			int pos  = atomicAdd(count, 1);
+			out[pos] = i;
+		}
+	}
+}
+
+}  // namespace dg
