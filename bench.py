@@ -1,0 +1,343 @@
+#!/usr/bin/env python
+"""Benchmark of the octree finite-volume step: leaf cell-updates/s on the 3D air-water shock-drop.
+
+Workload: the five-equation model (multi<3>) on an 8 x 4 x 4 mm box, 64 x 32 x 32 base cells and
+4 refinement levels, local time stepping on, Mach 1.5 shock into air hitting a water drop of radius
+0.5 mm (synthetic initial condition). A step is one global step of the LTS scheme
+(Integrator::integrate), i.e. every ACTI level substep it contains; leaf cell-updates are the
+cluster sizes of the executed substeps. The plain FP64 form runs here.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
+
+N > 1 runs one independent replica per GPU (weak scaling; the shock-drop step has no exchange in this
+build). `--impl reference` times the reference's own CPU solver (built from its sources by
+oracle/Makefile) on this box's host cores, in bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, HERE)
+
+METRIC = "leaf cell-updates/s at fixed L1 err vs FP64: mixed+batched+learned vs plain GPU"
+UNIT = "cell-updates/s"
+BYTES_PER_UPDATE = {2: 148, 3: 148}  # multi<3>: 16 E + 8 D + 12 with E = 7, D = 3
+REF_RUNNER = os.path.join(HERE, "oracle", "_ref", "dacti_ref_runner_fast")
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["gpu", "reference"], default="gpu")
+    ap.add_argument("--base-level", type=int, default=6)
+    ap.add_argument("--levels", type=int, default=4)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def workload_config(args) -> dict:
+    nb = 1 << args.base_level
+    return {
+        "workload": f"shock_drop_3d multi<3> {nb}x{nb // 2}x{nb // 2} base +{args.levels} levels, LTS, max_cfl 0.25, "
+                    f"Mach 1.5 shock on a 0.5 mm water drop, plain FP64 form",
+        "model": "multi<3> (five-equation, stiffened gas)",
+        "base_grid": [nb, nb // 2, nb // 2],
+        "levels": args.levels,
+        "step": "one global LTS step (all ACTI level substeps)",
+        "l2": "state resident in HBM and larger than L2 (no flush needed)",
+        "parallelism": f"replicas x{args.gpus}",
+    }
+
+
+def make_case(args):
+    from dacti_b200 import cases
+    return cases.shock_drop(base_level=args.base_level, levels=args.levels)
+
+
+def measured_peak():
+    path = os.path.join(HERE, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        self.out.flush()
+        self.out.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_samples(case_path: str, samples: int, substeps: int, threads: int) -> dict:
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([REF_RUNNER, case_path, os.path.join(tempfile.gettempdir(), "dg_ref"), "0",
+                        "--sample-substeps", str(substeps), "--samples", str(samples)],
+                       capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference runner failed: {r.stderr[-2000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def host_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+# ------------------------------------------------------------------------------------------------
+def bench_reference(args, rank: int, world: int) -> None:
+    if rank != 0:
+        return
+    from dacti_b200.casefile import write_case
+    case = make_case(args)
+    threads = host_threads()
+    sub = 60
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "case.bin")
+        write_case(case, path)
+        res = run_reference_samples(path, args.warmup + args.steps, sub, threads)
+    timed = res["samples"][args.warmup:]
+    upd = sum(s["updates"] for s in timed)
+    sec = sum(s["seconds"] for s in timed)
+    value = upd / sec if sec > 0 else 0.0
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sec / max(len(timed), 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"{len(timed)} samples of {sub} LTS substeps each of the first global step, "
+                                   f"reference Integrator (oracle/_ref/dacti_ref_runner_fast, -O3 -fopenmp) on "
+                                   f"{threads} threads of {cpu_model()}"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    import torch.distributed as dist
+    from dacti_b200.casefile import write_case
+    from dacti_b200.solver import KERNEL_KINDS, Solver
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    case = make_case(args)
+    D = case.shape.dims
+
+    solver = Solver(case, device=local_rank)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_profiling(True)
+    for _ in range(args.warmup):
+        solver.integrate()
+    st0 = solver.stats()
+
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            solver.integrate()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    st1 = solver.stats()
+    updates = float(st1.cell_updates - st0.cell_updates)
+    launches = int(st1.n_launches - st0.n_launches)
+
+    kms = {k: st1.kernel_ms[i] - st0.kernel_ms[i] for i, k in enumerate(KERNEL_KINDS)}
+    kl = {k: st1.kernel_launches[i] - st0.kernel_launches[i] for i, k in enumerate(KERNEL_KINDS)}
+    kc = {k: st1.kernel_cells[i] - st0.kernel_cells[i] for i, k in enumerate(KERNEL_KINDS)}
+
+    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    u_sum = torch.tensor([updates], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u_sum, op=dist.ReduceOp.SUM)
+    ms_max = float(t_max.item())
+    total_updates = float(u_sum.item())
+    value = total_updates / (ms_max * 1e-3)
+
+    # roofline of the dominant kernel (the flux stage): algorithmic bytes per cell update times the
+    # cells of its launches, over its CUDA-event time on the solver's stream
+    peak, peak_kind = measured_peak()
+    dom = max(kms, key=lambda k: kms[k])
+    b_per = BYTES_PER_UPDATE[D]
+    flux_ms = kms["flux"]
+    achieved = (b_per * kc["flux"]) / (flux_ms * 1e-3) / 1e9 if flux_ms > 0 else 0.0
+    traffic = None
+    tpath = os.path.join(HERE, "profiles", "flux_traffic.json")
+    if os.path.exists(tpath):
+        try:
+            with open(tpath) as f:
+                tj = json.load(f)
+            traffic = tj["bytes_per_cell"] * (kc["flux"] / max(kl["flux"], 1))
+        except Exception:
+            traffic = None
+    roofline = {
+        "bound": "hbm", "kernel": "k_flux (HLLC flux, cluster gather)", "achieved": achieved, "peak": peak,
+        "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+        "bytes_per_cell_update": b_per, "kernel_share": {k: round(v / max(sum(kms.values()), 1e-9), 4)
+                                                          for k, v in kms.items() if v > 0},
+        "dominant_kernel_by_time": dom,
+    }
+
+    result = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(args),
+        "form": "plain FP64", "gpu_launches": launches, "roofline": roofline, "clocks": clk.summary(),
+        "cells": solver.n_active_cells(), "substeps_timed": int(st1.n_substeps - st0.n_substeps),
+    }
+    solver.close()
+    del solver
+
+    # end to end through the public API: host tree -> device, K steps with the per-step scalars read
+    # back, then every active cell read back to the host
+    if not args.no_e2e:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s2 = Solver(case, device=local_rank)
+        s2.set_stream(stream.cuda_stream)
+        e_upd0 = s2.stats().cell_updates
+        for _ in range(args.steps):
+            s2.integrate()
+            s2.stats()
+        snap = s2.active_cells()
+        torch.cuda.synchronize()
+        e_sec = time.perf_counter() - t0
+        e_upd = float(s2.stats().cell_updates - e_upd0)
+        t_e = torch.tensor([e_sec], dtype=torch.float64, device="cuda")
+        u_e = torch.tensor([e_upd], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+            dist.all_reduce(u_e, op=dist.ReduceOp.SUM)
+        tree = case.tree
+        h2d = (tree.parent.nbytes + tree.children.nbytes + tree.level.nbytes + tree.flags.nbytes + tree.bc.nbytes +
+               tree.center.nbytes + tree.p.nbytes)
+        d2h = snap.n * (8 * (D + 1 + 2 * case.shape.E + 3) + 8)
+        result["e2e"] = {"value": float(u_e.item()) / float(t_e.item()), "unit": UNIT,
+                         "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
+                         "includes": "solver construction from the host tree, K steps, read-back of all cells"}
+        s2.close()
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_RUNNER):
+        threads = host_threads()
+        sub = 60
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "case.bin")
+            write_case(case, path)
+            res = run_reference_samples(path, 1, sub, threads)
+        s = res["samples"][0]
+        result["cpu_baseline"] = {
+            "value": s["updates"] / s["seconds"], "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"first {sub} LTS substeps of the first global step ({s['updates']:.0f} updates), reference "
+                      f"Integrator built from its sources (-O3 -fopenmp), {threads} threads of {cpu_model()}",
+        }
+    if rank == 0:
+        print(json.dumps(result), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        bench_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        bench_gpu(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

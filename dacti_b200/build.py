@@ -62,7 +62,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     with ThreadPoolExecutor(max_workers=len(UNITS)) as ex:
         objs = list(ex.map(compile_one, UNITS))
     tmp = LIB + ".tmp"
-    cmd = [cc, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    # the library carries its own (static) CUDA runtime, independent of any runtime a host process
+    # such as torch loads
+    cmd = [cc, *ARCH, "-shared", "-cudart", "static", "-o", tmp, *objs]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         raise RuntimeError(f"link failed:\n{r.stderr[-4000:]}")

@@ -180,3 +180,67 @@ def read_snapshot(path: str) -> Snapshot:
         d[:, D + 1: D + 1 + E].copy(), d[:, D + 1 + E: D + 1 + 2 * E].copy(), d[:, D + 1 + 2 * E].copy(),
         d[:, D + 2 + 2 * E].copy(), d[:, D + 3 + 2 * E].copy(),
     )
+
+
+def read_case(path: str) -> Case:
+    """Inverse of write_case."""
+    from .models import BcType
+    from .scene import BoundarySpec, RefineZone, Tree
+
+    with open(path, "rb") as f:
+        buf = f.read()
+    if buf[:8] != b"DGCASE01":
+        raise ValueError("bad case magic")
+    off = 8
+    hdr = np.frombuffer(buf, np.int32, 8, off)
+    off += 32
+    model, D, n, nbc, nz = (int(x) for x in hdr[:5])
+    shape = ModelShape(ModelId(model), D)
+    E, C, NF = shape.E, shape.C, shape.NF
+    prm = np.frombuffer(buf, np.float64, N_PARAMS, off)
+    off += 8 * N_PARAMS
+    weights = np.frombuffer(buf, np.float64, E, off).copy()
+    off += 8 * E
+    zones = []
+    for _ in range(nz):
+        z = np.frombuffer(buf, np.float64, 7, off)
+        off += 56
+        zones.append(RefineZone(list(z[:3]), list(z[3:6]), int(z[6])))
+    bcs = []
+    for _ in range(nbc):
+        tp = np.frombuffer(buf, np.int32, 2, off)
+        off += 8
+        pin = np.frombuffer(buf, np.float64, E, off).copy()
+        off += 8 * E
+        nrm = np.frombuffer(buf, np.float64, D, off).copy()
+        off += 8 * D
+        fade = float(np.frombuffer(buf, np.float64, 1, off)[0])
+        off += 8
+        bcs.append(BoundarySpec(BcType(int(tp[0])), list(pin), list(nrm), fade))
+
+    def take(dtype, count, shape_=None):
+        nonlocal off
+        a = np.frombuffer(buf, dtype, count, off).copy()
+        off += a.nbytes
+        return a.reshape(shape_) if shape_ else a
+
+    parent = take(np.int32, n)
+    children = take(np.int32, n * C, (n, C))
+    level = take(np.int32, n)
+    flags = take(np.uint32, n)
+    bc = take(np.int32, n * NF, (n, NF))
+    center = take(np.float64, n * D, (n, D))
+    p = take(np.float64, n * E, (n, E))
+    tree = Tree(shape, parent, children, level, flags, bc, center, p, bcs)
+    params = SolverParams(
+        side_length=float(prm[P["SIDE"]]), active_size=[float(prm[P["ACTIVE0"] + d]) for d in range(D)],
+        periodic=[bool(prm[P["PERIODIC0"] + d]) for d in range(D)], max_cfl=float(prm[P["MAX_CFL"]]),
+        max_dt=float(prm[P["MAX_DT"]]), error_threshold=(float(prm[P["MIN_ERR"]]), float(prm[P["MAX_ERR"]])),
+        max_level=int(prm[P["MAX_LEVEL"]]), min_level=int(prm[P["MIN_LEVEL"]]), weights=list(weights),
+        ns_mu=float(prm[P["NS_MU"]]), ns_lambda=float(prm[P["NS_LAMBDA"]]), gamma1=float(prm[P["GAMMA1"]]),
+        gamma2=float(prm[P["GAMMA2"]]), P1=float(prm[P["P1"]]), P2=float(prm[P["P2"]]), cp1=float(prm[P["CP1"]]),
+        cp2=float(prm[P["CP2"]]), cv1=float(prm[P["CV1"]]), cv2=float(prm[P["CV2"]]), mu1=float(prm[P["MU1"]]),
+        mu2=float(prm[P["MU2"]]), lambda1=float(prm[P["LAMBDA1"]]), lambda2=float(prm[P["LAMBDA2"]]),
+        sigma=float(prm[P["SIGMA"]]), zones=zones,
+    )
+    return Case(tree, params)

@@ -5,14 +5,18 @@
 
 struct dg_solver {
 	dg::SolverBase *impl;
+	int device;
 };
 
 namespace {
 thread_local std::string g_create_error;
+thread_local int g_device = 0;
 
 template<typename Fn>
 int guarded(dg_solver *s, Fn &&fn) {
 	try {
+		cudaError_t e = cudaSetDevice(s ? s->device : g_device);
+		if (e != cudaSuccess) throw dg::dg_error(DG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
 		fn();
 		return DG_OK;
 	} catch (const dg::dg_error &e) {
@@ -40,8 +44,14 @@ int dg_create(const dg_case *c, dg_solver **out) {
 			case DG_MULTI: impl = dg::make_solver_multi(*c); break;
 			default: throw dg::dg_error(DG_ERR_ARG, "unknown model id");
 		}
-		*out = new dg_solver{impl};
+		*out = new dg_solver{impl, g_device};
 	});
+}
+
+int dg_set_device(int ordinal) {
+	if (ordinal < 0) return DG_ERR_ARG;
+	g_device = ordinal;
+	return DG_OK;
 }
 
 int dg_set_stream(dg_solver *s, void *stream) {
@@ -72,6 +82,11 @@ int dg_get_stats(dg_solver *s, dg_stats *out) {
 	return guarded(s, [&] { s->impl->stats(out); });
 }
 
+int dg_set_profiling(dg_solver *s, int on) {
+	if (!s) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_profiling(on != 0); });
+}
+
 const char *dg_last_error(dg_solver *s) {
 	if (!s) return g_create_error.c_str();
 	return s->impl->last_error.c_str();
@@ -79,6 +94,7 @@ const char *dg_last_error(dg_solver *s) {
 
 void dg_destroy(dg_solver *s) {
 	if (!s) return;
+	cudaSetDevice(s->device);
 	delete s->impl;
 	delete s;
 }

@@ -37,6 +37,7 @@ public:
 	virtual long long read_cells(int *levels, double *data, long long max_cells) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
+	virtual void set_profiling(bool on) = 0;
 	std::string last_error;
 };
 
@@ -76,7 +77,63 @@ class Solver : public SolverBase {
 	long long n_split_total_ = 0, n_unsplit_total_ = 0;
 	int stamp_ = 0;
 
+	// launch accounting and optional per-kernel event timing
+	struct Pending {
+		int kind;
+		cudaEvent_t a, b;
+		long long cells;
+	};
+	bool prof_ = false;
+	std::vector<cudaEvent_t> ev_free_;
+	std::vector<Pending> pending_;
+	double kms_[DG_NK]          = {};
+	long long klaunch_[DG_NK]   = {};
+	long long kcells_[DG_NK]    = {};
+	long long n_launches_       = 0;
+
+	cudaEvent_t get_event() {
+		if (ev_free_.empty()) {
+			cudaEvent_t e;
+			DG_CUDA(cudaEventCreate(&e));
+			return e;
+		}
+		cudaEvent_t e = ev_free_.back();
+		ev_free_.pop_back();
+		return e;
+	}
+
+	template<class Fn>
+	void run_k(int kind, long long cells, Fn &&fn) {
+		cudaEvent_t a = nullptr, b = nullptr;
+		if (prof_) {
+			a = get_event();
+			b = get_event();
+			DG_CUDA(cudaEventRecord(a, st_));
+		}
+		fn();
+		n_launches_++;
+		klaunch_[kind]++;
+		kcells_[kind] += cells;
+		if (prof_) {
+			DG_CUDA(cudaEventRecord(b, st_));
+			pending_.push_back({kind, a, b, cells});
+		}
+	}
+
+	void drain_events() {
+		for (auto &p: pending_) {
+			float ms = 0.f;
+			DG_CUDA(cudaEventElapsedTime(&ms, p.a, p.b));
+			kms_[p.kind] += ms;
+			ev_free_.push_back(p.a);
+			ev_free_.push_back(p.b);
+		}
+		pending_.clear();
+	}
+
 public:
+	void set_profiling(bool on) override { prof_ = on; }
+
 	explicit Solver(const dg_case &c) {
 		limiter_ = c.limiter;
 		setup_consts(c);
@@ -101,6 +158,11 @@ public:
 		cudaFree(d_leaves_);
 		cudaFree(d_read_);
 		cudaFree(d_readlv_);
+		for (auto e: ev_free_) cudaEventDestroy(e);
+		for (auto &p: pending_) {
+			cudaEventDestroy(p.a);
+			cudaEventDestroy(p.b);
+		}
 	}
 
 	void set_stream(cudaStream_t s) override { st_ = s; }
@@ -374,19 +436,20 @@ private:
 		if constexpr (M::MULTI) {
 			const int g = grid_for(n);
 			for (int it = 0; it < 3; ++it) {
-				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
-				k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS);
+				run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS); });
 			}
-			k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
-			k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
-			k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_);
-			k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA);
+			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA); });
 		}
 	}
 
 	void sync_counters() {
 		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters), cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
+		drain_events();
 	}
 
 	void check_status() {
@@ -411,30 +474,51 @@ private:
 		int32_t *list      = Ls_.clu[L];
 		const int counterL = acti_counter_[L];
 
-		k_flux<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL, stamp_recv, 1, Ls_.recv, d_cnt_);
-		k_flux<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0, L, dtL,
-		                                                          stamp_recv, 0, Ls_.recv, d_cnt_);
-		k_update<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
-		k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		run_k(DG_K_FLUX, n, [&] {
+			k_flux<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL, stamp_recv, 1, Ls_.recv, d_cnt_);
+		});
+		run_k(DG_K_RECV, 0, [&] {
+			k_flux<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0, L, dtL,
+			                                                          stamp_recv, 0, Ls_.recv, d_cnt_);
+		});
+		run_k(DG_K_UPDATE, n, [&] { k_update<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_); });
+		run_k(DG_K_SLOPE, n, [&] { k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_); });
 		if constexpr (M::MULTI) multiphase_aux(list, n);
-		k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
-		k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_);
-		k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, d_cnt_);
-		k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, d_cnt_);
+		run_k(DG_K_ESTIMATE, n, [&] {
+			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
+		});
 		const int gf = grid_for((long long) n * (NC + 1));
-		k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
-		k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, 0, Ls_.upd, d_cnt_);
-		k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_);
-		k_reassign<M><<<gf, BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, &d_cnt_->n_new, 0, L, dtL, counterL, Ls_, d_cnt_);
+		run_k(DG_K_REGRID, n, [&] { k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_); });
+		run_k(DG_K_REGRID, 0, [&] {
+			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, d_cnt_);
+		});
+		run_k(DG_K_REGRID, 0, [&] {
+			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, d_cnt_);
+		});
+		run_k(DG_K_REGRID, 0, [&] {
+			k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
+		});
+		run_k(DG_K_REGRID, 0, [&] {
+			k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, 0, Ls_.upd,
+			                                                                          d_cnt_);
+		});
+		run_k(DG_K_REASSIGN, n, [&] {
+			k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_);
+		});
+		run_k(DG_K_REASSIGN, 0, [&] {
+			k_reassign<M><<<gf, BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, &d_cnt_->n_new, 0, L, dtL, counterL, Ls_, d_cnt_);
+		});
 		std::swap(Ls_.clu[L], Ls_.tmp);
-		k_set_count<<<1, 1, 0, st_>>>(&d_cnt_->clu[L], &d_cnt_->n_tmp);
+		run_k(DG_K_OTHER, 0, [&] { k_set_count<<<1, 1, 0, st_>>>(&d_cnt_->clu[L], &d_cnt_->n_tmp); });
 		DG_CUDA(cudaGetLastError());
 	}
 
 	void flush(int L) {
 		if (h_cnt_->buf[L] == 0) return;
-		k_flush<<<grid_for(h_cnt_->buf[L]), BLOCK, 0, st_>>>(P_, Ls_.buf[L], &d_cnt_->buf[L], Ls_.clu[L], &d_cnt_->clu[L], L,
-		                                                   d_cnt_);
+		run_k(DG_K_FLUSH, h_cnt_->buf[L], [&] {
+			k_flush<<<grid_for(h_cnt_->buf[L]), BLOCK, 0, st_>>>(P_, Ls_.buf[L], &d_cnt_->buf[L], Ls_.clu[L],
+			                                                   &d_cnt_->clu[L], L, d_cnt_);
+		});
 		DG_CUDA(cudaMemsetAsync(&d_cnt_->buf[L], 0, sizeof(int), st_));
 		DG_CUDA(cudaGetLastError());
 	}
@@ -594,6 +678,12 @@ public:
 		o->cell_updates   = updates_;
 		o->max_acti_level = max_acti_;
 		o->global_dt      = global_dt_;
+		o->n_launches     = n_launches_;
+		for (int k = 0; k < DG_NK; ++k) {
+			o->kernel_ms[k]       = kms_[k];
+			o->kernel_launches[k] = klaunch_[k];
+			o->kernel_cells[k]    = kcells_[k];
+		}
 	}
 };
 

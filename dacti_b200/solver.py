@@ -50,7 +50,13 @@ class DgStats(ctypes.Structure):
         ("n_gc", ctypes.c_longlong), ("n_substeps", ctypes.c_longlong), ("n_global_steps", ctypes.c_longlong),
         ("cell_updates", ctypes.c_longlong), ("max_acti_level", ctypes.c_int), ("global_dt", ctypes.c_double),
         ("acti_time", ctypes.c_double * 16), ("acti_counter", ctypes.c_int * 16),
+        ("n_launches", ctypes.c_longlong), ("kernel_ms", ctypes.c_double * 12),
+        ("kernel_launches", ctypes.c_longlong * 12), ("kernel_cells", ctypes.c_longlong * 12),
     ]
+
+
+KERNEL_KINDS = ("flux", "recv", "update", "slope", "aux", "estimate", "regrid", "reassign", "flush", "init", "gc",
+                "other")
 
 
 SUBSTEP_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.c_double,
@@ -69,6 +75,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib = ctypes.CDLL(path)
     vp = ctypes.c_void_p
     lib.dg_create.argtypes = [ctypes.POINTER(DgCase), ctypes.POINTER(vp)]
+    lib.dg_set_device.argtypes = [ctypes.c_int]
     lib.dg_set_stream.argtypes = [vp, vp]
     lib.dg_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                             SUBSTEP_FN, vp]
@@ -76,6 +83,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_read_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                   ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
+    lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_last_error.argtypes = [vp]
     lib.dg_last_error.restype = ctypes.c_char_p
     lib.dg_destroy.argtypes = [vp]
@@ -84,8 +92,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return lib
 
 
-EXPORTED_SYMBOLS = ("dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells", "dg_get_stats",
-                    "dg_last_error", "dg_destroy")
+EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells", "dg_get_stats",
+                    "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
 class DgError(RuntimeError):
@@ -99,8 +107,9 @@ def _ptr(a: np.ndarray, ctype):
 
 
 class Solver:
-    def __init__(self, case: Case, limiter: str = "minmod"):
+    def __init__(self, case: Case, limiter: str = "minmod", device: int = 0):
         self._lib = load_library()
+        self._check_plain(self._lib.dg_set_device(device))
         t, prm = case.tree, case.params
         sh = t.shape
         self.shape = sh
@@ -186,6 +195,9 @@ class Solver:
         self._check(self._lib.dg_get_stats(self._h, ctypes.byref(s)))
         return s
 
+    def set_profiling(self, on: bool = True) -> None:
+        self._check(self._lib.dg_set_profiling(self._h, 1 if on else 0))
+
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._lib.dg_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
 
@@ -199,6 +211,10 @@ class Solver:
             self.close()
         except Exception:
             pass
+
+    def _check_plain(self, rc: int) -> None:
+        if rc != DG_OK:
+            raise DgError(rc, "invalid device")
 
     def _check(self, rc: int) -> None:
         if rc != DG_OK:

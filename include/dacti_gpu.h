@@ -79,6 +79,12 @@ typedef struct dg_case {
 typedef void (*dg_substep_fn)(void *user, int level, double acti_time, int n_substeps, double dt_level,
                               long long cluster_size);
 
+/* kernel kinds reported in dg_stats.kernel_* */
+enum {
+	DG_K_FLUX = 0, DG_K_RECV, DG_K_UPDATE, DG_K_SLOPE, DG_K_AUX, DG_K_ESTIMATE, DG_K_REGRID, DG_K_REASSIGN,
+	DG_K_FLUSH, DG_K_INIT, DG_K_GC, DG_K_OTHER, DG_NK
+};
+
 typedef struct dg_stats {
 	long long n_clusters[16];   /* cells per ACTI cluster */
 	long long n_buffers[16];    /* cells waiting in ACTI buffers */
@@ -90,7 +96,15 @@ typedef struct dg_stats {
 	double global_dt;
 	double acti_time[16];
 	int acti_counter[16];
+	long long n_launches;        /* kernels launched by this solver so far */
+	double kernel_ms[DG_NK];     /* device time per kernel kind (when profiling is on) */
+	long long kernel_launches[DG_NK];
+	long long kernel_cells[DG_NK]; /* cells processed per kernel kind (cluster-sized launches) */
 } dg_stats;
+
+/* Selects the CUDA device on which the calling thread's next dg_create builds its solver; every
+ * later call on that solver runs on the same device. Default: device 0. */
+int dg_set_device(int ordinal);
 
 /* Integrator constructor (integrator/integrator.hpp:72-163) on a flattened initial tree. */
 int dg_create(const dg_case *c, dg_solver **out);
@@ -111,6 +125,9 @@ int dg_cell_count(dg_solver *s, long long *n);
 int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
 int dg_get_stats(dg_solver *s, dg_stats *out);
+
+/* Per-kernel device timing with CUDA events on the solver's stream (off by default). */
+int dg_set_profiling(dg_solver *s, int on);
 
 /* Text of the last error on this solver (or of the last failed dg_create when s is NULL). */
 const char *dg_last_error(dg_solver *s);

@@ -5,6 +5,7 @@
 //
 // Usage: dacti_ref_runner <case.bin> <out_prefix> <n_global_steps> [--check s1,s2,..]
 //                         [--t-end T] [--neighbor-audit] [--quiet]
+//                         [--sample-substeps S --samples N]   (bounded timing samples)
 // Prints one JSON line with timing (wall time of integrate() calls only), substep and
 // leaf-update counts. Leaf cell-updates are counted in the substep hook as the level's cluster
 // size, as impl/integrate.hpp:57-64 exposes it.
@@ -34,6 +35,8 @@ namespace {
 		std::set<int> checks;
 		bool neighbor_audit = false;
 		bool quiet = false;
+		int sample_substeps = 0;  // >0: each integrate() call is timed up to this many substeps
+		int samples = 0;
 	};
 
 	template<typename Model>
@@ -159,6 +162,34 @@ namespace {
 		bool force_break = false;
 		if (o.checks.count(0)) write_snapshot(in, o.out_prefix + "_0.snap", 0, time, updates);
 
+		if (o.sample_substeps > 0) {
+			// Bounded timing samples: each integrate() call is timed from its start to the hook of its
+			// sample_substeps-th substep; the hook then requests the early return the NaN path uses.
+			std::printf("{\"init_s\": %.6f, \"threads\": %d, \"samples\": [", init_s, omp_get_max_threads());
+			for (int s = 0; s < o.samples; ++s) {
+				int seen = 0;
+				double upd = 0.0, took = 0.0;
+				bool stop = false;
+				auto a = clk::now();
+				auto hook = [&](auto &itg, int level, scalar_t, int, scalar_t) {
+					if (stop) return;
+					upd += (double) itg.acti_clusters[level].size();
+					if (++seen == o.sample_substeps) {
+						took = std::chrono::duration<double>(clk::now() - a).count();
+						stop = true;
+						force_break = true;
+					}
+				};
+				in.integrate(hook, true, force_break);
+				if (!stop) took = std::chrono::duration<double>(clk::now() - a).count();
+				force_break = false;
+				std::printf("%s{\"substeps\": %d, \"updates\": %.0f, \"seconds\": %.6f}", s ? ", " : "", seen, upd, took);
+				std::fflush(stdout);
+			}
+			std::printf("]}\n");
+			return 0;
+		}
+
 		for (int step = 1; step <= o.n_steps; ++step) {
 			if (o.t_end > 0 && time >= o.t_end) break;
 			double step_updates = 0.0;
@@ -217,6 +248,10 @@ int main(int argc, char **argv) {
 			o.neighbor_audit = true;
 		} else if (a == "--quiet") {
 			o.quiet = true;
+		} else if (a == "--sample-substeps" && i + 1 < argc) {
+			o.sample_substeps = std::atoi(argv[++i]);
+		} else if (a == "--samples" && i + 1 < argc) {
+			o.samples = std::atoi(argv[++i]);
 		}
 	}
 	spdlog::set_level(spdlog::level::warn);

@@ -1,0 +1,48 @@
+"""Generates the golden fixtures of the parity tests by running the reference solver.
+
+Each fixture is a case file (the exact initial tree handed to both solvers) and the reference's
+snapshots of every active cell at the listed global steps, produced by DACTI's own Integrator
+compiled from its sources (oracle/_ref/dacti_ref_runner, single thread, no FMA contraction).
+
+    python tests/golden/make_golden.py        # rewrites tests/golden/*.case and *.snap
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from dacti_b200 import cases  # noqa: E402
+from dacti_b200.casefile import write_case  # noqa: E402
+from dacti_b200.models import ModelId  # noqa: E402
+
+RUNNER = os.path.join(ROOT, "oracle", "_ref", "dacti_ref_runner")
+
+# name -> (case factory, global steps, check steps)
+GOLDEN = {
+    "euler2": (lambda: cases.lax_liu3(base_level=3, levels=2), 6, [2, 6]),
+    "ns2": (lambda: cases.lax_liu3(base_level=3, levels=2, model=ModelId.NAVIER_STOKES, mu=2e-3, prandtl=0.72), 6,
+            [6]),
+    "multi2": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2), 4, [4]),
+    "multi3": (lambda: cases.shock_drop(dims=3, base_level=3, levels=1), 2, [2]),
+    "euler2_periodic": (lambda: cases.periodic_blob(base_level=3, levels=2), 6, [6]),
+}
+
+
+def generate(name: str) -> None:
+    factory, steps, checks = GOLDEN[name]
+    case = factory()
+    path = os.path.join(HERE, f"{name}.case")
+    write_case(case, path)
+    subprocess.run([RUNNER, path, os.path.join(HERE, name), str(steps), "--check", ",".join(map(str, checks))],
+                   check=True, capture_output=True, env=dict(os.environ, OMP_NUM_THREADS="1"))
+
+
+if __name__ == "__main__":
+    for n in GOLDEN:
+        generate(n)
+        print(n)

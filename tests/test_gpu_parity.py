@@ -1,0 +1,93 @@
+"""GPU parity with the reference solver: identical refinement decisions and ACTI levels, conserved
+fields within rel-L1 1e-10 (FP64 plain form)."""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, run_reference
+from dacti_b200 import cases
+from dacti_b200.casefile import read_case, read_snapshot, write_case
+from dacti_b200.parity import compare
+from dacti_b200.solver import Solver
+from tests.golden.make_golden import GOLDEN as CASES
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10  # relative L1 of every conserved component
+
+
+def _run(case, steps, checks):
+    s = Solver(case)
+    out = {}
+    for k in range(1, steps + 1):
+        _, fb = s.integrate()
+        assert not fb
+        if k in checks:
+            out[k] = s.active_cells()
+    stats = s.stats()
+    s.close()
+    return out, stats
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_parity(name):
+    _, steps, checks = CASES[name]
+    case = read_case(os.path.join(GOLDEN, f"{name}.case"))
+    got, _ = _run(case, steps, checks)
+    for k in checks:
+        ref = read_snapshot(os.path.join(GOLDEN, f"{name}_{k}.snap"))
+        rep = compare(ref, got[k], case.params.side_length)
+        assert rep.ok(TOL), f"{name} step {k}: {rep}"
+        assert got[k].n == ref.n
+
+
+def _live(case, steps, checks, tmp_path, name, threads=1):
+    path = str(tmp_path / f"{name}.case")
+    write_case(case, path)
+    run_reference(path, str(tmp_path / name), steps, checks, threads=threads)
+    got, stats = _run(case, steps, checks)
+    for k in checks:
+        ref = read_snapshot(str(tmp_path / f"{name}_{k}.snap"))
+        rep = compare(ref, got[k], case.params.side_length)
+        assert rep.ok(TOL), f"{name} step {k}: {rep}"
+        assert stats.cell_updates >= ref.updates or k != checks[-1]
+    return stats
+
+
+def test_lax_liu_config1_full_run(tmp_path):
+    """Config 1 at its full size (64^2 base, +3 levels) for the 26 global steps to t = 0.309."""
+    stats = _live(cases.lax_liu3(), 26, [1, 13, 26], tmp_path, "c1")
+    assert stats.n_global_steps == 26
+
+
+def test_garbage_collection_run(tmp_path):
+    """A run long enough for the reference's memory-efficiency trigger to compact the tree."""
+    stats = _live(cases.lax_liu3(base_level=5, levels=3), 43, [20, 43], tmp_path, "gc")
+    assert stats.n_gc >= 1
+
+
+def test_multi3_larger(tmp_path):
+    _live(cases.shock_drop(base_level=4, levels=2), 3, [1, 3], tmp_path, "sd3", threads=4)
+
+
+def test_periodic_without_refinement(tmp_path):
+    _live(cases.periodic_blob(base_level=5, refine=False), 8, [8], tmp_path, "pnr")
+
+
+def test_bitwise_determinism():
+    case = read_case(os.path.join(GOLDEN, "multi2.case"))
+    a, _ = _run(case, 4, [4])
+    b, _ = _run(case, 4, [4])
+    sa, sb = a[4].sorted(case.params.side_length), b[4].sorted(case.params.side_length)
+    assert np.array_equal(sa.u, sb.u) and np.array_equal(sa.p, sb.p)
+
+
+def test_nan_state_sets_force_break():
+    """Fault injection on the host: one cell with negative density makes the step report NaN."""
+    case = cases.lax_liu3(base_level=4, levels=1)
+    leaves = np.nonzero(case.tree.leaf_mask())[0]
+    case.tree.p[leaves[37], 0] = -1.0
+    s = Solver(case)
+    _, fb = s.integrate()
+    s.close()
+    assert fb
