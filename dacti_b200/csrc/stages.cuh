@@ -335,8 +335,8 @@ __device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uin
 		return;
 	}
 	if (!(P.flags[nb] & F_LEAF)) {
-		interp_p<M, INTERP_DEPTH>(P, status, nb, pv);
-		tv = interp_scalar<M::D, INTERP_DEPTH>(P, status, nb, P.t);
+		interp_p<M>(P, status, nb, pv);
+		tv = interp_scalar<M::D>(P, status, nb, P.t);
 	} else {
 		load_p<M>(P, nb, pv);
 		tv = P.t[nb];
@@ -445,7 +445,7 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 				}
 				double v[E];
 				if (!(P.flags[nb] & F_LEAF)) {
-					interp_p<M, INTERP_DEPTH>(P, &cnt->status, nb, v);
+					interp_p<M>(P, &cnt->status, nb, v);
 				} else if (P.level[nb] < li) {
 					double x[D];
 					for (int d = 0; d < D; ++d) x[d] = at(P.center, cap, d, i) + (d == dim ? h * (2 * dir - 1.0) : 0.0 * h);
@@ -686,7 +686,8 @@ __device__ void update_neighbors_leaf(const Pool &P, const Consts &C, int i) {
 template<class M>
 __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_t *status, int root) {
 	constexpr int NC = 1 << M::D;
-	int stack[64];
+	constexpr int CAP = 8 * MAX_TREE;
+	int stack[CAP];
 	int sp = 0;
 	stack[sp++] = root;
 	while (sp > 0) {
@@ -697,7 +698,7 @@ __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_
 			continue;
 		}
 		for (int c = NC - 1; c >= 0; --c) {
-			if (sp >= 64) {
+			if (sp >= CAP) {
 				set_status(status, ST_DEPTH);
 				break;
 			}
@@ -900,7 +901,7 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 	}
 	const double hn = C.size[P.level[nb]];
 	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
-	if (!(P.flags[nb] & F_LEAF)) return interp_scalar<M::D, INTERP_DEPTH>(P, status, nb, P.k + (size_t) comp * cap);
+	if (!(P.flags[nb] & F_LEAF)) return interp_scalar<M::D>(P, status, nb, P.k + (size_t) comp * cap);
 	return at(P.k, cap, comp, nb);
 }
 
@@ -996,8 +997,8 @@ __global__ void k_smooth_kappa(Pool P, Consts C, BcTable B, const int32_t *list,
 						av[dir] = pb[M::IA];
 					}
 				} else if (!(P.flags[nb] & F_LEAF)) {
-					kv[dir] = interp_scalar<M::D, INTERP_DEPTH>(P, &cnt->status, nb, P.k + (size_t) M::KAPPA * cap);
-					av[dir] = interp_scalar<M::D, INTERP_DEPTH>(P, &cnt->status, nb, P.p + (size_t) M::IA * cap);
+					kv[dir] = interp_scalar<M::D>(P, &cnt->status, nb, P.k + (size_t) M::KAPPA * cap);
+					av[dir] = interp_scalar<M::D>(P, &cnt->status, nb, P.p + (size_t) M::IA * cap);
 				} else {
 					kv[dir] = at(P.k, cap, M::KAPPA, nb);
 					av[dir] = at(P.p, cap, M::IA, nb);

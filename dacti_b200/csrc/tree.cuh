@@ -51,55 +51,101 @@ __device__ int find_neighbor(const Pool &P, const Consts &C, int i, int dim, int
 }
 
 // Domain::interpolate_p / interpolate_t / interpolate_k (integrator/domain.hpp:84-148): the value of
-// a leaf, or the mean over the active children of a non-leaf, recursively.
-template<class M, int DEPTH>
+// a leaf, or the mean over the active children of a non-leaf, recursively. Evaluated as an explicit
+// post-order walk (children in slot order, as the recursion visits them), so the depth below the
+// node is bounded only by the tree depth: cells may coarsen below the base level
+// (impl/adaptive_refinement.hpp:82 only requires tree_level > 0), next to much deeper subtrees.
+template<class M>
 __device__ void interp_p(const Pool &P, uint32_t *status, int n, double *out) {
+	constexpr int E = M::E, NC = 1 << M::D;
 	if (P.flags[n] & F_LEAF) {
 		load_p<M>(P, n, out);
 		return;
 	}
-	if constexpr (DEPTH == 0) {
-		set_status(status, ST_DEPTH);
-		for (int q = 0; q < M::E; ++q) out[q] = 0.0;
-	} else {
-		double f[M::E];
-		for (int q = 0; q < M::E; ++q) f[q] = 0.0;
-		int cnt = 0;
-		for (int c = 0; c < (1 << M::D); ++c) {
-			int ch = P.child[(size_t) c * P.cap + n];
-			if (P.flags[ch] & F_ACTIVE) {
-				double tmp[M::E];
-				interp_p<M, DEPTH - 1>(P, status, ch, tmp);
-				for (int q = 0; q < M::E; ++q) f[q] = f[q] + tmp[q];
-				cnt++;
+	struct Frame {
+		int node, next, cnt;
+		double f[E];
+	};
+	Frame st[MAX_TREE];
+	int sp = 0;
+	st[0].node = n;
+	st[0].next = 0;
+	st[0].cnt  = 0;
+	for (int q = 0; q < E; ++q) st[0].f[q] = 0.0;
+	sp = 1;
+	while (true) {
+		Frame &fr = st[sp - 1];
+		if (fr.next < NC) {
+			const int c = P.child[(size_t) fr.next * P.cap + fr.node];
+			fr.next++;
+			if (!(P.flags[c] & F_ACTIVE)) continue;
+			if (P.flags[c] & F_LEAF) {
+				for (int q = 0; q < E; ++q) fr.f[q] = fr.f[q] + at(P.p, P.cap, q, c);
+				fr.cnt++;
+			} else if (sp < MAX_TREE) {
+				Frame &nf = st[sp++];
+				nf.node   = c;
+				nf.next   = 0;
+				nf.cnt    = 0;
+				for (int q = 0; q < E; ++q) nf.f[q] = 0.0;
+			} else {
+				set_status(status, ST_DEPTH);
 			}
+			continue;
 		}
-		for (int q = 0; q < M::E; ++q) out[q] = f[q] / (double) cnt;
+		double r[E];
+		for (int q = 0; q < E; ++q) r[q] = fr.f[q] / (double) fr.cnt;
+		--sp;
+		if (sp == 0) {
+			for (int q = 0; q < E; ++q) out[q] = r[q];
+			return;
+		}
+		Frame &pf = st[sp - 1];
+		for (int q = 0; q < E; ++q) pf.f[q] = pf.f[q] + r[q];
+		pf.cnt++;
 	}
 }
 
 // Scalar field average (t, k[i] or p[i]); `arr` is the SoA base of that component.
-template<int D, int DEPTH>
+template<int D>
 __device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const double *arr) {
+	constexpr int NC = 1 << D;
 	if (P.flags[n] & F_LEAF) return arr[n];
-	if constexpr (DEPTH == 0) {
-		set_status(status, ST_DEPTH);
-		return 0.0;
-	} else {
-		double f = 0.0;
-		int cnt  = 0;
-		for (int c = 0; c < (1 << D); ++c) {
-			int ch = P.child[(size_t) c * P.cap + n];
-			if (P.flags[ch] & F_ACTIVE) {
-				f += interp_scalar<D, DEPTH - 1>(P, status, ch, arr);
-				cnt++;
+	int node[MAX_TREE], next[MAX_TREE], cnt[MAX_TREE];
+	double f[MAX_TREE];
+	int sp   = 1;
+	node[0]  = n;
+	next[0]  = 0;
+	cnt[0]   = 0;
+	f[0]     = 0.0;
+	while (true) {
+		const int k = sp - 1;
+		if (next[k] < NC) {
+			const int c = P.child[(size_t) next[k] * P.cap + node[k]];
+			next[k]++;
+			if (!(P.flags[c] & F_ACTIVE)) continue;
+			if (P.flags[c] & F_LEAF) {
+				f[k] += arr[c];
+				cnt[k]++;
+			} else if (sp < MAX_TREE) {
+				node[sp] = c;
+				next[sp] = 0;
+				cnt[sp]  = 0;
+				f[sp]    = 0.0;
+				++sp;
+			} else {
+				set_status(status, ST_DEPTH);
 			}
+			continue;
 		}
-		return f / (double) cnt;
+		const double r = f[k] / (double) cnt[k];
+		--sp;
+		if (sp == 0) return r;
+		f[sp - 1] += r;
+		cnt[sp - 1]++;
 	}
 }
 
-constexpr int INTERP_DEPTH = 4;
 
 // Boundary::boundary_value (integrator/boundary.hpp:75-123): ghost primitive state of a face.
 template<class M>

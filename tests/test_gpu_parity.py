@@ -67,7 +67,7 @@ def test_garbage_collection_run(tmp_path):
 
 
 def test_multi3_larger(tmp_path):
-    _live(cases.shock_drop(base_level=4, levels=2), 3, [1, 3], tmp_path, "sd3", threads=4)
+    _live(cases.shock_drop(base_level=4, levels=2), 3, [1, 3], tmp_path, "sd3")
 
 
 def test_periodic_without_refinement(tmp_path):
