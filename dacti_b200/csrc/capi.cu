@@ -1,12 +1,7 @@
 // extern "C" entry points of include/dacti_gpu.h.
-#include "solver.cuh"
+#include "capi_internal.h"
 
 #include <string>
-
-struct dg_solver {
-	dg::SolverBase *impl;
-	int device;
-};
 
 namespace {
 thread_local std::string g_create_error;

@@ -1,0 +1,9 @@
+// Layout of the opaque dg_solver handle, shared by the C-ABI translation units.
+#pragma once
+
+#include "solver.cuh"
+
+struct dg_solver {
+	dg::SolverBase *impl;
+	int device;
+};

@@ -35,6 +35,7 @@ public:
 	virtual void step(int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) = 0;
 	virtual long long cell_count() = 0;
 	virtual long long read_cells(int *levels, double *data, long long max_cells) = 0;
+	virtual long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void set_profiling(bool on) = 0;
@@ -657,6 +658,41 @@ public:
 		DG_CUDA(cudaGetLastError());
 		DG_CUDA(cudaMemcpyAsync(data, d_read_, sizeof(double) * W * n, cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaMemcpyAsync(levels, d_readlv_, sizeof(int32_t) * 2 * n, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaStreamSynchronize(st_));
+		return n;
+	}
+
+	// Same records as read_cells, gathered through caller-owned device scratch of `bytes` bytes;
+	// allocates nothing.
+	long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) override {
+		constexpr int W = D + 1 + 2 * E + 3;
+		const long long n = cell_count();
+		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
+		const size_t rec_bytes = align_up(sizeof(double) * W * (size_t) n);
+		const size_t need      = rec_bytes + sizeof(int32_t) * 2 * (size_t) n;
+		const size_t per_cell  = sizeof(double) * W + sizeof(int32_t) * 2;
+		if (need > bytes)
+			throw dg_error(DG_ERR_CAPACITY, "dg_read_cells_noalloc: " + std::to_string(n) + " active cells need " +
+			                                    std::to_string(need) + " bytes of scratch; the allocation-free scratch holds " +
+			                                    std::to_string(bytes) + " bytes (about " +
+			                                    std::to_string((bytes - 256) / per_cell) + " cells of this model)");
+		double *d_rec = (double *) scratch;
+		int32_t *d_lv = (int32_t *) ((char *) scratch + rec_bytes);
+		long long base = 0;
+		for (int pass = 0; pass < 2; ++pass) {
+			for (int l = 0; l < MAX_ACTI; ++l) {
+				int cnt = pass == 0 ? h_cnt_->clu[l] : h_cnt_->buf[l];
+				if (cnt == 0) continue;
+				const int32_t *list = pass == 0 ? Ls_.clu[l] : Ls_.buf[l];
+				k_gather_cells<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, (int) base, d_rec, d_lv);
+				base += cnt;
+			}
+		}
+		DG_CUDA(cudaGetLastError());
+		if (n > 0) {
+			DG_CUDA(cudaMemcpyAsync(data, d_rec, sizeof(double) * W * n, cudaMemcpyDeviceToHost, st_));
+			DG_CUDA(cudaMemcpyAsync(levels, d_lv, sizeof(int32_t) * 2 * n, cudaMemcpyDeviceToHost, st_));
+		}
 		DG_CUDA(cudaStreamSynchronize(st_));
 		return n;
 	}

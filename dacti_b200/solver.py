@@ -82,6 +82,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_cell_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_read_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                   ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.dg_read_cells_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
+                                          ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_last_error.argtypes = [vp]
@@ -92,7 +94,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return lib
 
 
-EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells", "dg_get_stats",
+EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells",
+                    "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
@@ -172,6 +175,9 @@ class Solver:
         return int(n.value)
 
     def active_cells(self) -> Snapshot:
+        return self._read(self._lib.dg_read_cells)
+
+    def _read(self, fn) -> Snapshot:
         sh = self.shape
         D, E = sh.dims, sh.E
         W = D + 1 + 2 * E + 3
@@ -179,8 +185,7 @@ class Solver:
         lv = np.zeros((max(n, 1), 2), np.int32)
         data = np.zeros((max(n, 1), W), np.float64)
         got = ctypes.c_longlong()
-        self._check(self._lib.dg_read_cells(self._h, _ptr(lv, ctypes.c_int), _ptr(data, ctypes.c_double), n,
-                                            ctypes.byref(got)))
+        self._check(fn(self._h, _ptr(lv, ctypes.c_int), _ptr(data, ctypes.c_double), n, ctypes.byref(got)))
         st = self.stats()
         n_in = int(sum(st.n_clusters))
         return Snapshot(
@@ -189,6 +194,10 @@ class Solver:
             data[:n, D + 1:D + 1 + E].copy(), data[:n, D + 1 + E:D + 1 + 2 * E].copy(), data[:n, D + 1 + 2 * E].copy(),
             data[:n, D + 2 + 2 * E].copy(), data[:n, D + 3 + 2 * E].copy(),
         )
+
+    def active_cells_noalloc(self) -> Snapshot:
+        """active_cells() through dg_read_cells_noalloc: no device allocation (bounded scratch)."""
+        return self._read(self._lib.dg_read_cells_noalloc)
 
     def stats(self) -> DgStats:
         s = DgStats()

@@ -124,6 +124,16 @@ int dg_cell_count(dg_solver *s, long long *n);
  * {center[D], t, u[E], p[E], error, max_dt, cfl}. */
 int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
+/* Allocation-free variant of dg_read_cells for hosts that cannot let the library call cudaMalloc
+ * (a fixed device-memory budget owned by the host's allocator, or a thread that must not take the
+ * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference: DACTI's
+ * Integrator hands out host references to its nodes. Same records and order as dg_read_cells,
+ * gathered through a 64 MiB scratch array that the library keeps resident on each device: read-backs
+ * larger than that (about 380 thousand multi<3> cells, 560 thousand euler<2> cells) return
+ * DG_ERR_CAPACITY. Calls share the scratch, so calls whose GPU work overlaps race; the first call on a
+ * device looks up the scratch's device address and should come before any stream capture. */
+int dg_read_cells_noalloc(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
+
 int dg_get_stats(dg_solver *s, dg_stats *out);
 
 /* Per-kernel device timing with CUDA events on the solver's stream (off by default). */
