@@ -15,7 +15,7 @@ import numpy as np
 
 from .casefile import Case, SolverParams
 from .models import BcType, ModelId, ModelShape
-from .scene import BoundarySpec, SceneSpec, SphereObject, build_tree
+from .scene import BoundarySpec, EllipseObject, SceneSpec, SphereObject, build_tree
 
 ZG = BoundarySpec(BcType.ZERO_GRADIENT)
 
@@ -76,7 +76,8 @@ def normal_shock(rho1: float, p1: float, mach: float, gamma: float = 1.4, P0: fl
 
 def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: float = 8e-3, aspect: int = 2,
                drop_radius: float = 0.5e-3, shock_x: float = -1.0e-3, mach: float = 1.5,
-               thresholds=(0.02, 0.05), max_cfl: float = 0.25, weights: Optional[tuple] = None) -> Case:
+               thresholds=(0.02, 0.05), max_cfl: float = 0.25, weights: Optional[tuple] = None,
+               mu: tuple = (0.0, 0.0), conductivity: tuple = (0.0, 0.0), sigma: float = 0.0) -> Case:
     """Config 2: five-equation air-water shock-drop.
 
     Domain ``length`` x ``length/aspect`` (x ``length/aspect``) with a ``2^base_level`` cell root
@@ -86,7 +87,9 @@ def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: floa
     it; volume fraction smeared with a tanh over the finest cell size. The inflow face carries the
     post-shock state; all other faces are zero-gradient. Surface tension and viscosity are zero.
     The CFL target 0.25 is the one of the reference's own cases/shockDrop3d.toml; at 0.5 the 3D
-    reference run floors the water pressure once the shock reaches the drop.
+    reference run floors the water pressure once the shock reaches the drop. ``mu``,
+    ``conductivity`` (water, air) and ``sigma`` switch on the viscous, heat and surface-tension terms
+    of model/multi.hpp.
     """
     shape = ModelShape(ModelId.MULTI, dims)
     E = shape.E
@@ -123,7 +126,8 @@ def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: floa
     prm = SolverParams(
         side_length=length, active_size=active, periodic=[False] * dims, max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=base_level + levels, min_level=base_level, weights=weights,
-        gamma1=4.4, gamma2=1.4, P1=6.0e8, P2=0.0,
+        gamma1=4.4, gamma2=1.4, P1=6.0e8, P2=0.0, mu1=mu[0], mu2=mu[1], lambda1=conductivity[0],
+        lambda2=conductivity[1], sigma=sigma,
     )
     return Case(build_tree(spec), prm)
 
@@ -151,5 +155,35 @@ def periodic_blob(base_level: int = 4, levels: int = 2, thresholds=(0.02, 0.05),
     prm = SolverParams(
         side_length=1.0, active_size=(1.0, 1.0), periodic=(True, True), max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=max_level, min_level=base_level, weights=(1.0, 0.0, 0.0, 0.0),
+    )
+    return Case(build_tree(spec), prm)
+
+
+def osc_drop(base_level: int = 4, levels: int = 2, thresholds=(1e-3, 1e-2), max_cfl: float = 0.4,
+             conductivity: tuple = (0.0, 0.0)) -> Case:
+    """2D oscillating drop in the non-dimensional units of the reference's cases/oscDrop.toml:
+    2 x 2 box, elliptic drop (a = 0.2, b = 0.12) of fluid 1 (rho 1, gamma 6.12, P0 500) in fluid 2
+    (rho 1e-3, gamma 1.4), p = 1 at rest, sigma = 0.1, Oh = 0.01 with L = 0.15825 and viscosity ratio
+    10 (mu1 = sqrt(rho1 sigma L) Oh, model/multi.hpp:531-535), tanh-smeared interface,
+    zero-gradient boundaries. Exercises surface tension (curvature, smoothing, source) and the
+    viscous terms of the five-equation model."""
+    shape = ModelShape(ModelId.MULTI, 2)
+    rho1, rho2, sigma, oh, L = 1.0, 1e-3, 0.1, 0.01, 0.15825
+    mu1 = math.sqrt(rho1 * sigma * L) * oh
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        out = np.zeros((c.shape[0], 6))
+        out[:, 1] = rho2
+        out[:, 4] = 1.0
+        return out
+
+    spec = SceneSpec(shape, (2.0, 2.0), base_level, base_level + levels, x2p, _zg_box(2),
+                     objects=[EllipseObject((0.0, 0.0), (0.2, 0.12), "droplet")], diffuse_ic=True,
+                     rho_ref=(rho1, rho2))
+    prm = SolverParams(
+        side_length=2.0, active_size=(2.0, 2.0), periodic=(False, False), max_cfl=max_cfl, max_dt=5e-3,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
+        weights=(1.0, 0.0, 0.0, 0.0, 0.0, 1.0), gamma1=6.12, gamma2=1.4, P1=500.0, P2=0.0,
+        mu1=mu1, mu2=mu1 / 10.0, lambda1=conductivity[0], lambda2=conductivity[1], sigma=sigma,
     )
     return Case(build_tree(spec), prm)

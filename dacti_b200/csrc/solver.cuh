@@ -68,6 +68,8 @@ class Solver : public SolverBase {
 	int32_t *d_readlv_ = nullptr;
 	long long read_cap_ = 0;
 	int limiter_ = 0;
+	bool visc_   = false;  // viscous/heat terms present (multiphase with any non-zero mu or lambda)
+	bool sigma_  = false;  // surface tension present
 
 	// scheduler state (integrator/integrator.hpp:46-58)
 	int acti_counter_[MAX_ACTI] = {};
@@ -198,6 +200,9 @@ public:
 		m.lambda1 = pr[DG_P_LAMBDA1];
 		m.lambda2 = pr[DG_P_LAMBDA2];
 		m.sigma = pr[DG_P_SIGMA];
+		if constexpr (M::MULTI) visc_ = m.mu1 != 0.0 || m.mu2 != 0.0 || m.lambda1 != 0.0 || m.lambda2 != 0.0;
+		else visc_ = M::VISC;
+		sigma_ = m.sigma != 0.0;
 		if (c.n_zones > MAX_ZONES) throw dg_error(DG_ERR_ARG, "too many refinement zones");
 		C_.n_zones = c.n_zones;
 		for (int z = 0; z < c.n_zones; ++z) {
@@ -409,7 +414,7 @@ public:
 		const int g = grid_for(n);
 		k_init_cells<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, d_cnt_);
 		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
-		k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, d_leaves_, n, limiter_, d_cnt_);
+		launch_slope(d_leaves_, n);
 		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n);
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
@@ -441,10 +446,19 @@ private:
 				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS); });
 			}
 			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
-			run_k(DG_K_AUX, n, [&] { k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
-			run_k(DG_K_AUX, n, [&] { k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
-			run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA); });
+			// The curvature only enters through sigma * kappa (model/multi.hpp:142, 216, 190-193); without
+			// surface tension those products are zeros and the curvature stages are skipped.
+			if (sigma_) {
+				run_k(DG_K_AUX, n, [&] { k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+				run_k(DG_K_AUX, n, [&] { k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA); });
+			}
 		}
+	}
+
+	void launch_slope(const int32_t *list, int n) {
+		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 	}
 
 	void sync_counters() {
@@ -475,15 +489,29 @@ private:
 		int32_t *list      = Ls_.clu[L];
 		const int counterL = acti_counter_[L];
 
+		constexpr int LPC = NF <= 4 ? 4 : 8;  // flux lanes per cell
 		run_k(DG_K_FLUX, n, [&] {
-			k_flux<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL, stamp_recv, 1, Ls_.recv, d_cnt_);
+			if (visc_)
+				k_flux<M, true><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL,
+				                                                                   stamp_recv, 1, Ls_.recv, d_cnt_);
+			else
+				k_flux<M, false><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL,
+				                                                                    stamp_recv, 1, Ls_.recv, d_cnt_);
 		});
 		run_k(DG_K_RECV, 0, [&] {
-			k_flux<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0, L, dtL,
-			                                                          stamp_recv, 0, Ls_.recv, d_cnt_);
+			if (visc_)
+				k_flux<M, true><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0,
+				                                                                   L, dtL, stamp_recv, 0, Ls_.recv, d_cnt_);
+			else
+				k_flux<M, false><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv,
+				                                                                    0, L, dtL, stamp_recv, 0, Ls_.recv,
+				                                                                    d_cnt_);
 		});
-		run_k(DG_K_UPDATE, n, [&] { k_update<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_); });
-		run_k(DG_K_SLOPE, n, [&] { k_slope<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_); });
+		run_k(DG_K_UPDATE, n, [&] {
+			if (visc_) k_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
+			else k_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
+		});
+		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) multiphase_aux(list, n);
 		run_k(DG_K_ESTIMATE, n, [&] {
 			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);

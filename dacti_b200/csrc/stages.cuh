@@ -30,7 +30,7 @@ __device__ __forceinline__ void append(int32_t *list, int *count, int value, int
 // the right state and the face keeps the owner's centre (the reference relabels face.dir = 1).
 // `shift` moves the non-owner's centre by the active size across a periodic wrap.
 // --------------------------------------------------------------------------------------------
-template<class M>
+template<class M, bool V = M::VISC>
 __device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
                                            double dtL, double *F) {
 	constexpr int E = M::E, D = M::D;
@@ -94,7 +94,7 @@ __device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int o
 			F[IA] += uc * (1 - a) * a;
 		}
 	}
-	if constexpr (M::VISC) {
+	if constexpr (M::VISC && V) {
 		constexpr int G = M::G;
 		double du[D * G], vel[D], fv[D + 1];
 		for (int i = 0; i < D; ++i)
@@ -120,7 +120,7 @@ __device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int o
 }
 
 // Boundary::boundary_flux (integrator/boundary.hpp:130-160), from the cell-centre state.
-template<class M>
+template<class M, bool V = M::VISC>
 __device__ __noinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
                                            int dir, double dtL, double *F) {
 	constexpr int E = M::E, D = M::D;
@@ -141,7 +141,7 @@ __device__ __noinline__ void boundary_flux(const Pool &P, const Consts &C, const
 		middle_state<M>(C.m, pb, pc, 0.0, dim, pm);
 		phys_flux<M>(C.m, pm, 0.0, dim, false, F);
 	}
-	if constexpr (M::VISC) {
+	if constexpr (M::VISC && V) {
 		constexpr int G = M::G;
 		double g[D * G], z[D], fv[D + 1];
 		for (int c = 0; c < D * G; ++c) g[c] = at(P.grad, cap, c, i);
@@ -164,7 +164,7 @@ __device__ __forceinline__ void acc_add(double *acc, const double *F, bool plus)
 
 // Adds to `acc` the fluxes owned by running-cluster cells across face (dim, dir) of cell i whose
 // neighbour slot is nb (a non-owning side's view of impl/flux.hpp:58-59).
-template<class M>
+template<class M, bool V = M::VISC>
 __device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t *status, int i, int nb, int dim,
                                        int dir, int L, double dtL, double *acc) {
 	const int cap = P.cap;
@@ -175,7 +175,7 @@ __device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t 
 		if (P.level[nb] == li && P.clu[nb] == L) {
 			const int an = P.acti[nb];
 			if (ai <= an && (dn == 1 || ai < an)) {
-				interior_flux<M>(P, C, nb, i, dim, dn, dtL, F);
+				interior_flux<M, V>(P, C, nb, i, dim, dn, dtL, F);
 				acc_add<M::F>(acc, F, dn == 1);
 			}
 		}
@@ -187,7 +187,7 @@ __device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t 
 		const int ch = P.child[(size_t) c * cap + nb];
 		if (P.flags[ch] & F_LEAF) {
 			if (P.clu[ch] == L && ai <= P.acti[ch]) {
-				interior_flux<M>(P, C, ch, i, dim, dn, dtL, F);
+				interior_flux<M, V>(P, C, ch, i, dim, dn, dtL, F);
 				acc_add<M::F>(acc, F, dn == 1);
 			}
 			continue;
@@ -200,64 +200,81 @@ __device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t 
 				continue;
 			}
 			if (P.clu[gc] == L && ai <= P.acti[gc]) {
-				interior_flux<M>(P, C, gc, i, dim, dn, dtL, F);
+				interior_flux<M, V>(P, C, gc, i, dim, dn, dtL, F);
 				acc_add<M::F>(acc, F, dn == 1);
 			}
 		}
 	}
 }
 
-// flux_update (impl/flux.hpp:11-97). cluster_mode: cells of cluster L (own faces + same-cluster
-// owners, marking receivers); otherwise: receivers (fluxes owned by cluster-L neighbours only).
-template<class M>
-__global__ void k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr, int n_host, int L,
-                       double dtL, int stamp, int cluster_mode, int32_t *recv, Counters *cnt) {
-	const int n   = n_ptr ? *n_ptr : n_host;
-	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
-		const int i  = list[tid];
-		const int li = P.level[i], ai = P.acti[i];
+// flux_update (impl/flux.hpp:11-97), face parallel. A group of 2D lanes (padded to 4 or 8) serves
+// one cell; lane f handles face (dim, dir) = (f / 2, f % 2): the flux the cell owns across it
+// (cluster_mode) and the fluxes running-cluster neighbours own across it. The lane sums are combined
+// with a fixed butterfly, so the per-cell total does not depend on scheduling. cluster_mode: cells of
+// cluster L (marking receivers); otherwise receivers, which only gather.
+template<class M, bool V>
+__global__ void __launch_bounds__(BLOCK) k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr,
+                                                int n_host, int L, double dtL, int stamp, int cluster_mode,
+                                                int32_t *recv, Counters *cnt) {
+	constexpr int NF = 2 * M::D;
+	constexpr int G  = NF <= 4 ? 4 : 8;
+	constexpr int GW = 32 / G;
+	const int n      = n_ptr ? *n_ptr : n_host;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot = wbase + lane / G;
 		double acc[M::F];
 		for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
-		double F[M::F];
-		for (int dim = 0; dim < M::D; ++dim) {
-			for (int dir = 0; dir < 2; ++dir) {
-				const int f  = 2 * dim + dir;
-				const int nb = P.nbr[(size_t) f * cap + i];
-				if (nb == 0) {
-					if (cluster_mode) {
-						const int b = P.bc[(size_t) f * cap + i];
-						if (b < 0) {
-							set_status(&cnt->status, ST_MISSING_BC);
-							continue;
-						}
-						boundary_flux<M>(P, C, B, i, b, dim, dir, dtL, F);
+		if (slot < n && sub < NF) {
+			const int i   = list[slot];
+			const int dim = sub >> 1, dir = sub & 1;
+			const int li = P.level[i], ai = P.acti[i];
+			const int nb = P.nbr[(size_t) sub * cap + i];
+			double F[M::F];
+			if (nb == 0) {
+				if (cluster_mode) {
+					const int b = P.bc[(size_t) sub * cap + i];
+					if (b < 0) {
+						set_status(&cnt->status, ST_MISSING_BC);
+					} else {
+						boundary_flux<M, V>(P, C, B, i, b, dim, dir, dtL, F);
 						acc_add<M::F>(acc, F, false);
 					}
-					continue;
 				}
+			} else {
+				bool done = false;
 				if (cluster_mode) {
 					const uint32_t fn = P.flags[nb];
 					const int ln = P.level[nb], an = P.acti[nb];
-					const bool owned = (fn & F_LEAF) && an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)));
-					if (owned) {
-						interior_flux<M>(P, C, i, nb, dim, dir, dtL, F);
+					if ((fn & F_LEAF) && an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
+						interior_flux<M, V>(P, C, i, nb, dim, dir, dtL, F);
 						acc_add<M::F>(acc, F, dir == 0);
 						if (P.clu[nb] != L) {
 							if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 						}
-						continue;
+						done = true;
 					}
 				}
-				gather_owned_by_others<M>(P, C, &cnt->status, i, nb, dim, dir, L, dtL, acc);
+				if (!done) gather_owned_by_others<M, V>(P, C, &cnt->status, i, nb, dim, dir, L, dtL, acc);
 			}
 		}
-		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] += acc[q];
+		// fixed-order butterfly over the group's lanes
+		for (int off = G / 2; off > 0; off >>= 1)
+			for (int q = 0; q < M::F; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+		if (slot < n) {
+			const int i = list[slot];
+			for (int q = sub; q < M::F; q += G) P.flux[(size_t) q * cap + i] += acc[q];
+		}
 	}
 }
 
-// cell_update (impl/cell_update.hpp:10-90)
-template<class M>
+// cell_update (impl/cell_update.hpp:10-90). Without viscous terms (V = false) the gradient inputs
+// are never read, so t_slope is not maintained.
+template<class M, bool V>
 __global__ void k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, Counters *cnt) {
 	constexpr int E = M::E;
 	const int cap = P.cap;
@@ -267,9 +284,9 @@ __global__ void k_update(Pool P, Consts C, const int32_t *list, int n, double dt
 		load_p<M>(P, i, pold);
 		for (int q = 0; q < E; ++q) u[q] = at(P.u, cap, q, i);
 		double gold[M::G > 0 ? M::G : 1];
-		grad_input<M>(C.m, pold, gold);
-		const double V = C.vol[P.level[i]];
-		for (int q = 0; q < M::F; ++q) du[q] = at(P.flux, cap, q, i) / V;
+		if constexpr (V) grad_input<M>(C.m, pold, gold);
+		const double vol = C.vol[P.level[i]];
+		for (int q = 0; q < M::F; ++q) du[q] = at(P.flux, cap, q, i) / vol;
 		for (int q = 0; q < E; ++q) u[q] += du[q];
 		if constexpr (M::MULTI) {
 			if (!C.signal) {
@@ -296,7 +313,7 @@ __global__ void k_update(Pool P, Consts C, const int32_t *list, int n, double dt
 		}
 		p[M::IP] = smax(p[M::IP], 1e-3);
 		cons_from_prim<M>(C.m, p, u);
-		if constexpr (M::G > 0) {
+		if constexpr (M::G > 0 && V) {
 			double gnew[M::G];
 			grad_input<M>(C.m, p, gnew);
 			for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = (gnew[g] - gold[g]) / dtL;
@@ -345,8 +362,9 @@ __device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uin
 	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
 }
 
-// compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients and the Hancock rhs.
-template<class M>
+// compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients (only read by the viscous
+// terms, so computed when V) and the Hancock rhs.
+template<class M, bool V = M::VISC>
 __device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim, int i) {
 	constexpr int E = M::E, D = M::D;
 	const int cap = P.cap;
@@ -363,7 +381,7 @@ __device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, 
 			double sp = (pp[q] - pc[q]) / (xp - xc);
 			slope[dim * E + q] = limit(lim, sn, sp);
 		}
-		if constexpr (M::G > 0) {
+		if constexpr (M::G > 0 && V) {
 			double gp[M::G], gn[M::G];
 			grad_input<M>(C.m, pp, gp);
 			grad_input<M>(C.m, pn, gn);
@@ -381,9 +399,9 @@ __device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, 
 	for (int q = 0; q < E; ++q) P.rhs[(size_t) q * cap + i] = rhs[q];
 }
 
-template<class M>
+template<class M, bool V>
 __global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
-	for (int tid = gtid(); tid < n; tid += gstride()) compute_slope<M>(P, C, B, &cnt->status, lim, list[tid]);
+	for (int tid = gtid(); tid < n; tid += gstride()) compute_slope<M, V>(P, C, B, &cnt->status, lim, list[tid]);
 }
 
 // Recompute the Hancock rhs from the stored slope (used for split parents, whose curvature may

@@ -63,6 +63,24 @@ class SphereObject:
 
 
 @dataclass
+class EllipseObject:
+    """Axis-aligned ellipse/ellipsoid with semi-axes `axes`; signed distance approximated by
+    (|x/a| - 1) * min(a) (exact on a circle), which is all the initial refinement and volume
+    fraction need."""
+
+    center: Sequence[float]
+    axes: Sequence[float]
+    type: str = "droplet"
+    bc: Optional[BoundarySpec] = None
+
+    def signed_distance(self, x: np.ndarray) -> np.ndarray:
+        D = x.shape[1]
+        c = np.asarray(self.center, dtype=np.float64)[:D]
+        a = np.asarray(self.axes, dtype=np.float64)[:D]
+        return (np.sqrt((((x - c) / a) ** 2).sum(axis=1)) - 1.0) * a.min()
+
+
+@dataclass
 class RefineZone:
     x0: Sequence[float]
     x1: Sequence[float]

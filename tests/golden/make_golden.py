@@ -30,6 +30,12 @@ GOLDEN = {
     "multi2": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2), 4, [4]),
     "multi3": (lambda: cases.shock_drop(dims=3, base_level=3, levels=1), 2, [2]),
     "euler2_periodic": (lambda: cases.periodic_blob(base_level=3, levels=2), 6, [6]),
+    # viscosity and heat conduction of the five-equation model
+    "multi2_visc": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2, mu=(1e-3, 1.8e-5),
+                                             conductivity=(0.6, 0.026)), 4, [4]),
+    # surface tension: the reference's own oscillating-drop setting reaches NaN at its third global step,
+    # so the fixture checks the two steps before that
+    "multi2_tension": (lambda: cases.osc_drop(), 2, [1, 2]),
 }
 
 
@@ -43,6 +49,6 @@ def generate(name: str) -> None:
 
 
 if __name__ == "__main__":
-    for n in GOLDEN:
+    for n in (sys.argv[1:] or GOLDEN):
         generate(n)
         print(n)
