@@ -293,7 +293,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         tree = case.tree
         h2d = (tree.parent.nbytes + tree.children.nbytes + tree.level.nbytes + tree.flags.nbytes + tree.bc.nbytes +
                tree.center.nbytes + tree.p.nbytes)
-        d2h = snap.n * (8 * (D + 1 + 2 * case.shape.E + 3) + 8)
+        d2h = snap.n * (8 * (D + 1 + 2 * case.shape.E + 3 + case.shape.P) + 8)
         result["e2e"] = {"value": float(u_e.item()) / float(t_e.item()), "unit": UNIT,
                          "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                          "includes": "solver construction from the host tree, K steps, read-back of all cells"}

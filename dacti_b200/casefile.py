@@ -140,6 +140,7 @@ class Snapshot:
     error: np.ndarray
     max_dt: np.ndarray
     cfl: np.ndarray
+    k: Optional[np.ndarray] = None  # model parameters (multi: mu, -, normal[D], kappa, smoothed alpha)
 
     @property
     def n(self) -> int:
@@ -153,7 +154,7 @@ class Snapshot:
         return Snapshot(
             self.dims, self.E, self.step, self.n_substeps, self.tree_size, self.n_in_clusters, self.time,
             self.global_dt, self.updates, self.tree_level[o], self.acti_level[o], self.center[o], self.t[o],
-            self.u[o], self.p[o], self.error[o], self.max_dt[o], self.cfl[o],
+            self.u[o], self.p[o], self.error[o], self.max_dt[o], self.cfl[o], None if self.k is None else self.k[o],
         )
 
 
@@ -171,14 +172,16 @@ def read_snapshot(path: str) -> Snapshot:
     hdr = np.frombuffer(buf, np.int32, 8, 8)
     D, E, n, n_in, step, nsub, tsz = (int(x) for x in hdr[:7])
     hd = np.frombuffer(buf, np.float64, 3, 40)
-    rec = np.dtype([("lv", np.int32, 2), ("d", np.float64, D + 1 + 2 * E + 3)])
+    base = D + 1 + 2 * E + 3
+    n_par = ((len(buf) - 64) // max(n, 1) - 8) // 8 - base if n > 0 else 0
+    rec = np.dtype([("lv", np.int32, 2), ("d", np.float64, base + n_par)])
     arr = np.frombuffer(buf, rec, n, 64)
     d = arr["d"]
     return Snapshot(
         D, E, step, nsub, tsz, n_in, float(hd[0]), float(hd[1]), float(hd[2]),
         arr["lv"][:, 0].copy(), arr["lv"][:, 1].copy(), d[:, :D].copy(), d[:, D].copy(),
         d[:, D + 1: D + 1 + E].copy(), d[:, D + 1 + E: D + 1 + 2 * E].copy(), d[:, D + 1 + 2 * E].copy(),
-        d[:, D + 2 + 2 * E].copy(), d[:, D + 3 + 2 * E].copy(),
+        d[:, D + 2 + 2 * E].copy(), d[:, D + 3 + 2 * E].copy(), d[:, base:].copy() if n_par > 0 else None,
     )
 
 

@@ -160,20 +160,21 @@ def periodic_blob(base_level: int = 4, levels: int = 2, thresholds=(0.02, 0.05),
 
 
 def osc_drop(base_level: int = 4, levels: int = 2, thresholds=(1e-3, 1e-2), max_cfl: float = 0.4,
-             conductivity: tuple = (0.0, 0.0)) -> Case:
+             conductivity: tuple = (0.0, 0.0), velocity: float = 0.0, sigma: float = 0.1, oh: float = 0.01) -> Case:
     """2D oscillating drop in the non-dimensional units of the reference's cases/oscDrop.toml:
     2 x 2 box, elliptic drop (a = 0.2, b = 0.12) of fluid 1 (rho 1, gamma 6.12, P0 500) in fluid 2
     (rho 1e-3, gamma 1.4), p = 1 at rest, sigma = 0.1, Oh = 0.01 with L = 0.15825 and viscosity ratio
     10 (mu1 = sqrt(rho1 sigma L) Oh, model/multi.hpp:531-535), tanh-smeared interface,
     zero-gradient boundaries. Exercises surface tension (curvature, smoothing, source) and the
-    viscous terms of the five-equation model."""
+    viscous terms of the five-equation model. ``velocity`` translates everything along x."""
     shape = ModelShape(ModelId.MULTI, 2)
-    rho1, rho2, sigma, oh, L = 1.0, 1e-3, 0.1, 0.01, 0.15825
+    rho1, rho2, L = 1.0, 1e-3, 0.15825
     mu1 = math.sqrt(rho1 * sigma * L) * oh
 
     def x2p(c: np.ndarray) -> np.ndarray:
         out = np.zeros((c.shape[0], 6))
         out[:, 1] = rho2
+        out[:, 2] = velocity
         out[:, 4] = 1.0
         return out
 

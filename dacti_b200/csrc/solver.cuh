@@ -663,7 +663,7 @@ public:
 	}
 
 	long long read_cells(int *levels, double *data, long long max_cells) override {
-		constexpr int W = D + 1 + 2 * E + 3;
+		constexpr int W = D + 1 + 2 * E + 3 + M::P;
 		long long n = cell_count();
 		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
 		if (n > read_cap_) {
@@ -693,7 +693,7 @@ public:
 	// Same records as read_cells, gathered through caller-owned device scratch of `bytes` bytes;
 	// allocates nothing.
 	long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) override {
-		constexpr int W = D + 1 + 2 * E + 3;
+		constexpr int W = D + 1 + 2 * E + 3 + M::P;
 		const long long n = cell_count();
 		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
 		const size_t rec_bytes = align_up(sizeof(double) * W * (size_t) n);

@@ -31,8 +31,8 @@ __device__ __forceinline__ void append(int32_t *list, int *count, int value, int
 // `shift` moves the non-owner's centre by the active size across a periodic wrap.
 // --------------------------------------------------------------------------------------------
 template<class M, bool V = M::VISC>
-__device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
-                                           double dtL, double *F) {
+__device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
+                                              double dtL, double *F) {
 	constexpr int E = M::E, D = M::D;
 	const int cap   = P.cap;
 	const int lo    = P.level[owner];
@@ -121,8 +121,8 @@ __device__ __noinline__ void interior_flux(const Pool &P, const Consts &C, int o
 
 // Boundary::boundary_flux (integrator/boundary.hpp:130-160), from the cell-centre state.
 template<class M, bool V = M::VISC>
-__device__ __noinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
-                                           int dir, double dtL, double *F) {
+__device__ __forceinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
+                                              int dir, double dtL, double *F) {
 	constexpr int E = M::E, D = M::D;
 	const int cap = P.cap;
 	double pc[E], pb[E];
@@ -154,71 +154,65 @@ __device__ __noinline__ void boundary_flux(const Pool &P, const Consts &C, const
 	for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * (t1 - t0) * dirn;
 }
 
-template<int NFL>
-__device__ __forceinline__ void acc_add(double *acc, const double *F, bool plus) {
-	if (plus)
-		for (int q = 0; q < NFL; ++q) acc[q] += F[q];
-	else
-		for (int q = 0; q < NFL; ++q) acc[q] -= F[q];
-}
-
-// Adds to `acc` the fluxes owned by running-cluster cells across face (dim, dir) of cell i whose
-// neighbour slot is nb (a non-owning side's view of impl/flux.hpp:58-59).
-template<class M, bool V = M::VISC>
-__device__ void gather_owned_by_others(const Pool &P, const Consts &C, uint32_t *status, int i, int nb, int dim,
-                                       int dir, int L, double dtL, double *acc) {
+// The c-th owner of a flux across face (dim, dir) of cell i at this substep (impl/flux.hpp:58-59 seen
+// from either side). c = 0: the cell itself (cluster_mode) or its same-level neighbour; c >= 1: the
+// finer cells behind a non-leaf neighbour, adjacent child a and, when that child is split, its
+// adjacent child b - 1 (c - 1 = a (2^(D-1) + 1) + b). Returns the owner or -1; `dn` is the owner's
+// direction towards the other cell and `plus` whether cell i adds the flux.
+template<class M>
+__device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i, int nb, int dim, int dir, int L, int li,
+                                          int ai, int c, bool cluster_mode, int &dn, bool &plus) {
+	constexpr int NSUB = 1 << (M::D - 1);
 	const int cap = P.cap;
-	const int li = P.level[i], ai = P.acti[i];
-	const int dn = 1 - dir;  // owner's direction towards i
-	double F[M::F];
-	if (P.flags[nb] & F_LEAF) {
-		if (P.level[nb] == li && P.clu[nb] == L) {
-			const int an = P.acti[nb];
-			if (ai <= an && (dn == 1 || ai < an)) {
-				interior_flux<M, V>(P, C, nb, i, dim, dn, dtL, F);
-				acc_add<M::F>(acc, F, dn == 1);
-			}
+	if (c == 0) {
+		const uint32_t fn = P.flags[nb];
+		if (!(fn & F_LEAF)) return -1;
+		const int ln = P.level[nb], an = P.acti[nb];
+		if (cluster_mode && an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
+			dn   = dir;
+			plus = dir == 0;
+			return i;
 		}
-		return;
+		if (ln == li && P.clu[nb] == L && ai <= an && ((1 - dir) == 1 || ai < an)) {
+			dn   = 1 - dir;
+			plus = dn == 1;
+			return nb;
+		}
+		return -1;
 	}
-	// finer cells across the face: the children (or grandchildren) of nb on its side facing i
-	for (int c = 0; c < (1 << M::D); ++c) {
-		if (((c >> dim) & 1) != dn) continue;
-		const int ch = P.child[(size_t) c * cap + nb];
-		if (P.flags[ch] & F_LEAF) {
-			if (P.clu[ch] == L && ai <= P.acti[ch]) {
-				interior_flux<M, V>(P, C, ch, i, dim, dn, dtL, F);
-				acc_add<M::F>(acc, F, dn == 1);
-			}
-			continue;
-		}
-		for (int g = 0; g < (1 << M::D); ++g) {
-			if (((g >> dim) & 1) != dn) continue;
-			const int gc = P.child[(size_t) g * cap + ch];
-			if (!(P.flags[gc] & F_LEAF)) {
-				set_status(status, ST_DEPTH);
-				continue;
-			}
-			if (P.clu[gc] == L && ai <= P.acti[gc]) {
-				interior_flux<M, V>(P, C, gc, i, dim, dn, dtL, F);
-				acc_add<M::F>(acc, F, dn == 1);
-			}
-		}
+	dn   = 1 - dir;
+	plus = dn == 1;
+	const int k = c - 1, a = k / (NSUB + 1), b = k % (NSUB + 1);
+	const int mask = (1 << dim) - 1;
+	const int ca   = (a & mask) | (dn << dim) | ((a >> dim) << (dim + 1));
+	const int ch   = P.child[(size_t) ca * cap + nb];
+	const bool ch_leaf = P.flags[ch] & F_LEAF;
+	if (b == 0) return (ch_leaf && P.clu[ch] == L && ai <= P.acti[ch]) ? ch : -1;
+	if (ch_leaf) return -1;
+	const int gb = b - 1;
+	const int cg = (gb & mask) | (dn << dim) | ((gb >> dim) << (dim + 1));
+	const int gc = P.child[(size_t) cg * cap + ch];
+	if (!(P.flags[gc] & F_LEAF)) {
+		set_status(status, ST_DEPTH);
+		return -1;
 	}
+	return (P.clu[gc] == L && ai <= P.acti[gc]) ? gc : -1;
 }
 
 // flux_update (impl/flux.hpp:11-97), face parallel. A group of 2D lanes (padded to 4 or 8) serves
 // one cell; lane f handles face (dim, dir) = (f / 2, f % 2): the flux the cell owns across it
-// (cluster_mode) and the fluxes running-cluster neighbours own across it. The lane sums are combined
-// with a fixed butterfly, so the per-cell total does not depend on scheduling. cluster_mode: cells of
-// cluster L (marking receivers); otherwise receivers, which only gather.
+// (cluster_mode) and the fluxes running-cluster neighbours own across it, all evaluated at one call
+// site. The lane sums are combined with a fixed butterfly, so the per-cell total does not depend on
+// scheduling. cluster_mode: cells of cluster L (marking receivers); otherwise receivers, which only
+// gather.
 template<class M, bool V>
-__global__ void __launch_bounds__(BLOCK) k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr,
+__global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr,
                                                 int n_host, int L, double dtL, int stamp, int cluster_mode,
                                                 int32_t *recv, Counters *cnt) {
-	constexpr int NF = 2 * M::D;
-	constexpr int G  = NF <= 4 ? 4 : 8;
-	constexpr int GW = 32 / G;
+	constexpr int NF   = 2 * M::D;
+	constexpr int G    = NF <= 4 ? 4 : 8;
+	constexpr int GW   = 32 / G;
+	constexpr int NSUB = 1 << (M::D - 1);
 	const int n      = n_ptr ? *n_ptr : n_host;
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
@@ -228,6 +222,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux(Pool P, Consts C, BcTable B, con
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
 		const int slot = wbase + lane / G;
 		double acc[M::F];
+#pragma unroll
 		for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
 		if (slot < n && sub < NF) {
 			const int i   = list[slot];
@@ -242,32 +237,42 @@ __global__ void __launch_bounds__(BLOCK) k_flux(Pool P, Consts C, BcTable B, con
 						set_status(&cnt->status, ST_MISSING_BC);
 					} else {
 						boundary_flux<M, V>(P, C, B, i, b, dim, dir, dtL, F);
-						acc_add<M::F>(acc, F, false);
+#pragma unroll
+						for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
 					}
 				}
 			} else {
-				bool done = false;
-				if (cluster_mode) {
-					const uint32_t fn = P.flags[nb];
-					const int ln = P.level[nb], an = P.acti[nb];
-					if ((fn & F_LEAF) && an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
-						interior_flux<M, V>(P, C, i, nb, dim, dir, dtL, F);
-						acc_add<M::F>(acc, F, dir == 0);
-						if (P.clu[nb] != L) {
-							if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
-						}
-						done = true;
+				const int ncand = (P.flags[nb] & F_LEAF) ? 1 : 1 + NSUB * (NSUB + 1);
+				for (int c = 0; c < ncand; ++c) {
+					int dn;
+					bool plus;
+					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, cluster_mode != 0, dn,
+					                                plus);
+					if (owner < 0) continue;
+					if (owner == i && P.clu[nb] != L) {
+						if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
+					}
+					interior_flux<M, V>(P, C, owner, owner == i ? nb : i, dim, dn, dtL, F);
+					if (plus) {
+#pragma unroll
+						for (int q = 0; q < M::F; ++q) acc[q] += F[q];
+					} else {
+#pragma unroll
+						for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
 					}
 				}
-				if (!done) gather_owned_by_others<M, V>(P, C, &cnt->status, i, nb, dim, dir, L, dtL, acc);
 			}
 		}
 		// fixed-order butterfly over the group's lanes
+#pragma unroll
 		for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
 			for (int q = 0; q < M::F; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
 		if (slot < n) {
 			const int i = list[slot];
-			for (int q = sub; q < M::F; q += G) P.flux[(size_t) q * cap + i] += acc[q];
+#pragma unroll
+			for (int q = 0; q < M::F; ++q)
+				if ((q & (G - 1)) == sub) P.flux[(size_t) q * cap + i] += acc[q];
 		}
 	}
 }
@@ -867,7 +872,7 @@ __global__ void k_assign(Pool P, Consts C, const int32_t *list, int n, double gl
 // Gather of active-cell records for the read-back API.
 template<class M>
 __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, double *out, int32_t *lv) {
-	constexpr int E = M::E, D = M::D, W = D + 1 + 2 * E + 3;
+	constexpr int E = M::E, D = M::D, W = D + 1 + 2 * E + 3 + M::P;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i = list[tid];
@@ -883,6 +888,7 @@ __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, dou
 		o[k++] = P.err[i];
 		o[k++] = P.maxdt[i];
 		o[k++] = P.cfl[i];
+		for (int q = 0; q < M::P; ++q) o[k++] = at(P.k, cap, q, i);
 	}
 }
 

@@ -180,7 +180,7 @@ class Solver:
     def _read(self, fn) -> Snapshot:
         sh = self.shape
         D, E = sh.dims, sh.E
-        W = D + 1 + 2 * E + 3
+        W = D + 1 + 2 * E + 3 + sh.P
         n = self.n_active_cells()
         lv = np.zeros((max(n, 1), 2), np.int32)
         data = np.zeros((max(n, 1), W), np.float64)
@@ -193,6 +193,7 @@ class Solver:
             float(st.cell_updates), lv[:n, 0].copy(), lv[:n, 1].copy(), data[:n, :D].copy(), data[:n, D].copy(),
             data[:n, D + 1:D + 1 + E].copy(), data[:n, D + 1 + E:D + 1 + 2 * E].copy(), data[:n, D + 1 + 2 * E].copy(),
             data[:n, D + 2 + 2 * E].copy(), data[:n, D + 3 + 2 * E].copy(),
+            data[:n, D + 4 + 2 * E:].copy() if sh.P > 0 else None,
         )
 
     def active_cells_noalloc(self) -> Snapshot:

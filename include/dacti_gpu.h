@@ -120,8 +120,9 @@ int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_su
 int dg_cell_count(dg_solver *s, long long *n);
 
 /* for_each_active_cell (integrator/integrator.hpp:172-191): clusters 0..15 then buffers 0..15.
- * levels[n][2] = {tree_level, acti_level}; data[n][D + 1 + 2E + 3] =
- * {center[D], t, u[E], p[E], error, max_dt, cfl}. */
+ * levels[n][2] = {tree_level, acti_level}; data[n][D + 1 + 2E + 3 + P] =
+ * {center[D], t, u[E], p[E], error, max_dt, cfl, k[P]} with P = NumParm (D + 4 for the
+ * multiphase model: mu, unused, interface normal[D], curvature, smoothed volume fraction; 0 otherwise). */
 int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
 /* Allocation-free variant of dg_read_cells for hosts that cannot let the library call cudaMalloc

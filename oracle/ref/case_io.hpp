@@ -142,7 +142,7 @@ namespace oracle {
 	// Snapshot of every active cell in for_each_active_cell order (integrator/integrator.hpp:172-191).
 	// Header: "DGSNAP01", int32 {dims, E, n_cells, n_in_clusters, step, n_substeps, tree_size, pad},
 	// double {time, global_dt, updates}. Then per cell int32 {tree_level, acti_level} and doubles
-	// {center[D], t, u[E], p[E], error, max_dt, cfl}.
+	// {center[D], t, u[E], p[E], error, max_dt, cfl, k[NumParm]}.
 	struct SnapWriter {
 		FILE *f = nullptr;
 		explicit SnapWriter(const std::string &path) {

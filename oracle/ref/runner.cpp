@@ -107,7 +107,8 @@ namespace {
 		in.for_each_active_cell([&](int, auto &node) {
 			int32_t lv[2] = {node.tree_level, node.acti_level};
 			w.put(lv, 2);
-			double buf[D + 1 + 2 * E + 3];
+			constexpr int NP = Model::NumParm;
+			double buf[D + 1 + 2 * E + 3 + NP];
 			int k = 0;
 			for (int d = 0; d < D; d++) buf[k++] = node.cell.center[d];
 			buf[k++] = node.cell.t;
@@ -116,6 +117,7 @@ namespace {
 			buf[k++] = node.error;
 			buf[k++] = node.max_dt;
 			buf[k++] = node.cfl;
+			for (int q = 0; q < NP; q++) buf[k++] = node.cell.k[q];
 			w.put(buf, k);
 		});
 	}
