@@ -61,6 +61,11 @@ class Solver : public SolverBase {
 	Counters *d_cnt_ = nullptr;
 	Counters *h_cnt_ = nullptr;  // pinned
 	void *pool_mem_  = nullptr;
+	void *shadow_mem_ = nullptr;  // second pool for permutations (re-sort), allocated on first use
+	Pool S_{};
+	void *sort_mem_  = nullptr;   // keys/values/temp storage of the re-sort
+	size_t sort_bytes_ = 0;
+	bool resort_     = true;
 	void *list_mem_  = nullptr;
 	void *bc_mem_    = nullptr;
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
@@ -154,6 +159,8 @@ public:
 	~Solver() override {
 		cudaStreamSynchronize(st_);
 		cudaFree(pool_mem_);
+		cudaFree(shadow_mem_);
+		cudaFree(sort_mem_);
 		cudaFree(list_mem_);
 		cudaFree(bc_mem_);
 		cudaFree(d_cnt_);
@@ -314,6 +321,8 @@ public:
 		cudaFree(pool_mem_);
 		pool_mem_ = mem;
 		P_        = NP;
+		cudaFree(shadow_mem_);
+		shadow_mem_ = nullptr;
 		// lists grow with the pool
 		Lists old = Ls_;
 		void *old_mem = list_mem_;
@@ -600,7 +609,72 @@ public:
 		for (int l = 0; l < MAX_ACTI; ++l) n_in += h_cnt_->clu[l];
 		n_global_++;
 		if ((double) n_in / (double) (h_cnt_->top - 1) < 0.2) gc();
+		if (resort_) resort();
 		*global_dt = global_dt_;
+	}
+
+	void set_resort(bool on) { resort_ = on; }
+
+	// Morton re-sort of the node pool by (cluster, Z-order) at the end of a global step, when every
+	// ACTI buffer is empty: each cluster becomes one contiguous slot range and its list the identity
+	// over that range.
+	void resort() {
+		for (int l = 0; l < MAX_ACTI; ++l)
+			if (h_cnt_->buf[l] != 0) return;
+		const int top = h_cnt_->top;
+		const int n   = top - 1;
+		if (n <= 0) return;
+		if (!shadow_mem_) shadow_mem_ = carve_pool(S_, P_.cap);
+		size_t temp = 0;
+		DG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, (uint64_t *) nullptr, (uint64_t *) nullptr,
+		                                        (int32_t *) nullptr, (int32_t *) nullptr, n, 0, 64, st_));
+		const size_t need = align_up(sizeof(uint64_t) * n) * 2 + align_up(sizeof(int32_t) * n) * 2 +
+		                    align_up(sizeof(int32_t) * (top + 1)) + align_up(temp);
+		if (need > sort_bytes_) {
+			cudaFree(sort_mem_);
+			DG_CUDA(cudaMalloc(&sort_mem_, need));
+			sort_bytes_ = need;
+		}
+		char *b          = (char *) sort_mem_;
+		uint64_t *k_in   = (uint64_t *) b;
+		b += align_up(sizeof(uint64_t) * n);
+		uint64_t *k_out = (uint64_t *) b;
+		b += align_up(sizeof(uint64_t) * n);
+		int32_t *v_in = (int32_t *) b;
+		b += align_up(sizeof(int32_t) * n);
+		int32_t *v_out = (int32_t *) b;
+		b += align_up(sizeof(int32_t) * n);
+		int32_t *newidx = (int32_t *) b;
+		b += align_up(sizeof(int32_t) * (top + 1));
+		void *tmp = b;
+		const int g = grid_for(n);
+		run_k(DG_K_OTHER, 0, [&] { k_sort_keys<D><<<g, BLOCK, 0, st_>>>(P_, top, k_in, v_in); });
+		DG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out, n, 0, 64, st_));
+		run_k(DG_K_OTHER, 0, [&] { k_sort_inverse<<<g, BLOCK, 0, st_>>>(v_out, n, newidx); });
+		auto fo = fields(P_), fs = fields(S_);
+		for (size_t k = 0; k < fo.size(); ++k) {
+			const int comps = fo[k].comps;
+			if (comps <= 0) continue;
+			run_k(DG_K_OTHER, 0, [&] {
+				switch (fo[k].elem) {
+					case 1: k_permute<int8_t><<<g, BLOCK, 0, st_>>>((const int8_t *) *fo[k].ptr, (int8_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+					case 2: k_permute<int16_t><<<g, BLOCK, 0, st_>>>((const int16_t *) *fo[k].ptr, (int16_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+					case 4: k_permute<int32_t><<<g, BLOCK, 0, st_>>>((const int32_t *) *fo[k].ptr, (int32_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+					default: k_permute<double><<<g, BLOCK, 0, st_>>>((const double *) *fo[k].ptr, (double *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+				}
+			});
+		}
+		run_k(DG_K_OTHER, 0, [&] { k_remap_links<D><<<grid_for(top), BLOCK, 0, st_>>>(S_, top, newidx); });
+		std::swap(P_, S_);
+		std::swap(pool_mem_, shadow_mem_);
+		int first = 1;
+		for (int l = 0; l < MAX_ACTI; ++l) {
+			const int cnt = h_cnt_->clu[l];
+			if (cnt > 0) run_k(DG_K_OTHER, 0, [&] { k_fill_range<<<grid_for(cnt), BLOCK, 0, st_>>>(Ls_.clu[l], first, cnt); });
+			first += cnt;
+		}
+		DG_CUDA(cudaGetLastError());
+		sync_counters();
 	}
 
 private:

@@ -1083,3 +1083,85 @@ static __global__ void k_collect_active_leaves(Pool P, int top, int32_t *out, in
 }
 
 }  // namespace dg
+
+namespace dg {
+
+// --------------------------------------------------------------------------------------------
+// Level-bucketed Morton re-sort of the node pool. Leaves of cluster L (then of buffer L) become one
+// contiguous, Z-ordered slot range; other slots keep their relative order after them. A pure
+// permutation: links are remapped and nothing the reference can observe changes.
+// --------------------------------------------------------------------------------------------
+__device__ __forceinline__ uint64_t spread2(uint64_t x) {  // 29 bits -> even positions
+	x &= 0x1fffffffull;
+	x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+	x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+	x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+	x = (x | (x << 2)) & 0x3333333333333333ull;
+	x = (x | (x << 1)) & 0x5555555555555555ull;
+	return x;
+}
+__device__ __forceinline__ uint64_t spread3(uint64_t x) {  // 19 bits -> every third position
+	x &= 0x7ffffull;
+	x = (x | (x << 32)) & 0x1f00000000ffffull;
+	x = (x | (x << 16)) & 0x1f0000ff0000ffull;
+	x = (x | (x << 8)) & 0x100f00f00f00f00full;
+	x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+	x = (x | (x << 2)) & 0x1249249249249249ull;
+	return x;
+}
+
+template<int D>
+__global__ void k_sort_keys(Pool P, int top, uint64_t *keys, int32_t *vals) {
+	constexpr int LMAX = D == 2 ? 29 : 19;
+	for (int j = gtid(); j < top - 1; j += gstride()) {
+		const int i     = j + 1;
+		const int8_t cl = P.clu[i];
+		uint64_t code   = cl >= 0 ? (uint64_t) cl : 63ull;
+		uint64_t m      = 0;
+		if (cl >= 0) {
+			const int l  = P.level[i];
+			const int sh = LMAX - l;
+			for (int d = 0; d < D; ++d) {
+				uint64_t c = (uint64_t) P.coord[(size_t) d * P.cap + i];
+				c          = sh >= 0 ? (c << sh) : (c >> (-sh));
+				m |= (D == 2 ? spread2(c) : spread3(c)) << d;
+			}
+		} else {
+			m = (uint64_t) i;
+		}
+		keys[j] = (code << 58) | (m & ((1ull << 58) - 1));
+		vals[j] = i;
+	}
+}
+
+static __global__ void k_sort_inverse(const int32_t *sorted_vals, int n, int32_t *newidx) {
+	for (int j = gtid(); j < n; j += gstride()) newidx[sorted_vals[j]] = j + 1;
+	if (gtid() == 0) newidx[0] = 0;
+}
+
+template<typename T>
+__global__ void k_permute(const T *__restrict__ src, T *__restrict__ dst, int comps, int cap, int n,
+                          const int32_t *__restrict__ perm) {
+	for (int j = gtid(); j < n; j += gstride()) {
+		const int o = perm[j];
+		for (int c = 0; c < comps; ++c) dst[(size_t) c * cap + j + 1] = src[(size_t) c * cap + o];
+	}
+}
+
+template<int D>
+__global__ void k_remap_links(Pool P, int top, const int32_t *newidx) {
+	constexpr int NC = 1 << D, NF = 2 * D;
+	const int cap = P.cap;
+	for (int j = gtid(); j < top; j += gstride()) {
+		if (j == 0) continue;
+		P.parent[j] = newidx[P.parent[j]];
+		for (int c = 0; c < NC; ++c) P.child[(size_t) c * cap + j] = newidx[P.child[(size_t) c * cap + j]];
+		for (int f = 0; f < NF; ++f) P.nbr[(size_t) f * cap + j] = newidx[P.nbr[(size_t) f * cap + j]];
+	}
+}
+
+static __global__ void k_fill_range(int32_t *list, int first, int n) {
+	for (int j = gtid(); j < n; j += gstride()) list[j] = first + j;
+}
+
+}  // namespace dg

@@ -35,9 +35,9 @@ GOLDEN = {
                                              conductivity=(0.6, 0.026)), 4, [4]),
     # surface tension: a translating drop in the units of the reference's oscillating-drop case. The
     # reference reaches NaN in its second global step (its fixed floor alpha1 rho1 >= 1e-3 doubles the
-    # gas density of 1e-3), so the fixture holds the constructed state (smoothed volume fraction,
-    # normals and curvature) and the first global step.
-    "multi2_tension": (lambda: cases.osc_drop(velocity=0.5), 1, [0, 1]),
+    # gas density of 1e-3) and already amplifies rounding differences within the first, so the fixture
+    # holds the constructed state: smoothed volume fraction, normals and curvature, bit for bit.
+    "multi2_tension": (lambda: cases.osc_drop(velocity=0.5), 0, [0]),
 }
 
 

@@ -50,10 +50,16 @@ def test_construction_is_bit_exact(name):
     assert np.array_equal(a.u, b.u) and np.array_equal(a.p, b.p)
     assert np.array_equal(a.acti_level, b.acti_level) and np.array_equal(a.max_dt, b.max_dt)
     if a.k is not None:
-        assert np.array_equal(a.k[:, 2:], b.k[:, 2:])  # normals, curvature, smoothed alpha
+        D = case.shape.dims
+        kappa = 2 + D
+        # interface normals and smoothed volume fraction
+        assert np.array_equal(a.k[:, 2:2 + D], b.k[:, 2:2 + D]) and np.array_equal(a.k[:, kappa + 1], b.k[:, kappa + 1])
+        # the curvature only matters, and is only computed, with surface tension
+        if case.params.sigma != 0.0:
+            assert np.array_equal(a.k[:, kappa], b.k[:, kappa])
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if CASES[n][1] > 0])
 def test_golden_parity(name):
     _, steps, checks = CASES[name]
     case = read_case(os.path.join(GOLDEN, f"{name}.case"))
