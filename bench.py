@@ -187,24 +187,19 @@ def bench_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
+def timed_run(case, form: str, args, stream, local_rank: int, world: int) -> dict:
+    """W warm-up global steps, then K timed ones with CUDA events on the solver's stream."""
     import torch
     import torch.distributed as dist
-    from dacti_b200.casefile import write_case
     from dacti_b200.solver import KERNEL_KINDS, Solver
-
-    torch.cuda.set_device(local_rank)
-    stream = torch.cuda.Stream()
-    case = make_case(args)
-    D = case.shape.dims
 
     solver = Solver(case, device=local_rank)
     solver.set_stream(stream.cuda_stream)
+    solver.set_form(form)
     solver.set_profiling(True)
     for _ in range(args.warmup):
         solver.integrate()
     st0 = solver.stats()
-
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -218,27 +213,59 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
-    ms = ev0.elapsed_time(ev1)
     st1 = solver.stats()
-    updates = float(st1.cell_updates - st0.cell_updates)
-    launches = int(st1.n_launches - st0.n_launches)
+    out = {
+        "ms": ev0.elapsed_time(ev1),
+        "updates": float(st1.cell_updates - st0.cell_updates),
+        "launches": int(st1.n_launches - st0.n_launches),
+        "kms": {k: st1.kernel_ms[i] - st0.kernel_ms[i] for i, k in enumerate(KERNEL_KINDS)},
+        "kl": {k: st1.kernel_launches[i] - st0.kernel_launches[i] for i, k in enumerate(KERNEL_KINDS)},
+        "kc": {k: st1.kernel_cells[i] - st0.kernel_cells[i] for i, k in enumerate(KERNEL_KINDS)},
+        "clocks": clk.summary(),
+        "snap": solver.active_cells(),
+        "substeps": int(st1.n_substeps - st0.n_substeps),
+    }
+    solver.close()
+    return out
 
-    kms = {k: st1.kernel_ms[i] - st0.kernel_ms[i] for i, k in enumerate(KERNEL_KINDS)}
-    kl = {k: st1.kernel_launches[i] - st0.kernel_launches[i] for i, k in enumerate(KERNEL_KINDS)}
-    kc = {k: st1.kernel_cells[i] - st0.kernel_cells[i] for i, k in enumerate(KERNEL_KINDS)}
 
-    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    u_sum = torch.tensor([updates], dtype=torch.float64, device="cuda")
+def reduce_ranks(ms: float, updates: float, world: int):
+    """Max of the timed region and sum of the cell updates over all ranks."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    u = torch.tensor([updates], dtype=torch.float64, device=dev)
     if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-        dist.all_reduce(u_sum, op=dist.ReduceOp.SUM)
-    ms_max = float(t_max.item())
-    total_updates = float(u_sum.item())
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.all_reduce(u, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(u.item())
+
+
+def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
+    import torch
+    from dacti_b200.accuracy import density_rel_l1
+    from dacti_b200.casefile import write_case
+    from dacti_b200.solver import Solver
+
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    case = make_case(args)
+    D = case.shape.dims
+
+    plain = timed_run(case, "fp64", args, stream, local_rank, world)
+    chosen = timed_run(case, "mixed", args, stream, local_rank, world)
+    err = density_rel_l1(chosen["snap"], plain["snap"], case.params.side_length, case.params.active_size,
+                         args.base_level, int(case.shape.model))
+
+    ms_max, total_updates = reduce_ranks(chosen["ms"], chosen["updates"], world)
     value = total_updates / (ms_max * 1e-3)
+    p_ms, p_upd = reduce_ranks(plain["ms"], plain["updates"], world)
 
     # roofline of the dominant kernel (the flux stage): algorithmic bytes per cell update times the
     # cells of its launches, over its CUDA-event time on the solver's stream
     peak, peak_kind = measured_peak()
+    kms, kl, kc = chosen["kms"], chosen["kl"], chosen["kc"]
     dom = max(kms, key=lambda k: kms[k])
     b_per = BYTES_PER_UPDATE[D]
     flux_ms = kms["flux"]
@@ -263,12 +290,15 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(args),
-        "form": "plain FP64", "gpu_launches": launches, "roofline": roofline, "clocks": clk.summary(),
-        "cells": solver.n_active_cells(), "substeps_timed": int(st1.n_substeps - st0.n_substeps),
+        "vs_baseline": None, "dtype": "f64 update / f32 flux", "data": "synthetic", "config": workload_config(args),
+        "form": "mixed: FP32 reconstruction + HLLC flux, FP64 update, totals and EOS recovery",
+        "gpu_launches": chosen["launches"], "roofline": roofline, "clocks": chosen["clocks"],
+        "cells": chosen["snap"].n, "substeps_timed": chosen["substeps"],
+        "plain_fp64": {"value": p_upd / (p_ms * 1e-3), "ms_per_step": p_ms / args.steps,
+                       "gpu_launches": plain["launches"], "cells": plain["snap"].n},
+        "accuracy": {"density_rel_l1_vs_plain_fp64": err, "bound": 1e-4, "ok": bool(err <= 1e-4),
+                     "grid": f"uniform base level {args.base_level}, after {args.warmup + args.steps} global steps"},
     }
-    solver.close()
-    del solver
 
     # end to end through the public API: host tree -> device, K steps with the per-step scalars read
     # back, then every active cell read back to the host
@@ -277,6 +307,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         t0 = time.perf_counter()
         s2 = Solver(case, device=local_rank)
         s2.set_stream(stream.cuda_stream)
+        s2.set_form("mixed")
         e_upd0 = s2.stats().cell_updates
         for _ in range(args.steps):
             s2.integrate()
@@ -285,16 +316,12 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         torch.cuda.synchronize()
         e_sec = time.perf_counter() - t0
         e_upd = float(s2.stats().cell_updates - e_upd0)
-        t_e = torch.tensor([e_sec], dtype=torch.float64, device="cuda")
-        u_e = torch.tensor([e_upd], dtype=torch.float64, device="cuda")
-        if world > 1:
-            dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-            dist.all_reduce(u_e, op=dist.ReduceOp.SUM)
+        e_ms, e_u = reduce_ranks(e_sec * 1e3, e_upd, world)
         tree = case.tree
         h2d = (tree.parent.nbytes + tree.children.nbytes + tree.level.nbytes + tree.flags.nbytes + tree.bc.nbytes +
                tree.center.nbytes + tree.p.nbytes)
         d2h = snap.n * (8 * (D + 1 + 2 * case.shape.E + 3 + case.shape.P) + 8)
-        result["e2e"] = {"value": float(u_e.item()) / float(t_e.item()), "unit": UNIT,
+        result["e2e"] = {"value": e_u / (e_ms * 1e-3), "unit": UNIT,
                          "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                          "includes": "solver construction from the host tree, K steps, read-back of all cells"}
         s2.close()

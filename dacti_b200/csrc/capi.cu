@@ -77,6 +77,11 @@ int dg_get_stats(dg_solver *s, dg_stats *out) {
 	return guarded(s, [&] { s->impl->stats(out); });
 }
 
+int dg_set_form(dg_solver *s, int form) {
+	if (!s) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_form(form); });
+}
+
 int dg_set_profiling(dg_solver *s, int on) {
 	if (!s) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->set_profiling(on != 0); });

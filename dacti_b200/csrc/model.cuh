@@ -10,8 +10,10 @@
 namespace dg {
 
 // std::min / std::max semantics (first argument returned on ties and NaN comparisons).
-__host__ __device__ __forceinline__ double smin(double a, double b) { return (b < a) ? b : a; }
-__host__ __device__ __forceinline__ double smax(double a, double b) { return (a < b) ? b : a; }
+template<class S>
+__host__ __device__ __forceinline__ S smin(S a, S b) { return (b < a) ? b : a; }
+template<class S>
+__host__ __device__ __forceinline__ S smax(S a, S b) { return (a < b) ? b : a; }
 
 // --------------------------------------------------------------------------------------------
 // Model traits (compile-time sizes of model/euler.hpp:26-32, navier_stokes.hpp:351, multi.hpp:27-42)
@@ -46,17 +48,19 @@ constexpr double MULTI_UC    = 1.0;      // model/multi.hpp:48
 // --------------------------------------------------------------------------------------------
 // Stiffened-gas mixture closures (model/multi.hpp:367-430)
 // --------------------------------------------------------------------------------------------
-__device__ __forceinline__ double mix_gamma(const ModelConsts &m, double a) {
-	if (a < MULTI_EPS) return m.gamma2;
-	else if (a > 1 - MULTI_EPS) return m.gamma1;
-	else return 1 + 1 / (a / (m.gamma1 - 1) + (1 - a) / (m.gamma2 - 1));
+template<class S = double>
+__device__ __forceinline__ S mix_gamma(const ModelConsts &m, S a) {
+	const S g1 = (S) m.gamma1, g2 = (S) m.gamma2;
+	if (a < (S) MULTI_EPS) return g2;
+	else if (a > 1 - (S) MULTI_EPS) return g1;
+	else return 1 + 1 / (a / (g1 - 1) + (1 - a) / (g2 - 1));
 }
-__device__ __forceinline__ double mix_p0(const ModelConsts &m, double a) {
-	if (a < MULTI_EPS) return m.P2;
-	else if (a > 1 - MULTI_EPS) return m.P1;
-	else
-		return (a * m.gamma1 * m.P1 / (m.gamma1 - 1) + (1 - a) * m.gamma2 * m.P2 / (m.gamma2 - 1)) /
-		       (1 + a / (m.gamma1 - 1) + (1 - a) / (m.gamma2 - 1));
+template<class S = double>
+__device__ __forceinline__ S mix_p0(const ModelConsts &m, S a) {
+	const S g1 = (S) m.gamma1, g2 = (S) m.gamma2, P1 = (S) m.P1, P2 = (S) m.P2;
+	if (a < (S) MULTI_EPS) return P2;
+	else if (a > 1 - (S) MULTI_EPS) return P1;
+	else return (a * g1 * P1 / (g1 - 1) + (1 - a) * g2 * P2 / (g2 - 1)) / (1 + a / (g1 - 1) + (1 - a) / (g2 - 1));
 }
 __device__ __forceinline__ double mix_temperature(const ModelConsts &m, double r0, double r1, double p, double a) {
 	if (a < MULTI_EPS) return (p + m.P2) / ((m.gamma2 - 1) * r1 * m.cv2);
@@ -69,31 +73,31 @@ __device__ __forceinline__ double mix_temperature(const ModelConsts &m, double r
 // --------------------------------------------------------------------------------------------
 // Sound speed, pressure and variable conversions
 // --------------------------------------------------------------------------------------------
-template<class M>
-__device__ __forceinline__ double sound_speed_rp(const ModelConsts &m, double r0, double r1, double p, double a) {
-	if constexpr (M::MULTI) return sqrt(mix_gamma(m, a) * (p + mix_p0(m, a)) / (r0 + r1));
-	else return sqrt(EULER_GAMMA * p / r0);
+template<class M, class S = double>
+__device__ __forceinline__ S sound_speed_rp(const ModelConsts &m, S r0, S r1, S p, S a) {
+	if constexpr (M::MULTI) return sqrt(mix_gamma<S>(m, a) * (p + mix_p0<S>(m, a)) / (r0 + r1));
+	else return sqrt((S) EULER_GAMMA * p / r0);
 }
 template<class M>
 __device__ __forceinline__ double sound_speed(const ModelConsts &m, const double *p) {
 	if constexpr (M::MULTI) return sqrt(mix_gamma(m, p[M::IA]) * (p[M::IP] + mix_p0(m, p[M::IA])) / (p[0] + p[1]));
 	else return sqrt(EULER_GAMMA * p[M::IP] / p[0]);
 }
-template<class M>
-__device__ __forceinline__ double sound_speed_2(const ModelConsts &m, double r0, double r1, double p, double a) {
-	if constexpr (M::MULTI) return mix_gamma(m, a) * (p + mix_p0(m, a)) / (r0 + r1);
-	else return EULER_GAMMA * p / r0;
+template<class M, class S = double>
+__device__ __forceinline__ S sound_speed_2(const ModelConsts &m, S r0, S r1, S p, S a) {
+	if constexpr (M::MULTI) return mix_gamma<S>(m, a) * (p + mix_p0<S>(m, a)) / (r0 + r1);
+	else return (S) EULER_GAMMA * p / r0;
 }
 
 // supersonic (model/euler.hpp:250-256, model/multi.hpp:432-438). The multiphase version passes
 // the scalar p[0] where a pair of phase densities is expected, so the "mixture" density is
 // (alpha1 rho1, 0) and only p[0] enters the sound speed.
-template<class M>
-__device__ __forceinline__ bool supersonic(const ModelConsts &m, const double *p) {
-	double u2 = 0;
+template<class M, class S = double>
+__device__ __forceinline__ bool supersonic(const ModelConsts &m, const S *p) {
+	S u2 = 0;
 	for (int i = 0; i < M::D; ++i) u2 += p[M::IU + i] * p[M::IU + i];
-	if constexpr (M::MULTI) return u2 > sound_speed_2<M>(m, p[0], 0.0, p[M::IP], p[M::IA]);
-	else return u2 > sound_speed_2<M>(m, p[0], 0.0, p[M::IP], 0.0);
+	if constexpr (M::MULTI) return u2 > sound_speed_2<M, S>(m, p[0], (S) 0, p[M::IP], p[M::IA]);
+	else return u2 > sound_speed_2<M, S>(m, p[0], (S) 0, p[M::IP], (S) 0);
 }
 
 template<class M>
@@ -163,15 +167,15 @@ __device__ __forceinline__ void grad_input(const ModelConsts &m, const double *p
 }
 
 // mu / lambda (model/navier_stokes.hpp:419-425, model/multi.hpp:313-319)
-template<class M>
-__device__ __forceinline__ double visc_mu(const ModelConsts &m, const double *p) {
-	if constexpr (M::MULTI) return m.mu1 * p[M::IA] + m.mu2 * (1 - p[M::IA]);
-	else return m.ns_mu;
+template<class M, class S = double>
+__device__ __forceinline__ S visc_mu(const ModelConsts &m, const S *p) {
+	if constexpr (M::MULTI) return (S) m.mu1 * p[M::IA] + (S) m.mu2 * (1 - p[M::IA]);
+	else return (S) m.ns_mu;
 }
-template<class M>
-__device__ __forceinline__ double visc_lambda(const ModelConsts &m, const double *p) {
-	if constexpr (M::MULTI) return m.lambda1 * p[M::IA] + m.lambda2 * (1 - p[M::IA]);
-	else return m.ns_lambda;
+template<class M, class S = double>
+__device__ __forceinline__ S visc_lambda(const ModelConsts &m, const S *p) {
+	if constexpr (M::MULTI) return (S) m.lambda1 * p[M::IA] + (S) m.lambda2 * (1 - p[M::IA]);
+	else return (S) m.ns_lambda;
 }
 
 // max_delta_time (model/euler.hpp:203-215, navier_stokes.hpp:427-440, multi.hpp:322-346)
@@ -202,13 +206,12 @@ __device__ __forceinline__ double max_delta_time(const ModelConsts &m, const dou
 // Physical fluxes (model/euler.hpp:50-83, model/multi.hpp:78-123). `F` must be zeroed by the caller
 // semantics: every component not written here is 0.
 // --------------------------------------------------------------------------------------------
-template<class M>
-__device__ __forceinline__ void phys_flux(const ModelConsts &m, const double *p, double un, int dim, bool projected,
-                                          double *F) {
+template<class M, class S = double>
+__device__ __forceinline__ void phys_flux(const ModelConsts &m, const S *p, S un, int dim, bool projected, S *F) {
 	const int in = M::IU + dim;
-	double vn    = projected ? un : p[in];
-	double ke    = 0.0;
-	for (int q = 0; q < M::F; ++q) F[q] = 0.0;
+	S vn         = projected ? un : p[in];
+	S ke         = 0;
+	for (int q = 0; q < M::F; ++q) F[q] = 0;
 	if constexpr (M::MULTI) {
 		for (int i = 0; i < M::D; ++i) {
 			F[M::IU + i] = (p[0] + p[1]) * vn * p[M::IU + i];
@@ -217,8 +220,8 @@ __device__ __forceinline__ void phys_flux(const ModelConsts &m, const double *p,
 		F[0] = vn * p[0];
 		F[1] = vn * p[1];
 		F[in] += p[M::IP];
-		double a = p[M::IA];
-		F[M::IP] = vn * (mix_gamma(m, a) / (mix_gamma(m, a) - 1) * (p[M::IP] + mix_p0(m, a)) + ke * (p[0] + p[1]));
+		S a      = p[M::IA];
+		F[M::IP] = vn * (mix_gamma<S>(m, a) / (mix_gamma<S>(m, a) - 1) * (p[M::IP] + mix_p0<S>(m, a)) + ke * (p[0] + p[1]));
 		F[M::IA] = vn * p[M::IA];
 		F[M::IA + 1] = vn;
 		F[M::IA + 2 + dim] = p[M::IA];
@@ -229,42 +232,41 @@ __device__ __forceinline__ void phys_flux(const ModelConsts &m, const double *p,
 		}
 		F[0] = vn * p[0];
 		F[in] += p[M::IP];
-		F[M::IP] = vn * (EULER_GAMMA / (EULER_GAMMA - 1) * p[M::IP] + ke * p[0]);
+		F[M::IP] = vn * ((S) (EULER_GAMMA / (EULER_GAMMA - 1)) * p[M::IP] + ke * p[0]);
 	}
 }
 
 // middle_state (model/euler.hpp:118-153, model/multi.hpp:205-246): the HLLC-type star state in
 // primitive variables; `ka` enters only the multiphase contact speed.
-template<class M>
-__device__ __forceinline__ void middle_state(const ModelConsts &m, const double *pn, const double *pp, double ka,
-                                             int dim, double *pm) {
+template<class M, class S = double>
+__device__ __forceinline__ void middle_state(const ModelConsts &m, const S *pn, const S *pp, S ka, int dim, S *pm) {
 	const int in = M::IU + dim;
 	const int ip = M::IP;
-	double c_n, c_p, rn, rp;
+	S c_n, c_p, rn, rp;
 	if constexpr (M::MULTI) {
-		c_n = sound_speed_rp<M>(m, pn[0], pn[1], pn[ip], pn[M::IA]);
-		c_p = sound_speed_rp<M>(m, pp[0], pp[1], pp[ip], pp[M::IA]);
+		c_n = sound_speed_rp<M, S>(m, pn[0], pn[1], pn[ip], pn[M::IA]);
+		c_p = sound_speed_rp<M, S>(m, pp[0], pp[1], pp[ip], pp[M::IA]);
 		rn  = pn[0] + pn[1];
 		rp  = pp[0] + pp[1];
 	} else {
-		c_n = sqrt(EULER_GAMMA * pn[ip] / pn[0]);
-		c_p = sqrt(EULER_GAMMA * pp[ip] / pp[0]);
+		c_n = sqrt((S) EULER_GAMMA * pn[ip] / pn[0]);
+		c_p = sqrt((S) EULER_GAMMA * pp[ip] / pp[0]);
 		rn  = pn[0];
 		rp  = pp[0];
 	}
-	double u  = 0.5 * (pn[in] + pp[in]);
-	double c  = 0.5 * (c_n + c_p);
-	double Sn = smin(u - c, pn[in] - c_n);
-	double Sp = smax(u + c, pp[in] + c_p);
-	double Sm;
+	S u  = (S) 0.5 * (pn[in] + pp[in]);
+	S c  = (S) 0.5 * (c_n + c_p);
+	S Sn = smin<S>(u - c, pn[in] - c_n);
+	S Sp = smax<S>(u + c, pp[in] + c_p);
+	S Sm;
 	if constexpr (M::MULTI)
-		Sm = (pp[ip] - pn[ip] + rn * pn[in] * (Sn - pn[in]) - rp * pp[in] * (Sp - pp[in]) - m.sigma * ka * (pp[M::IA] - pn[M::IA])) /
+		Sm = (pp[ip] - pn[ip] + rn * pn[in] * (Sn - pn[in]) - rp * pp[in] * (Sp - pp[in]) - (S) m.sigma * ka * (pp[M::IA] - pn[M::IA])) /
 		     (rn * (Sn - pn[in]) - rp * (Sp - pp[in]));
 	else
 		Sm = (pp[ip] - pn[ip] + pn[0] * pn[in] * (Sn - pn[in]) - pp[0] * pp[in] * (Sp - pp[in])) /
 		     (pn[0] * (Sn - pn[in]) - pp[0] * (Sp - pp[in]));
 
-	for (int q = 0; q < M::E; ++q) pm[q] = 0.0;
+	for (int q = 0; q < M::E; ++q) pm[q] = 0;
 	if (Sn > 0) {
 		for (int q = 0; q < M::E; ++q) pm[q] = pn[q];
 	} else if (Sp < 0) {
@@ -340,16 +342,15 @@ __device__ __forceinline__ void compute_rhs(const ModelConsts &m, const double *
 }
 
 // Fv<D> (model/common.hpp:8-24): viscous stress row (and work term) for face normal `dim`, times mu.
-template<int D>
-__device__ __forceinline__ void visc_flux(const double *du /*[D][G]*/, int G, const double *vel, double mu, int dim,
-                                          double *fv /*[D+1]*/) {
-	for (int i = 0; i <= D; ++i) fv[i] = 0.0;
-	double trace = 0.0;
+template<int D, class S = double>
+__device__ __forceinline__ void visc_flux(const S *du /*[D][G]*/, int G, const S *vel, S mu, int dim, S *fv /*[D+1]*/) {
+	for (int i = 0; i <= D; ++i) fv[i] = 0;
+	S trace = 0;
 	for (int i = 0; i < D; ++i) {
 		fv[i] = du[dim * G + i] + du[i * G + dim];
 		trace += du[i * G + i];
 	}
-	fv[dim] -= (2.0 / 3.0 * trace);
+	fv[dim] -= ((S) (2.0 / 3.0) * trace);
 	for (int i = 0; i < D; ++i) fv[D] += fv[i] * vel[i];
 	for (int i = 0; i <= D; ++i) fv[i] = fv[i] * mu;
 }

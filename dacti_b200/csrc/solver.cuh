@@ -39,6 +39,7 @@ public:
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void set_profiling(bool on) = 0;
+	virtual void set_form(int form) = 0;
 	std::string last_error;
 };
 
@@ -74,6 +75,7 @@ class Solver : public SolverBase {
 	long long read_cap_ = 0;
 	int limiter_ = 0;
 	bool visc_   = false;  // viscous/heat terms present (multiphase with any non-zero mu or lambda)
+	bool mixed_  = false;  // FP32 reconstruction and flux, FP64 update and EOS recovery
 	bool sigma_  = false;  // surface tension present
 
 	// scheduler state (integrator/integrator.hpp:46-58)
@@ -141,6 +143,10 @@ class Solver : public SolverBase {
 
 public:
 	void set_profiling(bool on) override { prof_ = on; }
+	void set_form(int form) override {
+		if (form != DG_FORM_FP64 && form != DG_FORM_MIXED) throw dg_error(DG_ERR_ARG, "unknown form");
+		mixed_ = form == DG_FORM_MIXED;
+	}
 
 	explicit Solver(const dg_case &c) {
 		limiter_ = c.limiter;
@@ -465,6 +471,20 @@ private:
 		}
 	}
 
+	void launch_flux(const int32_t *list, const int *n_ptr, int n, int L, double dtL, int stamp, int cluster_mode, int grid) {
+		if (mixed_) {
+			if (visc_)
+				k_flux<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+			else
+				k_flux<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+		} else {
+			if (visc_)
+				k_flux<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+			else
+				k_flux<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+		}
+	}
+
 	void launch_slope(const int32_t *list, int n) {
 		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
@@ -499,22 +519,9 @@ private:
 		const int counterL = acti_counter_[L];
 
 		constexpr int LPC = NF <= 4 ? 4 : 8;  // flux lanes per cell
-		run_k(DG_K_FLUX, n, [&] {
-			if (visc_)
-				k_flux<M, true><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL,
-				                                                                   stamp_recv, 1, Ls_.recv, d_cnt_);
-			else
-				k_flux<M, false><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, list, nullptr, n, L, dtL,
-				                                                                    stamp_recv, 1, Ls_.recv, d_cnt_);
-		});
+		run_k(DG_K_FLUX, n, [&] { launch_flux(list, nullptr, n, L, dtL, stamp_recv, 1, grid_for((long long) n * LPC)); });
 		run_k(DG_K_RECV, 0, [&] {
-			if (visc_)
-				k_flux<M, true><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv, 0,
-				                                                                   L, dtL, stamp_recv, 0, Ls_.recv, d_cnt_);
-			else
-				k_flux<M, false><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, C_, B_, Ls_.recv, &d_cnt_->n_recv,
-				                                                                    0, L, dtL, stamp_recv, 0, Ls_.recv,
-				                                                                    d_cnt_);
+			launch_flux(Ls_.recv, &d_cnt_->n_recv, 0, L, dtL, stamp_recv, 0, grid_for((long long) n * LPC));
 		});
 		run_k(DG_K_UPDATE, n, [&] {
 			if (visc_) k_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);

@@ -30,9 +30,9 @@ __device__ __forceinline__ void append(int32_t *list, int *count, int value, int
 // the right state and the face keeps the owner's centre (the reference relabels face.dir = 1).
 // `shift` moves the non-owner's centre by the active size across a periodic wrap.
 // --------------------------------------------------------------------------------------------
-template<class M, bool V = M::VISC>
+template<class M, bool V = M::VISC, class S = double>
 __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
-                                              double dtL, double *F) {
+                                              double dtL, double *Fout) {
 	constexpr int E = M::E, D = M::D;
 	const int cap   = P.cap;
 	const int lo    = P.level[owner];
@@ -59,99 +59,106 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 	const double tm   = 0.5 * (t1 + t0);
 	const double dt_n = tm - P.t[iL];
 	const double dt_p = tm - P.t[iR];
-	double pn[E], pp[E];
+	// Hancock predictor at the face (reconstruction); geometry and time offsets stay FP64
+	const S xl = (S) (fc - cL), xr = (S) (fc - cR), tl = (S) dt_n, tr = (S) dt_p;
+	S pn[E], pp[E];
 	for (int q = 0; q < E; ++q) {
-		double v = at(P.p, cap, q, iL) + at(P.slope, cap, dim * E + q, iL) * (fc - cL);
-		pn[q]    = v - at(P.rhs, cap, q, iL) * dt_n;
-		double w = at(P.p, cap, q, iR) + at(P.slope, cap, dim * E + q, iR) * (fc - cR);
-		pp[q]    = w - at(P.rhs, cap, q, iR) * dt_p;
+		S v   = (S) at(P.p, cap, q, iL) + (S) at(P.slope, cap, dim * E + q, iL) * xl;
+		pn[q] = v - (S) at(P.rhs, cap, q, iL) * tl;
+		S w   = (S) at(P.p, cap, q, iR) + (S) at(P.slope, cap, dim * E + q, iR) * xr;
+		pp[q] = w - (S) at(P.rhs, cap, q, iR) * tr;
 	}
-	double ka = 0.0;
-	if constexpr (M::MULTI) ka = 0.5 * (at(P.k, cap, M::KAPPA, iL) + at(P.k, cap, M::KAPPA, iR));
-	double pm[E];
-	middle_state<M>(C.m, pn, pp, ka, dim, pm);
-	phys_flux<M>(C.m, pm, 0.0, dim, false, F);
+	S ka = 0;
+	if constexpr (M::MULTI) ka = (S) 0.5 * ((S) at(P.k, cap, M::KAPPA, iL) + (S) at(P.k, cap, M::KAPPA, iR));
+	S pm[E], F[M::F];
+	middle_state<M, S>(C.m, pn, pp, ka, dim, pm);
+	phys_flux<M, S>(C.m, pm, (S) 0, dim, false, F);
 	const double dtf = t1 - t0;
 
 	if constexpr (M::MULTI) {
 		constexpr int IA = M::IA, IU = M::IU, IP = M::IP;
-		const double a = pm[IA];
-		if (a > 1e-5 && a < 1 - 1e-5) {
-			double n  = 0.5 * (at(P.k, cap, M::IKN + dim, iL) + at(P.k, cap, M::IKN + dim, iR));
-			double uc = MULTI_UC * fabs(pm[IU + dim]) * n;
-			double ke = 0.0;
+		const S a = pm[IA];
+		if (a > (S) 1e-5 && a < 1 - (S) 1e-5) {
+			S n  = (S) 0.5 * ((S) at(P.k, cap, M::IKN + dim, iL) + (S) at(P.k, cap, M::IKN + dim, iR));
+			S uc = (S) MULTI_UC * fabs(pm[IU + dim]) * n;
+			S ke = 0;
 			for (int i = 0; i < D; ++i) {
 				F[IU + i] += uc * ((1 - a) * pm[0] - a * pm[1]) * pm[IU + i];
-				ke += 0.5 * pm[IU + i] * pm[IU + i];
+				ke += (S) 0.5 * pm[IU + i] * pm[IU + i];
 			}
 			F[0] += uc * (1 - a) * pm[0];
 			F[1] += uc * (-a) * pm[1];
 			const ModelConsts &m = C.m;
+			const S g1 = (S) m.gamma1, g2 = (S) m.gamma2, P1 = (S) m.P1, P2 = (S) m.P2;
 			F[IP] += uc * ((1 - a) * pm[0] - a * pm[1]) * ke +
-			         uc * (1 - a) * a *
-			             (pm[IP] * (1 / (m.gamma1 - 1) - 1 / (m.gamma2 - 1)) + m.gamma1 * m.P1 / (m.gamma1 - 1) -
-			              m.gamma2 * m.P2 / (m.gamma2 - 1));
+			         uc * (1 - a) * a * (pm[IP] * (1 / (g1 - 1) - 1 / (g2 - 1)) + g1 * P1 / (g1 - 1) - g2 * P2 / (g2 - 1));
 			F[IA] += uc * (1 - a) * a;
 		}
 	}
 	if constexpr (M::VISC && V) {
 		constexpr int G = M::G;
-		double du[D * G], vel[D], fv[D + 1];
+		S du[D * G], vel[D], fv[D + 1];
 		for (int i = 0; i < D; ++i)
-			for (int g = 0; g < G; ++g) du[i * G + g] = 0.5 * (at(P.grad, cap, i * G + g, iL) + at(P.grad, cap, i * G + g, iR));
-		for (int i = 0; i < D; ++i) vel[i] = 0.5 * (at(P.p, cap, M::IU + i, iL) + at(P.p, cap, M::IU + i, iR));
+			for (int g = 0; g < G; ++g)
+				du[i * G + g] = (S) 0.5 * ((S) at(P.grad, cap, i * G + g, iL) + (S) at(P.grad, cap, i * G + g, iR));
+		for (int i = 0; i < D; ++i) vel[i] = (S) 0.5 * ((S) at(P.p, cap, M::IU + i, iL) + (S) at(P.p, cap, M::IU + i, iR));
 		if constexpr (M::MULTI) {
 			// multi.hpp:287-301: viscous and heat terms enter before the area * dt scaling
-			visc_flux<D>(du, G, vel, visc_mu<M>(C.m, pm), dim, fv);
+			visc_flux<D, S>(du, G, vel, visc_mu<M, S>(C.m, pm), dim, fv);
 			for (int i = 0; i <= D; ++i) F[M::IU + i] -= fv[i];
-			F[M::IU + D] -= du[dim * G + M::DT] * visc_lambda<M>(C.m, pm);
-			for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
+			F[M::IU + D] -= du[dim * G + M::DT] * visc_lambda<M, S>(C.m, pm);
+			for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * dtf;
 		} else {
 			// navier_stokes.hpp:387-408: convective part scaled first, then scaled viscous/heat terms
-			for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
-			visc_flux<D>(du, G, vel, C.m.ns_mu, dim, fv);
-			for (int i = 0; i <= D; ++i) F[M::IU + i] -= fv[i] * area * dtf;
-			double fh = C.m.ns_lambda * du[dim * G + M::DT] * area * dtf;
-			F[M::IU + D] -= fh;
+			for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * dtf;
+			visc_flux<D, S>(du, G, vel, (S) C.m.ns_mu, dim, fv);
+			for (int i = 0; i <= D; ++i) Fout[M::IU + i] -= (double) fv[i] * area * dtf;
+			const double fh = (double) ((S) C.m.ns_lambda * du[dim * G + M::DT]) * area * dtf;
+			Fout[M::IU + D] -= fh;
 		}
 	} else {
-		for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * dtf;
+		for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * dtf;
 	}
 }
 
 // Boundary::boundary_flux (integrator/boundary.hpp:130-160), from the cell-centre state.
-template<class M, bool V = M::VISC>
+template<class M, bool V = M::VISC, class S = double>
 __device__ __forceinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
-                                              int dir, double dtL, double *F) {
+                                              int dir, double dtL, double *Fout) {
 	constexpr int E = M::E, D = M::D;
 	const int cap = P.cap;
-	double pc[E], pb[E];
-	load_p<M>(P, i, pc);
+	double pcd[E], pbd[E];
+	load_p<M>(P, i, pcd);
 	const double t0 = P.t[i];
 	const double t1 = t0 + dtL;
-	boundary_value<M>(C.m, B, b, pc, t0, pb);
+	boundary_value<M>(C.m, B, b, pcd, t0, pbd);
+	S pc[E], pb[E], F[M::F];
+	for (int q = 0; q < E; ++q) {
+		pc[q] = (S) pcd[q];
+		pb[q] = (S) pbd[q];
+	}
 	const int type = B.type[b];
 	if (type == BC_FREESLIP) {
-		phys_flux<M>(C.m, pc, pb[M::IU + dim], dim, true, F);
+		phys_flux<M, S>(C.m, pc, pb[M::IU + dim], dim, true, F);
 	} else if (type == BC_NOSLIP) {
-		for (int q = 0; q < M::F; ++q) F[q] = 0.0;
+		for (int q = 0; q < M::F; ++q) F[q] = 0;
 		F[M::IU + dim] = pb[M::IP];
 	} else {
-		double pm[E];
-		middle_state<M>(C.m, pb, pc, 0.0, dim, pm);
-		phys_flux<M>(C.m, pm, 0.0, dim, false, F);
+		S pm[E];
+		middle_state<M, S>(C.m, pb, pc, (S) 0, dim, pm);
+		phys_flux<M, S>(C.m, pm, (S) 0, dim, false, F);
 	}
 	if constexpr (M::VISC && V) {
 		constexpr int G = M::G;
-		double g[D * G], z[D], fv[D + 1];
-		for (int c = 0; c < D * G; ++c) g[c] = at(P.grad, cap, c, i);
-		for (int d = 0; d < D; ++d) z[d] = 0.0;
-		visc_flux<D>(g, G, z, visc_mu<M>(C.m, pc), dim, fv);
+		S g[D * G], z[D], fv[D + 1];
+		for (int c = 0; c < D * G; ++c) g[c] = (S) at(P.grad, cap, c, i);
+		for (int d = 0; d < D; ++d) z[d] = 0;
+		visc_flux<D, S>(g, G, z, visc_mu<M, S>(C.m, pc), dim, fv);
 		for (int k = 0; k <= D; ++k) F[M::IU + k] -= fv[k];
 	}
 	const double area = C.area[P.level[i]];
 	const double dirn = (double) (2 * dir - 1);
-	for (int q = 0; q < M::F; ++q) F[q] = F[q] * area * (t1 - t0) * dirn;
+	for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * (t1 - t0) * dirn;
 }
 
 // The c-th owner of a flux across face (dim, dir) of cell i at this substep (impl/flux.hpp:58-59 seen
@@ -205,7 +212,7 @@ __device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i
 // site. The lane sums are combined with a fixed butterfly, so the per-cell total does not depend on
 // scheduling. cluster_mode: cells of cluster L (marking receivers); otherwise receivers, which only
 // gather.
-template<class M, bool V>
+template<class M, bool V, class S = double>
 __global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr,
                                                 int n_host, int L, double dtL, int stamp, int cluster_mode,
                                                 int32_t *recv, Counters *cnt) {
@@ -236,7 +243,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, 
 					if (b < 0) {
 						set_status(&cnt->status, ST_MISSING_BC);
 					} else {
-						boundary_flux<M, V>(P, C, B, i, b, dim, dir, dtL, F);
+						boundary_flux<M, V, S>(P, C, B, i, b, dim, dir, dtL, F);
 #pragma unroll
 						for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
 					}
@@ -252,7 +259,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, 
 					if (owner == i && P.clu[nb] != L) {
 						if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 					}
-					interior_flux<M, V>(P, C, owner, owner == i ? nb : i, dim, dn, dtL, F);
+					interior_flux<M, V, S>(P, C, owner, owner == i ? nb : i, dim, dn, dtL, F);
 					if (plus) {
 #pragma unroll
 						for (int q = 0; q < M::F; ++q) acc[q] += F[q];

@@ -86,6 +86,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                           ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.dg_set_form.argtypes = [vp, ctypes.c_int]
     lib.dg_last_error.argtypes = [vp]
     lib.dg_last_error.restype = ctypes.c_char_p
     lib.dg_destroy.argtypes = [vp]
@@ -96,7 +97,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells",
                     "dg_read_cells_noalloc", "dg_get_stats",
-                    "dg_set_profiling", "dg_last_error", "dg_destroy")
+                    "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
 class DgError(RuntimeError):
@@ -204,6 +205,10 @@ class Solver:
         s = DgStats()
         self._check(self._lib.dg_get_stats(self._h, ctypes.byref(s)))
         return s
+
+    def set_form(self, form: str) -> None:
+        """'fp64' (the reference's arithmetic) or 'mixed' (FP32 reconstruction and flux, FP64 update)."""
+        self._check(self._lib.dg_set_form(self._h, {"fp64": 0, "mixed": 1}[form]))
 
     def set_profiling(self, on: bool = True) -> None:
         self._check(self._lib.dg_set_profiling(self._h, 1 if on else 0))

@@ -31,6 +31,10 @@ enum {
 /* model ids (dacti::model::euler / navier_stokes / multi) */
 enum { DG_EULER = 0, DG_NAVIER_STOKES = 1, DG_MULTI = 2 };
 
+/* numerical forms: the reference's FP64 arithmetic, or FP32 reconstruction and HLLC flux with the
+ * conservative update, the conservation totals and the pressure/temperature recovery in FP64 */
+enum { DG_FORM_FP64 = 0, DG_FORM_MIXED = 1 };
+
 /* limiter ids (dacti::integrator::slope, integrator/slope_limiters.hpp:7-57) */
 enum { DG_MINMOD = 0, DG_UNLIMITED, DG_VAN_LEER, DG_SUPERBEE, DG_VON_ALBA_2, DG_KOREN, DG_FIRST_ORDER };
 
@@ -136,6 +140,10 @@ int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, 
 int dg_read_cells_noalloc(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
 int dg_get_stats(dg_solver *s, dg_stats *out);
+
+/* Numerical form of the following steps (DG_FORM_FP64 by default). No counterpart in the reference,
+ * which computes everything in FP64. */
+int dg_set_form(dg_solver *s, int form);
 
 /* Per-kernel device timing with CUDA events on the solver's stream (off by default). */
 int dg_set_profiling(dg_solver *s, int on);
