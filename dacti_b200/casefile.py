@@ -57,6 +57,7 @@ class SolverParams:
     lambda2: float = 0.0
     sigma: float = 0.0
     zones: Sequence[RefineZone] = field(default_factory=list)
+    limiter: int = 0  # dacti::integrator::slope id: minmod, unlimited, van_leer, superbee, von_alba_2, koren, first_order
 
     def param_vector(self) -> np.ndarray:
         v = np.zeros(N_PARAMS, np.float64)
@@ -96,7 +97,7 @@ def write_case(case: Case, path: str) -> None:
     E, D = sh.E, sh.dims
     with open(path, "wb") as f:
         f.write(b"DGCASE01")
-        hdr = np.array([int(sh.model), D, t.n_nodes, len(t.bcs), len(prm.zones), 0, 0, 0], np.int32)
+        hdr = np.array([int(sh.model), D, t.n_nodes, len(t.bcs), len(prm.zones), int(prm.limiter), 0, 0], np.int32)
         f.write(hdr.tobytes())
         f.write(prm.param_vector().tobytes())
         f.write(np.asarray(prm.weights, np.float64).reshape(E).tobytes())
@@ -197,7 +198,7 @@ def read_case(path: str) -> Case:
     off = 8
     hdr = np.frombuffer(buf, np.int32, 8, off)
     off += 32
-    model, D, n, nbc, nz = (int(x) for x in hdr[:5])
+    model, D, n, nbc, nz, lim = (int(x) for x in hdr[:6])
     shape = ModelShape(ModelId(model), D)
     E, C, NF = shape.E, shape.C, shape.NF
     prm = np.frombuffer(buf, np.float64, N_PARAMS, off)
@@ -244,6 +245,6 @@ def read_case(path: str) -> Case:
         gamma2=float(prm[P["GAMMA2"]]), P1=float(prm[P["P1"]]), P2=float(prm[P["P2"]]), cp1=float(prm[P["CP1"]]),
         cp2=float(prm[P["CP2"]]), cv1=float(prm[P["CV1"]]), cv2=float(prm[P["CV2"]]), mu1=float(prm[P["MU1"]]),
         mu2=float(prm[P["MU2"]]), lambda1=float(prm[P["LAMBDA1"]]), lambda2=float(prm[P["LAMBDA2"]]),
-        sigma=float(prm[P["SIGMA"]]), zones=zones,
+        sigma=float(prm[P["SIGMA"]]), zones=zones, limiter=lim,
     )
     return Case(tree, params)

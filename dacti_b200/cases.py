@@ -25,7 +25,8 @@ def _zg_box(D: int):
 
 
 def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
-             model: ModelId = ModelId.EULER, mu: float = 0.0, prandtl: Optional[float] = None) -> Case:
+             model: ModelId = ModelId.EULER, mu: float = 0.0, prandtl: Optional[float] = None,
+             domain_bc=None, limiter: int = 0) -> Case:
     """Config 1: 2D Euler Lax-Liu configuration 3 on the unit square, quadrants split at x=y=0.
 
     States (rho, u, v, p): TR (1.5,0,0,1.5), TL (0.5323,1.206,0,0.3), BL (0.138,1.206,1.206,0.029),
@@ -34,7 +35,9 @@ def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_
     to t = 0.3 (tighter pairs make the reference itself produce NaN near t = 0.29).
 
     With ``model=ModelId.NAVIER_STOKES`` the same problem runs with constant viscosity ``mu`` and
-    conductivity ``mu * cp / prandtl`` (model/navier_stokes.hpp:454-459).
+    conductivity ``mu * cp / prandtl`` (model/navier_stokes.hpp:454-459). ``domain_bc`` replaces the
+    zero-gradient faces with (neg, pos) BoundarySpec pairs per dimension; ``limiter`` selects the
+    slope limiter by id.
     """
     shape = ModelShape(model, 2)
 
@@ -51,12 +54,12 @@ def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_
         out[br] = (0.5323, 0.0, 1.206, 0.3)
         return out
 
-    spec = SceneSpec(shape, (1.0, 1.0), base_level, base_level + levels, x2p, _zg_box(2))
+    spec = SceneSpec(shape, (1.0, 1.0), base_level, base_level + levels, x2p, domain_bc or _zg_box(2))
     prm = SolverParams(
         side_length=1.0, active_size=(1.0, 1.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
         weights=(1.0, 0.0, 0.0, 0.0),
-        ns_mu=mu, ns_lambda=(mu * 1005.0 / prandtl) if prandtl else 0.0,
+        ns_mu=mu, ns_lambda=(mu * 1005.0 / prandtl) if prandtl else 0.0, limiter=limiter,
     )
     return Case(build_tree(spec), prm)
 
@@ -132,6 +135,37 @@ def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: floa
     return Case(build_tree(spec), prm)
 
 
+def box_blast(base_level: int = 3, levels: int = 2, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
+              p_in: float = 5.0, model: ModelId = ModelId.EULER, mu: float = 0.0, prandtl: float = 0.72,
+              domain_bc=None) -> Case:
+    """2D Euler / Navier-Stokes blast in the unit box: rho 1.5, p = ``p_in`` inside a disc of radius
+    0.2 at (0.1, -0.05), rho 1, p 1 outside, uniform drift (0.2, -0.1). Its waves reach every face of
+    the box within one time unit, which exercises the wall treatments (integrator/boundary.hpp:
+    76-89, 128-142): ``domain_bc`` gives (neg, pos) BoundarySpec pairs per dimension, freeslip
+    on x and noslip on y by default. (The Lax-Liu configuration 3 runs into the reference's wall
+    boundary fluxes at Mach ~1 and breaks down with NaN after a few steps, so it is not used here.)"""
+    shape = ModelShape(model, 2)
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        inside = np.hypot(c[:, 0] - 0.1, c[:, 1] + 0.05) < 0.2
+        out = np.empty((c.shape[0], 4))
+        out[:, 0] = np.where(inside, 1.5, 1.0)
+        out[:, 1] = 0.2
+        out[:, 2] = -0.1
+        out[:, 3] = np.where(inside, p_in, 1.0)
+        return out
+
+    if domain_bc is None:
+        domain_bc = [(BoundarySpec(BcType.FREESLIP),) * 2, (BoundarySpec(BcType.NOSLIP),) * 2]
+    spec = SceneSpec(shape, (1.0, 1.0), base_level, base_level + levels, x2p, domain_bc)
+    prm = SolverParams(
+        side_length=1.0, active_size=(1.0, 1.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
+        weights=(1.0, 0.0, 0.0, 0.0), ns_mu=mu, ns_lambda=mu * 1005.0 / prandtl if mu else 0.0,
+    )
+    return Case(build_tree(spec), prm)
+
+
 def periodic_blob(base_level: int = 4, levels: int = 2, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
                   refine: bool = True) -> Case:
     """2D Euler on a doubly periodic unit square: a dense square (rho 2 inside |x|,|y| < 0.15, else 1)
@@ -155,6 +189,35 @@ def periodic_blob(base_level: int = 4, levels: int = 2, thresholds=(0.02, 0.05),
     prm = SolverParams(
         side_length=1.0, active_size=(1.0, 1.0), periodic=(True, True), max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=max_level, min_level=base_level, weights=(1.0, 0.0, 0.0, 0.0),
+    )
+    return Case(build_tree(spec), prm)
+
+
+def smooth_periodic(base_level: int = 3, levels: int = 2, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
+                    limiter: int = 0) -> Case:
+    """2D Euler on a doubly periodic unit square with every primitive varying smoothly: a periodic
+    Gaussian density bump of width 0.1 on a background of sines, sheared velocity, pressure wave.
+    No two neighbouring cells hold equal values, so the slope limiters whose formula is 0/0 on
+    equal slopes (van Leer, van Albada 2 in integrator/slope_limiters.hpp) stay finite; the
+    reference produces NaN on them wherever the flow is piecewise constant."""
+    shape = ModelShape(ModelId.EULER, 2)
+    tp = 2.0 * math.pi
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        x, y = c[:, 0], c[:, 1]
+        bump = np.exp(-(np.sin(math.pi * x) ** 2 + np.sin(math.pi * y) ** 2) / 0.01)
+        out = np.empty((c.shape[0], 4))
+        out[:, 0] = 1.0 + 0.5 * bump + 0.1 * np.sin(tp * x + 0.3) * np.sin(tp * y + 1.1) + 0.05 * np.cos(tp * (x + 2 * y))
+        out[:, 1] = 0.3 + 0.1 * np.cos(tp * y + 0.4) + 0.02 * np.sin(tp * (x - y) + 0.9)
+        out[:, 2] = -0.2 + 0.1 * np.sin(tp * x + 0.2) + 0.03 * np.cos(tp * (2 * x + y) + 0.5) + 0.02 * np.sin(tp * y + 0.7)
+        out[:, 3] = 1.0 + 0.1 * np.sin(tp * (x - y) + 0.6) + 0.03 * np.cos(tp * (x + y) + 0.8) + 0.2 * bump
+        return out
+
+    spec = SceneSpec(shape, (1.0, 1.0), base_level, base_level + levels, x2p, [None, None])
+    prm = SolverParams(
+        side_length=1.0, active_size=(1.0, 1.0), periodic=(True, True), max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
+        weights=(1.0, 0.0, 0.0, 0.0), limiter=limiter,
     )
     return Case(build_tree(spec), prm)
 

@@ -298,6 +298,14 @@ __device__ __forceinline__ void middle_state(const ModelConsts &m, const S *pn, 
 	}
 }
 
+// multi::A receives the curvature through a `const size_t ka` parameter (model/multi.hpp:126): the
+// double is truncated to an integer and a negative value wraps modulo 2^64 before re-entering the
+// product as a double. Reproduced as the reference build converts it (signed 64-bit truncation read as
+// unsigned).
+__device__ __forceinline__ double jacobian_kappa(double k) {
+	return (double) (unsigned long long) (long long) k;
+}
+
 // compute_rhs (model/euler.hpp:105-116, model/multi.hpp:158-169): rhs = sum_j A_j(p) slope_j with
 // the primitive Jacobians A (model/euler.hpp:86-103, model/multi.hpp:126-145). Products with
 // structurally zero entries of A are skipped: adding an exact zero never changes a running sum
@@ -313,7 +321,7 @@ __device__ __forceinline__ void compute_rhs(const ModelConsts &m, const double *
 	double a_pin = M::MULTI ? rho * c2 : p[0] * c2;  // A[ip][in]
 	double a_inp = 1.0 / rho;                         // A[in][ip]
 	double a_ina = 0.0;                               // A[in][ia]
-	if constexpr (M::MULTI) a_ina = m.sigma * kappa / (p[0] + p[1]);
+	if constexpr (M::MULTI) a_ina = m.sigma * jacobian_kappa(kappa) / (p[0] + p[1]);
 	for (int i = 0; i < E; ++i) {
 		double r = 0.0;
 		for (int j = 0; j < D; ++j) {

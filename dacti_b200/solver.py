@@ -111,7 +111,7 @@ def _ptr(a: np.ndarray, ctype):
 
 
 class Solver:
-    def __init__(self, case: Case, limiter: str = "minmod", device: int = 0):
+    def __init__(self, case: Case, limiter: Optional[str] = None, device: int = 0):
         self._lib = load_library()
         self._check_plain(self._lib.dg_set_device(device))
         t, prm = case.tree, case.params
@@ -139,7 +139,8 @@ class Solver:
         )
         c = DgCase()
         c.model, c.dims, c.n_nodes = int(sh.model), D, t.n_nodes
-        c.n_bc, c.n_zones, c.limiter = len(t.bcs), len(prm.zones), LIMITERS[limiter]
+        lim_id = LIMITERS[limiter] if limiter is not None else int(prm.limiter)
+        c.n_bc, c.n_zones, c.limiter = len(t.bcs), len(prm.zones), lim_id
         dbl, it = ctypes.c_double, ctypes.c_int
         c.params, c.weights, c.zones = _ptr(keep["params"], dbl), _ptr(keep["weights"], dbl), _ptr(keep["zones"], dbl)
         c.bc_type, c.bc_p_in = _ptr(keep["bc_type"], it), _ptr(keep["bc_p_in"], dbl)

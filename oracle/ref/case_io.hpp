@@ -69,7 +69,7 @@ namespace oracle {
 	};
 
 	struct CaseData {
-		int32_t model = 0, dims = 0, n_nodes = 0, n_bc = 0, n_zones = 0;
+		int32_t model = 0, dims = 0, n_nodes = 0, n_bc = 0, n_zones = 0, limiter = 0;
 		int E = 0, C = 0, NF = 0;
 		double params[N_PARAMS] = {};
 		std::vector<double> weights;
@@ -96,7 +96,7 @@ namespace oracle {
 		if (std::memcmp(magic, "DGCASE01", 8) != 0) throw std::runtime_error("bad case magic");
 		int32_t hdr[8];
 		rd(f, hdr, 8);
-		c.model = hdr[0], c.dims = hdr[1], c.n_nodes = hdr[2], c.n_bc = hdr[3], c.n_zones = hdr[4];
+		c.model = hdr[0], c.dims = hdr[1], c.n_nodes = hdr[2], c.n_bc = hdr[3], c.n_zones = hdr[4], c.limiter = hdr[5];
 		c.E  = num_eqns(c.model, c.dims);
 		c.C  = 1 << c.dims;
 		c.NF = 2 * c.dims;

@@ -85,20 +85,20 @@ namespace {
 		return bad;
 	}
 
-	template<typename Model>
-	struct Runner : public integrator::Integrator<Model, integrator::slope::minmod, integrator::error::weighted_laplacian<Model::NumEqns>> {
-		using Base     = integrator::Integrator<Model, integrator::slope::minmod, integrator::error::weighted_laplacian<Model::NumEqns>>;
+	template<typename Model, typename Limiter = integrator::slope::minmod>
+	struct Runner : public integrator::Integrator<Model, Limiter, integrator::error::weighted_laplacian<Model::NumEqns>> {
+		using Base       = integrator::Integrator<Model, Limiter, integrator::error::weighted_laplacian<Model::NumEqns>>;
 		using vecn_t_pub = linalg::vec<scalar_t, Model::NumDims>;
 		using Base::Base;
 	};
 
-	template<typename Model>
-	void write_snapshot(Runner<Model> &in, const std::string &path, int step, double time, double updates) {
+	template<typename Model, typename R>
+	void write_snapshot(R &in, const std::string &path, int step, double time, double updates) {
 		constexpr int D = Model::NumDims;
 		constexpr int E = Model::NumEqns;
 		oracle::SnapWriter w(path);
 		size_t n_clusters = 0;
-		for (int l = 0; l < Runner<Model>::MAX_LEVEL; l++) n_clusters += in.acti_clusters[l].size();
+		for (int l = 0; l < R::MAX_LEVEL; l++) n_clusters += in.acti_clusters[l].size();
 		int32_t hdr[8] = {D, E, (int32_t) in.n_active_cells(), (int32_t) n_clusters, step, in.n_substeps, (int32_t) in.domain.tree.size(), 0};
 		w.put("DGSNAP01", 8);
 		w.put(hdr, 8);
@@ -122,8 +122,9 @@ namespace {
 		});
 	}
 
-	template<typename Model>
+	template<typename Model, typename Limiter = integrator::slope::minmod>
 	int run(const oracle::CaseData &c, const Options &o) {
+		using R = Runner<Model, Limiter>;
 		using namespace oracle;
 		constexpr int D = Model::NumDims;
 		constexpr int E = Model::NumEqns;
@@ -155,14 +156,14 @@ namespace {
 		scene::Scene<Model> scene(cfg);
 		using clk = std::chrono::steady_clock;
 		auto t0   = clk::now();
-		Runner<Model> in{integrator::slope::minmod{}, integrator::error::weighted_laplacian<E>{w}, scene, cfg};
+		R in{Limiter{}, integrator::error::weighted_laplacian<E>{w}, scene, cfg};
 		double init_s = std::chrono::duration<double>(clk::now() - t0).count();
 
 		double time = 0.0, updates = 0.0, integ_s = 0.0;
 		long substeps = 0, gc_events = 0, audit_bad = 0;
 		int steps_done   = 0;
 		bool force_break = false;
-		if (o.checks.count(0)) write_snapshot(in, o.out_prefix + "_0.snap", 0, time, updates);
+		if (o.checks.count(0)) write_snapshot<Model>(in, o.out_prefix + "_0.snap", 0, time, updates);
 
 		if (o.sample_substeps > 0) {
 			// Bounded timing samples: each integrate() call is timed from its start to the hook of its
@@ -201,7 +202,7 @@ namespace {
                 substeps++;
                 if (level == 0) {
                     size_t n = 0;
-                    for (int l = 0; l < Runner<Model>::MAX_LEVEL; l++) n += itg.acti_clusters[l].size();
+                    for (int l = 0; l < R::MAX_LEVEL; l++) n += itg.acti_clusters[l].size();
                     will_gc = (double) n / (double) (itg.domain.tree.size() - 1) < 0.2;
                 }
 			};
@@ -213,7 +214,7 @@ namespace {
 			steps_done = step;
 			if (will_gc) gc_events++;
 			if (o.neighbor_audit) audit_bad += audit_neighbors(in);
-			if (o.checks.count(step)) write_snapshot(in, o.out_prefix + "_" + std::to_string(step) + ".snap", step, time, updates);
+			if (o.checks.count(step)) write_snapshot<Model>(in, o.out_prefix + "_" + std::to_string(step) + ".snap", step, time, updates);
 			if (force_break) break;
 		}
 
@@ -258,8 +259,21 @@ int main(int argc, char **argv) {
 	}
 	spdlog::set_level(spdlog::level::warn);
 	oracle::CaseData c = oracle::read_case(o.case_path);
+	if (c.limiter != 0 && !(c.model == 0 && c.dims == 2)) {
+		std::fprintf(stderr, "limiters other than minmod are built for euler<2> only\n");
+		return 2;
+	}
 	switch (c.model * 10 + c.dims) {
-		case 2: return run<model::euler<2>>(c, o);
+		case 2:
+			switch (c.limiter) {
+				case 0: return run<model::euler<2>, integrator::slope::minmod>(c, o);
+				case 1: return run<model::euler<2>, integrator::slope::unlimited>(c, o);
+				case 2: return run<model::euler<2>, integrator::slope::van_leer>(c, o);
+				case 3: return run<model::euler<2>, integrator::slope::superbee>(c, o);
+				case 4: return run<model::euler<2>, integrator::slope::von_alba_2>(c, o);
+				case 5: return run<model::euler<2>, integrator::slope::koren>(c, o);
+				default: return run<model::euler<2>, integrator::slope::first_order>(c, o);
+			}
 		case 3: return run<model::euler<3>>(c, o);
 		case 12: return run<model::navier_stokes<2>>(c, o);
 		case 13: return run<model::navier_stokes<3>>(c, o);

@@ -18,7 +18,17 @@ sys.path.insert(0, ROOT)
 
 from dacti_b200 import cases  # noqa: E402
 from dacti_b200.casefile import write_case  # noqa: E402
-from dacti_b200.models import ModelId  # noqa: E402
+from dacti_b200.models import BcType, ModelId  # noqa: E402
+from dacti_b200.scene import BoundarySpec  # noqa: E402
+
+# Fixed-state conditions sit on the negative faces: the reference's boundary flux passes the
+# boundary state as the left Riemann state on every face (integrator/boundary.hpp:143-149), which
+# is unstable on positive faces for these inflow states.
+OUT = BoundarySpec(BcType.OUTFLOW, (0.0, 0.0, 0.0, 1.0))
+OPEN_A = [(BoundarySpec(BcType.INFLOW, (1.0, 0.4, -0.1, 1.0), None, 0.3), OUT),
+          (BoundarySpec(BcType.INFLOW_R, (1.2, 0.0, 0.3, 1.1), None, 0.0), OUT)]
+OPEN_B = [(BoundarySpec(BcType.DIRICHLET, (1.0, 0.2, -0.1, 1.0)), BoundarySpec(BcType.ZERO_GRADIENT)),
+          (BoundarySpec(BcType.INFLOW, (1.1, 0.0, 0.2, 1.2), None, 0.0), OUT)]
 
 RUNNER = os.path.join(ROOT, "oracle", "_ref", "dacti_ref_runner")
 
@@ -30,6 +40,14 @@ GOLDEN = {
     "multi2": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2), 4, [0, 4]),
     "multi3": (lambda: cases.shock_drop(dims=3, base_level=3, levels=1), 2, [0, 2]),
     "euler2_periodic": (lambda: cases.periodic_blob(base_level=3, levels=2), 6, [6]),
+    # boundary conditions: freeslip / noslip walls, inflow with fade-in, inflow_r, Dirichlet, outflow
+    "euler2_walls": (lambda: cases.box_blast(base_level=3, levels=2), 10, [5, 10]),
+    "euler2_open_a": (lambda: cases.box_blast(base_level=3, levels=2, domain_bc=OPEN_A), 10, [5, 10]),
+    "euler2_open_b": (lambda: cases.box_blast(base_level=3, levels=2, domain_bc=OPEN_B), 10, [10]),
+    "ns2_walls": (lambda: cases.box_blast(base_level=3, levels=2, model=ModelId.NAVIER_STOKES, mu=2e-3), 10, [10]),
+    # slope limiters other than minmod (integrator/slope_limiters.hpp:18-57)
+    **{f"euler2_lim{k}": (lambda k=k: cases.smooth_periodic(base_level=4, levels=2, limiter=k), 6, [6])
+       for k in range(1, 7)},
     # viscosity and heat conduction of the five-equation model
     "multi2_visc": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2, mu=(1e-3, 1.8e-5),
                                              conductivity=(0.6, 0.026)), 4, [4]),
