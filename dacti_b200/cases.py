@@ -223,15 +223,17 @@ def smooth_periodic(base_level: int = 3, levels: int = 2, thresholds=(0.02, 0.05
 
 
 def osc_drop(base_level: int = 4, levels: int = 2, thresholds=(1e-3, 1e-2), max_cfl: float = 0.4,
-             conductivity: tuple = (0.0, 0.0), velocity: float = 0.0, sigma: float = 0.1, oh: float = 0.01) -> Case:
+             conductivity: tuple = (0.0, 0.0), velocity: float = 0.0, sigma: float = 0.1, oh: float = 0.01,
+             rho_gas: float = 1e-3) -> Case:
     """2D oscillating drop in the non-dimensional units of the reference's cases/oscDrop.toml:
     2 x 2 box, elliptic drop (a = 0.2, b = 0.12) of fluid 1 (rho 1, gamma 6.12, P0 500) in fluid 2
     (rho 1e-3, gamma 1.4), p = 1 at rest, sigma = 0.1, Oh = 0.01 with L = 0.15825 and viscosity ratio
     10 (mu1 = sqrt(rho1 sigma L) Oh, model/multi.hpp:531-535), tanh-smeared interface,
     zero-gradient boundaries. Exercises surface tension (curvature, smoothing, source) and the
-    viscous terms of the five-equation model. ``velocity`` translates everything along x."""
+    viscous terms of the five-equation model. ``velocity`` translates everything along x;
+    ``rho_gas`` replaces the gas density."""
     shape = ModelShape(ModelId.MULTI, 2)
-    rho1, rho2, L = 1.0, 1e-3, 0.15825
+    rho1, rho2, L = 1.0, rho_gas, 0.15825
     mu1 = math.sqrt(rho1 * sigma * L) * oh
 
     def x2p(c: np.ndarray) -> np.ndarray:
