@@ -18,6 +18,9 @@
 #include "model/multi.hpp"
 #include "model/navier_stokes.hpp"
 #include "scene/scene.hpp"
+#ifdef DACTI_ADAPTER_CHECK
+#include "dacti_gpu/integrator.hpp"
+#endif
 
 #include <chrono>
 #include <cstdio>
@@ -37,6 +40,7 @@ namespace {
 		bool quiet = false;
 		int sample_substeps = 0;  // >0: each integrate() call is timed up to this many substeps
 		int samples = 0;
+		bool adapter_check = false;  // side-by-side run against the GPU adapter (adapter build only)
 	};
 
 	template<typename Model>
@@ -60,6 +64,36 @@ namespace {
 			Model::mu_     = c.params[P_NS_MU];
 			Model::lambda_ = c.params[P_NS_LAMBDA];
 		}
+	}
+
+	template<typename Model>
+	std::shared_ptr<config::Config<Model>> make_config(const oracle::CaseData &c) {
+		using namespace oracle;
+		constexpr int D = Model::NumDims;
+		constexpr int E = Model::NumEqns;
+		auto cfg         = std::make_shared<config::Config<Model>>();
+		cfg->case_data   = &c;
+		cfg->side_length = c.params[P_SIDE];
+		for (int d = 0; d < D; d++) {
+			cfg->active_size[d] = c.params[P_ACTIVE0 + d];
+			cfg->IsPeriodic[d]  = c.params[P_PERIODIC0 + d] != 0.0;
+		}
+		cfg->max_cfl              = c.params[P_MAX_CFL];
+		cfg->max_dt               = c.params[P_MAX_DT];
+		cfg->error_threshold      = vec2_t{c.params[P_MIN_ERR], c.params[P_MAX_ERR]};
+		cfg->max_refinement_level = (int) c.params[P_MAX_LEVEL];
+		cfg->min_refinement_level = (int) c.params[P_MIN_LEVEL];
+		typename Model::prim_t w;
+		for (int q = 0; q < E; q++) w[q] = c.weights[q];
+		cfg->error_weights = w;
+		for (auto &z: c.zones) {
+			typename config::Config<Model>::RefineZone rz;
+			rz.x0               = vec3_t{z.x0[0], z.x0[1], z.x0[2]};
+			rz.x1               = vec3_t{z.x1[0], z.x1[1], z.x1[2]};
+			rz.refinement_level = (size_t) z.level;
+			cfg->refine_zones.push_back(rz);
+		}
+		return cfg;
 	}
 
 	// Counts active leaves whose stored neighbour index differs from a fresh Domain::find, i.e.
@@ -122,6 +156,76 @@ namespace {
 		});
 	}
 
+#ifdef DACTI_ADAPTER_CHECK
+	// Integer cell coordinates at the cell's own level: the key under which both sides' cells are
+	// matched (centres are (i + 1/2) size - side/2 on both sides).
+	template<typename Node>
+	std::vector<double> cell_row(const Node &node, double side, int D, int E) {
+		std::vector<double> r;
+		r.push_back(node.tree_level);
+		for (int d = 0; d < D; ++d) r.push_back(std::nearbyint((node.cell.center[d] + 0.5 * side) / node.cell.size - 0.5));
+		r.push_back(node.acti_level);
+		for (int q = 0; q < E; ++q) r.push_back(node.cell.u[q]);
+		return r;
+	}
+
+	// Runs the reference Integrator and dacti::gpu::Integrator (the C++ adapter over the GPU library)
+	// side by side from the same Scene and Config and compares, after construction and after every
+	// global step: the substep hook sequence (level, level time, substep count, cluster size), the
+	// force_break flag, global_dt, the active cell set with its ACTI levels, and the conserved state.
+	template<typename Model, typename Limiter>
+	int adapter_check(const oracle::CaseData &c, const Options &o, std::shared_ptr<config::Config<Model>> cfg) {
+		constexpr int D = Model::NumDims;
+		constexpr int E = Model::NumEqns;
+		using Est       = integrator::error::weighted_laplacian<E>;
+		scene::Scene<Model> scene_ref(cfg), scene_gpu(cfg);
+		Runner<Model, Limiter> ref{Limiter{}, Est{cfg->error_weights}, scene_ref, cfg};
+		dacti::gpu::Integrator<Model, Limiter, Est> gpu{Limiter{}, Est{cfg->error_weights}, scene_gpu, cfg};
+		const double side = cfg->side_length;
+		int failures      = 0;
+		auto rows         = [&](auto &itg) {
+            std::vector<std::vector<double>> v;
+            itg.for_each_active_cell([&](int, auto &node) { v.push_back(cell_row(node, side, D, E)); });
+            std::sort(v.begin(), v.end(), [&](const auto &a, const auto &b) {
+                return std::lexicographical_compare(a.begin(), a.begin() + D + 1, b.begin(), b.begin() + D + 1);
+            });
+            return v;
+		};
+		auto compare = [&](int step, bool hooks_equal, bool fb_equal) {
+			auto a = rows(ref), b = rows(gpu);
+			bool cells_equal = a.size() == b.size();
+			double num = 0.0, den = 0.0;
+			for (size_t i = 0; cells_equal && i < a.size(); ++i) {
+				for (int k = 0; k < D + 2; ++k) cells_equal = cells_equal && a[i][k] == b[i][k];
+				for (int q = 0; q < E; ++q) num += std::abs(a[i][D + 2 + q] - b[i][D + 2 + q]), den += std::abs(a[i][D + 2 + q]);
+			}
+			double rel = den > 0 ? num / den : num;
+			bool ok    = hooks_equal && fb_equal && cells_equal && ref.global_dt == gpu.global_dt &&
+			          ref.n_active_cells() == gpu.n_active_cells() && rel <= 1e-10;
+			if (!ok) failures++;
+			std::printf("{\"step\": %d, \"hooks_equal\": %s, \"force_break_equal\": %s, \"cells_equal\": %s, "
+			            "\"n_ref\": %zu, \"n_gpu\": %zu, \"global_dt_equal\": %s, \"rel_l1_u\": %.3e}\n",
+			            step, hooks_equal ? "true" : "false", fb_equal ? "true" : "false", cells_equal ? "true" : "false",
+			            ref.n_active_cells(), gpu.n_active_cells(), ref.global_dt == gpu.global_dt ? "true" : "false", rel);
+		};
+		compare(0, true, true);
+		for (int step = 1; step <= o.n_steps; ++step) {
+			std::vector<std::array<double, 4>> hr, hg;
+			auto rec = [](auto &out) {
+				return [&out](auto &itg, int level, scalar_t at, int ns, scalar_t) {
+					out.push_back({(double) level, at, (double) ns, (double) itg.acti_clusters[level].size()});
+				};
+			};
+			bool fr = false, fg = false;
+			ref.integrate(rec(hr), true, fr);
+			gpu.integrate(rec(hg), true, fg);
+			compare(step, hr == hg, fr == fg);
+			if (fr || fg) break;
+		}
+		return failures ? 1 : 0;
+	}
+#endif
+
 	template<typename Model, typename Limiter = integrator::slope::minmod>
 	int run(const oracle::CaseData &c, const Options &o) {
 		using R = Runner<Model, Limiter>;
@@ -130,33 +234,15 @@ namespace {
 		constexpr int E = Model::NumEqns;
 		set_model_constants<Model>(c);
 
-		auto cfg         = std::make_shared<config::Config<Model>>();
-		cfg->case_data   = &c;
-		cfg->side_length = c.params[P_SIDE];
-		for (int d = 0; d < D; d++) {
-			cfg->active_size[d] = c.params[P_ACTIVE0 + d];
-			cfg->IsPeriodic[d]  = c.params[P_PERIODIC0 + d] != 0.0;
-		}
-		cfg->max_cfl              = c.params[P_MAX_CFL];
-		cfg->max_dt               = c.params[P_MAX_DT];
-		cfg->error_threshold      = vec2_t{c.params[P_MIN_ERR], c.params[P_MAX_ERR]};
-		cfg->max_refinement_level = (int) c.params[P_MAX_LEVEL];
-		cfg->min_refinement_level = (int) c.params[P_MIN_LEVEL];
-		typename Model::prim_t w;
-		for (int q = 0; q < E; q++) w[q] = c.weights[q];
-		cfg->error_weights = w;
-		for (auto &z: c.zones) {
-			typename config::Config<Model>::RefineZone rz;
-			rz.x0               = vec3_t{z.x0[0], z.x0[1], z.x0[2]};
-			rz.x1               = vec3_t{z.x1[0], z.x1[1], z.x1[2]};
-			rz.refinement_level = (size_t) z.level;
-			cfg->refine_zones.push_back(rz);
-		}
+		auto cfg = make_config<Model>(c);
+#ifdef DACTI_ADAPTER_CHECK
+		if (o.adapter_check) return adapter_check<Model, Limiter>(c, o, cfg);
+#endif
 
 		scene::Scene<Model> scene(cfg);
 		using clk = std::chrono::steady_clock;
 		auto t0   = clk::now();
-		R in{Limiter{}, integrator::error::weighted_laplacian<E>{w}, scene, cfg};
+		R in{Limiter{}, integrator::error::weighted_laplacian<E>{cfg->error_weights}, scene, cfg};
 		double init_s = std::chrono::duration<double>(clk::now() - t0).count();
 
 		double time = 0.0, updates = 0.0, integ_s = 0.0;
@@ -255,6 +341,8 @@ int main(int argc, char **argv) {
 			o.sample_substeps = std::atoi(argv[++i]);
 		} else if (a == "--samples" && i + 1 < argc) {
 			o.samples = std::atoi(argv[++i]);
+		} else if (a == "--adapter-check") {
+			o.adapter_check = true;
 		}
 	}
 	spdlog::set_level(spdlog::level::warn);

@@ -1,0 +1,38 @@
+"""The C++ adapter include/dacti_gpu/integrator.hpp is a drop-in for the reference's Integrator.
+
+oracle/_ref/dacti_adapter_check holds, in one process, the reference's
+dacti::integrator::Integrator (integrator/integrator.hpp:14-225, compiled from its own headers) and
+dacti::gpu::Integrator over the GPU library, both built from the same Scene and Config, and drives
+them with the same calls a DACTI driver makes (integrate with a substep hook, n_active_cells,
+for_each_active_cell, global_dt). After construction and after every global step it compares the
+hook sequence, force_break, global_dt, the active cell set with ACTI levels, and the conserved state
+(relative L1 <= 1e-10), printing one JSON line per step.
+"""
+import json
+import os
+import subprocess
+
+import pytest
+
+from conftest import GOLDEN, ROOT
+
+CHECK = os.path.join(ROOT, "oracle", "_ref", "dacti_adapter_check")
+
+CASES = [("euler2", 4), ("ns2", 4), ("multi2", 3), ("multi3", 2), ("euler2_periodic", 4), ("euler2_walls", 6),
+         ("euler2_open_a", 6), ("euler2_lim2", 4), ("euler2_lim5", 4), ("multi2_tension_run", 2)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,steps", CASES)
+def test_adapter_matches_reference_integrator(name, steps, tmp_path):
+    if not os.path.exists(CHECK):
+        pytest.fail("oracle/_ref/dacti_adapter_check is not built (make -C oracle after building the library)")
+    r = subprocess.run([CHECK, os.path.join(GOLDEN, f"{name}.case"), str(tmp_path / name), str(steps),
+                        "--adapter-check"], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
+    lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert len(lines) == steps + 1
+    for rec in lines:
+        assert rec["hooks_equal"] and rec["force_break_equal"] and rec["cells_equal"], rec
+        assert rec["global_dt_equal"] and rec["n_ref"] == rec["n_gpu"] and rec["rel_l1_u"] <= 1e-10, rec
