@@ -97,8 +97,7 @@ struct Pool {
 	double *t;
 	double *u;        // [E][cap]
 	double *p;        // [E][cap]
-	double *rhs;      // [E][cap]
-	double *slope;    // [D][E][cap]
+	double *rec;      // [cap][W] reconstruction record: p copy, Hancock rhs, slope rows, multiphase k part
 	double *k;        // [P][cap]
 	double *tslope;   // [G][cap]
 	double *grad;     // [D][G][cap]
@@ -107,6 +106,9 @@ struct Pool {
 	int32_t *stamp;   // per-node dedup stamp for list building
 	uint8_t *op;      // refinement op code
 	double *tmp;      // per-node scratch scalar (Jacobi smoothing)
+	// Per-substep scratch outside the permuted fields:
+	double *ff;       // [cap][2D][F] flux of each face a cell owns, written in the running substep
+	int32_t *plan;    // [cap][2D] source of each face's flux for the running cluster's cells
 };
 
 // Device counters, copied back to the host after each substep.
@@ -120,6 +122,8 @@ struct Counters {
 	int n_new;        // new cluster members (children + coarsened parents)
 	int n_upd;        // neighbour-update list
 	int n_tmp;        // rebuilt cluster list
+	int n_task;       // owned interior faces of the running substep
+	int n_btask;      // owned boundary faces of the running substep
 	uint32_t status;
 	unsigned long long n_split_total, n_unsplit_total;
 	double dmax;      // reduction result
@@ -135,6 +139,8 @@ struct Lists {
 	int32_t *unsplit;  // parents to coarsen
 	int32_t *fresh;    // new children and coarsened parents
 	int32_t *upd;      // neighbour-update list
+	int32_t *task;     // owned interior faces (cell * 2D + face) of the running substep
+	int32_t *btask;    // owned boundary faces
 };
 
 }  // namespace dg

@@ -15,6 +15,29 @@ __host__ __device__ __forceinline__ S smin(S a, S b) { return (b < a) ? b : a; }
 template<class S>
 __host__ __device__ __forceinline__ S smax(S a, S b) { return (a < b) ? b : a; }
 
+// a[LO + k] and a[LO + k] (+)= v for a run-time k in [0, N): unrolled selects keep small state arrays in
+// registers where a dynamic index would move them to local memory.
+template<int LO, int N, class S>
+__device__ __forceinline__ S pick(const S *a, int k) {
+	S r = a[LO];
+#pragma unroll
+	for (int j = 1; j < N; ++j)
+		if (k == j) r = a[LO + j];
+	return r;
+}
+template<int LO, int N, class S>
+__device__ __forceinline__ void put(S *a, int k, S v) {
+#pragma unroll
+	for (int j = 0; j < N; ++j)
+		if (k == j) a[LO + j] = v;
+}
+template<int LO, int N, class S>
+__device__ __forceinline__ void put_add(S *a, int k, S v) {
+#pragma unroll
+	for (int j = 0; j < N; ++j)
+		if (k == j) a[LO + j] += v;
+}
+
 // --------------------------------------------------------------------------------------------
 // Model traits (compile-time sizes of model/euler.hpp:26-32, navier_stokes.hpp:351, multi.hpp:27-42)
 // --------------------------------------------------------------------------------------------
@@ -208,8 +231,8 @@ __device__ __forceinline__ double max_delta_time(const ModelConsts &m, const dou
 // --------------------------------------------------------------------------------------------
 template<class M, class S = double>
 __device__ __forceinline__ void phys_flux(const ModelConsts &m, const S *p, S un, int dim, bool projected, S *F) {
-	const int in = M::IU + dim;
-	S vn         = projected ? un : p[in];
+	constexpr int D = M::D;
+	S vn         = projected ? un : pick<M::IU, D>(p, dim);
 	S ke         = 0;
 	for (int q = 0; q < M::F; ++q) F[q] = 0;
 	if constexpr (M::MULTI) {
@@ -219,19 +242,19 @@ __device__ __forceinline__ void phys_flux(const ModelConsts &m, const S *p, S un
 		}
 		F[0] = vn * p[0];
 		F[1] = vn * p[1];
-		F[in] += p[M::IP];
+		put_add<M::IU, D>(F, dim, p[M::IP]);
 		S a      = p[M::IA];
 		F[M::IP] = vn * (mix_gamma<S>(m, a) / (mix_gamma<S>(m, a) - 1) * (p[M::IP] + mix_p0<S>(m, a)) + ke * (p[0] + p[1]));
 		F[M::IA] = vn * p[M::IA];
 		F[M::IA + 1] = vn;
-		F[M::IA + 2 + dim] = p[M::IA];
+		put<M::IA + 2, D>(F, dim, p[M::IA]);
 	} else {
 		for (int i = 0; i < M::D; ++i) {
 			F[M::IU + i] = p[0] * vn * p[M::IU + i];
 			ke += 0.5 * p[M::IU + i] * p[M::IU + i];
 		}
 		F[0] = vn * p[0];
-		F[in] += p[M::IP];
+		put_add<M::IU, D>(F, dim, p[M::IP]);
 		F[M::IP] = vn * ((S) (EULER_GAMMA / (EULER_GAMMA - 1)) * p[M::IP] + ke * p[0]);
 	}
 }
@@ -240,8 +263,9 @@ __device__ __forceinline__ void phys_flux(const ModelConsts &m, const S *p, S un
 // primitive variables; `ka` enters only the multiphase contact speed.
 template<class M, class S = double>
 __device__ __forceinline__ void middle_state(const ModelConsts &m, const S *pn, const S *pp, S ka, int dim, S *pm) {
-	const int in = M::IU + dim;
+	constexpr int D = M::D;
 	const int ip = M::IP;
+	const S un = pick<M::IU, D>(pn, dim), up = pick<M::IU, D>(pp, dim);
 	S c_n, c_p, rn, rp;
 	if constexpr (M::MULTI) {
 		c_n = sound_speed_rp<M, S>(m, pn[0], pn[1], pn[ip], pn[M::IA]);
@@ -254,17 +278,17 @@ __device__ __forceinline__ void middle_state(const ModelConsts &m, const S *pn, 
 		rn  = pn[0];
 		rp  = pp[0];
 	}
-	S u  = (S) 0.5 * (pn[in] + pp[in]);
+	S u  = (S) 0.5 * (un + up);
 	S c  = (S) 0.5 * (c_n + c_p);
-	S Sn = smin<S>(u - c, pn[in] - c_n);
-	S Sp = smax<S>(u + c, pp[in] + c_p);
+	S Sn = smin<S>(u - c, un - c_n);
+	S Sp = smax<S>(u + c, up + c_p);
 	S Sm;
 	if constexpr (M::MULTI)
-		Sm = (pp[ip] - pn[ip] + rn * pn[in] * (Sn - pn[in]) - rp * pp[in] * (Sp - pp[in]) - (S) m.sigma * ka * (pp[M::IA] - pn[M::IA])) /
-		     (rn * (Sn - pn[in]) - rp * (Sp - pp[in]));
+		Sm = (pp[ip] - pn[ip] + rn * un * (Sn - un) - rp * up * (Sp - up) - (S) m.sigma * ka * (pp[M::IA] - pn[M::IA])) /
+		     (rn * (Sn - un) - rp * (Sp - up));
 	else
-		Sm = (pp[ip] - pn[ip] + pn[0] * pn[in] * (Sn - pn[in]) - pp[0] * pp[in] * (Sp - pp[in])) /
-		     (pn[0] * (Sn - pn[in]) - pp[0] * (Sp - pp[in]));
+		Sm = (pp[ip] - pn[ip] + pn[0] * un * (Sn - un) - pp[0] * up * (Sp - up)) /
+		     (pn[0] * (Sn - un) - pp[0] * (Sp - up));
 
 	for (int q = 0; q < M::E; ++q) pm[q] = 0;
 	if (Sn > 0) {
@@ -273,28 +297,28 @@ __device__ __forceinline__ void middle_state(const ModelConsts &m, const S *pn, 
 		for (int q = 0; q < M::E; ++q) pm[q] = pp[q];
 	} else if (Sm > 0 && Sn < 0) {
 		if constexpr (M::MULTI) {
-			pm[0]      = pn[0] * (Sn - pn[in]) / (Sn - Sm);
-			pm[1]      = pn[1] * (Sn - pn[in]) / (Sn - Sm);
-			pm[ip]     = pn[ip] + (pn[0] + pn[1]) * (Sn - pn[in]) * (Sm - pn[in]);
+			pm[0]      = pn[0] * (Sn - un) / (Sn - Sm);
+			pm[1]      = pn[1] * (Sn - un) / (Sn - Sm);
+			pm[ip]     = pn[ip] + (pn[0] + pn[1]) * (Sn - un) * (Sm - un);
 			pm[M::IA]  = pn[M::IA];
 		} else {
-			pm[0]  = pn[0] * (Sn - pn[in]) / (Sn - Sm);
-			pm[ip] = pn[ip] + pn[0] * (Sn - pn[in]) * (Sm - pn[in]);
+			pm[0]  = pn[0] * (Sn - un) / (Sn - Sm);
+			pm[ip] = pn[ip] + pn[0] * (Sn - un) * (Sm - un);
 		}
 		for (int i = 0; i < M::D; ++i) pm[M::IU + i] = pn[M::IU + i];
-		pm[in] = Sm;
+		put<M::IU, D>(pm, dim, Sm);
 	} else {
 		if constexpr (M::MULTI) {
-			pm[0]     = pp[0] * (Sp - pp[in]) / (Sp - Sm);
-			pm[1]     = pp[1] * (Sp - pp[in]) / (Sp - Sm);
-			pm[ip]    = pp[ip] + (pp[0] + pp[1]) * (Sp - pp[in]) * (Sm - pp[in]);
+			pm[0]     = pp[0] * (Sp - up) / (Sp - Sm);
+			pm[1]     = pp[1] * (Sp - up) / (Sp - Sm);
+			pm[ip]    = pp[ip] + (pp[0] + pp[1]) * (Sp - up) * (Sm - up);
 			pm[M::IA] = pp[M::IA];
 		} else {
-			pm[0]  = pp[0] * (Sp - pp[in]) / (Sp - Sm);
-			pm[ip] = pp[ip] + pp[0] * (Sp - pp[in]) * (Sm - pp[in]);
+			pm[0]  = pp[0] * (Sp - up) / (Sp - Sm);
+			pm[ip] = pp[ip] + pp[0] * (Sp - up) * (Sm - up);
 		}
 		for (int i = 0; i < M::D; ++i) pm[M::IU + i] = pp[M::IU + i];
-		pm[in] = Sm;
+		put<M::IU, D>(pm, dim, Sm);
 	}
 }
 
@@ -350,15 +374,21 @@ __device__ __forceinline__ void compute_rhs(const ModelConsts &m, const double *
 }
 
 // Fv<D> (model/common.hpp:8-24): viscous stress row (and work term) for face normal `dim`, times mu.
-template<int D, class S = double>
-__device__ __forceinline__ void visc_flux(const S *du /*[D][G]*/, int G, const S *vel, S mu, int dim, S *fv /*[D+1]*/) {
+// du is [D][G].
+template<int D, int G, class S = double>
+__device__ __forceinline__ void visc_flux(const S *du, const S *vel, S mu, int dim, S *fv /*[D+1]*/) {
 	for (int i = 0; i <= D; ++i) fv[i] = 0;
 	S trace = 0;
+#pragma unroll
 	for (int i = 0; i < D; ++i) {
-		fv[i] = du[dim * G + i] + du[i * G + dim];
+		S row = du[i], col = du[i * G];  // du[dim * G + i] and du[i * G + dim] for dim == 0
+#pragma unroll
+		for (int j = 1; j < D; ++j)
+			if (dim == j) row = du[j * G + i], col = du[i * G + j];
+		fv[i] = row + col;
 		trace += du[i * G + i];
 	}
-	fv[dim] -= ((S) (2.0 / 3.0) * trace);
+	put_add<0, D>(fv, dim, -((S) (2.0 / 3.0) * trace));
 	for (int i = 0; i < D; ++i) fv[D] += fv[i] * vel[i];
 	for (int i = 0; i <= D; ++i) fv[i] = fv[i] * mu;
 }

@@ -69,6 +69,8 @@ class Solver : public SolverBase {
 	bool resort_     = true;
 	void *list_mem_  = nullptr;
 	void *bc_mem_    = nullptr;
+	double *ff_mem_    = nullptr;  // face fluxes (Pool::ff)
+	int32_t *plan_mem_ = nullptr;  // face-flux sources (Pool::plan)
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
 	double *d_read_    = nullptr;
 	int32_t *d_readlv_ = nullptr;
@@ -169,6 +171,8 @@ public:
 		cudaFree(sort_mem_);
 		cudaFree(list_mem_);
 		cudaFree(bc_mem_);
+		cudaFree(ff_mem_);
+		cudaFree(plan_mem_);
 		cudaFree(d_cnt_);
 		cudaFreeHost(h_cnt_);
 		cudaFree(d_leaves_);
@@ -285,7 +289,7 @@ public:
 		    {(void **) &P.acti, 1, 1}, {(void **) &P.clu, 1, 1}, {(void **) &P.flags, 4, 1},
 		    {(void **) &P.coord, 4, D}, {(void **) &P.nbr, 4, NF}, {(void **) &P.bc, 2, NF},
 		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
-		    {(void **) &P.p, 8, E}, {(void **) &P.rhs, 8, E}, {(void **) &P.slope, 8, D * E},
+		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1},
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.op, 1, 1},
@@ -311,7 +315,26 @@ public:
 		return mem;
 	}
 
-	void alloc_pool(int cap) { pool_mem_ = carve_pool(P_, cap); }
+	void alloc_pool(int cap) {
+		pool_mem_ = carve_pool(P_, cap);
+		alloc_derived(cap);
+	}
+
+	// Per-substep scratch sized with the pool: face fluxes and face-flux sources.
+	void alloc_derived(int cap) {
+		cudaFree(ff_mem_);
+		cudaFree(plan_mem_);
+		ff_mem_   = nullptr;
+		plan_mem_ = nullptr;
+		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) cap));
+		DG_CUDA(cudaMalloc(&plan_mem_, sizeof(int32_t) * NF * (size_t) cap));
+		attach_derived();
+	}
+
+	void attach_derived() {
+		P_.ff   = ff_mem_;
+		P_.plan = plan_mem_;
+	}
 
 	void grow_pool(int new_cap) {
 		Pool NP{};
@@ -329,6 +352,7 @@ public:
 		P_        = NP;
 		cudaFree(shadow_mem_);
 		shadow_mem_ = nullptr;
+		alloc_derived(new_cap);
 		// lists grow with the pool
 		Lists old = Ls_;
 		void *old_mem = list_mem_;
@@ -346,7 +370,8 @@ public:
 	void alloc_lists(int cap) {
 		const int nlists = 2 * MAX_ACTI + 6;
 		size_t one       = align_up(sizeof(int32_t) * (size_t) cap);
-		DG_CUDA(cudaMalloc(&list_mem_, one * nlists));
+		size_t faces     = align_up(sizeof(int32_t) * (size_t) cap * NF);
+		DG_CUDA(cudaMalloc(&list_mem_, one * nlists + 2 * faces));
 		char *b = (char *) list_mem_;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			Ls_.clu[l] = (int32_t *) b;
@@ -365,6 +390,10 @@ public:
 		Ls_.fresh   = (int32_t *) b;
 		b += one;
 		Ls_.upd     = (int32_t *) b;
+		b += one;
+		Ls_.task    = (int32_t *) b;
+		b += faces;
+		Ls_.btask   = (int32_t *) b;
 		list_cap_   = cap;
 	}
 
@@ -430,7 +459,10 @@ public:
 		k_init_cells<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, d_cnt_);
 		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
 		launch_slope(d_leaves_, n);
-		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n);
+		if constexpr (M::MULTI) {
+			multiphase_aux(d_leaves_, n);
+			k_rec_k<M><<<g, BLOCK, 0, st_>>>(P_, d_leaves_, n);
+		}
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
 		global_dt_ = std::fmax(-INFINITY, h_cnt_->dmax);
@@ -471,23 +503,31 @@ private:
 		}
 	}
 
-	void launch_flux(const int32_t *list, const int *n_ptr, int n, int L, double dtL, int stamp, int cluster_mode, int grid) {
+	void launch_flux_faces(int grid, double dtL) {
 		if (mixed_) {
-			if (visc_)
-				k_flux<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
-			else
-				k_flux<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+			if (visc_) k_flux_faces<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
+			else k_flux_faces<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
 		} else {
-			if (visc_)
-				k_flux<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
-			else
-				k_flux<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, list, n_ptr, n, L, dtL, stamp, cluster_mode, Ls_.recv, d_cnt_);
+			if (visc_) k_flux_faces<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
+			else k_flux_faces<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
+		}
+	}
+
+	void launch_flux_bfaces(int grid, double dtL) {
+		if (mixed_) {
+			if (visc_) k_flux_bfaces<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
+			else k_flux_bfaces<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
+		} else {
+			if (visc_) k_flux_bfaces<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
+			else k_flux_bfaces<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
 		}
 	}
 
 	void launch_slope(const int32_t *list, int n) {
-		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
-		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		const long long b = (n + SLOPE_BLOCK - 1) / SLOPE_BLOCK;
+		const int grid    = (int) std::max(1LL, std::min(b, 148LL * 32));
+		if (visc_) k_slope<M, true><<<grid, SLOPE_BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		else k_slope<M, false><<<grid, SLOPE_BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 	}
 
 	void sync_counters() {
@@ -513,22 +553,31 @@ private:
 		if (need > P_.cap) grow_pool((int) std::min<long long>(std::max<long long>(need, (long long) P_.cap * 3 / 2), 2000000000LL));
 		const int stamp_recv = ++stamp_;
 		const int stamp_upd  = ++stamp_;
-		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_recv, 0, sizeof(int) * 7, st_));
+		// n_recv .. n_btask and status
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_recv, 0, (char *) (&d_cnt_->status + 1) - (char *) &d_cnt_->n_recv, st_));
 		const int g        = grid_for(n);
 		int32_t *list      = Ls_.clu[L];
 		const int counterL = acti_counter_[L];
 
-		constexpr int LPC = NF <= 4 ? 4 : 8;  // flux lanes per cell
-		run_k(DG_K_FLUX, n, [&] { launch_flux(list, nullptr, n, L, dtL, stamp_recv, 1, grid_for((long long) n * LPC)); });
+		constexpr int LPC = NF <= 4 ? 4 : 8;  // receive lanes per cell
+		run_k(DG_K_FLUX, n, [&] {
+			k_flux_tasks<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, list, n, L, stamp_recv, Ls_.task, Ls_.btask,
+			                                                                  Ls_.recv, d_cnt_);
+		});
+		run_k(DG_K_FLUX, 0, [&] { launch_flux_faces(grid_for((long long) n * NF / 2 + 1), dtL); });
+		run_k(DG_K_FLUX, 0, [&] { launch_flux_bfaces(grid_for(n / 4 + 1), dtL); });
 		run_k(DG_K_RECV, 0, [&] {
-			launch_flux(Ls_.recv, &d_cnt_->n_recv, 0, L, dtL, stamp_recv, 0, grid_for((long long) n * LPC));
+			k_flux_receive<M><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
-			if (visc_) k_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
-			else k_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, d_cnt_);
+			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, dtL, d_cnt_);
+			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, dtL, d_cnt_);
 		});
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
-		if constexpr (M::MULTI) multiphase_aux(list, n);
+		if constexpr (M::MULTI) {
+			multiphase_aux(list, n);
+			run_k(DG_K_AUX, n, [&] { k_rec_k<M><<<g, BLOCK, 0, st_>>>(P_, list, n); });
+		}
 		run_k(DG_K_ESTIMATE, n, [&] {
 			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
 		});
@@ -667,13 +716,18 @@ public:
 					case 1: k_permute<int8_t><<<g, BLOCK, 0, st_>>>((const int8_t *) *fo[k].ptr, (int8_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
 					case 2: k_permute<int16_t><<<g, BLOCK, 0, st_>>>((const int16_t *) *fo[k].ptr, (int16_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
 					case 4: k_permute<int32_t><<<g, BLOCK, 0, st_>>>((const int32_t *) *fo[k].ptr, (int32_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
-					default: k_permute<double><<<g, BLOCK, 0, st_>>>((const double *) *fo[k].ptr, (double *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+					case 8: k_permute<double><<<g, BLOCK, 0, st_>>>((const double *) *fo[k].ptr, (double *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+					default:  // one record of elem bytes per node
+						k_permute_words<<<grid_for((long long) n * (fo[k].elem / 8)), BLOCK, 0, st_>>>(
+						    (const double *) *fo[k].ptr, (double *) *fs[k].ptr, (int) (fo[k].elem / 8), n, v_out);
+						break;
 				}
 			});
 		}
 		run_k(DG_K_OTHER, 0, [&] { k_remap_links<D><<<grid_for(top), BLOCK, 0, st_>>>(S_, top, newidx); });
 		std::swap(P_, S_);
 		std::swap(pool_mem_, shadow_mem_);
+		attach_derived();
 		int first = 1;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			const int cnt = h_cnt_->clu[l];
@@ -717,6 +771,7 @@ private:
 		cudaFree(pool_mem_);
 		pool_mem_ = mem;
 		P_        = NP;
+		attach_derived();
 		// full ACTI reassignment
 		Counters z{};
 		z.top    = new_top;

@@ -1,11 +1,11 @@
-// Stage kernels of one ACTI-level substep (impl/integrate.hpp:26-67), one thread per cell.
+// Stage kernels of one ACTI-level substep (impl/integrate.hpp:26-67).
 //
-// Flux accumulation is gather based and free of floating-point atomics: every cell of the running
-// cluster sums, in a fixed face order, the fluxes it owns plus the fluxes its same-cluster
-// neighbours own across shared faces (re-evaluating them with identical inputs gives identical
-// values); cells of slower time levels that receive fluxes (the coarse side of the LTS coupling,
-// impl/flux.hpp:82-91) are collected into a receiver list and gather the same way in a second pass.
-// The result is independent of list order and of scheduling, so runs are bitwise reproducible.
+// Flux accumulation is free of floating-point atomics. Every face that carries a flux in a substep
+// has one owner (impl/flux.hpp:58-59), which evaluates it once into its face-flux slot; each cell of
+// the running cluster then sums the slots of its faces in a fixed order, and the cells of slower
+// time levels that receive fluxes (the coarse side of the LTS coupling, impl/flux.hpp:82-91) are
+// collected into a receiver list and gather the same way. The result is independent of list order
+// and of scheduling, so runs are bitwise reproducible.
 #pragma once
 
 #include "tree.cuh"
@@ -24,13 +24,94 @@ __device__ __forceinline__ void append(int32_t *list, int *count, int value, int
 }
 
 // --------------------------------------------------------------------------------------------
+// Reconstruction records. Everything a face flux needs from one side, apart from centre and time,
+// sits in one contiguous FP64 record per node: the primitive state (a copy of the pool's p), the
+// Hancock rhs, the limited slope rows (each padded to an even length so that rows start on 16-byte
+// boundaries) and, for the multiphase model, the curvature and interface normal. A neighbour's
+// face state is then a handful of 16-byte vector loads from a few cache lines instead of 3E + 2
+// scattered structure-of-arrays loads. The record is the only storage of slope and rhs.
+// --------------------------------------------------------------------------------------------
+template<class M>
+struct Rec {
+	static constexpr int E = M::E, D = M::D;
+	static constexpr int ES  = (E + 1) & ~1;  // slope row stride
+	static constexpr int P0  = 0, R0 = E;     // p and rhs, adjacent (2E doubles)
+	static constexpr int S0  = 2 * E;         // slope row d at S0 + d * ES
+	static constexpr int K0  = S0 + D * ES;   // multiphase: curvature, then the normal's D components
+	static constexpr int RAW = K0 + (M::MULTI ? 1 + D : 0);
+	static constexpr int W   = (RAW + 1) & ~1;
+};
+
+__device__ __forceinline__ double *rec_of(const Pool &P, int i, int W) { return P.rec + (size_t) i * W; }
+
+// Loads the face-dim part of node i's record, rounded to S: p, rhs, slope row `dim`, and (multiphase)
+// curvature and normal component `dim`.
+template<class M, class S>
+__device__ __forceinline__ void load_face_rec(const Pool &P, int i, int dim, S *p, S *rhs, S *sl, S &kap, S &nrm) {
+	using R = Rec<M>;
+	constexpr int E = M::E;
+	const double2 *r = reinterpret_cast<const double2 *>(rec_of(P, i, R::W));
+	double a[2 * E];
+#pragma unroll
+	for (int k = 0; k < E; ++k) {
+		const double2 v = __ldg(r + k);
+		a[2 * k] = v.x, a[2 * k + 1] = v.y;
+	}
+#pragma unroll
+	for (int q = 0; q < E; ++q) p[q] = (S) a[R::P0 + q], rhs[q] = (S) a[R::R0 + q];
+	const double2 *sr = r + (R::S0 + dim * R::ES) / 2;
+#pragma unroll
+	for (int k = 0; k < R::ES / 2; ++k) {
+		const double2 v = __ldg(sr + k);
+		if (2 * k < E) sl[2 * k] = (S) v.x;
+		if (2 * k + 1 < E) sl[2 * k + 1] = (S) v.y;
+	}
+	if constexpr (M::MULTI) {
+		const double *kr = rec_of(P, i, R::W) + R::K0;
+		kap = (S) __ldg(kr);
+		nrm = (S) pick<0, M::D>(kr + 1, dim);
+	}
+}
+
+// Slope component q along d of node i.
+template<class M>
+__device__ __forceinline__ double rec_slope(const Pool &P, int i, int d, int q) {
+	return rec_of(P, i, Rec<M>::W)[Rec<M>::S0 + d * Rec<M>::ES + q];
+}
+
+// Multiphase k part of the record (curvature, normal) from the pool's parameters.
+template<class M>
+__device__ __forceinline__ void write_rec_k(const Pool &P, int i) {
+	if constexpr (M::MULTI) {
+		double *kr = rec_of(P, i, Rec<M>::W) + Rec<M>::K0;
+		kr[0] = at(P.k, P.cap, M::KAPPA, i);
+		for (int d = 0; d < M::D; ++d) kr[1 + d] = at(P.k, P.cap, M::IKN + d, i);
+	}
+}
+
+template<class M>
+__global__ void k_rec_k(Pool P, const int32_t *list, int n) {
+	for (int tid = gtid(); tid < n; tid += gstride()) write_rec_k<M>(P, list[tid]);
+}
+
+// du[dim * G + DT] (temperature gradient along the face normal) for a run-time dim.
+template<class M, class S>
+__device__ __forceinline__ S pick_row_dt(const S *du, int dim) {
+	S r = du[M::DT];
+#pragma unroll
+	for (int j = 1; j < M::D; ++j)
+		if (dim == j) r = du[j * M::G + M::DT];
+	return r;
+}
+
+// --------------------------------------------------------------------------------------------
 // Interior face flux: Model::flux(left, right, face) with the face of the owning cell
 // (impl/flux.hpp:32-39, 80-91; model/euler.hpp:156-200, navier_stokes.hpp:387-408,
 // multi.hpp:249-302). `dir_o` is the owner's direction towards `other`; for dir_o == 0 the owner is
 // the right state and the face keeps the owner's centre (the reference relabels face.dir = 1).
-// `shift` moves the non-owner's centre by the active size across a periodic wrap.
+// Across a periodic wrap the non-owner's centre moves by the active size.
 // --------------------------------------------------------------------------------------------
-template<class M, bool V = M::VISC, class S = double>
+template<class M, bool V, class S>
 __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, int owner, int other, int dim, int dir_o,
                                               double dtL, double *Fout) {
 	constexpr int E = M::E, D = M::D;
@@ -56,6 +137,9 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 	const double cL = dir_o == 1 ? co : cx;
 	const double cR = dir_o == 1 ? cx : co;
 
+	S pl[E], hl[E], sl[E], pr[E], hr[E], sr[E], kl = 0, kr = 0, nl = 0, nr = 0;
+	load_face_rec<M, S>(P, iL, dim, pl, hl, sl, kl, nl);
+	load_face_rec<M, S>(P, iR, dim, pr, hr, sr, kr, nr);
 	const double tm   = 0.5 * (t1 + t0);
 	const double dt_n = tm - P.t[iL];
 	const double dt_p = tm - P.t[iR];
@@ -63,13 +147,13 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 	const S xl = (S) (fc - cL), xr = (S) (fc - cR), tl = (S) dt_n, tr = (S) dt_p;
 	S pn[E], pp[E];
 	for (int q = 0; q < E; ++q) {
-		S v   = (S) at(P.p, cap, q, iL) + (S) at(P.slope, cap, dim * E + q, iL) * xl;
-		pn[q] = v - (S) at(P.rhs, cap, q, iL) * tl;
-		S w   = (S) at(P.p, cap, q, iR) + (S) at(P.slope, cap, dim * E + q, iR) * xr;
-		pp[q] = w - (S) at(P.rhs, cap, q, iR) * tr;
+		S v   = pl[q] + sl[q] * xl;
+		pn[q] = v - hl[q] * tl;
+		S w   = pr[q] + sr[q] * xr;
+		pp[q] = w - hr[q] * tr;
 	}
 	S ka = 0;
-	if constexpr (M::MULTI) ka = (S) 0.5 * ((S) at(P.k, cap, M::KAPPA, iL) + (S) at(P.k, cap, M::KAPPA, iR));
+	if constexpr (M::MULTI) ka = (S) 0.5 * (kl + kr);
 	S pm[E], F[M::F];
 	middle_state<M, S>(C.m, pn, pp, ka, dim, pm);
 	phys_flux<M, S>(C.m, pm, (S) 0, dim, false, F);
@@ -79,8 +163,8 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 		constexpr int IA = M::IA, IU = M::IU, IP = M::IP;
 		const S a = pm[IA];
 		if (a > (S) 1e-5 && a < 1 - (S) 1e-5) {
-			S n  = (S) 0.5 * ((S) at(P.k, cap, M::IKN + dim, iL) + (S) at(P.k, cap, M::IKN + dim, iR));
-			S uc = (S) MULTI_UC * fabs(pm[IU + dim]) * n;
+			S n  = (S) 0.5 * (nl + nr);
+			S uc = (S) MULTI_UC * fabs(pick<IU, D>(pm, dim)) * n;
 			S ke = 0;
 			for (int i = 0; i < D; ++i) {
 				F[IU + i] += uc * ((1 - a) * pm[0] - a * pm[1]) * pm[IU + i];
@@ -101,19 +185,19 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 		for (int i = 0; i < D; ++i)
 			for (int g = 0; g < G; ++g)
 				du[i * G + g] = (S) 0.5 * ((S) at(P.grad, cap, i * G + g, iL) + (S) at(P.grad, cap, i * G + g, iR));
-		for (int i = 0; i < D; ++i) vel[i] = (S) 0.5 * ((S) at(P.p, cap, M::IU + i, iL) + (S) at(P.p, cap, M::IU + i, iR));
+		for (int i = 0; i < D; ++i) vel[i] = (S) 0.5 * (pl[M::IU + i] + pr[M::IU + i]);
 		if constexpr (M::MULTI) {
 			// multi.hpp:287-301: viscous and heat terms enter before the area * dt scaling
-			visc_flux<D, S>(du, G, vel, visc_mu<M, S>(C.m, pm), dim, fv);
+			visc_flux<D, G, S>(du, vel, visc_mu<M, S>(C.m, pm), dim, fv);
 			for (int i = 0; i <= D; ++i) F[M::IU + i] -= fv[i];
-			F[M::IU + D] -= du[dim * G + M::DT] * visc_lambda<M, S>(C.m, pm);
+			F[M::IU + D] -= pick_row_dt<M, S>(du, dim) * visc_lambda<M, S>(C.m, pm);
 			for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * dtf;
 		} else {
 			// navier_stokes.hpp:387-408: convective part scaled first, then scaled viscous/heat terms
 			for (int q = 0; q < M::F; ++q) Fout[q] = (double) F[q] * area * dtf;
-			visc_flux<D, S>(du, G, vel, (S) C.m.ns_mu, dim, fv);
+			visc_flux<D, G, S>(du, vel, (S) C.m.ns_mu, dim, fv);
 			for (int i = 0; i <= D; ++i) Fout[M::IU + i] -= (double) fv[i] * area * dtf;
-			const double fh = (double) ((S) C.m.ns_lambda * du[dim * G + M::DT]) * area * dtf;
+			const double fh = (double) ((S) C.m.ns_lambda * pick_row_dt<M, S>(du, dim)) * area * dtf;
 			Fout[M::IU + D] -= fh;
 		}
 	} else {
@@ -122,7 +206,7 @@ __device__ __forceinline__ void interior_flux(const Pool &P, const Consts &C, in
 }
 
 // Boundary::boundary_flux (integrator/boundary.hpp:130-160), from the cell-centre state.
-template<class M, bool V = M::VISC, class S = double>
+template<class M, bool V, class S>
 __device__ __forceinline__ void boundary_flux(const Pool &P, const Consts &C, const BcTable &B, int i, int b, int dim,
                                               int dir, double dtL, double *Fout) {
 	constexpr int E = M::E, D = M::D;
@@ -139,10 +223,10 @@ __device__ __forceinline__ void boundary_flux(const Pool &P, const Consts &C, co
 	}
 	const int type = B.type[b];
 	if (type == BC_FREESLIP) {
-		phys_flux<M, S>(C.m, pc, pb[M::IU + dim], dim, true, F);
+		phys_flux<M, S>(C.m, pc, pick<M::IU, D>(pb, dim), dim, true, F);
 	} else if (type == BC_NOSLIP) {
 		for (int q = 0; q < M::F; ++q) F[q] = 0;
-		F[M::IU + dim] = pb[M::IP];
+		put<M::IU, D>(F, dim, pb[M::IP]);
 	} else {
 		S pm[E];
 		middle_state<M, S>(C.m, pb, pc, (S) 0, dim, pm);
@@ -153,7 +237,7 @@ __device__ __forceinline__ void boundary_flux(const Pool &P, const Consts &C, co
 		S g[D * G], z[D], fv[D + 1];
 		for (int c = 0; c < D * G; ++c) g[c] = (S) at(P.grad, cap, c, i);
 		for (int d = 0; d < D; ++d) z[d] = 0;
-		visc_flux<D, S>(g, G, z, visc_mu<M, S>(C.m, pc), dim, fv);
+		visc_flux<D, G, S>(g, z, visc_mu<M, S>(C.m, pc), dim, fv);
 		for (int k = 0; k <= D; ++k) F[M::IU + k] -= fv[k];
 	}
 	const double area = C.area[P.level[i]];
@@ -206,21 +290,108 @@ __device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i
 	return (P.clu[gc] == L && ai <= P.acti[gc]) ? gc : -1;
 }
 
-// flux_update (impl/flux.hpp:11-97), face parallel. A group of 2D lanes (padded to 4 or 8) serves
-// one cell; lane f handles face (dim, dir) = (f / 2, f % 2): the flux the cell owns across it
-// (cluster_mode) and the fluxes running-cluster neighbours own across it, all evaluated at one call
-// site. The lane sums are combined with a fixed butterfly, so the per-cell total does not depend on
-// scheduling. cluster_mode: cells of cluster L (marking receivers); otherwise receivers, which only
-// gather.
+__device__ __forceinline__ double *face_flux(const Pool &P, int i, int f, int nflux, int nfaces) {
+	return P.ff + ((size_t) i * nfaces + f) * nflux;
+}
+
+// Face-flux source codes of plan[]: (owner * 2D + owner's face) * 2 + (1 if the cell subtracts it);
+// PLAN_NONE when no flux crosses the face in this substep, PLAN_WALK when finer owners behind a
+// non-leaf neighbour have to be enumerated.
+constexpr int32_t PLAN_NONE = -1, PLAN_WALK = -2;
+
+// flux_update (impl/flux.hpp:11-97), first part. One thread per (cell, face) of the running cluster
+// decides whether the cell owns the face (the finer side, or at equal levels the slower cell, or the
+// cell on the left) and queues it as a dense task, interior and boundary faces apart; it records in
+// plan[] where the face's flux will come from, and owners next to cells of slower clusters queue
+// those as receivers. Task order is scheduling dependent, task results are not.
+template<class M>
+__global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stamp, int32_t *tasks, int32_t *btasks,
+                             int32_t *recv, Counters *cnt) {
+	constexpr int NF = 2 * M::D;
+	const int cap   = P.cap;
+	const long long total = (long long) n * NF;
+	for (long long t = gtid(); t < total; t += gstride()) {
+		const int slot = (int) (t / NF), f = (int) (t % NF);
+		const int i    = list[slot];
+		const int dir  = f & 1;
+		const int nb   = P.nbr[(size_t) f * cap + i];
+		int32_t *pl    = P.plan + (size_t) i * NF + f;
+		if (nb == 0) {
+			if (P.bc[(size_t) f * cap + i] < 0) {
+				set_status(&cnt->status, ST_MISSING_BC);
+				*pl = PLAN_NONE;
+			} else {
+				append(btasks, &cnt->n_btask, i * NF + f, cap * NF, &cnt->status);
+				*pl = (i * NF + f) * 2 + 1;
+			}
+			continue;
+		}
+		if (!(P.flags[nb] & F_LEAF)) {
+			*pl = PLAN_WALK;
+			continue;
+		}
+		const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
+		if (an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
+			if (P.clu[nb] != L) {
+				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
+			}
+			append(tasks, &cnt->n_task, i * NF + f, cap * NF, &cnt->status);
+			*pl = (i * NF + f) * 2 + dir;
+		} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
+			*pl = (nb * NF + (f ^ 1)) * 2 + dir;
+		} else {
+			*pl = PLAN_NONE;
+		}
+	}
+}
+
+// Interior face fluxes of the queued tasks, one thread per face, into the owner's face-flux slot.
 template<class M, bool V, class S = double>
-__global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, const int32_t *list, const int *n_ptr,
-                                                int n_host, int L, double dtL, int stamp, int cluster_mode,
-                                                int32_t *recv, Counters *cnt) {
+__global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const int32_t *tasks, const int *n_ptr,
+                                                      double dtL) {
+	constexpr int NF = 2 * M::D;
+	const int n = *n_ptr;
+	for (int t = gtid(); t < n; t += gstride()) {
+		const int code = tasks[t];
+		const int i = code / NF, f = code % NF;
+		const int nb = P.nbr[(size_t) f * P.cap + i];
+		double F[M::F];
+		interior_flux<M, V, S>(P, C, i, nb, f >> 1, f & 1, dtL, F);
+		double *dst = face_flux(P, i, f, M::F, NF);
+#pragma unroll
+		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
+	}
+}
+
+// Boundary face fluxes of the queued tasks.
+template<class M, bool V, class S = double>
+__global__ void k_flux_bfaces(Pool P, Consts C, BcTable B, const int32_t *tasks, const int *n_ptr, double dtL) {
+	constexpr int NF = 2 * M::D;
+	const int n = *n_ptr;
+	for (int t = gtid(); t < n; t += gstride()) {
+		const int code = tasks[t];
+		const int i = code / NF, f = code % NF;
+		const int b = P.bc[(size_t) f * P.cap + i];
+		double F[M::F];
+		boundary_flux<M, V, S>(P, C, B, i, b, f >> 1, f & 1, dtL, F);
+		double *dst = face_flux(P, i, f, M::F, NF);
+#pragma unroll
+		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
+	}
+}
+
+// flux_update, receiving side: each queued receiver sums, in a fixed face order, the fluxes that
+// running-cluster cells own across its faces. A group of 2D lanes (padded to 4 or 8) serves one
+// cell; lane f walks the owners across face (dim, dir) = (f / 2, f % 2) and the lane sums are
+// combined with a fixed butterfly, so the total does not depend on scheduling.
+template<class M>
+__global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *list, const int *n_ptr, int L,
+                                                        Counters *cnt) {
 	constexpr int NF   = 2 * M::D;
 	constexpr int G    = NF <= 4 ? 4 : 8;
 	constexpr int GW   = 32 / G;
 	constexpr int NSUB = 1 << (M::D - 1);
-	const int n      = n_ptr ? *n_ptr : n_host;
+	const int n      = *n_ptr;
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
 	const int sub    = lane & (G - 1);
@@ -236,30 +407,14 @@ __global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, 
 			const int dim = sub >> 1, dir = sub & 1;
 			const int li = P.level[i], ai = P.acti[i];
 			const int nb = P.nbr[(size_t) sub * cap + i];
-			double F[M::F];
-			if (nb == 0) {
-				if (cluster_mode) {
-					const int b = P.bc[(size_t) sub * cap + i];
-					if (b < 0) {
-						set_status(&cnt->status, ST_MISSING_BC);
-					} else {
-						boundary_flux<M, V, S>(P, C, B, i, b, dim, dir, dtL, F);
-#pragma unroll
-						for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
-					}
-				}
-			} else {
+			if (nb != 0) {
 				const int ncand = (P.flags[nb] & F_LEAF) ? 1 : 1 + NSUB * (NSUB + 1);
 				for (int c = 0; c < ncand; ++c) {
 					int dn;
 					bool plus;
-					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, cluster_mode != 0, dn,
-					                                plus);
+					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, false, dn, plus);
 					if (owner < 0) continue;
-					if (owner == i && P.clu[nb] != L) {
-						if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
-					}
-					interior_flux<M, V, S>(P, C, owner, owner == i ? nb : i, dim, dn, dtL, F);
+					const double *F = face_flux(P, owner, 2 * dim + dn, M::F, NF);
 					if (plus) {
 #pragma unroll
 						for (int q = 0; q < M::F; ++q) acc[q] += F[q];
@@ -284,21 +439,86 @@ __global__ void __launch_bounds__(BLOCK, 2) k_flux(Pool P, Consts C, BcTable B, 
 	}
 }
 
-// cell_update (impl/cell_update.hpp:10-90). Without viscous terms (V = false) the gradient inputs
-// are never read, so t_slope is not maintained.
+// The flux sum of face f of a running-cluster cell: the planned source, or the finer owners behind a
+// non-leaf neighbour in candidate order.
+template<class M>
+__device__ __forceinline__ void face_sum(const Pool &P, uint32_t *status, int i, int f, int L, int li, int ai, double *acc) {
+	constexpr int NF = 2 * M::D, NSUB = 1 << (M::D - 1);
+#pragma unroll
+	for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
+	const int pl = P.plan[(size_t) i * NF + f];
+	if (pl >= 0) {
+		const double *F = P.ff + (size_t) (pl >> 1) * M::F;
+		if (pl & 1) {
+#pragma unroll
+			for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
+		} else {
+#pragma unroll
+			for (int q = 0; q < M::F; ++q) acc[q] += F[q];
+		}
+	} else if (pl == PLAN_WALK) {
+		const int nb = P.nbr[(size_t) f * P.cap + i];
+		for (int c = 1; c < 1 + NSUB * (NSUB + 1); ++c) {
+			int dn;
+			bool plus;
+			const int owner = face_owner<M>(P, status, i, nb, f >> 1, f & 1, L, li, ai, c, true, dn, plus);
+			if (owner < 0) continue;
+			const double *F = face_flux(P, owner, (f & ~1) | dn, M::F, NF);
+			if (plus) {
+#pragma unroll
+				for (int q = 0; q < M::F; ++q) acc[q] += F[q];
+			} else {
+#pragma unroll
+				for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
+			}
+		}
+	}
+}
+
+// flux_update's gather for the running cluster fused with cell_update (impl/cell_update.hpp:10-90),
+// one thread per cell. The face sums combine in the pairing order of a butterfly over 4 (2D) or 8
+// (3D) lanes, the last two contributing zeros in 3D. Without viscous terms (V = false) the gradient
+// inputs are never read, so t_slope is not maintained.
 template<class M, bool V>
-__global__ void k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, Counters *cnt) {
-	constexpr int E = M::E;
+__global__ void k_gather_update(Pool P, Consts C, const int32_t *list, int n, int L, double dtL, Counters *cnt) {
+	constexpr int E = M::E, NF = 2 * M::D;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
-		const int i = list[tid];
-		double pold[E], u[E], du[M::F], p[E];
+		const int i  = list[tid];
+		const int li = P.level[i], ai = P.acti[i];
+		double a[M::F], b[M::F], c[M::F];
+		if constexpr (NF <= 4) {
+			// (f0 + f2) + (f1 + f3)
+			face_sum<M>(P, &cnt->status, i, 0, L, li, ai, a);
+			face_sum<M>(P, &cnt->status, i, 2, L, li, ai, b);
+			for (int q = 0; q < M::F; ++q) a[q] += b[q];
+			face_sum<M>(P, &cnt->status, i, 1, L, li, ai, b);
+			face_sum<M>(P, &cnt->status, i, 3, L, li, ai, c);
+			for (int q = 0; q < M::F; ++q) b[q] += c[q];
+		} else {
+			// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0))
+			face_sum<M>(P, &cnt->status, i, 0, L, li, ai, a);
+			face_sum<M>(P, &cnt->status, i, 4, L, li, ai, b);
+			for (int q = 0; q < M::F; ++q) a[q] += b[q];
+			face_sum<M>(P, &cnt->status, i, 2, L, li, ai, b);
+			for (int q = 0; q < M::F; ++q) b[q] += 0.0;
+			for (int q = 0; q < M::F; ++q) a[q] += b[q];
+			face_sum<M>(P, &cnt->status, i, 1, L, li, ai, b);
+			face_sum<M>(P, &cnt->status, i, 5, L, li, ai, c);
+			for (int q = 0; q < M::F; ++q) b[q] += c[q];
+			face_sum<M>(P, &cnt->status, i, 3, L, li, ai, c);
+			for (int q = 0; q < M::F; ++q) c[q] += 0.0;
+			for (int q = 0; q < M::F; ++q) b[q] += c[q];
+		}
+		double du[M::F];
+		const double vol = C.vol[li];
+		for (int q = 0; q < M::F; ++q) du[q] = (at(P.flux, cap, q, i) + (a[q] + b[q])) / vol;
+
+		double pold[E], u[E], p[E];
 		load_p<M>(P, i, pold);
 		for (int q = 0; q < E; ++q) u[q] = at(P.u, cap, q, i);
 		double gold[M::G > 0 ? M::G : 1];
 		if constexpr (V) grad_input<M>(C.m, pold, gold);
-		const double vol = C.vol[P.level[i]];
-		for (int q = 0; q < M::F; ++q) du[q] = at(P.flux, cap, q, i) / vol;
 		for (int q = 0; q < E; ++q) u[q] += du[q];
 		if constexpr (M::MULTI) {
 			if (!C.signal) {
@@ -375,10 +595,13 @@ __device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uin
 }
 
 // compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients (only read by the viscous
-// terms, so computed when V) and the Hancock rhs.
+// terms, so computed when V) and the Hancock rhs. Writes the record values [0, K0) of cell i (p, rhs,
+// slope rows) to `out`; the gradients go to the pool.
 template<class M, bool V = M::VISC>
-__device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim, int i) {
+__device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim,
+                                              int i, double *out) {
 	constexpr int E = M::E, D = M::D;
+	using R = Rec<M>;
 	const int cap = P.cap;
 	double pc[E];
 	load_p<M>(P, i, pc);
@@ -403,17 +626,48 @@ __device__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, 
 			}
 		}
 	}
-	for (int c = 0; c < D * E; ++c) P.slope[(size_t) c * cap + i] = slope[c];
 	double rhs[E];
 	double kap = 0.0;
 	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
 	compute_rhs<M>(C.m, pc, slope, kap, rhs);
-	for (int q = 0; q < E; ++q) P.rhs[(size_t) q * cap + i] = rhs[q];
+	for (int q = 0; q < E; ++q) out[R::P0 + q] = pc[q], out[R::R0 + q] = rhs[q];
+	for (int d = 0; d < D; ++d)
+		for (int q = 0; q < R::ES; ++q) out[R::S0 + d * R::ES + q] = q < E ? slope[d * E + q] : 0.0;
 }
 
+// Slope stage over a cell list, one thread per cell. The record values are staged per warp in
+// shared memory and written back as consecutive 8-byte words, so that a warp of consecutive cells
+// stores whole cache lines (cells of the running cluster are mostly consecutive pool slots).
+constexpr int SLOPE_BLOCK = 128;
+
 template<class M, bool V>
-__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
-	for (int tid = gtid(); tid < n; tid += gstride()) compute_slope<M, V>(P, C, B, &cnt->status, lim, list[tid]);
+__global__ void __launch_bounds__(SLOPE_BLOCK) k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim,
+                                                       Counters *cnt) {
+	using R = Rec<M>;
+	constexpr int K  = R::K0;  // staged values per cell
+	constexpr int SK = K | 1;  // odd row stride against bank conflicts
+	__shared__ double stage[SLOPE_BLOCK / 32][32 * SK];
+	__shared__ int cells[SLOPE_BLOCK];
+	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+	double *st = stage[wib];
+	int *wc    = cells + wib * 32;
+	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int base = warp * 32; base < n; base += nwarps * 32) {
+		const int slot = base + lane;
+		if (slot < n) {
+			const int i = list[slot];
+			wc[lane]    = i;
+			compute_slope<M, V>(P, C, B, &cnt->status, lim, i, st + lane * SK);
+		}
+		__syncwarp();
+		const int live = min(32, n - base);
+		for (int j = lane; j < live * K; j += 32) {
+			const int c = j / K, k = j - c * K;
+			rec_of(P, wc[c], R::W)[k] = st[c * SK + k];
+		}
+		__syncwarp();
+	}
 }
 
 // Recompute the Hancock rhs from the stored slope (used for split parents, whose curvature may
@@ -424,11 +678,13 @@ __device__ void recompute_rhs(const Pool &P, const Consts &C, int i) {
 	const int cap = P.cap;
 	double pc[E], slope[D * E], rhs[E];
 	load_p<M>(P, i, pc);
-	for (int c = 0; c < D * E; ++c) slope[c] = at(P.slope, cap, c, i);
+	for (int d = 0; d < D; ++d)
+		for (int q = 0; q < E; ++q) slope[d * E + q] = rec_slope<M>(P, i, d, q);
 	double kap = 0.0;
 	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
 	compute_rhs<M>(C.m, pc, slope, kap, rhs);
-	for (int q = 0; q < E; ++q) P.rhs[(size_t) q * cap + i] = rhs[q];
+	double *r = rec_of(P, i, Rec<M>::W);
+	for (int q = 0; q < E; ++q) r[Rec<M>::R0 + q] = rhs[q];
 }
 
 // Scene::can_split (scene/scene.hpp:50-61) with identity-transform refinement zones.
@@ -484,7 +740,7 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 					load_p<M>(P, nb, v);
 					for (int d = 0; d < D; ++d) {
 						const double off = x[d] - at(P.center, cap, d, nb);
-						for (int q = 0; q < E; ++q) v[q] = v[q] + at(P.slope, cap, d * E + q, nb) * off;
+						for (int q = 0; q < E; ++q) v[q] = v[q] + rec_slope<M>(P, nb, d, q) * off;
 					}
 				} else {
 					load_p<M>(P, nb, v);
@@ -587,9 +843,11 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 				P.child[(size_t) c * cap + par] = first + c;
 			}
 		}
+		using R = Rec<M>;
 		double pp[E], pc[D];
 		load_p<M>(P, par, pp);
 		for (int d = 0; d < D; ++d) pc[d] = at(P.center, cap, d, par);
+		const double *rp = rec_of(P, par, R::W);
 		for (int c = 0; c < NC; ++c) {
 			const int s = slots[c];
 			P.parent[s] = par;
@@ -609,16 +867,19 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 			for (int k = 0; k < E; ++k) p[k] = pp[k];
 			for (int d = 0; d < D; ++d) {
 				const double off = cc[d] - pc[d];
-				for (int k = 0; k < E; ++k) p[k] = p[k] + at(P.slope, cap, d * E + k, par) * off;
+				for (int k = 0; k < E; ++k) p[k] = p[k] + rp[R::S0 + d * R::ES + k] * off;
 			}
 			cons_from_prim<M>(C.m, p, u);
+			double *rs = rec_of(P, s, R::W);
 			for (int k = 0; k < E; ++k) {
-				P.p[(size_t) k * cap + s]   = p[k];
-				P.u[(size_t) k * cap + s]   = u[k];
-				P.rhs[(size_t) k * cap + s] = 0.0;
+				P.p[(size_t) k * cap + s] = p[k];
+				P.u[(size_t) k * cap + s] = u[k];
+				rs[R::P0 + k]             = p[k];
+				rs[R::R0 + k]             = 0.0;
 			}
-			for (int k = 0; k < D * E; ++k) P.slope[(size_t) k * cap + s] = at(P.slope, cap, k, par);
+			for (int k = 0; k < D * R::ES; ++k) rs[R::S0 + k] = rp[R::S0 + k];
 			for (int k = 0; k < M::P; ++k) P.k[(size_t) k * cap + s] = at(P.k, cap, k, par);
+			write_rec_k<M>(P, s);
 			for (int k = 0; k < M::G; ++k) P.tslope[(size_t) k * cap + s] = at(P.tslope, cap, k, par);
 			for (int k = 0; k < D * M::G; ++k) P.grad[(size_t) k * cap + s] = at(P.grad, cap, k, par);
 			for (int k = 0; k < M::F; ++k) P.flux[(size_t) k * cap + s] = 0.0;
@@ -676,11 +937,14 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		for (int q = 0; q < M::P; ++q) kk[q] = kk[q] / (double) NC;
 		for (int q = 0; q < D * G; ++q) gr[q] = gr[q] / (double) NC;
 		P.t[par] = t;
+		double *rpar = rec_of(P, par, Rec<M>::W);
 		for (int q = 0; q < E; ++q) {
 			P.u[(size_t) q * cap + par] = u[q];
 			P.p[(size_t) q * cap + par] = p[q];
+			rpar[Rec<M>::P0 + q]        = p[q];
 		}
 		for (int q = 0; q < M::P; ++q) P.k[(size_t) q * cap + par] = kk[q];
+		write_rec_k<M>(P, par);
 		for (int q = 0; q < G; ++q) P.tslope[(size_t) q * cap + par] = ts[q];
 		for (int q = 0; q < D * G; ++q) P.grad[(size_t) q * cap + par] = gr[q];
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + par] = 0.0;
@@ -1060,7 +1324,11 @@ static __global__ void k_gc_move(const char *src, char *dst, int elem, int comps
 		const int j = newidx[i];
 		for (int c = 0; c < comps; ++c) {
 			const size_t so = ((size_t) c * cap + i) * elem, dof = ((size_t) c * cap + j) * elem;
-			for (int b = 0; b < elem; ++b) dst[dof + b] = src[so + b];
+			if (elem % 8 == 0) {
+				for (int b = 0; b < elem; b += 8) *(double *) (dst + dof + b) = *(const double *) (src + so + b);
+			} else {
+				for (int b = 0; b < elem; ++b) dst[dof + b] = src[so + b];
+			}
 		}
 	}
 }
@@ -1152,6 +1420,16 @@ __global__ void k_permute(const T *__restrict__ src, T *__restrict__ dst, int co
 	for (int j = gtid(); j < n; j += gstride()) {
 		const int o = perm[j];
 		for (int c = 0; c < comps; ++c) dst[(size_t) c * cap + j + 1] = src[(size_t) c * cap + o];
+	}
+}
+
+// Permutation of a field holding one record of w 8-byte words per node: word-parallel copies.
+static __global__ void k_permute_words(const double *__restrict__ src, double *__restrict__ dst, int w, int n,
+                                       const int32_t *__restrict__ perm) {
+	const long long total = (long long) n * w;
+	for (long long t = gtid(); t < total; t += gstride()) {
+		const int j = (int) (t / w), k = (int) (t % w);
+		dst[(size_t) (j + 1) * w + k] = src[(size_t) perm[j] * w + k];
 	}
 }
 
