@@ -524,10 +524,8 @@ private:
 	}
 
 	void launch_slope(const int32_t *list, int n) {
-		const long long b = (n + SLOPE_BLOCK - 1) / SLOPE_BLOCK;
-		const int grid    = (int) std::max(1LL, std::min(b, 148LL * 32));
-		if (visc_) k_slope<M, true><<<grid, SLOPE_BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
-		else k_slope<M, false><<<grid, SLOPE_BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 	}
 
 	void sync_counters() {

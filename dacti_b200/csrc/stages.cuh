@@ -635,38 +635,20 @@ __device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, co
 		for (int q = 0; q < R::ES; ++q) out[R::S0 + d * R::ES + q] = q < E ? slope[d * E + q] : 0.0;
 }
 
-// Slope stage over a cell list, one thread per cell. The record values are staged per warp in
-// shared memory and written back as consecutive 8-byte words, so that a warp of consecutive cells
-// stores whole cache lines (cells of the running cluster are mostly consecutive pool slots).
-constexpr int SLOPE_BLOCK = 128;
-
+// Slope stage over a cell list, one thread per cell; each thread writes its record's [0, K0) part
+// with 16-byte stores.
 template<class M, bool V>
-__global__ void __launch_bounds__(SLOPE_BLOCK) k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim,
-                                                       Counters *cnt) {
+__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
 	using R = Rec<M>;
-	constexpr int K  = R::K0;  // staged values per cell
-	constexpr int SK = K | 1;  // odd row stride against bank conflicts
-	__shared__ double stage[SLOPE_BLOCK / 32][32 * SK];
-	__shared__ int cells[SLOPE_BLOCK];
-	const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-	double *st = stage[wib];
-	int *wc    = cells + wib * 32;
-	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
-	for (int base = warp * 32; base < n; base += nwarps * 32) {
-		const int slot = base + lane;
-		if (slot < n) {
-			const int i = list[slot];
-			wc[lane]    = i;
-			compute_slope<M, V>(P, C, B, &cnt->status, lim, i, st + lane * SK);
-		}
-		__syncwarp();
-		const int live = min(32, n - base);
-		for (int j = lane; j < live * K; j += 32) {
-			const int c = j / K, k = j - c * K;
-			rec_of(P, wc[c], R::W)[k] = st[c * SK + k];
-		}
-		__syncwarp();
+	constexpr int K = R::K0;
+	static_assert(K % 2 == 0, "record rows are 16-byte aligned");
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double out[K];
+		compute_slope<M, V>(P, C, B, &cnt->status, lim, i, out);
+		double2 *dst = reinterpret_cast<double2 *>(rec_of(P, i, R::W));
+#pragma unroll
+		for (int k = 0; k < K / 2; ++k) dst[k] = make_double2(out[2 * k], out[2 * k + 1]);
 	}
 }
 
