@@ -47,6 +47,11 @@ def parse_args():
     ap.add_argument("--levels", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--forms", default="fp64,mixed", help="numerical forms to time (the last one is `value`)")
+    ap.add_argument("--profile-substep", type=int, default=-1,
+                    help="bracket only this substep of the first timed step of the last form with "
+                         "cudaProfilerStart/Stop (for ncu --profile-from-start off); -2 brackets the whole timed "
+                         "region of the last form")
     return ap.parse_args()
 
 
@@ -187,7 +192,14 @@ def bench_reference(args, rank: int, world: int) -> None:
     print(json.dumps(line), flush=True)
 
 
-def timed_run(case, form: str, args, stream, local_rank: int, world: int) -> dict:
+def profiler_range(on: bool) -> None:
+    """cudaProfilerStart/Stop, so that `ncu --profile-from-start off` captures only the chosen range."""
+    import ctypes
+    rt = ctypes.CDLL("libcudart.so.12")
+    (rt.cudaProfilerStart if on else rt.cudaProfilerStop)()
+
+
+def timed_run(case, form: str, args, stream, local_rank: int, world: int, profile: int = -1) -> dict:
     """W warm-up global steps, then K timed ones with CUDA events on the solver's stream."""
     import torch
     import torch.distributed as dist
@@ -205,12 +217,28 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int) -> dic
     torch.cuda.synchronize()
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
+    seen = [0]
+
+    def hook(_s, level, at, n, dt, size):
+        # substep k of the first timed step: start after substep k - 1, stop after substep k
+        if seen[0] == profile - 1:
+            profiler_range(True)
+        if seen[0] == profile:
+            profiler_range(False)
+        seen[0] += 1
+
     with ClockSampler(local_rank) as clk:
+        if profile == -2:
+            profiler_range(True)
+        if profile == 0:
+            profiler_range(True)
         ev0.record(stream)
-        for _ in range(args.steps):
-            solver.integrate()
+        for k in range(args.steps):
+            solver.integrate(hook if (profile >= 0 and k == 0) else None)
         ev1.record(stream)
         torch.cuda.synchronize()
+        if profile == -2:
+            profiler_range(False)
     if world > 1:
         dist.barrier()
     st1 = solver.stats()
@@ -253,8 +281,13 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     case = make_case(args)
     D = case.shape.dims
 
-    plain = timed_run(case, "fp64", args, stream, local_rank, world)
-    chosen = timed_run(case, "mixed", args, stream, local_rank, world)
+    forms = args.forms.split(",")
+    runs = {}
+    for k, f in enumerate(forms):
+        runs[f] = timed_run(case, f, args, stream, local_rank, world,
+                            profile=args.profile_substep if k == len(forms) - 1 else -1)
+    chosen = runs[forms[-1]]
+    plain = runs.get("fp64", chosen)
     err = density_rel_l1(chosen["snap"], plain["snap"], case.params.side_length, case.params.active_size,
                          args.base_level, int(case.shape.model))
 
@@ -262,29 +295,35 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     value = total_updates / (ms_max * 1e-3)
     p_ms, p_upd = reduce_ranks(plain["ms"], plain["updates"], world)
 
-    # roofline of the dominant kernel (the flux stage): algorithmic bytes per cell update times the
-    # cells of its launches, over its CUDA-event time on the solver's stream
+    # Roofline of the cell-update kernel (k_gather_update: face-flux gather fused with the conservative
+    # update, EOS recovery and floors): algorithmic bytes per leaf cell-update (16 E + 8 D + 12: U read
+    # and written in FP64, 2D neighbour ids, level and time) times the cells of its launches, over its
+    # CUDA-event time on the solver's stream. `traffic` is the DRAM bytes per launch from the committed
+    # ncu summary of the same kernel, scaled to this run's cells per launch.
     peak, peak_kind = measured_peak()
     kms, kl, kc = chosen["kms"], chosen["kl"], chosen["kc"]
     dom = max(kms, key=lambda k: kms[k])
     b_per = BYTES_PER_UPDATE[D]
-    flux_ms = kms["flux"]
-    achieved = (b_per * kc["flux"]) / (flux_ms * 1e-3) / 1e9 if flux_ms > 0 else 0.0
+    upd_ms = kms["update"]
+    launches = max(kl["update"], 1)
+    achieved = (b_per * kc["update"] / launches) / (upd_ms * 1e-3 / launches) / 1e9 if upd_ms > 0 else 0.0
     traffic = None
-    tpath = os.path.join(HERE, "profiles", "flux_traffic.json")
+    tpath = os.path.join(HERE, "profiles", "gather_update_traffic.json")
     if os.path.exists(tpath):
         try:
             with open(tpath) as f:
                 tj = json.load(f)
-            traffic = tj["bytes_per_cell"] * (kc["flux"] / max(kl["flux"], 1))
+            traffic = tj["dram_bytes_per_cell"] * (kc["update"] / launches)
         except Exception:
             traffic = None
+    step_achieved = b_per * chosen["updates"] / (chosen["ms"] * 1e-3) / 1e9
     roofline = {
-        "bound": "hbm", "kernel": "k_flux (HLLC flux, cluster gather)", "achieved": achieved, "peak": peak,
-        "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
-        "bytes_per_cell_update": b_per, "kernel_share": {k: round(v / max(sum(kms.values()), 1e-9), 4)
-                                                          for k, v in kms.items() if v > 0},
-        "dominant_kernel_by_time": dom,
+        "bound": "hbm", "kernel": "k_gather_update (face-flux gather + cell update)", "achieved": achieved,
+        "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+        "bytes_per_cell_update": b_per, "launches": kl["update"], "avg_launch_us": 1e3 * upd_ms / launches,
+        "whole_step": {"achieved": step_achieved, "frac": step_achieved / peak},
+        "kernel_share": {k: round(v / max(sum(kms.values()), 1e-9), 4) for k, v in kms.items() if v > 0},
+        "dominant_kernel_kind_by_time": dom,
     }
 
     result = {

@@ -98,6 +98,9 @@ struct Pool {
 	double *u;        // [E][cap]
 	double *p;        // [E][cap]
 	double *rec;      // [cap][W] reconstruction record: p copy, Hancock rhs, slope rows, multiphase k part
+	double *avg;      // [cap][AW] non-leaf nodes: mean primitive state and time over the active subtree
+	int32_t *mark;    // refresh epoch in which the node was queued for a subtree-mean refresh
+	int32_t *pending; // queued children whose subtree mean is not yet refreshed
 	double *k;        // [P][cap]
 	double *tslope;   // [G][cap]
 	double *grad;     // [D][G][cap]
@@ -116,6 +119,8 @@ struct Counters {
 	int clu[MAX_ACTI];
 	int buf[MAX_ACTI];
 	int top;          // next free node slot (== reference tree.size())
+	int n_dirty;      // non-leaf nodes whose subtree mean is stale (kept across substeps until refreshed)
+	int n_seed;       // queued nodes without queued children
 	int n_recv;
 	int n_split;
 	int n_unsplit;
@@ -124,6 +129,7 @@ struct Counters {
 	int n_tmp;        // rebuilt cluster list
 	int n_task;       // owned interior faces of the running substep
 	int n_btask;      // owned boundary faces of the running substep
+	int n_wtask;      // faces of running-cluster cells with finer owners behind a non-leaf neighbour
 	uint32_t status;
 	unsigned long long n_split_total, n_unsplit_total;
 	double dmax;      // reduction result
@@ -141,6 +147,9 @@ struct Lists {
 	int32_t *upd;      // neighbour-update list
 	int32_t *task;     // owned interior faces (cell * 2D + face) of the running substep
 	int32_t *btask;    // owned boundary faces
+	int32_t *wtask;    // faces whose flux sum walks finer owners
+	int32_t *dirty;    // non-leaf nodes whose subtree mean is stale
+	int32_t *seed;     // the refresh's starting nodes
 };
 
 }  // namespace dg

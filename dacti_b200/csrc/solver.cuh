@@ -88,6 +88,8 @@ class Solver : public SolverBase {
 	long long n_substeps_ = 0, n_global_ = 0, updates_ = 0, n_gc_ = 0;
 	long long n_split_total_ = 0, n_unsplit_total_ = 0;
 	int stamp_ = 0;
+	int epoch_ = 1;           // subtree-mean refresh epoch (dedup stamp of Pool::mark)
+	int max_tree_level_ = 0;  // deepest tree level any node can reach
 
 	// launch accounting and optional per-kernel event timing
 	struct Pending {
@@ -289,7 +291,8 @@ public:
 		    {(void **) &P.acti, 1, 1}, {(void **) &P.clu, 1, 1}, {(void **) &P.flags, 4, 1},
 		    {(void **) &P.coord, 4, D}, {(void **) &P.nbr, 4, NF}, {(void **) &P.bc, 2, NF},
 		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
-		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1},
+		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1}, {(void **) &P.avg, 8 * Avg<M>::W, 1},
+		    {(void **) &P.mark, 4, 1}, {(void **) &P.pending, 4, 1},
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.op, 1, 1},
@@ -362,6 +365,7 @@ public:
 			DG_CUDA(cudaMemcpyAsync(Ls_.clu[l], old.clu[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
 			DG_CUDA(cudaMemcpyAsync(Ls_.buf[l], old.buf[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
 		}
+		DG_CUDA(cudaMemcpyAsync(Ls_.dirty, old.dirty, sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
 		cudaFree(old_mem);
 	}
@@ -371,7 +375,7 @@ public:
 		const int nlists = 2 * MAX_ACTI + 6;
 		size_t one       = align_up(sizeof(int32_t) * (size_t) cap);
 		size_t faces     = align_up(sizeof(int32_t) * (size_t) cap * NF);
-		DG_CUDA(cudaMalloc(&list_mem_, one * nlists + 2 * faces));
+		DG_CUDA(cudaMalloc(&list_mem_, one * (nlists + 2) + 3 * faces));
 		char *b = (char *) list_mem_;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			Ls_.clu[l] = (int32_t *) b;
@@ -391,9 +395,15 @@ public:
 		b += one;
 		Ls_.upd     = (int32_t *) b;
 		b += one;
+		Ls_.dirty   = (int32_t *) b;
+		b += one;
+		Ls_.seed    = (int32_t *) b;
+		b += one;
 		Ls_.task    = (int32_t *) b;
 		b += faces;
 		Ls_.btask   = (int32_t *) b;
+		b += faces;
+		Ls_.wtask   = (int32_t *) b;
 		list_cap_   = cap;
 	}
 
@@ -415,8 +425,11 @@ public:
 		std::vector<int8_t> lv(n), ac(n, -1), cl(n, CLU_NONE);
 		std::vector<int32_t> coord((size_t) n * D, 0);
 		std::vector<int16_t> bc((size_t) n * NF);
+		max_tree_level_ = C_.max_refinement_level;
+		for (int z = 0; z < C_.n_zones; ++z) max_tree_level_ = std::max(max_tree_level_, C_.zlevel[z]);
 		for (int i = 0; i < n; ++i) {
 			lv[i] = (int8_t) c.level[i];
+			max_tree_level_ = std::max(max_tree_level_, (int) c.level[i]);
 			for (int f = 0; f < NF; ++f) bc[(size_t) i * NF + f] = (int16_t) c.bc[(size_t) i * NF + f];
 		}
 		// integer coordinates, parents before children
@@ -458,6 +471,7 @@ public:
 		const int g = grid_for(n);
 		k_init_cells<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, d_cnt_);
 		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
+		all_avgs();
 		launch_slope(d_leaves_, n);
 		if constexpr (M::MULTI) {
 			multiphase_aux(d_leaves_, n);
@@ -523,6 +537,27 @@ private:
 		}
 	}
 
+	// Subtree means of every non-leaf node, deepest level first (construction, after re-sort and
+	// compaction); pending refresh marks are dropped.
+	void all_avgs() {
+		const int top = h_cnt_->top;
+		for (int l = max_tree_level_; l >= 0; --l)
+			run_k(DG_K_OTHER, 0, [&] { k_avg_all_level<M><<<grid_for(top), BLOCK, 0, st_>>>(P_, top, l); });
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_dirty, 0, sizeof(int), st_));
+		DG_CUDA(cudaMemsetAsync(P_.pending, 0, sizeof(int32_t) * (size_t) P_.cap, st_));
+		epoch_++;
+	}
+
+	// Subtree means of the queued non-leaf nodes, deepest level first.
+	void refresh_avgs(long long bound) {
+		const int grid = grid_for(bound);
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_seed, 0, sizeof(int), st_));
+		run_k(DG_K_OTHER, 0, [&] { k_avg_seed<<<grid, BLOCK, 0, st_>>>(P_, Ls_.dirty, &d_cnt_->n_dirty, Ls_.seed, &d_cnt_->n_seed); });
+		run_k(DG_K_OTHER, 0, [&] { k_avg_climb<M><<<grid, BLOCK, 0, st_>>>(P_, Ls_.seed, &d_cnt_->n_seed); });
+		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_dirty, 0, sizeof(int), st_));
+		epoch_++;
+	}
+
 	void launch_slope(const int32_t *list, int n) {
 		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
@@ -560,17 +595,19 @@ private:
 		constexpr int LPC = NF <= 4 ? 4 : 8;  // receive lanes per cell
 		run_k(DG_K_FLUX, n, [&] {
 			k_flux_tasks<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, list, n, L, stamp_recv, Ls_.task, Ls_.btask,
-			                                                                  Ls_.recv, d_cnt_);
+			                                                                  Ls_.wtask, Ls_.recv, d_cnt_);
 		});
 		run_k(DG_K_FLUX, 0, [&] { launch_flux_faces(grid_for((long long) n * NF / 2 + 1), dtL); });
 		run_k(DG_K_FLUX, 0, [&] { launch_flux_bfaces(grid_for(n / 4 + 1), dtL); });
+		run_k(DG_K_FLUX, 0, [&] { k_flux_walk<M><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_); });
 		run_k(DG_K_RECV, 0, [&] {
 			k_flux_receive<M><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
-			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, dtL, d_cnt_);
-			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, dtL, d_cnt_);
+			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, epoch_, Ls_.dirty, d_cnt_);
+			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, epoch_, Ls_.dirty, d_cnt_);
 		});
+		refresh_avgs((long long) n / 4 + (long long) NC * h_cnt_->n_split + 1);
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) {
 			multiphase_aux(list, n);
@@ -582,10 +619,11 @@ private:
 		const int gf = grid_for((long long) n * (NC + 1));
 		run_k(DG_K_REGRID, n, [&] { k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_); });
 		run_k(DG_K_REGRID, 0, [&] {
-			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, d_cnt_);
+			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, epoch_, Ls_.dirty, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
-			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, d_cnt_);
+			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, epoch_, Ls_.dirty,
+			                                   d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
 			k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
@@ -726,6 +764,7 @@ public:
 		std::swap(P_, S_);
 		std::swap(pool_mem_, shadow_mem_);
 		attach_derived();
+		all_avgs();
 		int first = 1;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			const int cnt = h_cnt_->clu[l];
@@ -770,6 +809,8 @@ private:
 		pool_mem_ = mem;
 		P_        = NP;
 		attach_derived();
+		h_cnt_->top = new_top;
+		all_avgs();
 		// full ACTI reassignment
 		Counters z{};
 		z.top    = new_top;

@@ -294,10 +294,12 @@ __device__ __forceinline__ double *face_flux(const Pool &P, int i, int f, int nf
 	return P.ff + ((size_t) i * nfaces + f) * nflux;
 }
 
-// Face-flux source codes of plan[]: (owner * 2D + owner's face) * 2 + (1 if the cell subtracts it);
-// PLAN_NONE when no flux crosses the face in this substep, PLAN_WALK when finer owners behind a
-// non-leaf neighbour have to be enumerated.
-constexpr int32_t PLAN_NONE = -1, PLAN_WALK = -2;
+// Face-flux source codes of plan[]: (owner * 2D + owner's face) * 2 + (1 if the cell subtracts it),
+// or PLAN_NONE when no flux crosses the face in this substep. A face with finer owners behind a
+// non-leaf neighbour is queued as a walk task; the walk stores the face's signed sum in the cell's own
+// slot for that face (unused otherwise: the cell owns no face towards a non-leaf) and plans it as a
+// plain source.
+constexpr int32_t PLAN_NONE = -1;
 
 // flux_update (impl/flux.hpp:11-97), first part. One thread per (cell, face) of the running cluster
 // decides whether the cell owns the face (the finer side, or at equal levels the slower cell, or the
@@ -306,7 +308,7 @@ constexpr int32_t PLAN_NONE = -1, PLAN_WALK = -2;
 // those as receivers. Task order is scheduling dependent, task results are not.
 template<class M>
 __global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stamp, int32_t *tasks, int32_t *btasks,
-                             int32_t *recv, Counters *cnt) {
+                             int32_t *wtasks, int32_t *recv, Counters *cnt) {
 	constexpr int NF = 2 * M::D;
 	const int cap   = P.cap;
 	const long long total = (long long) n * NF;
@@ -327,7 +329,8 @@ __global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stam
 			continue;
 		}
 		if (!(P.flags[nb] & F_LEAF)) {
-			*pl = PLAN_WALK;
+			append(wtasks, &cnt->n_wtask, i * NF + f, cap * NF, &cnt->status);
+			*pl = (i * NF + f) * 2;
 			continue;
 		}
 		const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
@@ -439,29 +442,24 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 	}
 }
 
-// The flux sum of face f of a running-cluster cell: the planned source, or the finer owners behind a
-// non-leaf neighbour in candidate order.
+// Walk tasks: the flux sum of a running-cluster cell's face whose finer owners sit behind a non-leaf
+// neighbour, in candidate order, stored in the cell's own slot for that face.
 template<class M>
-__device__ __forceinline__ void face_sum(const Pool &P, uint32_t *status, int i, int f, int L, int li, int ai, double *acc) {
+__global__ void k_flux_walk(Pool P, const int32_t *wtasks, const int *n_ptr, int L, Counters *cnt) {
 	constexpr int NF = 2 * M::D, NSUB = 1 << (M::D - 1);
-#pragma unroll
-	for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
-	const int pl = P.plan[(size_t) i * NF + f];
-	if (pl >= 0) {
-		const double *F = P.ff + (size_t) (pl >> 1) * M::F;
-		if (pl & 1) {
-#pragma unroll
-			for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
-		} else {
-#pragma unroll
-			for (int q = 0; q < M::F; ++q) acc[q] += F[q];
-		}
-	} else if (pl == PLAN_WALK) {
+	const int n = *n_ptr;
+	for (int t = gtid(); t < n; t += gstride()) {
+		const int code = wtasks[t];
+		const int i = code / NF, f = code % NF;
+		const int li = P.level[i], ai = P.acti[i];
 		const int nb = P.nbr[(size_t) f * P.cap + i];
+		double acc[M::F];
+#pragma unroll
+		for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
 		for (int c = 1; c < 1 + NSUB * (NSUB + 1); ++c) {
 			int dn;
 			bool plus;
-			const int owner = face_owner<M>(P, status, i, nb, f >> 1, f & 1, L, li, ai, c, true, dn, plus);
+			const int owner = face_owner<M>(P, &cnt->status, i, nb, f >> 1, f & 1, L, li, ai, c, true, dn, plus);
 			if (owner < 0) continue;
 			const double *F = face_flux(P, owner, (f & ~1) | dn, M::F, NF);
 			if (plus) {
@@ -472,47 +470,53 @@ __device__ __forceinline__ void face_sum(const Pool &P, uint32_t *status, int i,
 				for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
 			}
 		}
+		double *dst = face_flux(P, i, f, M::F, NF);
+#pragma unroll
+		for (int q = 0; q < M::F; ++q) dst[q] = acc[q];
 	}
 }
 
+// Signed contribution of a planned face source to component q, as a gather lane forms it from +0.
+__device__ __forceinline__ double face_term(const double *F, int pl, int q) {
+	if (pl < 0) return 0.0;
+	const double v = F[q];
+	return (pl & 1) ? 0.0 - v : 0.0 + v;
+}
+
 // flux_update's gather for the running cluster fused with cell_update (impl/cell_update.hpp:10-90),
-// one thread per cell. The face sums combine in the pairing order of a butterfly over 4 (2D) or 8
-// (3D) lanes, the last two contributing zeros in 3D. Without viscous terms (V = false) the gradient
-// inputs are never read, so t_slope is not maintained.
+// one thread per cell, component by component so that all face-slot loads are independent. The face
+// terms combine in the pairing order of a butterfly over 4 (2D) or 8 (3D) lanes, the last two
+// contributing zeros in 3D. Without viscous terms (V = false) the gradient inputs are never read, so
+// t_slope is not maintained.
 template<class M, bool V>
-__global__ void k_gather_update(Pool P, Consts C, const int32_t *list, int n, int L, double dtL, Counters *cnt) {
+__global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, const int32_t *list, int n, double dtL,
+                                                            int epoch, int32_t *dirty, Counters *cnt) {
 	constexpr int E = M::E, NF = 2 * M::D;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i  = list[tid];
-		const int li = P.level[i], ai = P.acti[i];
-		double a[M::F], b[M::F], c[M::F];
-		if constexpr (NF <= 4) {
-			// (f0 + f2) + (f1 + f3)
-			face_sum<M>(P, &cnt->status, i, 0, L, li, ai, a);
-			face_sum<M>(P, &cnt->status, i, 2, L, li, ai, b);
-			for (int q = 0; q < M::F; ++q) a[q] += b[q];
-			face_sum<M>(P, &cnt->status, i, 1, L, li, ai, b);
-			face_sum<M>(P, &cnt->status, i, 3, L, li, ai, c);
-			for (int q = 0; q < M::F; ++q) b[q] += c[q];
-		} else {
-			// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0))
-			face_sum<M>(P, &cnt->status, i, 0, L, li, ai, a);
-			face_sum<M>(P, &cnt->status, i, 4, L, li, ai, b);
-			for (int q = 0; q < M::F; ++q) a[q] += b[q];
-			face_sum<M>(P, &cnt->status, i, 2, L, li, ai, b);
-			for (int q = 0; q < M::F; ++q) b[q] += 0.0;
-			for (int q = 0; q < M::F; ++q) a[q] += b[q];
-			face_sum<M>(P, &cnt->status, i, 1, L, li, ai, b);
-			face_sum<M>(P, &cnt->status, i, 5, L, li, ai, c);
-			for (int q = 0; q < M::F; ++q) b[q] += c[q];
-			face_sum<M>(P, &cnt->status, i, 3, L, li, ai, c);
-			for (int q = 0; q < M::F; ++q) c[q] += 0.0;
-			for (int q = 0; q < M::F; ++q) b[q] += c[q];
+		const int li = P.level[i];
+		int pl[NF];
+		const double *src[NF];
+#pragma unroll
+		for (int f = 0; f < NF; ++f) {
+			pl[f]  = P.plan[(size_t) i * NF + f];
+			src[f] = P.ff + (size_t) (pl[f] < 0 ? 0 : pl[f] >> 1) * M::F;
 		}
-		double du[M::F];
 		const double vol = C.vol[li];
-		for (int q = 0; q < M::F; ++q) du[q] = (at(P.flux, cap, q, i) + (a[q] + b[q])) / vol;
+		double du[M::F];
+#pragma unroll
+		for (int q = 0; q < M::F; ++q) {
+			double s;
+			if constexpr (NF <= 4) {
+				s = (face_term(src[0], pl[0], q) + face_term(src[2], pl[2], q)) +
+				    (face_term(src[1], pl[1], q) + face_term(src[3], pl[3], q));
+			} else {
+				s = ((face_term(src[0], pl[0], q) + face_term(src[4], pl[4], q)) + (face_term(src[2], pl[2], q) + 0.0)) +
+				    ((face_term(src[1], pl[1], q) + face_term(src[5], pl[5], q)) + (face_term(src[3], pl[3], q) + 0.0));
+			}
+			du[q] = (at(P.flux, cap, q, i) + s) / vol;
+		}
 
 		double pold[E], u[E], p[E];
 		load_p<M>(P, i, pold);
@@ -560,6 +564,46 @@ __global__ void k_gather_update(Pool P, Consts C, const int32_t *list, int n, in
 		}
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
 		P.t[i] = P.t[i] + dtL;
+		mark_from(P, P.parent[i], epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
+	}
+}
+
+// Subtree-mean refresh, first pass: the queued nodes without queued children start the refresh.
+static __global__ void k_avg_seed(Pool P, const int32_t *dirty, const int *n_ptr, int32_t *seed, int *n_seed) {
+	const int n = *n_ptr;
+	for (int t = gtid(); t < n; t += gstride()) {
+		const int a = dirty[t];
+		if (P.pending[a] == 0) seed[atomicAdd(n_seed, 1)] = a;
+	}
+}
+
+// Second pass: each start node is refreshed, then its thread climbs while it is the last queued child
+// to finish, refreshing each ancestor after all of that ancestor's queued children (children before
+// parents, as the recursion of interpolate_p orders them).
+template<class M>
+__global__ void k_avg_climb(Pool P, const int32_t *seed, const int *n_ptr) {
+	const int n = *n_ptr;
+	for (int t = gtid(); t < n; t += gstride()) {
+		int a = seed[t];
+		for (int guard = 0; guard < MAX_TREE; ++guard) {
+			const uint32_t fl = P.flags[a];
+			if (!(fl & F_LEAF) && !(fl & F_GARBAGE)) refresh_avg<M>(P, a);
+			__threadfence();
+			const int b = P.parent[a];
+			if (b == 0 || atomicSub(&P.pending[b], 1) != 1) break;
+			__threadfence();  // the other children's means, written before their own decrements
+			a = b;
+		}
+	}
+}
+
+// Subtree means of every non-leaf node of one tree level.
+template<class M>
+__global__ void k_avg_all_level(Pool P, int top, int level) {
+	for (int a = 1 + gtid(); a < top; a += gstride()) {
+		if (P.level[a] != level) continue;
+		const uint32_t fl = P.flags[a];
+		if (!(fl & F_LEAF) && !(fl & F_GARBAGE)) refresh_avg<M>(P, a);
 	}
 }
 
@@ -585,7 +629,7 @@ __device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uin
 	}
 	if (!(P.flags[nb] & F_LEAF)) {
 		interp_p<M>(P, status, nb, pv);
-		tv = interp_scalar<M::D>(P, status, nb, P.t);
+		tv = interp_t<M>(P, nb);
 	} else {
 		load_p<M>(P, nb, pv);
 		tv = P.t[nb];
@@ -606,6 +650,7 @@ __device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, co
 	double pc[E];
 	load_p<M>(P, i, pc);
 	double slope[D * E];
+#pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
 		double pn[E], pp[E], xn, xp, tn, tp;
 		const double xc = 0.0;
@@ -630,8 +675,11 @@ __device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, co
 	double kap = 0.0;
 	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
 	compute_rhs<M>(C.m, pc, slope, kap, rhs);
+#pragma unroll
 	for (int q = 0; q < E; ++q) out[R::P0 + q] = pc[q], out[R::R0 + q] = rhs[q];
+#pragma unroll
 	for (int d = 0; d < D; ++d)
+#pragma unroll
 		for (int q = 0; q < R::ES; ++q) out[R::S0 + d * R::ES + q] = q < E ? slope[d * E + q] : 0.0;
 }
 
@@ -801,7 +849,7 @@ __global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int3
 // rhs, and join the running cluster.
 template<class M>
 __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
-                        Counters *cnt) {
+                        int epoch, int32_t *dirty, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D;
 	const int n   = *n_ptr;
 	const int cap = P.cap;
@@ -878,6 +926,7 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 			append(fresh, &cnt->n_new, s, cap, &cnt->status);
 		}
 		P.flags[par] &= ~(F_LEAF | F_SHOULD_SPLIT);
+		mark_from(P, par, epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
 	}
 }
 
@@ -886,7 +935,7 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 // stale gradient, as interpolated_cell does not reset it) and keeps its old slope and rhs.
 template<class M>
 __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh,
-                          Counters *cnt) {
+                          int epoch, int32_t *dirty, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D, G = M::G;
 	const int n   = *n_ptr;
 	const int cap = P.cap;
@@ -936,6 +985,7 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		P.acti[par]  = (int8_t) L;
 		P.clu[par]   = (int8_t) L;
 		append(fresh, &cnt->n_new, par, cap, &cnt->status);
+		mark_from(P, P.parent[par], epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
 	}
 }
 
