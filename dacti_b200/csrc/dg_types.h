@@ -98,9 +98,9 @@ struct Pool {
 	double *u;        // [E][cap]
 	double *p;        // [E][cap]
 	double *rec;      // [cap][W] reconstruction record: p copy, Hancock rhs, slope rows, multiphase k part
-	double *avg;      // [cap][AW] non-leaf nodes: mean primitive state and time over the active subtree
-	int32_t *mark;    // refresh epoch in which the node was queued for a subtree-mean refresh
-	int32_t *pending; // queued children whose subtree mean is not yet refreshed
+	double *avg;      // [cap][AW] non-leaf nodes: memo of the mean primitive state and time of the subtree
+	int32_t *mod;     // epoch of the latest change of any leaf below the node
+	int32_t *cst;     // epoch at which `avg` was computed
 	double *k;        // [P][cap]
 	double *tslope;   // [G][cap]
 	double *grad;     // [D][G][cap]
@@ -112,6 +112,8 @@ struct Pool {
 	// Per-substep scratch outside the permuted fields:
 	double *ff;       // [cap][2D][F] flux of each face a cell owns, written in the running substep
 	int32_t *plan;    // [cap][2D] source of each face's flux for the running cluster's cells
+	double *nbv;      // [slot][2D][NW] neighbour values of the running list's cells (p, t, centre distance)
+	int32_t *nbi;     // [slot][2D] neighbour level, leaf flag, presence and ACTI level
 };
 
 // Device counters, copied back to the host after each substep.
@@ -119,8 +121,6 @@ struct Counters {
 	int clu[MAX_ACTI];
 	int buf[MAX_ACTI];
 	int top;          // next free node slot (== reference tree.size())
-	int n_dirty;      // non-leaf nodes whose subtree mean is stale (kept across substeps until refreshed)
-	int n_seed;       // queued nodes without queued children
 	int n_recv;
 	int n_split;
 	int n_unsplit;
@@ -148,8 +148,6 @@ struct Lists {
 	int32_t *task;     // owned interior faces (cell * 2D + face) of the running substep
 	int32_t *btask;    // owned boundary faces
 	int32_t *wtask;    // faces whose flux sum walks finer owners
-	int32_t *dirty;    // non-leaf nodes whose subtree mean is stale
-	int32_t *seed;     // the refresh's starting nodes
 };
 
 }  // namespace dg

@@ -71,6 +71,8 @@ class Solver : public SolverBase {
 	void *bc_mem_    = nullptr;
 	double *ff_mem_    = nullptr;  // face fluxes (Pool::ff)
 	int32_t *plan_mem_ = nullptr;  // face-flux sources (Pool::plan)
+	double *nbv_mem_   = nullptr;  // neighbour values (Pool::nbv)
+	int32_t *nbi_mem_  = nullptr;  // neighbour facts (Pool::nbi)
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
 	double *d_read_    = nullptr;
 	int32_t *d_readlv_ = nullptr;
@@ -88,7 +90,7 @@ class Solver : public SolverBase {
 	long long n_substeps_ = 0, n_global_ = 0, updates_ = 0, n_gc_ = 0;
 	long long n_split_total_ = 0, n_unsplit_total_ = 0;
 	int stamp_ = 0;
-	int epoch_ = 1;           // subtree-mean refresh epoch (dedup stamp of Pool::mark)
+	int epoch_ = 2;           // kernel epochs of the subtree-mean memo (Pool::mod / Pool::cst)
 	int max_tree_level_ = 0;  // deepest tree level any node can reach
 
 	// launch accounting and optional per-kernel event timing
@@ -175,6 +177,8 @@ public:
 		cudaFree(bc_mem_);
 		cudaFree(ff_mem_);
 		cudaFree(plan_mem_);
+		cudaFree(nbv_mem_);
+		cudaFree(nbi_mem_);
 		cudaFree(d_cnt_);
 		cudaFreeHost(h_cnt_);
 		cudaFree(d_leaves_);
@@ -292,7 +296,7 @@ public:
 		    {(void **) &P.coord, 4, D}, {(void **) &P.nbr, 4, NF}, {(void **) &P.bc, 2, NF},
 		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
 		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1}, {(void **) &P.avg, 8 * Avg<M>::W, 1},
-		    {(void **) &P.mark, 4, 1}, {(void **) &P.pending, 4, 1},
+		    {(void **) &P.mod, 4, 1}, {(void **) &P.cst, 4, 1},
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.op, 1, 1},
@@ -301,6 +305,13 @@ public:
 	}
 
 	static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
+
+	size_t pool_bytes(int cap) {
+		Pool tmp{};
+		size_t total = 0;
+		for (auto &f: fields(tmp)) total += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
+		return total;
+	}
 
 	void *carve_pool(Pool &P, int cap) {
 		P.cap        = cap;
@@ -327,19 +338,29 @@ public:
 	void alloc_derived(int cap) {
 		cudaFree(ff_mem_);
 		cudaFree(plan_mem_);
+		cudaFree(nbv_mem_);
+		cudaFree(nbi_mem_);
 		ff_mem_   = nullptr;
 		plan_mem_ = nullptr;
+		nbv_mem_  = nullptr;
+		nbi_mem_  = nullptr;
 		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) cap));
 		DG_CUDA(cudaMalloc(&plan_mem_, sizeof(int32_t) * NF * (size_t) cap));
+		DG_CUDA(cudaMalloc(&nbv_mem_, sizeof(double) * Nbv<M>::W * NF * (size_t) cap));
+		DG_CUDA(cudaMalloc(&nbi_mem_, sizeof(int32_t) * NF * (size_t) cap));
 		attach_derived();
 	}
 
 	void attach_derived() {
 		P_.ff   = ff_mem_;
 		P_.plan = plan_mem_;
+		P_.nbv  = nbv_mem_;
+		P_.nbi  = nbi_mem_;
 	}
 
 	void grow_pool(int new_cap) {
+		cudaFree(shadow_mem_);
+		shadow_mem_ = nullptr;
 		Pool NP{};
 		void *mem = carve_pool(NP, new_cap);
 		auto fo = fields(P_), fn = fields(NP);
@@ -353,19 +374,22 @@ public:
 		cudaFree(pool_mem_);
 		pool_mem_ = mem;
 		P_        = NP;
-		cudaFree(shadow_mem_);
-		shadow_mem_ = nullptr;
 		alloc_derived(new_cap);
 		// lists grow with the pool
 		Lists old = Ls_;
 		void *old_mem = list_mem_;
 		int old_cap   = list_cap_;
 		alloc_lists(new_cap);
+		const size_t bytes = sizeof(int32_t) * old_cap;
 		for (int l = 0; l < MAX_ACTI; ++l) {
-			DG_CUDA(cudaMemcpyAsync(Ls_.clu[l], old.clu[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
-			DG_CUDA(cudaMemcpyAsync(Ls_.buf[l], old.buf[l], sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
+			DG_CUDA(cudaMemcpyAsync(Ls_.clu[l], old.clu[l], bytes, cudaMemcpyDeviceToDevice, st_));
+			DG_CUDA(cudaMemcpyAsync(Ls_.buf[l], old.buf[l], bytes, cudaMemcpyDeviceToDevice, st_));
 		}
-		DG_CUDA(cudaMemcpyAsync(Ls_.dirty, old.dirty, sizeof(int32_t) * old_cap, cudaMemcpyDeviceToDevice, st_));
+		// the per-substep lists too: the pool can grow between the indicator and the split
+		for (auto pr: {std::make_pair(Ls_.tmp, old.tmp), std::make_pair(Ls_.recv, old.recv),
+		               std::make_pair(Ls_.split, old.split), std::make_pair(Ls_.unsplit, old.unsplit),
+		               std::make_pair(Ls_.fresh, old.fresh), std::make_pair(Ls_.upd, old.upd)})
+			DG_CUDA(cudaMemcpyAsync(pr.first, pr.second, bytes, cudaMemcpyDeviceToDevice, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
 		cudaFree(old_mem);
 	}
@@ -375,7 +399,7 @@ public:
 		const int nlists = 2 * MAX_ACTI + 6;
 		size_t one       = align_up(sizeof(int32_t) * (size_t) cap);
 		size_t faces     = align_up(sizeof(int32_t) * (size_t) cap * NF);
-		DG_CUDA(cudaMalloc(&list_mem_, one * (nlists + 2) + 3 * faces));
+		DG_CUDA(cudaMalloc(&list_mem_, one * nlists + 3 * faces));
 		char *b = (char *) list_mem_;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			Ls_.clu[l] = (int32_t *) b;
@@ -394,10 +418,6 @@ public:
 		Ls_.fresh   = (int32_t *) b;
 		b += one;
 		Ls_.upd     = (int32_t *) b;
-		b += one;
-		Ls_.dirty   = (int32_t *) b;
-		b += one;
-		Ls_.seed    = (int32_t *) b;
 		b += one;
 		Ls_.task    = (int32_t *) b;
 		b += faces;
@@ -471,7 +491,8 @@ public:
 		const int g = grid_for(n);
 		k_init_cells<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n, d_cnt_);
 		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
-		all_avgs();
+		// every memo starts stale: mod = 1 > cst = 0
+		k_fill_i32<<<grid_for(P_.cap), BLOCK, 0, st_>>>(P_.mod, 1, P_.cap);
 		launch_slope(d_leaves_, n);
 		if constexpr (M::MULTI) {
 			multiphase_aux(d_leaves_, n);
@@ -537,28 +558,9 @@ private:
 		}
 	}
 
-	// Subtree means of every non-leaf node, deepest level first (construction, after re-sort and
-	// compaction); pending refresh marks are dropped.
-	void all_avgs() {
-		const int top = h_cnt_->top;
-		for (int l = max_tree_level_; l >= 0; --l)
-			run_k(DG_K_OTHER, 0, [&] { k_avg_all_level<M><<<grid_for(top), BLOCK, 0, st_>>>(P_, top, l); });
-		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_dirty, 0, sizeof(int), st_));
-		DG_CUDA(cudaMemsetAsync(P_.pending, 0, sizeof(int32_t) * (size_t) P_.cap, st_));
-		epoch_++;
-	}
-
-	// Subtree means of the queued non-leaf nodes, deepest level first.
-	void refresh_avgs(long long bound) {
-		const int grid = grid_for(bound);
-		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_seed, 0, sizeof(int), st_));
-		run_k(DG_K_OTHER, 0, [&] { k_avg_seed<<<grid, BLOCK, 0, st_>>>(P_, Ls_.dirty, &d_cnt_->n_dirty, Ls_.seed, &d_cnt_->n_seed); });
-		run_k(DG_K_OTHER, 0, [&] { k_avg_climb<M><<<grid, BLOCK, 0, st_>>>(P_, Ls_.seed, &d_cnt_->n_seed); });
-		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_dirty, 0, sizeof(int), st_));
-		epoch_++;
-	}
-
+	// Neighbour values of the list (kept for the estimator), then slopes.
 	void launch_slope(const int32_t *list, int n) {
+		k_nbvals<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, list, n, ++epoch_, d_cnt_);
 		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
 	}
@@ -581,9 +583,9 @@ private:
 	void substep(int L) {
 		const int n      = h_cnt_->clu[L];
 		const double dtL = global_dt_ / (double) (1 << L);
-		// room for every cell of the cluster to split
-		const long long need = (long long) h_cnt_->top + (long long) NC * n + 16;
-		if (need > P_.cap) grow_pool((int) std::min<long long>(std::max<long long>(need, (long long) P_.cap * 3 / 2), 2000000000LL));
+		// A split takes 2^D new slots. When the pool cannot take a split of every cluster cell, the
+		// split requests are read back after the indicator and the pool grown to fit them.
+		const bool tight = (long long) h_cnt_->top + (long long) NC * n + 16 > P_.cap;
 		const int stamp_recv = ++stamp_;
 		const int stamp_upd  = ++stamp_;
 		// n_recv .. n_btask and status
@@ -604,10 +606,10 @@ private:
 			k_flux_receive<M><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
-			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, epoch_, Ls_.dirty, d_cnt_);
-			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, epoch_, Ls_.dirty, d_cnt_);
+			const int e = ++epoch_;
+			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e, d_cnt_);
+			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e, d_cnt_);
 		});
-		refresh_avgs((long long) n / 4 + (long long) NC * h_cnt_->n_split + 1);
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) {
 			multiphase_aux(list, n);
@@ -616,14 +618,23 @@ private:
 		run_k(DG_K_ESTIMATE, n, [&] {
 			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
 		});
+		if (tight) {
+			sync_counters();
+			check_status();
+			const long long need = (long long) h_cnt_->top + (long long) NC * h_cnt_->n_split + 16;
+			if (need > P_.cap) {
+				const long long want = std::max(need + need / 4, (long long) P_.cap * 5 / 4);
+				grow_pool((int) std::min<long long>(want, 2000000000LL));
+				list = Ls_.clu[L];
+			}
+		}
 		const int gf = grid_for((long long) n * (NC + 1));
 		run_k(DG_K_REGRID, n, [&] { k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_); });
 		run_k(DG_K_REGRID, 0, [&] {
-			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, epoch_, Ls_.dirty, d_cnt_);
+			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, ++epoch_, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
-			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, epoch_, Ls_.dirty,
-			                                   d_cnt_);
+			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, ++epoch_, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
 			k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
@@ -764,7 +775,6 @@ public:
 		std::swap(P_, S_);
 		std::swap(pool_mem_, shadow_mem_);
 		attach_derived();
-		all_avgs();
 		int first = 1;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			const int cnt = h_cnt_->clu[l];
@@ -795,22 +805,20 @@ private:
 		DG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, keep, newidx, top + 1, st_));
 		int new_top = 0;
 		DG_CUDA(cudaMemcpyAsync(&new_top, newidx + top, sizeof(int), cudaMemcpyDeviceToHost, st_));
-		Pool NP{};
-		void *mem = carve_pool(NP, P_.cap);
-		auto fo = fields(P_), fn = fields(NP);
+		// compact into the re-sort's second pool (zeroed), which then becomes the live one
+		if (!shadow_mem_) shadow_mem_ = carve_pool(S_, P_.cap);
+		else DG_CUDA(cudaMemsetAsync(shadow_mem_, 0, pool_bytes(P_.cap), st_));
+		auto fo = fields(P_), fn = fields(S_);
 		for (size_t k = 0; k < fo.size(); ++k) {
 			if (fo[k].comps <= 0) continue;
 			k_gc_move<<<g, BLOCK, 0, st_>>>((const char *) *fo[k].ptr, (char *) *fn[k].ptr, (int) fo[k].elem, fo[k].comps,
 			                                 P_.cap, top, keep, newidx);
 		}
 		DG_CUDA(cudaStreamSynchronize(st_));
-		k_gc_remap<D><<<grid_for(new_top), BLOCK, 0, st_>>>(NP, new_top, keep, newidx);
-		cudaFree(pool_mem_);
-		pool_mem_ = mem;
-		P_        = NP;
+		k_gc_remap<D><<<grid_for(new_top), BLOCK, 0, st_>>>(S_, new_top, keep, newidx);
+		std::swap(P_, S_);
+		std::swap(pool_mem_, shadow_mem_);
 		attach_derived();
-		h_cnt_->top = new_top;
-		all_avgs();
 		// full ACTI reassignment
 		Counters z{};
 		z.top    = new_top;

@@ -490,7 +490,7 @@ __device__ __forceinline__ double face_term(const double *F, int pl, int q) {
 // t_slope is not maintained.
 template<class M, bool V>
 __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, const int32_t *list, int n, double dtL,
-                                                            int epoch, int32_t *dirty, Counters *cnt) {
+                                                            int epoch, Counters *cnt) {
 	constexpr int E = M::E, NF = 2 * M::D;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
@@ -564,78 +564,52 @@ __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, co
 		}
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
 		P.t[i] = P.t[i] + dtL;
-		mark_from(P, P.parent[i], epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
+		mark_up(P, P.parent[i], epoch);
 	}
 }
 
-// Subtree-mean refresh, first pass: the queued nodes without queued children start the refresh.
-static __global__ void k_avg_seed(Pool P, const int32_t *dirty, const int *n_ptr, int32_t *seed, int *n_seed) {
-	const int n = *n_ptr;
-	for (int t = gtid(); t < n; t += gstride()) {
-		const int a = dirty[t];
-		if (P.pending[a] == 0) seed[atomicAdd(n_seed, 1)] = a;
-	}
-}
 
-// Second pass: each start node is refreshed, then its thread climbs while it is the last queued child
-// to finish, refreshing each ancestor after all of that ancestor's queued children (children before
-// parents, as the recursion of interpolate_p orders them).
+// Neighbour values of a cell list: for each (cell, face) the neighbour's primitive state and time as
+// compute_slope and the error estimator see them (the leaf's own, or the mean over a non-leaf
+// neighbour's subtree), the centre distance 0.5 (h + h_n), and packed neighbour facts. One thread per
+// (cell, face), so the dependent neighbour loads of all faces proceed in parallel; the slope and
+// estimation stages then read their cell's 2D entries contiguously.
 template<class M>
-__global__ void k_avg_climb(Pool P, const int32_t *seed, const int *n_ptr) {
-	const int n = *n_ptr;
-	for (int t = gtid(); t < n; t += gstride()) {
-		int a = seed[t];
-		for (int guard = 0; guard < MAX_TREE; ++guard) {
-			const uint32_t fl = P.flags[a];
-			if (!(fl & F_LEAF) && !(fl & F_GARBAGE)) refresh_avg<M>(P, a);
-			__threadfence();
-			const int b = P.parent[a];
-			if (b == 0 || atomicSub(&P.pending[b], 1) != 1) break;
-			__threadfence();  // the other children's means, written before their own decrements
-			a = b;
+struct Nbv {
+	static constexpr int W = (M::E + 2 + 1) & ~1;  // p[E], t, centre distance
+};
+constexpr int32_t NB_LEAF = 1 << 8, NB_PRESENT = 1 << 9;
+
+__device__ __forceinline__ int nb_level(int32_t code) { return code & 0xff; }
+__device__ __forceinline__ int nb_acti(int32_t code) { return ((code >> 16) & 0xff) - 1; }
+
+template<class M>
+__global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch, Counters *cnt) {
+	constexpr int E = M::E, NF = 2 * M::D, W = Nbv<M>::W;
+	const long long total = (long long) n * NF;
+	for (long long t = gtid(); t < total; t += gstride()) {
+		const int slot = (int) (t / NF), f = (int) (t % NF);
+		const int i    = list[slot];
+		const int nb   = P.nbr[(size_t) f * P.cap + i];
+		int32_t *oi    = P.nbi + t;
+		if (nb == 0) {
+			*oi = 0;
+			continue;
 		}
-	}
-}
-
-// Subtree means of every non-leaf node of one tree level.
-template<class M>
-__global__ void k_avg_all_level(Pool P, int top, int level) {
-	for (int a = 1 + gtid(); a < top; a += gstride()) {
-		if (P.level[a] != level) continue;
-		const uint32_t fl = P.flags[a];
-		if (!(fl & F_LEAF) && !(fl & F_GARBAGE)) refresh_avg<M>(P, a);
-	}
-}
-
-// State of the neighbour across face (dim, dir) as compute_slope sees it (impl/slopes.hpp:208-246):
-// a ghost at distance h for boundaries, the recursive child mean for finer neighbours.
-template<class M>
-__device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int i, int dim, int dir,
-                           const double *pc, double *pv, double &x, double &tv) {
-	const int cap = P.cap;
-	const int nb  = P.nbr[(size_t) (2 * dim + dir) * cap + i];
-	const double h = C.size[P.level[i]];
-	if (nb == 0) {
-		const int b = P.bc[(size_t) (2 * dim + dir) * cap + i];
-		if (b < 0) {
-			set_status(status, ST_MISSING_BC);
-			for (int q = 0; q < M::E; ++q) pv[q] = pc[q];
+		const uint32_t fl = P.flags[nb];
+		const int ln      = P.level[nb];
+		double v[E + 1];
+		if (!(fl & F_LEAF)) {
+			interp_pt<M>(P, &cnt->status, nb, epoch, v);
 		} else {
-			boundary_value<M>(C.m, B, b, pc, P.t[i], pv);
+			load_p<M>(P, nb, v);
+			v[E] = P.t[nb];
 		}
-		x  = dir == 0 ? -h : h;
-		tv = P.t[i];
-		return;
+		double *o = P.nbv + t * W;
+		for (int q = 0; q <= E; ++q) o[q] = v[q];
+		o[E + 1] = 0.5 * (C.size[P.level[i]] + C.size[ln]);
+		*oi      = NB_PRESENT | ((fl & F_LEAF) ? NB_LEAF : 0) | ln | ((P.acti[nb] + 1) << 16);
 	}
-	if (!(P.flags[nb] & F_LEAF)) {
-		interp_p<M>(P, status, nb, pv);
-		tv = interp_t<M>(P, nb);
-	} else {
-		load_p<M>(P, nb, pv);
-		tv = P.t[nb];
-	}
-	const double hn = C.size[P.level[nb]];
-	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
 }
 
 // compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients (only read by the viscous
@@ -643,19 +617,43 @@ __device__ void slope_side(const Pool &P, const Consts &C, const BcTable &B, uin
 // slope rows) to `out`; the gradients go to the pool.
 template<class M, bool V = M::VISC>
 __device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim,
-                                              int i, double *out) {
-	constexpr int E = M::E, D = M::D;
+                                              int i, int slot, double *out) {
+	constexpr int E = M::E, D = M::D, NF = 2 * D, NW = Nbv<M>::W;
 	using R = Rec<M>;
 	const int cap = P.cap;
 	double pc[E];
 	load_p<M>(P, i, pc);
+	const double h = C.size[P.level[i]];
 	double slope[D * E];
 #pragma unroll
 	for (int dim = 0; dim < D; ++dim) {
 		double pn[E], pp[E], xn, xp, tn, tp;
 		const double xc = 0.0;
-		slope_side<M>(P, C, B, status, i, dim, 0, pc, pn, xn, tn);
-		slope_side<M>(P, C, B, status, i, dim, 1, pc, pp, xp, tp);
+		// impl/slopes.hpp:24-58: a ghost at distance h for boundaries, else the neighbour value
+#pragma unroll
+		for (int dir = 0; dir < 2; ++dir) {
+			const int f = 2 * dim + dir;
+			double *pv = dir == 0 ? pn : pp;
+			double &x  = dir == 0 ? xn : xp;
+			double &tv = dir == 0 ? tn : tp;
+			const int32_t code = P.nbi[(size_t) slot * NF + f];
+			if (!(code & NB_PRESENT)) {
+				const int b = P.bc[(size_t) f * cap + i];
+				if (b < 0) {
+					set_status(status, ST_MISSING_BC);
+					for (int q = 0; q < E; ++q) pv[q] = pc[q];
+				} else {
+					boundary_value<M>(C.m, B, b, pc, P.t[i], pv);
+				}
+				x  = dir == 0 ? -h : h;
+				tv = P.t[i];
+			} else {
+				const double *nv = P.nbv + ((size_t) slot * NF + f) * NW;
+				for (int q = 0; q < E; ++q) pv[q] = nv[q];
+				tv = nv[E];
+				x  = dir == 0 ? -nv[E + 1] : nv[E + 1];
+			}
+		}
 		for (int q = 0; q < E; ++q) {
 			double sn = (pc[q] - pn[q]) / (xc - xn);
 			double sp = (pp[q] - pc[q]) / (xp - xc);
@@ -693,7 +691,7 @@ __global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n,
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i = list[tid];
 		double out[K];
-		compute_slope<M, V>(P, C, B, &cnt->status, lim, i, out);
+		compute_slope<M, V>(P, C, B, &cnt->status, lim, i, tid, out);
 		double2 *dst = reinterpret_cast<double2 *>(rec_of(P, i, R::W));
 #pragma unroll
 		for (int k = 0; k < K / 2; ++k) dst[k] = make_double2(out[2 * k], out[2 * k + 1]);
@@ -740,7 +738,7 @@ __device__ bool can_split_at(const Pool &P, const Consts &C, int i) {
 template<class M>
 __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list,
                            Counters *cnt) {
-	constexpr int E = M::E, D = M::D;
+	constexpr int E = M::E, D = M::D, NF = 2 * D;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i  = list[tid];
@@ -754,26 +752,26 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 			for (int q = 0; q < E; ++q) d2[q] = pc[q] * -2.0;
 			bool missing = false;
 			for (int dir = 0; dir < 2; ++dir) {
-				const int nb = P.nbr[(size_t) (2 * dim + dir) * cap + i];
-				if (nb == 0) {
+				const int f = 2 * dim + dir;
+				const int32_t code = P.nbi[(size_t) tid * NF + f];
+				if (!(code & NB_PRESENT)) {
 					missing = true;
 					break;
 				}
+				const double *nv = P.nbv + ((size_t) tid * NF + f) * Nbv<M>::W;
 				double v[E];
-				if (!(P.flags[nb] & F_LEAF)) {
-					interp_p<M>(P, &cnt->status, nb, v);
-				} else if (P.level[nb] < li) {
+				for (int q = 0; q < E; ++q) v[q] = nv[q];
+				if ((code & NB_LEAF) && nb_level(code) < li) {
+					// a coarser leaf: its state extrapolated to the same-level position
+					const int nb = P.nbr[(size_t) f * cap + i];
 					double x[D];
 					for (int d = 0; d < D; ++d) x[d] = at(P.center, cap, d, i) + (d == dim ? h * (2 * dir - 1.0) : 0.0 * h);
 					if (C.periodic[dim] && dir == 0 && x[dim] < -0.5 * C.active[dim]) x[dim] += C.active[dim];
 					if (C.periodic[dim] && dir == 1 && x[dim] > 0.5 * C.active[dim]) x[dim] -= C.active[dim];
-					load_p<M>(P, nb, v);
 					for (int d = 0; d < D; ++d) {
 						const double off = x[d] - at(P.center, cap, d, nb);
 						for (int q = 0; q < E; ++q) v[q] = v[q] + rec_slope<M>(P, nb, d, q) * off;
 					}
-				} else {
-					load_p<M>(P, nb, v);
 				}
 				for (int q = 0; q < E; ++q) d2[q] = d2[q] + v[q];
 			}
@@ -800,17 +798,17 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 		const bool want_split = (error > C.max_err && (fl & F_CAN_SPLIT)) || (fl & F_SHOULD_SPLIT);
 		if (want_split) {
 			bool ready = true;
-			for (int f = 0; f < 2 * D; ++f) {
-				const int nb = P.nbr[(size_t) f * cap + i];
-				if (nb != 0 && P.level[nb] < li - 1) ready = false;
+			for (int f = 0; f < NF; ++f) {
+				const int32_t code = P.nbi[(size_t) tid * NF + f];
+				if ((code & NB_PRESENT) && nb_level(code) < li - 1) ready = false;
 			}
 			if (ready) op |= OP_SPLIT;
 		}
 		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1) {
 			bool ok = true;
-			for (int f = 0; f < 2 * D; ++f) {
-				const int nb = P.nbr[(size_t) f * cap + i];
-				if (nb != 0 && (!(P.flags[nb] & F_LEAF) || P.acti[nb] > L)) ok = false;
+			for (int f = 0; f < NF; ++f) {
+				const int32_t code = P.nbi[(size_t) tid * NF + f];
+				if ((code & NB_PRESENT) && (!(code & NB_LEAF) || nb_acti(code) > L)) ok = false;
 			}
 			if (ok) op |= OP_UCAND;
 		}
@@ -849,7 +847,7 @@ __global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int3
 // rhs, and join the running cluster.
 template<class M>
 __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
-                        int epoch, int32_t *dirty, Counters *cnt) {
+                        int epoch, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D;
 	const int n   = *n_ptr;
 	const int cap = P.cap;
@@ -926,7 +924,7 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 			append(fresh, &cnt->n_new, s, cap, &cnt->status);
 		}
 		P.flags[par] &= ~(F_LEAF | F_SHOULD_SPLIT);
-		mark_from(P, par, epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
+		mark_up(P, par, epoch);
 	}
 }
 
@@ -935,7 +933,7 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 // stale gradient, as interpolated_cell does not reset it) and keeps its old slope and rhs.
 template<class M>
 __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh,
-                          int epoch, int32_t *dirty, Counters *cnt) {
+                          int epoch, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D, G = M::G;
 	const int n   = *n_ptr;
 	const int cap = P.cap;
@@ -985,7 +983,7 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		P.acti[par]  = (int8_t) L;
 		P.clu[par]   = (int8_t) L;
 		append(fresh, &cnt->n_new, par, cap, &cnt->status);
-		mark_from(P, P.parent[par], epoch, dirty, &cnt->n_dirty, cap, &cnt->status);
+		mark_up(P, P.parent[par], epoch);
 	}
 }
 
@@ -1475,6 +1473,10 @@ __global__ void k_remap_links(Pool P, int top, const int32_t *newidx) {
 		for (int c = 0; c < NC; ++c) P.child[(size_t) c * cap + j] = newidx[P.child[(size_t) c * cap + j]];
 		for (int f = 0; f < NF; ++f) P.nbr[(size_t) f * cap + j] = newidx[P.nbr[(size_t) f * cap + j]];
 	}
+}
+
+static __global__ void k_fill_i32(int32_t *a, int v, int n) {
+	for (int j = gtid(); j < n; j += gstride()) a[j] = v;
 }
 
 static __global__ void k_fill_range(int32_t *list, int first, int n) {

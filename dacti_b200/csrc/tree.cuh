@@ -52,74 +52,93 @@ __device__ int find_neighbor(const Pool &P, const Consts &C, int i, int dim, int
 
 // Subtree means of non-leaf nodes. Domain::interpolate_p / interpolate_t (integrator/domain.hpp:
 // 84-148) return, for a non-leaf node, the mean over its active children of the child's value (a
-// leaf's own state, or recursively the child's mean). The pool keeps that mean for every non-leaf
-// node in `avg` ({p[E], t}), refreshed bottom-up whenever a leaf below changes, so that a lookup is
-// one record read instead of a walk over the subtree; the refresh adds the children in slot order
-// from +0 and divides by their count, exactly as the recursion does.
+// leaf's own state, or recursively the child's mean). The walk below computes the same recursion
+// (children in slot order, sums from +0, divided by the count), but memoises every non-leaf mean it
+// forms in `avg` with the epoch of the computing kernel (`cst`), and reuses a memo instead of
+// descending when no leaf below has changed since (`mod`, stamped upwards by every kernel that changes
+// a leaf's state or the tree). A memo is only trusted when a previous kernel wrote it, so threads of
+// one kernel never read each other's partial writes.
 template<class M>
 struct Avg {
 	static constexpr int W = (M::E + 1 + 1) & ~1;  // p[E], t, padded to 16 bytes
 };
 
+__device__ __forceinline__ bool memo_ok(const Pool &P, int n, int epoch) {
+	const int c = __ldcg(P.cst + n);
+	return c > __ldcg(P.mod + n) && c < epoch;
+}
+
+// Mean primitive state and time of node n ({p[E], t} in out); `epoch` is the calling kernel's.
 template<class M>
-__device__ __forceinline__ void interp_p(const Pool &P, uint32_t *, int n, double *out) {
+__device__ void interp_pt(const Pool &P, uint32_t *status, int n, int epoch, double *out) {
+	constexpr int E = M::E, NC = 1 << M::D, AW = Avg<M>::W;
 	if (P.flags[n] & F_LEAF) {
 		load_p<M>(P, n, out);
+		out[E] = P.t[n];
 		return;
 	}
-	const double *a = P.avg + (size_t) n * Avg<M>::W;
-	for (int q = 0; q < M::E; ++q) out[q] = a[q];
-}
-
-template<class M>
-__device__ __forceinline__ double interp_t(const Pool &P, int n) {
-	if (P.flags[n] & F_LEAF) return P.t[n];
-	return P.avg[(size_t) n * Avg<M>::W + M::E];
-}
-
-// Recomputes the subtree mean of non-leaf node n from its children (whose own means are current).
-// Child means may have been written moments before by threads on other SMs, so they are read past
-// the non-coherent L1.
-template<class M>
-__device__ __forceinline__ void refresh_avg(const Pool &P, int n) {
-	constexpr int E = M::E, NC = 1 << M::D;
-	double f[E + 1];
-	for (int q = 0; q <= E; ++q) f[q] = 0.0;
-	int cnt = 0;
-	for (int c = 0; c < NC; ++c) {
-		const int ch = P.child[(size_t) c * P.cap + n];
-		const uint32_t fl = P.flags[ch];
-		if (!(fl & F_ACTIVE)) continue;
-		if (fl & F_LEAF) {
-			for (int q = 0; q < E; ++q) f[q] = f[q] + at(P.p, P.cap, q, ch);
-			f[E] = f[E] + P.t[ch];
-		} else {
-			const double *a = P.avg + (size_t) ch * Avg<M>::W;
-			for (int q = 0; q <= E; ++q) f[q] = f[q] + __ldcg(a + q);
-		}
-		cnt++;
+	if (memo_ok(P, n, epoch)) {
+		for (int q = 0; q <= E; ++q) out[q] = __ldcg(P.avg + (size_t) n * AW + q);
+		return;
 	}
-	double *a = P.avg + (size_t) n * Avg<M>::W;
-	for (int q = 0; q <= E; ++q) a[q] = f[q] / (double) cnt;
+	struct Frame {
+		int node, next, cnt;
+		double f[E + 1];
+	};
+	Frame st[MAX_TREE];
+	st[0].node = n;
+	st[0].next = 0;
+	st[0].cnt  = 0;
+	for (int q = 0; q <= E; ++q) st[0].f[q] = 0.0;
+	int sp = 1;
+	while (true) {
+		Frame &fr = st[sp - 1];
+		if (fr.next < NC) {
+			const int c = P.child[(size_t) fr.next * P.cap + fr.node];
+			fr.next++;
+			const uint32_t fl = P.flags[c];
+			if (!(fl & F_ACTIVE)) continue;
+			if (fl & F_LEAF) {
+				for (int q = 0; q < E; ++q) fr.f[q] = fr.f[q] + at(P.p, P.cap, q, c);
+				fr.f[E] = fr.f[E] + P.t[c];
+				fr.cnt++;
+			} else if (memo_ok(P, c, epoch)) {
+				for (int q = 0; q <= E; ++q) fr.f[q] = fr.f[q] + __ldcg(P.avg + (size_t) c * AW + q);
+				fr.cnt++;
+			} else if (sp < MAX_TREE) {
+				Frame &nf = st[sp++];
+				nf.node   = c;
+				nf.next   = 0;
+				nf.cnt    = 0;
+				for (int q = 0; q <= E; ++q) nf.f[q] = 0.0;
+			} else {
+				set_status(status, ST_DEPTH);
+			}
+			continue;
+		}
+		double r[E + 1];
+		for (int q = 0; q <= E; ++q) r[q] = fr.f[q] / (double) fr.cnt;
+		double *memo = P.avg + (size_t) fr.node * AW;
+		for (int q = 0; q <= E; ++q) memo[q] = r[q];
+		P.cst[fr.node] = epoch;
+		--sp;
+		if (sp == 0) {
+			for (int q = 0; q <= E; ++q) out[q] = r[q];
+			return;
+		}
+		Frame &pf = st[sp - 1];
+		for (int q = 0; q <= E; ++q) pf.f[q] = pf.f[q] + r[q];
+		pf.cnt++;
+	}
 }
 
-// Queues a node whose subtree changed and its ancestors for the next refresh. Every queued node counts
-// its queued children in `pending`; a walk stops at the first ancestor that an earlier walk of the same
-// refresh epoch queued (that walk went on to the root). `first` is the lowest node whose mean changed:
-// the parent of a changed leaf, or a cell that has just been split.
-__device__ __forceinline__ void mark_from(const Pool &P, int first, int epoch, int32_t *dirty, int *n_dirty, int cap,
-                                          uint32_t *status) {
-	int a = first;
-	if (a == 0 || atomicExch(&P.mark[a], epoch) == epoch) return;
-	for (int guard = 0; guard < MAX_TREE; ++guard) {
-		const int pos = atomicAdd(n_dirty, 1);
-		if (pos < cap) dirty[pos] = a;
-		else atomicOr(status, ST_CAPACITY);
-		const int b = P.parent[a];
-		if (b == 0) return;
-		atomicAdd(&P.pending[b], 1);
-		if (atomicExch(&P.mark[b], epoch) == epoch) return;
-		a = b;
+// Stamps a changed subtree: `first` (the parent of a changed leaf, or a cell that has just been
+// split) and its ancestors get mod = epoch; a walk stops at the first ancestor already stamped in this
+// epoch (that walk continues to the root).
+__device__ __forceinline__ void mark_up(const Pool &P, int first, int epoch) {
+	for (int a = first, guard = 0; a != 0 && guard < MAX_TREE; a = P.parent[a], ++guard) {
+		if (__ldcg(P.mod + a) == epoch) break;
+		P.mod[a] = epoch;
 	}
 }
 
