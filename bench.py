@@ -51,7 +51,8 @@ def parse_args():
     ap.add_argument("--profile-substep", type=int, default=-1,
                     help="bracket only this substep of the first timed step of the last form with "
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off); -2 brackets the whole timed "
-                         "region of the last form")
+                         "region of the last form, -3 the substep that ran the largest cluster in the last "
+                         "warm-up step")
     return ap.parse_args()
 
 
@@ -209,8 +210,16 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
     solver.set_stream(stream.cuda_stream)
     solver.set_form(form)
     solver.set_profiling(True)
-    for _ in range(args.warmup):
-        solver.integrate()
+    sizes = []
+    for k in range(args.warmup):
+        if k == args.warmup - 1:
+            solver.integrate(lambda _s, level, at, n, dt, size: sizes.append((size, level)))
+        else:
+            solver.integrate()
+    if profile == -3 and sizes:
+        profile = max(range(len(sizes)), key=lambda j: sizes[j][0])
+        print(f"profiled substep {profile}: level {sizes[profile][1]}, {sizes[profile][0]} cells in the warm-up "
+              f"step", file=sys.stderr)
     st0 = solver.stats()
     if world > 1:
         dist.barrier()
