@@ -317,14 +317,12 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     launches = max(kl["update"], 1)
     achieved = (b_per * kc["update"] / launches) / (upd_ms * 1e-3 / launches) / 1e9 if upd_ms > 0 else 0.0
     traffic = None
-    tpath = os.path.join(HERE, "profiles", "gather_update_traffic.json")
+    tpath = os.path.join(HERE, "profiles", "gather_update_shock_drop_3d_small.md")
     if os.path.exists(tpath):
-        try:
-            with open(tpath) as f:
-                tj = json.load(f)
-            traffic = tj["dram_bytes_per_cell"] * (kc["update"] / launches)
-        except Exception:
-            traffic = None
+        with open(tpath) as f:
+            for line in f:
+                if line.startswith("traffic_dram_bytes_per_cell"):
+                    traffic = float(line.split("=")[1]) * (kc["update"] / launches)
     step_achieved = b_per * chosen["updates"] / (chosen["ms"] * 1e-3) / 1e9
     roofline = {
         "bound": "hbm", "kernel": "k_gather_update (face-flux gather + cell update)", "achieved": achieved,
