@@ -209,7 +209,6 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
     solver = Solver(case, device=local_rank)
     solver.set_stream(stream.cuda_stream)
     solver.set_form(form)
-    solver.set_profiling(True)
     sizes = []
     for k in range(args.warmup):
         if k == args.warmup - 1:
@@ -251,13 +250,19 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
     if world > 1:
         dist.barrier()
     st1 = solver.stats()
+    # per-kernel-kind device times from CUDA events around every launch, over one more global step
+    # outside the timed region (the events add host work per launch)
+    solver.set_profiling(True)
+    solver.integrate()
+    st2 = solver.stats()
+    solver.set_profiling(False)
     out = {
         "ms": ev0.elapsed_time(ev1),
         "updates": float(st1.cell_updates - st0.cell_updates),
         "launches": int(st1.n_launches - st0.n_launches),
-        "kms": {k: st1.kernel_ms[i] - st0.kernel_ms[i] for i, k in enumerate(KERNEL_KINDS)},
-        "kl": {k: st1.kernel_launches[i] - st0.kernel_launches[i] for i, k in enumerate(KERNEL_KINDS)},
-        "kc": {k: st1.kernel_cells[i] - st0.kernel_cells[i] for i, k in enumerate(KERNEL_KINDS)},
+        "kms": {k: st2.kernel_ms[i] - st1.kernel_ms[i] for i, k in enumerate(KERNEL_KINDS)},
+        "kl": {k: st2.kernel_launches[i] - st1.kernel_launches[i] for i, k in enumerate(KERNEL_KINDS)},
+        "kc": {k: st2.kernel_cells[i] - st1.kernel_cells[i] for i, k in enumerate(KERNEL_KINDS)},
         "clocks": clk.summary(),
         "snap": solver.active_cells(),
         "substeps": int(st1.n_substeps - st0.n_substeps),
@@ -343,7 +348,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "plain_fp64": {"value": p_upd / (p_ms * 1e-3), "ms_per_step": p_ms / args.steps,
                        "gpu_launches": plain["launches"], "cells": plain["snap"].n},
         "accuracy": {"density_rel_l1_vs_plain_fp64": err, "bound": 1e-4, "ok": bool(err <= 1e-4),
-                     "grid": f"uniform base level {args.base_level}, after {args.warmup + args.steps} global steps"},
+                     "grid": f"uniform base level {args.base_level}, after {args.warmup + args.steps + 1} global steps"},
     }
 
     # end to end through the public API: host tree -> device, K steps with the per-step scalars read

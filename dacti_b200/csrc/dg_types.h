@@ -107,6 +107,7 @@ struct Pool {
 	double *flux;     // [F][cap]
 	double *err, *maxdt, *cfl;
 	int32_t *stamp;   // per-node dedup stamp for list building
+	uint32_t *fmask;  // faces (bit 2 dim + dir) whose neighbour changed in the running regrid; 0 otherwise
 	uint8_t *op;      // refinement op code
 	double *tmp;      // per-node scratch scalar (Jacobi smoothing)
 	// Per-substep scratch outside the permuted fields:

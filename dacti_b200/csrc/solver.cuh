@@ -299,7 +299,7 @@ public:
 		    {(void **) &P.mod, 4, 1}, {(void **) &P.cst, 4, 1},
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
-		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.op, 1, 1},
+		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.fmask, 4, 1}, {(void **) &P.op, 1, 1},
 		    {(void **) &P.tmp, 8, 1},
 		};
 	}
@@ -587,7 +587,6 @@ private:
 		// split requests are read back after the indicator and the pool grown to fit them.
 		const bool tight = (long long) h_cnt_->top + (long long) NC * n + 16 > P_.cap;
 		const int stamp_recv = ++stamp_;
-		const int stamp_upd  = ++stamp_;
 		// n_recv .. n_btask and status
 		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_recv, 0, (char *) (&d_cnt_->status + 1) - (char *) &d_cnt_->n_recv, st_));
 		const int g        = grid_for(n);
@@ -637,11 +636,10 @@ private:
 			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, ++epoch_, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
-			k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, stamp_upd, Ls_.upd, d_cnt_);
+			k_nbr_fresh<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_new, Ls_.fresh, Ls_.upd, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
-			k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, 0, Ls_.upd,
-			                                                                          d_cnt_);
+			k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, Ls_.upd, d_cnt_);
 		});
 		run_k(DG_K_REASSIGN, n, [&] {
 			k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_);

@@ -991,17 +991,47 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 // boundary get the node found at the same level (or the coarser leaf); a neighbour more than one
 // level coarser is flagged should_split.
 template<class M>
-__device__ void update_neighbors_leaf(const Pool &P, const Consts &C, int i) {
+__device__ void update_neighbor_face(const Pool &P, const Consts &C, int i, int dim, int dir) {
 	const int cap = P.cap;
-	const int li  = P.level[i];
-	for (int dim = 0; dim < M::D; ++dim) {
-		for (int dir = 0; dir < 2; ++dir) {
-			const int f = 2 * dim + dir;
-			if (P.bc[(size_t) f * cap + i] >= 0) continue;
-			const int nb = find_neighbor<M::D>(P, C, i, dim, dir);
-			if (nb == 0 || !(P.flags[nb] & F_ACTIVE)) continue;
-			P.nbr[(size_t) f * cap + i] = nb;
-			if (P.level[nb] < li - 1) atomicOr(&P.flags[nb], (uint32_t) F_SHOULD_SPLIT);
+	const int f   = 2 * dim + dir;
+	if (P.bc[(size_t) f * cap + i] >= 0) return;
+	const int nb = find_neighbor<M::D>(P, C, i, dim, dir);
+	if (nb == 0 || !(P.flags[nb] & F_ACTIVE)) return;
+	P.nbr[(size_t) f * cap + i] = nb;
+	if (P.level[nb] < P.level[i] - 1) atomicOr(&P.flags[nb], (uint32_t) F_SHOULD_SPLIT);
+}
+
+template<class M>
+__device__ void update_neighbors_leaf(const Pool &P, const Consts &C, int i) {
+	for (int dim = 0; dim < M::D; ++dim)
+		for (int dir = 0; dir < 2; ++dir) update_neighbor_face<M>(P, C, i, dim, dir);
+}
+
+// update_neighbors restricted to one face of a node: the leaves of its subtree that touch face
+// (dim, dir) get that face's neighbour recomputed. Used for the neighbours of new cells: a leaf of such a
+// neighbour's subtree that does not touch the face towards the new cell finds the same neighbours as
+// before, so the reference's full subtree update leaves it unchanged.
+template<class M>
+__device__ void update_face_subtree(const Pool &P, const Consts &C, uint32_t *status, int root, int dim, int dir) {
+	constexpr int NC = 1 << M::D, NH = NC / 2;
+	constexpr int CAP = NH * MAX_TREE;
+	int stack[CAP];
+	int sp = 0;
+	stack[sp++] = root;
+	while (sp > 0) {
+		const int x = stack[--sp];
+		const uint32_t fl = P.flags[x];
+		if (fl & F_LEAF) {
+			if (fl & F_ACTIVE) update_neighbor_face<M>(P, C, x, dim, dir);
+			continue;
+		}
+		for (int c = NC - 1; c >= 0; --c) {
+			if (((c >> dim) & 1) != dir) continue;
+			if (sp >= CAP) {
+				set_status(status, ST_DEPTH);
+				break;
+			}
+			stack[sp++] = P.child[(size_t) c * P.cap + x];
 		}
 	}
 }
@@ -1033,9 +1063,9 @@ __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_
 
 // Neighbour repair, first pass (impl/adaptive_refinement.hpp:236-249): new children and coarsened
 // parents, then queue their neighbours for the second pass.
+// Each neighbour is queued once with the mask of its faces towards new cells.
 template<class M>
-__global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *fresh, int stamp, int32_t *upd,
-                            Counters *cnt) {
+__global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *fresh, int32_t *upd, Counters *cnt) {
 	const int n   = *n_ptr;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
@@ -1044,16 +1074,23 @@ __global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *f
 		for (int f = 0; f < 2 * M::D; ++f) {
 			const int nb = P.nbr[(size_t) f * cap + i];
 			if (nb != 0 && ((P.flags[nb] & F_ACTIVE) || !(P.flags[nb] & F_LEAF))) {
-				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(upd, &cnt->n_upd, nb, cap, &cnt->status);
+				if (atomicOr(&P.fmask[nb], 1u << (f ^ 1)) == 0) append(upd, &cnt->n_upd, nb, cap, &cnt->status);
 			}
 		}
 	}
 }
 
+// Neighbour repair, second pass: the queued neighbours' faces towards new cells.
 template<class M>
-__global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, int n_host, const int32_t *list, Counters *cnt) {
-	const int n = n_ptr ? *n_ptr : n_host;
-	for (int tid = gtid(); tid < n; tid += gstride()) update_neighbors_subtree<M>(P, C, &cnt->status, list[tid]);
+__global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, const int32_t *list, Counters *cnt) {
+	const int n = *n_ptr;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int x       = list[tid];
+		const uint32_t m  = P.fmask[x];
+		for (int f = 0; f < 2 * M::D; ++f)
+			if (m & (1u << f)) update_face_subtree<M>(P, C, &cnt->status, x, f >> 1, f & 1);
+		P.fmask[x] = 0;
+	}
 }
 
 // ACTI reassignment (impl/adaptive_refinement.hpp:264-322): per-cell CFL decides whether a cell
