@@ -47,6 +47,10 @@ def parse_args():
     ap.add_argument("--levels", type=int, default=4)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--profile-level", type=int, default=-1,
+                    help="with --profile-substep -3: the largest substep of this ACTI level instead")
+    ap.add_argument("--batch-trees", type=int, default=256, help="trees of the batched 2D Riemann workload")
+    ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--forms", default="fp64,mixed", help="numerical forms to time (the last one is `value`)")
     ap.add_argument("--profile-substep", type=int, default=-1,
                     help="bracket only this substep of the first timed step of the last form with "
@@ -216,7 +220,8 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
         else:
             solver.integrate()
     if profile == -3 and sizes:
-        profile = max(range(len(sizes)), key=lambda j: sizes[j][0])
+        cand = [j for j in range(len(sizes)) if args.profile_level < 0 or sizes[j][1] == args.profile_level]
+        profile = max(cand, key=lambda j: sizes[j][0])
         print(f"profiled substep {profile}: level {sizes[profile][1]}, {sizes[profile][0]} cells in the warm-up "
               f"step", file=sys.stderr)
     st0 = solver.stats()
@@ -269,6 +274,50 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
     }
     solver.close()
     return out
+
+
+def batched_run(args, local_rank: int, world: int) -> dict:
+    """Batched 2D Euler quadtree Riemann problems (seeded, see cases.riemann_batch): one global step of
+    every tree per call of dg_step_many (host threads, one stream per tree), against the same trees
+    stepped one after another on one host thread. Mixed form."""
+    import torch
+    from dacti_b200 import cases
+    from dacti_b200.solver import Solver, step_many
+
+    threads = 32
+    batch = cases.riemann_batch(args.batch_trees, seed=3)
+    solvers = [Solver(c, device=local_rank) for c in batch]
+    for s in solvers:
+        s.set_form("mixed")
+    step_many(solvers, threads=threads)  # warm-up; every solver gets its own stream here
+
+    def updates():
+        return float(sum(s.stats().cell_updates for s in solvers))
+
+    torch.cuda.synchronize()
+    u0, t0 = updates(), time.perf_counter()
+    for _ in range(args.steps):
+        step_many(solvers, threads=threads)
+    torch.cuda.synchronize()
+    b_sec, b_upd = time.perf_counter() - t0, updates() - u0
+    u0, t0 = updates(), time.perf_counter()
+    for s in solvers:
+        s.integrate()
+    torch.cuda.synchronize()
+    s_sec, s_upd = time.perf_counter() - t0, updates() - u0
+    cells = sum(s.n_active_cells() for s in solvers)
+    for s in solvers:
+        s.close()
+    b_ms, b_u = reduce_ranks(b_sec * 1e3, b_upd, world)
+    s_ms, s_u = reduce_ranks(s_sec * 1e3, s_upd, world)
+    return {
+        "workload": f"{args.batch_trees} independent 2D Euler quadtree Riemann problems, base 2^k, k ~ U{{5..8}}, "
+                    f"+2..4 levels, seeded quadrant states (seed 3), LTS, mixed form",
+        "value": b_u / (b_ms * 1e-3), "unit": UNIT, "steps": args.steps, "threads": threads,
+        "timing": "host wall clock around synchronous dg_step_many calls (each tree synchronises per substep)",
+        "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
+        "speedup": (b_u / b_ms) / (s_u / s_ms) if s_u > 0 else None, "active_cells": cells,
+    }
 
 
 def reduce_ranks(ms: float, updates: float, world: int):
@@ -376,6 +425,9 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
                          "h2d_bytes_per_step": int(h2d / args.steps), "d2h_bytes_per_step": int(d2h / args.steps),
                          "includes": "solver construction from the host tree, K steps, read-back of all cells"}
         s2.close()
+
+    if not args.no_batched:
+        result["batched"] = batched_run(args, local_rank, world)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_RUNNER):
         threads = host_threads()

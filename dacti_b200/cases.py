@@ -64,6 +64,40 @@ def lax_liu3(base_level: int = 6, levels: int = 3, thresholds=(0.02, 0.05), max_
     return Case(build_tree(spec), prm)
 
 
+def riemann_batch(n_trees: int = 256, seed: int = 3, base_levels=(5, 8), extra_levels=(2, 4),
+                  thresholds=(0.02, 0.05), max_cfl: float = 0.5) -> list:
+    """Config 3: independent 2D Euler quadtree Riemann problems on the unit square, split at x = y = 0.
+
+    Per tree, seeded: base grid 2^k x 2^k with k ~ U{base_levels}, 2-4 extra levels, and four quadrant
+    states with rho ~ U(0.1, 2), p ~ U(0.02, 2), u, v ~ U(-1.5, 1.5); zero-gradient boundaries, CFL
+    `max_cfl`, density-weighted Laplacian indicator. Each tree is one Integrator of the reference.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    shape = ModelShape(ModelId.EULER, 2)
+    for _ in range(n_trees):
+        base = int(rng.integers(base_levels[0], base_levels[1] + 1))
+        levels = int(rng.integers(extra_levels[0], extra_levels[1] + 1))
+        q = np.empty((4, 4))
+        q[:, 0] = rng.uniform(0.1, 2.0, 4)
+        q[:, 1] = rng.uniform(-1.5, 1.5, 4)
+        q[:, 2] = rng.uniform(-1.5, 1.5, 4)
+        q[:, 3] = rng.uniform(0.02, 2.0, 4)
+
+        def x2p(c: np.ndarray, q=q) -> np.ndarray:
+            x, y = c[:, 0], c[:, 1]
+            k = np.where(x > 0, np.where(y > 0, 0, 3), np.where(y > 0, 1, 2))
+            return q[k].copy()
+
+        spec = SceneSpec(shape, (1.0, 1.0), base, base + levels, x2p, _zg_box(2))
+        prm = SolverParams(
+            side_length=1.0, active_size=(1.0, 1.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
+            error_threshold=thresholds, max_level=base + levels, min_level=base, weights=(1.0, 0.0, 0.0, 0.0),
+        )
+        out.append(Case(build_tree(spec), prm))
+    return out
+
+
 def normal_shock(rho1: float, p1: float, mach: float, gamma: float = 1.4, P0: float = 0.0):
     """Post-shock (rho, u, p) behind a normal shock moving into gas at rest.
 

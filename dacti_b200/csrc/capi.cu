@@ -1,7 +1,10 @@
 // extern "C" entry points of include/dacti_gpu.h.
 #include "capi_internal.h"
 
+#include <atomic>
 #include <string>
+#include <thread>
+#include <vector>
 
 namespace {
 thread_local std::string g_create_error;
@@ -57,6 +60,32 @@ int dg_set_stream(dg_solver *s, void *stream) {
 int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) {
 	if (!s || !force_break || !global_dt) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->step(signal, force_break, global_dt, fn, user); });
+}
+
+int dg_step_many(dg_solver **s, int n, int threads, int signal, int *force_break, double *global_dt, int *status) {
+	if (!s || n < 0 || threads < 1 || !force_break || !global_dt || !status) return DG_ERR_ARG;
+	for (int k = 0; k < n; ++k)
+		if (!s[k]) return DG_ERR_ARG;
+	// every solver on a stream of its own, so that the solvers' kernels can overlap on the device
+	for (int k = 0; k < n; ++k) {
+		const int rc = guarded(s[k], [&] { s[k]->impl->own_stream(); });
+		if (rc != DG_OK) return rc;
+	}
+	std::atomic<int> next{0};
+	auto worker = [&] {
+		for (int k = next++; k < n; k = next++) {
+			force_break[k] = 0;
+			status[k]      = guarded(s[k], [&] { s[k]->impl->step(signal, &force_break[k], &global_dt[k], nullptr, nullptr); });
+		}
+	};
+	const int nt = threads < n ? threads : (n > 0 ? n : 1);
+	std::vector<std::thread> pool;
+	for (int t = 1; t < nt; ++t) pool.emplace_back(worker);
+	worker();
+	for (auto &th: pool) th.join();
+	for (int k = 0; k < n; ++k)
+		if (status[k] != DG_OK) return status[k];
+	return DG_OK;
 }
 
 int dg_cell_count(dg_solver *s, long long *n) {

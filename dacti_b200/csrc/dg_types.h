@@ -109,7 +109,7 @@ struct Pool {
 	int32_t *stamp;   // per-node dedup stamp for list building
 	uint32_t *fmask;  // faces (bit 2 dim + dir) whose neighbour changed in the running regrid; 0 otherwise
 	uint8_t *op;      // refinement op code
-	double *tmp;      // per-node scratch scalar (Jacobi smoothing)
+	double *tmp, *tmp2;  // per-node scratch scalars (Jacobi smoothing sweeps, alternately)
 	// Per-substep scratch outside the permuted fields:
 	double *ff;       // [cap][2D][F] flux of each face a cell owns, written in the running substep
 	int32_t *plan;    // [cap][2D] source of each face's flux for the running cluster's cells

@@ -38,6 +38,7 @@ public:
 	virtual long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
+	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
 	virtual void set_profiling(bool on) = 0;
 	virtual void set_form(int form) = 0;
 	std::string last_error;
@@ -184,6 +185,7 @@ public:
 		cudaFree(d_leaves_);
 		cudaFree(d_read_);
 		cudaFree(d_readlv_);
+		if (owned_stream_) cudaStreamDestroy(owned_stream_);
 		for (auto e: ev_free_) cudaEventDestroy(e);
 		for (auto &p: pending_) {
 			cudaEventDestroy(p.a);
@@ -192,6 +194,13 @@ public:
 	}
 
 	void set_stream(cudaStream_t s) override { st_ = s; }
+
+	cudaStream_t owned_stream_ = nullptr;
+	void own_stream() override {
+		if (st_ != 0) return;
+		if (!owned_stream_) DG_CUDA(cudaStreamCreateWithFlags(&owned_stream_, cudaStreamNonBlocking));
+		st_ = owned_stream_;
+	}
 
 	// ---------------------------------------------------------------------------------------
 	void setup_consts(const dg_case &c) {
@@ -300,7 +309,7 @@ public:
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.fmask, 4, 1}, {(void **) &P.op, 1, 1},
-		    {(void **) &P.tmp, 8, 1},
+		    {(void **) &P.tmp, 8, 1}, {(void **) &P.tmp2, 8, 1},
 		};
 	}
 
@@ -494,10 +503,7 @@ public:
 		// every memo starts stale: mod = 1 > cst = 0
 		k_fill_i32<<<grid_for(P_.cap), BLOCK, 0, st_>>>(P_.mod, 1, P_.cap);
 		launch_slope(d_leaves_, n);
-		if constexpr (M::MULTI) {
-			multiphase_aux(d_leaves_, n);
-			k_rec_k<M><<<g, BLOCK, 0, st_>>>(P_, d_leaves_, n);
-		}
+		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n, -1);
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
 		global_dt_ = std::fmax(-INFINITY, h_cnt_->dmax);
@@ -520,20 +526,22 @@ public:
 private:
 	// smooth_alpha x3, normal_update, curvature_update, smooth_curvature over one cell list
 	// (impl/integrate.hpp:284-289, integrator/integrator.hpp:134-143).
-	void multiphase_aux(const int32_t *list, int n) {
+	// Lm: the ACTI level whose cluster `list` is, or -1 when the list holds every leaf (constructor).
+	void multiphase_aux(const int32_t *list, int n, int Lm) {
 		if constexpr (M::MULTI) {
 			const int g = grid_for(n);
-			for (int it = 0; it < 3; ++it) {
-				run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
-				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS); });
-			}
+			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, nullptr, P_.tmp, Lm, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp, P_.tmp2, Lm, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp2, P_.tmp, Lm, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS, P_.tmp); });
 			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
 			// The curvature only enters through sigma * kappa (model/multi.hpp:142, 216, 190-193); without
 			// surface tension those products are zeros and the curvature stages are skipped.
 			if (sigma_) {
 				run_k(DG_K_AUX, n, [&] { k_curvature<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
 				run_k(DG_K_AUX, n, [&] { k_smooth_kappa<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
-				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA); });
+				run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::KAPPA, P_.tmp); });
+				run_k(DG_K_AUX, n, [&] { k_rec_k<M><<<g, BLOCK, 0, st_>>>(P_, list, n); });
 			}
 		}
 	}
@@ -610,10 +618,7 @@ private:
 			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e, d_cnt_);
 		});
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
-		if constexpr (M::MULTI) {
-			multiphase_aux(list, n);
-			run_k(DG_K_AUX, n, [&] { k_rec_k<M><<<g, BLOCK, 0, st_>>>(P_, list, n); });
-		}
+		if constexpr (M::MULTI) multiphase_aux(list, n, L);
 		run_k(DG_K_ESTIMATE, n, [&] {
 			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
 		});

@@ -338,10 +338,14 @@ __global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stam
 			if (P.clu[nb] != L) {
 				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 			}
-			append(tasks, &cnt->n_task, i * NF + f, cap * NF, &cnt->status);
+			// a same-level neighbour of the running cluster does not own its side of the face: the owner
+			// also writes the flux into the neighbour's own slot for that face, so that every cell of the
+			// cluster gathers from its own contiguous slots
+			const int mirror = (ln == li && P.clu[nb] == L) ? 1 : 0;
+			append(tasks, &cnt->n_task, (i * NF + f) * 2 + mirror, cap * NF, &cnt->status);
 			*pl = (i * NF + f) * 2 + dir;
 		} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
-			*pl = (nb * NF + (f ^ 1)) * 2 + dir;
+			*pl = (i * NF + f) * 2 + dir;  // written by the owner nb into this cell's slot
 		} else {
 			*pl = PLAN_NONE;
 		}
@@ -355,7 +359,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const in
 	constexpr int NF = 2 * M::D;
 	const int n = *n_ptr;
 	for (int t = gtid(); t < n; t += gstride()) {
-		const int code = tasks[t];
+		const int code = tasks[t] >> 1;
 		const int i = code / NF, f = code % NF;
 		const int nb = P.nbr[(size_t) f * P.cap + i];
 		double F[M::F];
@@ -363,6 +367,11 @@ __global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const in
 		double *dst = face_flux(P, i, f, M::F, NF);
 #pragma unroll
 		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
+		if (tasks[t] & 1) {
+			double *mir = face_flux(P, nb, f ^ 1, M::F, NF);
+#pragma unroll
+			for (int q = 0; q < M::F; ++q) mir[q] = F[q];
+		}
 	}
 }
 
@@ -1242,9 +1251,18 @@ namespace dg {
 // fraction, the recursive child mean of k[comp] for finer neighbours, else the neighbour's k[comp].
 // `x` receives the centre distance used by compute_normal/compute_curvature (half a cell at a
 // boundary, impl/normal_curvature.hpp:161-183).
+// The smoothed volume fraction of node x during the Jacobi sweeps of a cell list: the previous sweep's
+// result for members of the list (cur, after the first sweep), the stored k[ALPHAS] for everyone else.
+// Lm >= 0: members are the cells of cluster Lm; Lm < 0: every leaf (the constructor's list).
+template<class M>
+__device__ __forceinline__ double alpha_now(const Pool &P, int x, const double *cur, int Lm) {
+	if (cur && (Lm < 0 || P.clu[x] == Lm)) return cur[x];
+	return at(P.k, P.cap, M::ALPHAS, x);
+}
+
 template<class M>
 __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int i, int dim, int dir,
-                         int comp, bool zero_at_boundary, double &x) {
+                         int comp, bool zero_at_boundary, double &x, const double *cur = nullptr, int Lm = -1) {
 	const int cap  = P.cap;
 	const int nb   = P.nbr[(size_t) (2 * dim + dir) * cap + i];
 	const double h = C.size[P.level[i]];
@@ -1263,32 +1281,38 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 	}
 	const double hn = C.size[P.level[nb]];
 	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
+	if (comp == M::ALPHAS && cur) {
+		if (!(P.flags[nb] & F_LEAF)) return interp_fn<M::D>(P, status, nb, [&](int y) { return alpha_now<M>(P, y, cur, Lm); });
+		return alpha_now<M>(P, nb, cur, Lm);
+	}
 	if (!(P.flags[nb] & F_LEAF)) return interp_scalar<M::D>(P, status, nb, P.k + (size_t) comp * cap);
 	return at(P.k, cap, comp, nb);
 }
 
-// smooth_alpha, one Jacobi sweep into P.tmp (impl/smooth.hpp:10-51)
+// smooth_alpha, one Jacobi sweep (impl/smooth.hpp:10-51): reads the previous sweep's values of the
+// list's cells from `cur` (nullptr for the first sweep: everything from k[ALPHAS]) and writes `out`;
+// the sweeps alternate between two scratch arrays and only the result of the last is stored.
 template<class M>
-__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
-	const int cap = P.cap;
+__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, const double *cur, double *out,
+                               int Lm, Counters *cnt) {
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i     = list[tid];
-		const double ac = at(P.k, cap, M::ALPHAS, i);
+		const double ac = cur ? cur[i] : at(P.k, P.cap, M::ALPHAS, i);
 		double s        = 0.0;
 		for (int dim = 0; dim < M::D; ++dim) {
 			double x;
-			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x);
-			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x);
+			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x, cur, Lm);
+			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x, cur, Lm);
 			s += 0.5 * (an + ap) + ac;
 		}
-		P.tmp[i] = s / (double) (2 * M::D);
+		out[i] = s / (double) (2 * M::D);
 	}
 }
 
-static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp) {
+static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp, const double *src) {
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i = list[tid];
-		P.k[(size_t) comp * P.cap + i] = P.tmp[i];
+		P.k[(size_t) comp * P.cap + i] = src[i];
 	}
 }
 
@@ -1311,6 +1335,10 @@ __global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n
 		const double len = sqrt(sq);
 		for (int d = 0; d < D; ++d) nrm[d] = (len < 1e-10) ? 0.0 : nrm[d] / len;
 		for (int d = 0; d < D; ++d) P.k[(size_t) (M::IKN + d) * cap + i] = nrm[d];
+		// the record's multiphase part (curvature is final here unless surface tension recomputes it)
+		double *kr = rec_of(P, i, Rec<M>::W) + Rec<M>::K0;
+		kr[0] = at(P.k, cap, M::KAPPA, i);
+		for (int d = 0; d < D; ++d) kr[1 + d] = nrm[d];
 	}
 }
 

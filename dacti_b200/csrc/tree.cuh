@@ -142,11 +142,12 @@ __device__ __forceinline__ void mark_up(const Pool &P, int first, int epoch) {
 	}
 }
 
-// Scalar field average (t, k[i] or p[i]); `arr` is the SoA base of that component.
-template<int D>
-__device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const double *arr) {
+// Mean of a per-node scalar over the subtree of n (the leaf's own value for a leaf), children in slot
+// order as the recursion of interpolate_k visits them; `val(x)` gives a leaf's value.
+template<int D, class Val>
+__device__ double interp_fn(const Pool &P, uint32_t *status, int n, Val val) {
 	constexpr int NC = 1 << D;
-	if (P.flags[n] & F_LEAF) return arr[n];
+	if (P.flags[n] & F_LEAF) return val(n);
 	int node[MAX_TREE], next[MAX_TREE], cnt[MAX_TREE];
 	double f[MAX_TREE];
 	int sp   = 1;
@@ -161,7 +162,7 @@ __device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const do
 			next[k]++;
 			if (!(P.flags[c] & F_ACTIVE)) continue;
 			if (P.flags[c] & F_LEAF) {
-				f[k] += arr[c];
+				f[k] += val(c);
 				cnt[k]++;
 			} else if (sp < MAX_TREE) {
 				node[sp] = c;
@@ -180,6 +181,12 @@ __device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const do
 		f[sp - 1] += r;
 		cnt[sp - 1]++;
 	}
+}
+
+// Scalar field average (t, k[i] or p[i]); `arr` is the SoA base of that component.
+template<int D>
+__device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const double *arr) {
+	return interp_fn<D>(P, status, n, [arr](int x) { return arr[x]; });
 }
 
 

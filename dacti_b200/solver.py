@@ -79,6 +79,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_set_stream.argtypes = [vp, vp]
     lib.dg_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                             SUBSTEP_FN, vp]
+    lib.dg_step_many.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                 ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_int)]
     lib.dg_cell_count.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_read_cells.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                   ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
@@ -95,7 +97,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     return lib
 
 
-EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_cell_count", "dg_read_cells",
+EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
+                    "dg_read_cells",
                     "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
@@ -235,3 +238,21 @@ class Solver:
     def _check(self, rc: int) -> None:
         if rc != DG_OK:
             raise DgError(rc, self._lib.dg_last_error(self._h).decode())
+
+
+def step_many(solvers, threads: int = 32, signal: bool = True) -> list:
+    """dg_step_many: one global step of every solver, concurrently (host threads, one stream each).
+    Returns the force_break flags; raises DgError with the first failing solver's message."""
+    lib = load_library()
+    n = len(solvers)
+    hs = (ctypes.c_void_p * max(n, 1))(*[s._h for s in solvers])
+    fb = (ctypes.c_int * max(n, 1))()
+    gdt = (ctypes.c_double * max(n, 1))()
+    st = (ctypes.c_int * max(n, 1))()
+    rc = lib.dg_step_many(hs, n, threads, 1 if signal else 0, fb, gdt, st)
+    if rc != 0:
+        for k in range(n):
+            if st[k] != 0:
+                raise DgError(st[k], lib.dg_last_error(solvers[k]._h).decode())
+        raise DgError(rc, "dg_step_many failed")
+    return [bool(fb[k]) for k in range(n)]

@@ -120,6 +120,15 @@ int dg_set_stream(dg_solver *s, void *cuda_stream);
  * force_break is set when a cell update produced NaN (the step stops at that substep). */
 int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user);
 
+/* One global step of each of n independent solvers (a batch of trees, each one Integrator of the
+ * reference stepped on its own), driven by up to `threads` host threads with every solver on a stream
+ * of its own so that the trees' kernels overlap on the device. Results per tree are those of dg_step
+ * (bitwise: the kernels are deterministic); force_break[k], global_dt[k] and status[k] per solver; the
+ * return value is the first non-DG_OK status or DG_OK. A solver still on the legacy default stream gets
+ * a stream of its own. No substep callback. */
+int dg_step_many(dg_solver **solvers, int n, int threads, int signal, int *force_break, double *global_dt,
+                 int *status);
+
 /* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */
 int dg_cell_count(dg_solver *s, long long *n);
 
