@@ -284,7 +284,7 @@ def batched_run(args, local_rank: int, world: int) -> dict:
     from dacti_b200 import cases
     from dacti_b200.solver import Solver, step_many
 
-    threads = 32
+    threads = 8
     batch = cases.riemann_batch(args.batch_trees, seed=3)
     solvers = [Solver(c, device=local_rank) for c in batch]
     for s in solvers:

@@ -1,6 +1,7 @@
 // extern "C" entry points of include/dacti_gpu.h.
 #include "capi_internal.h"
 
+#include <algorithm>
 #include <atomic>
 #include <string>
 #include <thread>
@@ -71,9 +72,18 @@ int dg_step_many(dg_solver **s, int n, int threads, int signal, int *force_break
 		const int rc = guarded(s[k], [&] { s[k]->impl->own_stream(); });
 		if (rc != DG_OK) return rc;
 	}
+	// largest trees first (cells as the work estimate), so that no large tree is left for the end
+	std::vector<long long> cells(n, 0);
+	std::vector<int> order(n);
+	for (int k = 0; k < n; ++k) {
+		order[k] = k;
+		guarded(s[k], [&] { cells[k] = s[k]->impl->cell_count(); });
+	}
+	std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cells[a] > cells[b]; });
 	std::atomic<int> next{0};
 	auto worker = [&] {
-		for (int k = next++; k < n; k = next++) {
+		for (int j = next++; j < n; j = next++) {
+			const int k    = order[j];
 			force_break[k] = 0;
 			status[k]      = guarded(s[k], [&] { s[k]->impl->step(signal, &force_break[k], &global_dt[k], nullptr, nullptr); });
 		}

@@ -101,6 +101,8 @@ struct Pool {
 	double *avg;      // [cap][AW] non-leaf nodes: memo of the mean primitive state and time of the subtree
 	int32_t *mod;     // epoch of the latest change of any leaf below the node
 	int32_t *cst;     // epoch at which `avg` was computed
+	double *avga;     // non-leaf nodes: memo of the mean smoothed volume fraction of the subtree
+	int32_t *csta;    // epoch at which `avga` was computed
 	double *k;        // [P][cap]
 	double *tslope;   // [G][cap]
 	double *grad;     // [D][G][cap]

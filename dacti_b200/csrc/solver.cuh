@@ -305,7 +305,7 @@ public:
 		    {(void **) &P.coord, 4, D}, {(void **) &P.nbr, 4, NF}, {(void **) &P.bc, 2, NF},
 		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
 		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1}, {(void **) &P.avg, 8 * Avg<M>::W, 1},
-		    {(void **) &P.mod, 4, 1}, {(void **) &P.cst, 4, 1},
+		    {(void **) &P.mod, 4, 1}, {(void **) &P.cst, 4, 1}, {(void **) &P.avga, 8, 1}, {(void **) &P.csta, 4, 1},
 		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.fmask, 4, 1}, {(void **) &P.op, 1, 1},
@@ -503,7 +503,7 @@ public:
 		// every memo starts stale: mod = 1 > cst = 0
 		k_fill_i32<<<grid_for(P_.cap), BLOCK, 0, st_>>>(P_.mod, 1, P_.cap);
 		launch_slope(d_leaves_, n);
-		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n, -1);
+		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n, -1, 0);
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
 		global_dt_ = std::fmax(-INFINITY, h_cnt_->dmax);
@@ -527,14 +527,21 @@ private:
 	// smooth_alpha x3, normal_update, curvature_update, smooth_curvature over one cell list
 	// (impl/integrate.hpp:284-289, integrator/integrator.hpp:134-143).
 	// Lm: the ACTI level whose cluster `list` is, or -1 when the list holds every leaf (constructor).
-	void multiphase_aux(const int32_t *list, int n, int Lm) {
+	// e_upd: epoch of the substep's cell update (0: no memoised volume-fraction means).
+	void multiphase_aux(const int32_t *list, int n, int Lm, int e_upd) {
 		if constexpr (M::MULTI) {
 			const int g = grid_for(n);
-			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, nullptr, P_.tmp, Lm, d_cnt_); });
-			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp, P_.tmp2, Lm, d_cnt_); });
-			run_k(DG_K_AUX, n, [&] { k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp2, P_.tmp, Lm, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] {
+				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, nullptr, P_.tmp, Lm, ++epoch_, e_upd, d_cnt_);
+			});
+			run_k(DG_K_AUX, n, [&] {
+				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp, P_.tmp2, Lm, ++epoch_, e_upd, d_cnt_);
+			});
+			run_k(DG_K_AUX, n, [&] {
+				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp2, P_.tmp, Lm, ++epoch_, e_upd, d_cnt_);
+			});
 			run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS, P_.tmp); });
-			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, ++epoch_, e_upd, d_cnt_); });
 			// The curvature only enters through sigma * kappa (model/multi.hpp:142, 216, 190-193); without
 			// surface tension those products are zeros and the curvature stages are skipped.
 			if (sigma_) {
@@ -602,6 +609,7 @@ private:
 		const int counterL = acti_counter_[L];
 
 		constexpr int LPC = NF <= 4 ? 4 : 8;  // receive lanes per cell
+		int e_upd = 0;                       // epoch of this substep's cell update
 		run_k(DG_K_FLUX, n, [&] {
 			k_flux_tasks<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, list, n, L, stamp_recv, Ls_.task, Ls_.btask,
 			                                                                  Ls_.wtask, Ls_.recv, d_cnt_);
@@ -613,12 +621,12 @@ private:
 			k_flux_receive<M><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
-			const int e = ++epoch_;
-			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e, d_cnt_);
-			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e, d_cnt_);
+			e_upd = ++epoch_;
+			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
 		});
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
-		if constexpr (M::MULTI) multiphase_aux(list, n, L);
+		if constexpr (M::MULTI) multiphase_aux(list, n, L, e_upd);
 		run_k(DG_K_ESTIMATE, n, [&] {
 			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
 		});
@@ -635,7 +643,7 @@ private:
 		const int gf = grid_for((long long) n * (NC + 1));
 		run_k(DG_K_REGRID, n, [&] { k_unsplit_select<M><<<g, BLOCK, 0, st_>>>(P_, list, n, L, Ls_.unsplit, d_cnt_); });
 		run_k(DG_K_REGRID, 0, [&] {
-			k_split<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, ++epoch_, d_cnt_);
+			k_split<M><<<gf, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_split, Ls_.split, L, Ls_.fresh, ++epoch_, d_cnt_);
 		});
 		run_k(DG_K_REGRID, 0, [&] {
 			k_unsplit<M><<<g, BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_unsplit, Ls_.unsplit, L, Ls_.fresh, ++epoch_, d_cnt_);

@@ -338,14 +338,10 @@ __global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stam
 			if (P.clu[nb] != L) {
 				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 			}
-			// a same-level neighbour of the running cluster does not own its side of the face: the owner
-			// also writes the flux into the neighbour's own slot for that face, so that every cell of the
-			// cluster gathers from its own contiguous slots
-			const int mirror = (ln == li && P.clu[nb] == L) ? 1 : 0;
-			append(tasks, &cnt->n_task, (i * NF + f) * 2 + mirror, cap * NF, &cnt->status);
+			append(tasks, &cnt->n_task, i * NF + f, cap * NF, &cnt->status);
 			*pl = (i * NF + f) * 2 + dir;
 		} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
-			*pl = (i * NF + f) * 2 + dir;  // written by the owner nb into this cell's slot
+			*pl = (nb * NF + (f ^ 1)) * 2 + dir;
 		} else {
 			*pl = PLAN_NONE;
 		}
@@ -359,7 +355,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const in
 	constexpr int NF = 2 * M::D;
 	const int n = *n_ptr;
 	for (int t = gtid(); t < n; t += gstride()) {
-		const int code = tasks[t] >> 1;
+		const int code = tasks[t];
 		const int i = code / NF, f = code % NF;
 		const int nb = P.nbr[(size_t) f * P.cap + i];
 		double F[M::F];
@@ -367,11 +363,6 @@ __global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const in
 		double *dst = face_flux(P, i, f, M::F, NF);
 #pragma unroll
 		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
-		if (tasks[t] & 1) {
-			double *mir = face_flux(P, nb, f ^ 1, M::F, NF);
-#pragma unroll
-			for (int q = 0; q < M::F; ++q) mir[q] = F[q];
-		}
 	}
 }
 
@@ -857,36 +848,44 @@ __global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int3
 template<class M>
 __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
                         int epoch, Counters *cnt) {
-	constexpr int E = M::E, D = M::D, NC = 1 << D;
-	const int n   = *n_ptr;
-	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
-		const int par = split_list[tid];
-		if constexpr (M::MULTI) recompute_rhs<M>(P, C, par);
-		const int lp   = P.level[par];
-		const double q = 0.25 * C.size[lp];
-		int slots[NC];
-		bool reuse = P.child[par] != 0;
-		if (reuse) {
-			for (int c = 0; c < NC; ++c) slots[c] = P.child[(size_t) c * cap + par];
-		} else {
-			const int first = atomicAdd(&cnt->top, NC);
-			if (first + NC > cap) {
-				set_status(&cnt->status, ST_CAPACITY);
-				continue;
-			}
-			for (int c = 0; c < NC; ++c) {
-				slots[c]                             = first + c;
-				P.child[(size_t) c * cap + par] = first + c;
+	constexpr int E = M::E, D = M::D, NC = 1 << D, GW = 32 / NC;
+	using R = Rec<M>;
+	const int n      = *n_ptr;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int c      = lane & (NC - 1);  // the child this lane sets up
+	const int lead   = lane & ~(NC - 1);
+	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	// one group of 2^D lanes per parent: the group's first lane allocates, every lane builds one child
+	for (int base = warp * GW; base < n; base += nwarps * GW) {
+		const int slot    = base + lane / NC;
+		const bool active = slot < n;
+		const int par     = active ? split_list[slot] : 0;
+		int first = 0, reuse = 0, fail = 0;
+		if (active && c == 0) {
+			if constexpr (M::MULTI) recompute_rhs<M>(P, C, par);
+			reuse = P.child[par] != 0;
+			if (!reuse) {
+				first = atomicAdd(&cnt->top, NC);
+				if (first + NC > cap) {
+					set_status(&cnt->status, ST_CAPACITY);
+					fail = 1;
+				}
 			}
 		}
-		using R = Rec<M>;
-		double pp[E], pc[D];
-		load_p<M>(P, par, pp);
-		for (int d = 0; d < D; ++d) pc[d] = at(P.center, cap, d, par);
-		const double *rp = rec_of(P, par, R::W);
-		for (int c = 0; c < NC; ++c) {
-			const int s = slots[c];
+		first = __shfl_sync(0xffffffffu, first, lead);
+		reuse = __shfl_sync(0xffffffffu, reuse, lead);
+		fail  = __shfl_sync(0xffffffffu, fail, lead);
+		if (active && !fail) {
+			const int s = reuse ? P.child[(size_t) c * cap + par] : first + c;
+			if (!reuse) P.child[(size_t) c * cap + par] = s;
+			const int lp   = P.level[par];
+			const double q = 0.25 * C.size[lp];
+			double pp[E], pc[D];
+			load_p<M>(P, par, pp);
+			for (int d = 0; d < D; ++d) pc[d] = at(P.center, cap, d, par);
+			const double *rp = rec_of(P, par, R::W);
 			P.parent[s] = par;
 			P.level[s]  = (int8_t) (lp + 1);
 			P.acti[s]   = (int8_t) L;
@@ -932,8 +931,11 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 				for (int k = 0; k < NC; ++k) P.child[(size_t) k * cap + s] = 0;
 			append(fresh, &cnt->n_new, s, cap, &cnt->status);
 		}
-		P.flags[par] &= ~(F_LEAF | F_SHOULD_SPLIT);
-		mark_up(P, par, epoch);
+		__syncwarp();
+		if (active && !fail && c == 0) {
+			P.flags[par] &= ~(F_LEAF | F_SHOULD_SPLIT);
+			mark_up(P, par, epoch);
+		}
 	}
 }
 
@@ -1262,7 +1264,8 @@ __device__ __forceinline__ double alpha_now(const Pool &P, int x, const double *
 
 template<class M>
 __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int i, int dim, int dir,
-                         int comp, bool zero_at_boundary, double &x, const double *cur = nullptr, int Lm = -1) {
+                         int comp, bool zero_at_boundary, double &x, const double *cur = nullptr, int Lm = -1,
+                         int epoch = 0, int e_upd = 0) {
 	const int cap  = P.cap;
 	const int nb   = P.nbr[(size_t) (2 * dim + dir) * cap + i];
 	const double h = C.size[P.level[i]];
@@ -1281,9 +1284,10 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 	}
 	const double hn = C.size[P.level[nb]];
 	x = dir == 0 ? -0.5 * (h + hn) : 0.5 * (h + hn);
-	if (comp == M::ALPHAS && cur) {
-		if (!(P.flags[nb] & F_LEAF)) return interp_fn<M::D>(P, status, nb, [&](int y) { return alpha_now<M>(P, y, cur, Lm); });
-		return alpha_now<M>(P, nb, cur, Lm);
+	if (comp == M::ALPHAS) {
+		auto val = [&](int y) { return alpha_now<M>(P, y, cur, Lm); };
+		if (!(P.flags[nb] & F_LEAF)) return interp_alpha<M::D>(P, status, nb, val, epoch, e_upd);
+		return val(nb);
 	}
 	if (!(P.flags[nb] & F_LEAF)) return interp_scalar<M::D>(P, status, nb, P.k + (size_t) comp * cap);
 	return at(P.k, cap, comp, nb);
@@ -1294,15 +1298,15 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 // the sweeps alternate between two scratch arrays and only the result of the last is stored.
 template<class M>
 __global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, const double *cur, double *out,
-                               int Lm, Counters *cnt) {
+                               int Lm, int epoch, int e_upd, Counters *cnt) {
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i     = list[tid];
 		const double ac = cur ? cur[i] : at(P.k, P.cap, M::ALPHAS, i);
 		double s        = 0.0;
 		for (int dim = 0; dim < M::D; ++dim) {
 			double x;
-			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x, cur, Lm);
-			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x, cur, Lm);
+			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
+			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
 			s += 0.5 * (an + ap) + ac;
 		}
 		out[i] = s / (double) (2 * M::D);
@@ -1318,7 +1322,7 @@ static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp,
 
 // compute_normal (impl/normal_curvature.hpp:7-55)
 template<class M>
-__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
 	constexpr int D = M::D;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
@@ -1326,8 +1330,8 @@ __global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n
 		double nrm[D];
 		for (int dim = 0; dim < D; ++dim) {
 			double xn, xp;
-			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, xn);
-			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, xp);
+			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, xn, nullptr, -1, epoch, e_upd);
+			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, xp, nullptr, -1, epoch, e_upd);
 			nrm[dim] = (ap - an) / (xp - xn);
 		}
 		double sq = 0.0;

@@ -183,6 +183,62 @@ __device__ double interp_fn(const Pool &P, uint32_t *status, int n, Val val) {
 	}
 }
 
+// The same recursion for the smoothed volume fraction, memoised like the primitive-state means but
+// only for subtrees without a leaf changed in the running substep (mod below `e_upd`, the epoch of the
+// substep's cell update): below those, the list's cells change from one Jacobi sweep to the next.
+// e_upd = 0 disables the memo.
+template<int D, class Val>
+__device__ double interp_alpha(const Pool &P, uint32_t *status, int n, Val val, int epoch, int e_upd) {
+	constexpr int NC = 1 << D;
+	auto ok = [&](int x) {
+		const int c = __ldcg(P.csta + x), m = __ldcg(P.mod + x);
+		return c > m && c < epoch && m < e_upd;
+	};
+	if (P.flags[n] & F_LEAF) return val(n);
+	if (ok(n)) return __ldcg(P.avga + n);
+	int node[MAX_TREE], next[MAX_TREE], cnt[MAX_TREE];
+	double f[MAX_TREE];
+	int sp  = 1;
+	node[0] = n;
+	next[0] = 0;
+	cnt[0]  = 0;
+	f[0]    = 0.0;
+	while (true) {
+		const int k = sp - 1;
+		if (next[k] < NC) {
+			const int c = P.child[(size_t) next[k] * P.cap + node[k]];
+			next[k]++;
+			const uint32_t fl = P.flags[c];
+			if (!(fl & F_ACTIVE)) continue;
+			if (fl & F_LEAF) {
+				f[k] += val(c);
+				cnt[k]++;
+			} else if (ok(c)) {
+				f[k] += __ldcg(P.avga + c);
+				cnt[k]++;
+			} else if (sp < MAX_TREE) {
+				node[sp] = c;
+				next[sp] = 0;
+				cnt[sp]  = 0;
+				f[sp]    = 0.0;
+				++sp;
+			} else {
+				set_status(status, ST_DEPTH);
+			}
+			continue;
+		}
+		const double r = f[k] / (double) cnt[k];
+		if (__ldcg(P.mod + node[k]) < e_upd) {
+			P.avga[node[k]] = r;
+			P.csta[node[k]] = epoch;
+		}
+		--sp;
+		if (sp == 0) return r;
+		f[sp - 1] += r;
+		cnt[sp - 1]++;
+	}
+}
+
 // Scalar field average (t, k[i] or p[i]); `arr` is the SoA base of that component.
 template<int D>
 __device__ double interp_scalar(const Pool &P, uint32_t *status, int n, const double *arr) {
