@@ -111,6 +111,14 @@ int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, 
 	});
 }
 
+int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long *n_out) {
+	if (!s || !slopes) return DG_ERR_ARG;
+	return guarded(s, [&] {
+		long long n = s->impl->read_slopes(slopes, max_cells);
+		if (n_out) *n_out = n;
+	});
+}
+
 int dg_get_stats(dg_solver *s, dg_stats *out) {
 	if (!s || !out) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->stats(out); });

@@ -36,6 +36,7 @@ public:
 	virtual long long cell_count() = 0;
 	virtual long long read_cells(int *levels, double *data, long long max_cells) = 0;
 	virtual long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) = 0;
+	virtual long long read_slopes(double *data, long long max_cells) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
@@ -881,6 +882,30 @@ public:
 		DG_CUDA(cudaMemcpyAsync(data, d_read_, sizeof(double) * W * n, cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaMemcpyAsync(levels, d_readlv_, sizeof(int32_t) * 2 * n, cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
+		return n;
+	}
+
+	// Limited slopes of the active cells, [D][E] per cell, in read_cells' order.
+	long long read_slopes(double *data, long long max_cells) override {
+		const long long n = cell_count();
+		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
+		double *d_out = nullptr;
+		DG_CUDA(cudaMalloc(&d_out, sizeof(double) * D * E * (n > 0 ? n : 1)));
+		long long base = 0;
+		for (int pass = 0; pass < 2; ++pass) {
+			for (int l = 0; l < MAX_ACTI; ++l) {
+				const int cnt = pass == 0 ? h_cnt_->clu[l] : h_cnt_->buf[l];
+				if (cnt == 0) continue;
+				const int32_t *list = pass == 0 ? Ls_.clu[l] : Ls_.buf[l];
+				k_gather_slopes<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, (int) base, d_out);
+				base += cnt;
+			}
+		}
+		cudaError_t e = cudaGetLastError();
+		if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(data, d_out, sizeof(double) * D * E * n, cudaMemcpyDeviceToHost, st_);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+		cudaFree(d_out);
+		if (e != cudaSuccess) throw dg_error(DG_ERR_CUDA, std::string("read_slopes: ") + cudaGetErrorString(e));
 		return n;
 	}
 

@@ -1218,6 +1218,18 @@ __global__ void k_assign(Pool P, Consts C, const int32_t *list, int n, double gl
 	}
 }
 
+// Gather of the active cells' limited slopes ([D][E] per cell) for the read-back API.
+template<class M>
+__global__ void k_gather_slopes(Pool P, const int32_t *list, int n, int base, double *out) {
+	constexpr int E = M::E, D = M::D;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double *o   = out + (size_t) (base + tid) * D * E;
+		for (int d = 0; d < D; ++d)
+			for (int q = 0; q < E; ++q) o[d * E + q] = rec_slope<M>(P, i, d, q);
+	}
+}
+
 // Gather of active-cell records for the read-back API.
 template<class M>
 __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, double *out, int32_t *lv) {

@@ -1,0 +1,94 @@
+"""The simulation loop of DACTI's default_driver (driver/default_driver.hpp:77-217) over the GPU solver.
+
+`run()` advances global steps until `end_time` (or a converged steady state), calling `integrate` with
+`signal = time > signal_time`; after every step it decides, as the reference does, whether to write a
+frame (simulation time advanced by at least `io_interval` since the last one, convergence, or NaN), and
+then appends a row (time, frame, step, n_cells and the observers' integral variables) to
+`<out_dir>/<name>_observables.csv` and writes `<out_dir>/<name>_<frame:04>.vtu`. Frame 0 is the initial
+state. A NaN (force_break) ends the run after its frame, as in the reference.
+"""
+from __future__ import annotations
+
+import os
+import time as _time
+from typing import Optional, Sequence
+
+import numpy as np
+
+from .io import write_vtu
+from .solver import Solver
+
+
+class Totals:
+    """Integral observer: conserved totals sum(u * volume) per component, named u_0 .. u_{E-1}."""
+
+    name = "Totals"
+
+    def __init__(self, E: int):
+        self.names = [f"u_{q}" for q in range(E)]
+
+    def observe(self, snap, side_length: float) -> list:
+        vol = (side_length * 0.5 ** snap.tree_level.astype(np.float64)) ** snap.dims
+        return list((snap.u * vol[:, None]).sum(axis=0))
+
+
+class DefaultDriver:
+    def __init__(self, solver: Solver, name: str, out_dir: str, end_time: Optional[float] = None,
+                 io_interval: float = 0.0, observers: Sequence = (), convergence_tol: float = 0.0,
+                 signal_time: float = 0.0, write_frames: bool = True, max_steps: Optional[int] = None):
+        self.s, self.name, self.out_dir = solver, name, out_dir
+        self.end_time, self.io_interval = end_time, io_interval
+        self.observers, self.convergence_tol, self.signal_time = list(observers), convergence_tol, signal_time
+        self.write_frames, self.max_steps = write_frames, max_steps
+        self.log: list = []
+
+    def _observe(self, snap) -> list:
+        vals = []
+        for ob in self.observers:
+            vals += ob.observe(snap, self.s.side_length)
+        return vals
+
+    def _frame(self, frame: int, snap) -> None:
+        if self.write_frames:
+            write_vtu(os.path.join(self.out_dir, f"{self.name}_{frame:04d}.vtu"), snap, self.s.active_slopes(),
+                      self.s.side_length)
+
+    def run(self) -> dict:
+        os.makedirs(self.out_dir, exist_ok=True)
+        t_start = _time.perf_counter()
+        names = [n for ob in self.observers for n in ob.names]
+        csv = open(os.path.join(self.out_dir, f"{self.name}_observables.csv"), "w")
+        csv.write("time,frame,step," + ",".join(["n_cells"] + names) + "\n")
+        snap = self.s.active_cells()
+        integ = self._observe(snap)
+        self._frame(0, snap)
+        sim_time, last_print, frame, step, last_step = 0.0, 0.0, 0, 0, 0
+        converged = force_break = False
+        while (self.end_time is None or sim_time < self.end_time) and not converged:
+            if self.max_steps is not None and step >= self.max_steps:
+                break
+            gdt, force_break = self.s.integrate(signal=sim_time > self.signal_time)
+            sim_time += gdt
+            snap = None
+            if self.convergence_tol > 0:
+                snap = self.s.active_cells()
+                old, integ = integ, self._observe(snap)
+                csv.write(",".join(map(repr, [sim_time, frame, step, snap.n] + integ)) + "\n")
+                delta = max((abs(a - b) / gdt for a, b in zip(integ, old)), default=0.0)
+                converged = delta < self.convergence_tol
+            if sim_time - last_print >= self.io_interval or converged or force_break:
+                frame += 1
+                snap = snap or self.s.active_cells()
+                integ = self._observe(snap)
+                csv.write(",".join(map(repr, [sim_time, frame, step, snap.n] + integ)) + "\n")
+                csv.flush()
+                self.log.append({"frame": frame, "time": sim_time, "steps": step - last_step, "cells": snap.n,
+                                 "global_dt": gdt, "seconds": _time.perf_counter() - t_start})
+                last_print, last_step = sim_time, step
+                self._frame(frame, snap)
+            if force_break:
+                break
+            step += 1
+        csv.close()
+        return {"time": sim_time, "steps": step, "frames": frame, "force_break": bool(force_break),
+                "converged": converged}

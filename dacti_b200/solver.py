@@ -86,6 +86,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                   ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_read_cells_noalloc.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double),
                                           ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+    lib.dg_read_slopes.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_longlong,
+                                   ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_set_form.argtypes = [vp, ctypes.c_int]
@@ -98,7 +100,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
-                    "dg_read_cells",
+                    "dg_read_cells", "dg_read_slopes",
                     "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
@@ -204,6 +206,15 @@ class Solver:
     def active_cells_noalloc(self) -> Snapshot:
         """active_cells() through dg_read_cells_noalloc: no device allocation (bounded scratch)."""
         return self._read(self._lib.dg_read_cells_noalloc)
+
+    def active_slopes(self) -> np.ndarray:
+        """dg_read_slopes: the active cells' limited slopes, shape (n, D, E), in active_cells() order."""
+        sh = self.shape
+        n = self.n_active_cells()
+        out = np.zeros((max(n, 1), sh.dims, sh.E))
+        got = ctypes.c_longlong(0)
+        self._check(self._lib.dg_read_slopes(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
+        return out[: got.value]
 
     def stats(self) -> DgStats:
         s = DgStats()

@@ -138,6 +138,11 @@ int dg_cell_count(dg_solver *s, long long *n);
  * multiphase model: mu, unused, interface normal[D], curvature, smoothed volume fraction; 0 otherwise). */
 int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
+/* The limited slopes (Cell::slope, integrator/cell.hpp:19) of the active cells, slopes[n][D][E], in the
+ * order of dg_read_cells: what a writer needs to evaluate Cell::get_p(x, t) (cell.hpp:23-31) at points
+ * of the cell, as DACTI's VTU writer does at the cell vertices (driver/io/vtu_writer.hpp:40-62). */
+int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long *n_out);
+
 /* Allocation-free variant of dg_read_cells for hosts that cannot let the library call cudaMalloc
  * (a fixed device-memory budget owned by the host's allocator, or a thread that must not take the
  * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference: DACTI's
