@@ -119,6 +119,14 @@ int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long 
 	});
 }
 
+int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out) {
+	if (!s || !gradients) return DG_ERR_ARG;
+	return guarded(s, [&] {
+		long long n = s->impl->read_gradients(gradients, max_cells);
+		if (n_out) *n_out = n;
+	});
+}
+
 int dg_get_stats(dg_solver *s, dg_stats *out) {
 	if (!s || !out) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->stats(out); });

@@ -183,6 +183,7 @@ __device__ __forceinline__ void grad_input(const ModelConsts &m, const double *p
 		if constexpr (M::MULTI) {
 			g[M::DT] = mix_temperature(m, p[0], p[1], p[M::IP], p[M::IA]);
 			g[M::DA] = p[M::IA];
+			g[M::DA + 1] = 0.0;  // dbeta: never read; left unset by multi::get_grad_input
 		} else {
 			g[M::DT] = p[M::IP] / (p[0] * NS_R);
 		}

@@ -37,6 +37,7 @@ public:
 	virtual long long read_cells(int *levels, double *data, long long max_cells) = 0;
 	virtual long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) = 0;
 	virtual long long read_slopes(double *data, long long max_cells) = 0;
+	virtual long long read_gradients(double *data, long long max_cells) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
@@ -885,28 +886,50 @@ public:
 		return n;
 	}
 
-	// Limited slopes of the active cells, [D][E] per cell, in read_cells' order.
-	long long read_slopes(double *data, long long max_cells) override {
+	// `width` doubles per active cell, gathered by `launch(list, count, base, out)` in read_cells' order.
+	template<class F>
+	long long read_per_cell(double *data, long long max_cells, int width, const char *what, F launch) {
 		const long long n = cell_count();
 		if (n > max_cells) throw dg_error(DG_ERR_ARG, "read buffer too small");
 		double *d_out = nullptr;
-		DG_CUDA(cudaMalloc(&d_out, sizeof(double) * D * E * (n > 0 ? n : 1)));
+		DG_CUDA(cudaMalloc(&d_out, sizeof(double) * width * (n > 0 ? n : 1)));
 		long long base = 0;
 		for (int pass = 0; pass < 2; ++pass) {
 			for (int l = 0; l < MAX_ACTI; ++l) {
 				const int cnt = pass == 0 ? h_cnt_->clu[l] : h_cnt_->buf[l];
 				if (cnt == 0) continue;
-				const int32_t *list = pass == 0 ? Ls_.clu[l] : Ls_.buf[l];
-				k_gather_slopes<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, (int) base, d_out);
+				launch(pass == 0 ? Ls_.clu[l] : Ls_.buf[l], cnt, (int) base, d_out);
 				base += cnt;
 			}
 		}
 		cudaError_t e = cudaGetLastError();
-		if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(data, d_out, sizeof(double) * D * E * n, cudaMemcpyDeviceToHost, st_);
+		if (e == cudaSuccess && n > 0) e = cudaMemcpyAsync(data, d_out, sizeof(double) * width * n, cudaMemcpyDeviceToHost, st_);
 		if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
 		cudaFree(d_out);
-		if (e != cudaSuccess) throw dg_error(DG_ERR_CUDA, std::string("read_slopes: ") + cudaGetErrorString(e));
+		if (e != cudaSuccess) throw dg_error(DG_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
 		return n;
+	}
+
+	// Limited slopes of the active cells, [D][E] per cell, in read_cells' order.
+	long long read_slopes(double *data, long long max_cells) override {
+		return read_per_cell(data, max_cells, D * E, "read_slopes", [&](const int32_t *list, int cnt, int base, double *o) {
+			k_gather_slopes<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, base, o);
+		});
+	}
+
+	// Gradients of the gradient inputs, [D][G] per active cell, in read_cells' order.
+	long long read_gradients(double *data, long long max_cells) override {
+		if constexpr (M::G == 0) {
+			throw dg_error(DG_ERR_UNSUPPORTED, "dg_read_gradients: the Euler model has no gradient inputs");
+		} else {
+			if (!visc_)
+				throw dg_error(DG_ERR_UNSUPPORTED, "dg_read_gradients: gradients are kept only when the case has viscous "
+				                                   "or heat-conduction terms");
+			return read_per_cell(data, max_cells, D * M::G, "read_gradients",
+			                     [&](const int32_t *list, int cnt, int base, double *o) {
+				                     k_gather_grads<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, base, o);
+			                     });
+		}
 	}
 
 	// Same records as read_cells, gathered through caller-owned device scratch of `bytes` bytes;

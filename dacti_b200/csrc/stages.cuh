@@ -1230,6 +1230,17 @@ __global__ void k_gather_slopes(Pool P, const int32_t *list, int n, int base, do
 	}
 }
 
+// Gradients (Cell::gradient, [D][G]) of the listed cells, for the read-back API.
+template<class M>
+__global__ void k_gather_grads(Pool P, const int32_t *list, int n, int base, double *out) {
+	constexpr int G = M::G, D = M::D;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double *o   = out + (size_t) (base + tid) * D * G;
+		for (int k = 0; k < D * G; ++k) o[k] = at(P.grad, P.cap, k, i);
+	}
+}
+
 // Gather of active-cell records for the read-back API.
 template<class M>
 __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, double *out, int32_t *lv) {

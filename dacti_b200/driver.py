@@ -19,6 +19,17 @@ from .io import write_vtu
 from .solver import Solver
 
 
+def _row(vals) -> str:
+    """One CSV row; floats (numpy scalars included) in shortest round-trip form, integers as they are."""
+    out = []
+    for v in vals:
+        if isinstance(v, (int, np.integer)) and not isinstance(v, bool):
+            out.append(str(int(v)))
+        else:
+            out.append(repr(float(v)))
+    return ",".join(out) + "\n"
+
+
 class Totals:
     """Integral observer: conserved totals sum(u * volume) per component, named u_0 .. u_{E-1}."""
 
@@ -27,9 +38,31 @@ class Totals:
     def __init__(self, E: int):
         self.names = [f"u_{q}" for q in range(E)]
 
-    def observe(self, snap, side_length: float) -> list:
-        vol = (side_length * 0.5 ** snap.tree_level.astype(np.float64)) ** snap.dims
+    def observe(self, solver, snap) -> list:
+        vol = (solver.side_length * 0.5 ** snap.tree_level.astype(np.float64)) ** snap.dims
         return list((snap.u * vol[:, None]).sum(axis=0))
+
+
+class DropEnergy:
+    """DACTI's DropEnergy observer (driver/observer/drop_energy.hpp:8-34) for the multiphase model:
+    ke = sum vol 0.5 rho |v|^2 and Etot = sum vol (0.5 rho |v|^2 + sigma |grad alpha|), rho = p0 + p1,
+    with |grad alpha| from the cell's stored volume-fraction gradient along x and y only (as the
+    reference, also in 3D). The gradients come from dg_read_gradients, so the case needs viscous or
+    conduction terms (the steps skip the gradient computation otherwise)."""
+
+    name = "Droplet Energy"
+    names = ["ke", "Etot"]
+
+    def observe(self, solver, snap) -> list:
+        sh = solver.shape
+        D, iu, da = sh.dims, sh.iu, sh.dims + 1
+        grad = solver.active_gradients()
+        vol = (solver.side_length * 0.5 ** snap.tree_level.astype(np.float64)) ** D
+        rho = snap.p[:, 0] + snap.p[:, 1]
+        v2 = (snap.p[:, iu:iu + D] ** 2).sum(axis=1)
+        norm = np.sqrt(grad[:, 0, da] ** 2 + grad[:, 1, da] ** 2)
+        ke = vol * 0.5 * rho * v2
+        return [float(ke.sum()), float((ke + vol * solver.params.sigma * norm).sum())]
 
 
 class DefaultDriver:
@@ -45,7 +78,7 @@ class DefaultDriver:
     def _observe(self, snap) -> list:
         vals = []
         for ob in self.observers:
-            vals += ob.observe(snap, self.s.side_length)
+            vals += ob.observe(self.s, snap)
         return vals
 
     def _frame(self, frame: int, snap) -> None:
@@ -73,14 +106,14 @@ class DefaultDriver:
             if self.convergence_tol > 0:
                 snap = self.s.active_cells()
                 old, integ = integ, self._observe(snap)
-                csv.write(",".join(map(repr, [sim_time, frame, step, snap.n] + integ)) + "\n")
+                csv.write(_row([sim_time, frame, step, snap.n] + integ))
                 delta = max((abs(a - b) / gdt for a, b in zip(integ, old)), default=0.0)
                 converged = delta < self.convergence_tol
             if sim_time - last_print >= self.io_interval or converged or force_break:
                 frame += 1
                 snap = snap or self.s.active_cells()
                 integ = self._observe(snap)
-                csv.write(",".join(map(repr, [sim_time, frame, step, snap.n] + integ)) + "\n")
+                csv.write(_row([sim_time, frame, step, snap.n] + integ))
                 csv.flush()
                 self.log.append({"frame": frame, "time": sim_time, "steps": step - last_step, "cells": snap.n,
                                  "global_dt": gdt, "seconds": _time.perf_counter() - t_start})

@@ -21,6 +21,7 @@ boundaries, which is what that pass intends.
 """
 from __future__ import annotations
 
+import math
 from dataclasses import dataclass, field
 from typing import Callable, Optional, Sequence
 
@@ -64,27 +65,75 @@ class SphereObject:
 
 @dataclass
 class EllipseObject:
-    """Axis-aligned ellipse/ellipsoid with semi-axes `axes`; signed distance approximated by
-    (|x/a| - 1) * min(a) (exact on a circle), which is all the initial refinement and volume
-    fraction need."""
+    """Ellipse/ellipsoid with semi-axes `axes`, turned by `angle_deg` about z (2D), centred at `center`;
+    signed distance approximated by (|y/a| - 1) * min(a) in the body frame y (exact on a circle), which
+    is all the initial refinement and volume fraction need."""
 
     center: Sequence[float]
     axes: Sequence[float]
     type: str = "droplet"
     bc: Optional[BoundarySpec] = None
+    angle_deg: float = 0.0
 
     def signed_distance(self, x: np.ndarray) -> np.ndarray:
         D = x.shape[1]
         c = np.asarray(self.center, dtype=np.float64)[:D]
         a = np.asarray(self.axes, dtype=np.float64)[:D]
-        return (np.sqrt((((x - c) / a) ** 2).sum(axis=1)) - 1.0) * a.min()
+        y = x - c
+        if self.angle_deg != 0.0:
+            if D != 2:
+                raise NotImplementedError("rotated ellipsoids are supported in 2D only")
+            th = self.angle_deg * math.pi / 180.0
+            cs, sn = math.cos(th), math.sin(th)
+            # body frame: R^T (x - c) with R the rotation by +angle about z
+            y = np.stack([cs * y[:, 0] + sn * y[:, 1], -sn * y[:, 0] + cs * y[:, 1]], axis=1)
+        return (np.sqrt(((y / a) ** 2).sum(axis=1)) - 1.0) * a.min()
+
+
+@dataclass
+class PolygonObject:
+    """Closed 2D polygon (vertices in order, either orientation): exact signed distance, negative
+    inside (even-odd rule)."""
+
+    vertices: Sequence[Sequence[float]]
+    type: str = "droplet"
+    bc: Optional[BoundarySpec] = None
+
+    def signed_distance(self, x: np.ndarray) -> np.ndarray:
+        if x.shape[1] != 2:
+            raise NotImplementedError("polygon objects are 2D")
+        v = np.asarray(self.vertices, np.float64)
+        w = np.roll(v, -1, axis=0)
+        dist = np.full(x.shape[0], np.inf)
+        inside = np.zeros(x.shape[0], bool)
+        for a, b in zip(v, w):
+            ab = b - a
+            t = np.clip(((x - a) @ ab) / (ab @ ab), 0.0, 1.0)
+            dist = np.minimum(dist, np.sqrt(((x - (a + t[:, None] * ab)) ** 2).sum(axis=1)))
+            crosses = (a[1] > x[:, 1]) != (b[1] > x[:, 1])
+            with np.errstate(divide="ignore", invalid="ignore"):
+                xc = a[0] + (x[:, 1] - a[1]) * ab[0] / ab[1]
+            inside ^= crosses & (x[:, 0] < xc)
+        return np.where(inside, -dist, dist)
 
 
 @dataclass
 class RefineZone:
+    """Refinement zone (config/config.hpp:77-86): cells whose centre, padded to 3D with zeros, lies
+    strictly inside the box (x0, x1) may refine up to `level`."""
+
     x0: Sequence[float]
     x1: Sequence[float]
     level: int
+
+    def __post_init__(self):
+        if len(self.x0) != 3 or len(self.x1) != 3:
+            raise ValueError("refinement zone corners are 3D points (vec3_t), also in 1D and 2D cases")
+
+    def contains(self, ctr: np.ndarray) -> np.ndarray:
+        x = np.zeros((ctr.shape[0], 3))
+        x[:, : ctr.shape[1]] = ctr
+        return np.all((x < np.asarray(self.x1, np.float64)) & (x > np.asarray(self.x0, np.float64)), axis=1)
 
 
 @dataclass
@@ -102,6 +151,9 @@ class SceneSpec:
     zones: Sequence[RefineZone] = field(default_factory=list)
     diffuse_ic: bool = False
     rho_ref: Optional[Sequence[float]] = None  # multiphase phase densities (model/multi.hpp:479-483)
+    # init_interface sets the gas density to rho_ref[1] (scene.cpp:362); True keeps a gas density the
+    # initial condition already set (a shocked gas region) instead
+    keep_ic_gas_density: bool = True
 
     @property
     def side_length(self) -> float:
@@ -278,10 +330,7 @@ def build_tree(spec: SceneSpec) -> Tree:
             split |= m4
             cu[m4] = True
         for z in spec.zones:
-            x0 = np.asarray(z.x0, np.float64)[:D]
-            x1 = np.asarray(z.x1, np.float64)[:D]
-            inside = np.all((ctr < x1) & (ctr > x0), axis=1)
-            split |= inside & (lvl < z.level)
+            split |= z.contains(ctr) & (lvl < z.level)
         fl = np.where(cu, fl | F_CAN_UNSPLIT, fl & ~np.uint32(F_CAN_UNSPLIT)).astype(np.uint32)
         g.flags[frontier] = fl
 
@@ -366,8 +415,11 @@ def _init_interface(spec: SceneSpec, g: _Grow, idx: np.ndarray, center: np.ndarr
         alpha = np.where(sm & ~np.isnan(alpha), 0.5 * (1.0 - np.tanh(sd / h)), alpha)
     keep = np.isnan(alpha)
     ia = shape.ia
-    air = p[idx, 1] / np.where(p[idx, ia] < 1.0, 1.0 - p[idx, ia], 1.0)
-    air = np.where(air > 0, air, rho2)
+    if spec.keep_ic_gas_density:
+        air = p[idx, 1] / np.where(p[idx, ia] < 1.0, 1.0 - p[idx, ia], 1.0)
+        air = np.where(air > 0, air, rho2)
+    else:
+        air = np.full(idx.size, float(rho2))
     new = p[idx].copy()
     new[:, 0] = rho1 * alpha
     new[:, 1] = air * (1.0 - alpha)

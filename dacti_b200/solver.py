@@ -88,6 +88,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                           ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_read_slopes.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_longlong,
                                    ctypes.POINTER(ctypes.c_longlong)]
+    lib.dg_read_gradients.argtypes = lib.dg_read_slopes.argtypes
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_set_form.argtypes = [vp, ctypes.c_int]
@@ -100,7 +101,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
-                    "dg_read_cells", "dg_read_slopes",
+                    "dg_read_cells", "dg_read_slopes", "dg_read_gradients",
                     "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
@@ -123,6 +124,7 @@ class Solver:
         sh = t.shape
         self.shape = sh
         self.side_length = prm.side_length
+        self.params = prm
         E, D = sh.E, sh.dims
         nb = max(len(t.bcs), 1)
         keep = dict(
@@ -214,6 +216,16 @@ class Solver:
         out = np.zeros((max(n, 1), sh.dims, sh.E))
         got = ctypes.c_longlong(0)
         self._check(self._lib.dg_read_slopes(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
+        return out[: got.value]
+
+    def active_gradients(self) -> np.ndarray:
+        """dg_read_gradients: the active cells' gradients of the gradient inputs, shape (n, D, G), in
+        active_cells() order (Navier-Stokes and viscous multiphase cases only)."""
+        sh = self.shape
+        n = self.n_active_cells()
+        out = np.zeros((max(n, 1), sh.dims, sh.G))
+        got = ctypes.c_longlong(0)
+        self._check(self._lib.dg_read_gradients(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
         return out[: got.value]
 
     def stats(self) -> DgStats:

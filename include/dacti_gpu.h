@@ -143,6 +143,16 @@ int dg_read_cells(dg_solver *s, int *levels, double *data, long long max_cells, 
  * of the cell, as DACTI's VTU writer does at the cell vertices (driver/io/vtu_writer.hpp:40-62). */
 int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long *n_out);
 
+/* The gradients of the gradient inputs (Cell::gradient, integrator/cell.hpp:20; written by
+ * compute_slope, impl/slopes.hpp:68-70) of the active cells, gradients[n][D][G], in the order of
+ * dg_read_cells. G is NumGrad: D + 1 for Navier-Stokes (velocity, temperature), D + 3 for the
+ * multiphase model (velocity, temperature, volume fraction, and a last slot that is zero here and
+ * indeterminate in the reference, whose get_grad_input leaves it unset, model/multi.hpp:148-156). What
+ * DACTI's DropEnergy observer reads (driver/observer/drop_energy.hpp:25-26). DG_ERR_UNSUPPORTED for
+ * the Euler model (no gradient inputs) and for multiphase cases without viscosity or conduction,
+ * whose steps skip the gradient computation. */
+int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out);
+
 /* Allocation-free variant of dg_read_cells for hosts that cannot let the library call cudaMalloc
  * (a fixed device-memory budget owned by the host's allocator, or a thread that must not take the
  * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference: DACTI's

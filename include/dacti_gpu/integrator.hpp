@@ -346,6 +346,25 @@ namespace dacti::gpu {
 				nd.is_leaf = nd.is_active = true;
 				cells_.push_back(nd);
 			}
+			// slopes for Cell::get_p (vtu_writer), gradients for DropEnergy; a case whose steps keep no
+			// gradients leaves them zero
+			std::vector<double> sl((size_t) D * E * (got > 0 ? got : 1));
+			long long gs = 0;
+			detail::check(dg_read_slopes(solver_.get(), sl.data(), got, &gs), solver_.get(), "dg_read_slopes");
+			for (long long i = 0; i < gs; ++i)
+				for (int d = 0; d < D; ++d)
+					for (int q = 0; q < E; ++q) cells_[1 + i].cell.slope[d][q] = sl[(i * D + d) * E + q];
+			if constexpr (Model::NumGrad > 0) {
+				constexpr int G = Model::NumGrad;
+				std::vector<double> gr((size_t) D * G * (got > 0 ? got : 1));
+				const int rc = dg_read_gradients(solver_.get(), gr.data(), got, &gs);
+				if (rc != DG_ERR_UNSUPPORTED) {
+					detail::check(rc, solver_.get(), "dg_read_gradients");
+					for (long long i = 0; i < gs; ++i)
+						for (int d = 0; d < D; ++d)
+							for (int g = 0; g < G; ++g) cells_[1 + i].cell.gradient[d][g] = gr[(i * D + d) * G + g];
+				}
+			}
 			cache_valid_ = true;
 		}
 	};

@@ -159,13 +159,19 @@ namespace {
 #ifdef DACTI_ADAPTER_CHECK
 	// Integer cell coordinates at the cell's own level: the key under which both sides' cells are
 	// matched (centres are (i + 1/2) size - side/2 on both sides).
+	// Row: level, cell coordinates, ACTI level, u[E], slope[D][E], gradient[D][G].
 	template<typename Node>
-	std::vector<double> cell_row(const Node &node, double side, int D, int E) {
+	std::vector<double> cell_row(const Node &node, double side, int D, int E, int G) {
 		std::vector<double> r;
 		r.push_back(node.tree_level);
 		for (int d = 0; d < D; ++d) r.push_back(std::nearbyint((node.cell.center[d] + 0.5 * side) / node.cell.size - 0.5));
 		r.push_back(node.acti_level);
 		for (int q = 0; q < E; ++q) r.push_back(node.cell.u[q]);
+		for (int d = 0; d < D; ++d)
+			for (int q = 0; q < E; ++q) r.push_back(node.cell.slope[d][q]);
+		if constexpr (requires { node.cell.gradient[0][0]; })
+			for (int d = 0; d < D; ++d)
+				for (int g = 0; g < G; ++g) r.push_back(node.cell.gradient[d][g]);
 		return r;
 	}
 
@@ -183,9 +189,14 @@ namespace {
 		dacti::gpu::Integrator<Model, Limiter, Est> gpu{Limiter{}, Est{cfg->error_weights}, scene_gpu, cfg};
 		const double side = cfg->side_length;
 		int failures      = 0;
+		constexpr int G   = Model::NumGrad;
+		// the GPU keeps gradients only where a viscous or conduction term reads them
+		bool grad_kept = G > 0;
+		if constexpr (Model::Multiphase)
+			grad_kept = Model::mu1 != 0.0 || Model::mu2 != 0.0 || Model::lambda1 != 0.0 || Model::lambda2 != 0.0;
 		auto rows         = [&](auto &itg) {
             std::vector<std::vector<double>> v;
-            itg.for_each_active_cell([&](int, auto &node) { v.push_back(cell_row(node, side, D, E)); });
+            itg.for_each_active_cell([&](int, auto &node) { v.push_back(cell_row(node, side, D, E, G)); });
             std::sort(v.begin(), v.end(), [&](const auto &a, const auto &b) {
                 return std::lexicographical_compare(a.begin(), a.begin() + D + 1, b.begin(), b.begin() + D + 1);
             });
@@ -194,19 +205,31 @@ namespace {
 		auto compare = [&](int step, bool hooks_equal, bool fb_equal) {
 			auto a = rows(ref), b = rows(gpu);
 			bool cells_equal = a.size() == b.size();
-			double num = 0.0, den = 0.0;
-			for (size_t i = 0; cells_equal && i < a.size(); ++i) {
+			// relative L1 difference over columns [k0, k0 + n) of every row
+			auto rel_l1 = [&](int k0, int n) {
+				double num = 0.0, den = 0.0;
+				for (size_t i = 0; cells_equal && i < a.size(); ++i)
+					for (int k = k0; k < k0 + n; ++k) num += std::abs(a[i][k] - b[i][k]), den += std::abs(a[i][k]);
+				return den > 0 ? num / den : num;
+			};
+			for (size_t i = 0; cells_equal && i < a.size(); ++i)
 				for (int k = 0; k < D + 2; ++k) cells_equal = cells_equal && a[i][k] == b[i][k];
-				for (int q = 0; q < E; ++q) num += std::abs(a[i][D + 2 + q] - b[i][D + 2 + q]), den += std::abs(a[i][D + 2 + q]);
-			}
-			double rel = den > 0 ? num / den : num;
-			bool ok    = hooks_equal && fb_equal && cells_equal && ref.global_dt == gpu.global_dt &&
+			const double rel   = rel_l1(D + 2, E);
+			const double rel_s = rel_l1(D + 2 + E, D * E);
+			// multi::get_grad_input leaves its last slot (dbeta) unset (model/multi.hpp:148-156), so the
+			// reference's value there is indeterminate: compare velocity, temperature and alpha only
+			const int g_cmp = Model::Multiphase ? D + 2 : G;
+			double rel_g    = 0.0;
+			for (int d = 0; grad_kept && d < D; ++d) rel_g += rel_l1(D + 2 + E + D * E + d * G, g_cmp);
+			bool ok            = hooks_equal && fb_equal && cells_equal && ref.global_dt == gpu.global_dt &&
 			          ref.n_active_cells() == gpu.n_active_cells() && rel <= 1e-10;
 			if (!ok) failures++;
 			std::printf("{\"step\": %d, \"hooks_equal\": %s, \"force_break_equal\": %s, \"cells_equal\": %s, "
-			            "\"n_ref\": %zu, \"n_gpu\": %zu, \"global_dt_equal\": %s, \"rel_l1_u\": %.3e}\n",
+			            "\"n_ref\": %zu, \"n_gpu\": %zu, \"global_dt_equal\": %s, \"rel_l1_u\": %.3e, "
+			            "\"rel_l1_slope\": %.3e, \"rel_l1_grad\": %.3e, \"grad_compared\": %s}\n",
 			            step, hooks_equal ? "true" : "false", fb_equal ? "true" : "false", cells_equal ? "true" : "false",
-			            ref.n_active_cells(), gpu.n_active_cells(), ref.global_dt == gpu.global_dt ? "true" : "false", rel);
+			            ref.n_active_cells(), gpu.n_active_cells(), ref.global_dt == gpu.global_dt ? "true" : "false", rel,
+			            rel_s, rel_g, grad_kept ? "true" : "false");
 		};
 		compare(0, true, true);
 		for (int step = 1; step <= o.n_steps; ++step) {

@@ -5,8 +5,9 @@ dacti::integrator::Integrator (integrator/integrator.hpp:14-225, compiled from i
 dacti::gpu::Integrator over the GPU library, both built from the same Scene and Config, and drives
 them with the same calls a DACTI driver makes (integrate with a substep hook, n_active_cells,
 for_each_active_cell, global_dt). After construction and after every global step it compares the
-hook sequence, force_break, global_dt, the active cell set with ACTI levels, and the conserved state
-(relative L1 <= 1e-10), printing one JSON line per step.
+hook sequence, force_break, global_dt, the active cell set with ACTI levels, the conserved state
+(relative L1 <= 1e-10), and the slopes and gradients the adapter's nodes carry (relative L1 <= 1e-8;
+gradients where the case has viscous or conduction terms), printing one JSON line per step.
 """
 import json
 import os
@@ -36,3 +37,5 @@ def test_adapter_matches_reference_integrator(name, steps, tmp_path):
     for rec in lines:
         assert rec["hooks_equal"] and rec["force_break_equal"] and rec["cells_equal"], rec
         assert rec["global_dt_equal"] and rec["n_ref"] == rec["n_gpu"] and rec["rel_l1_u"] <= 1e-10, rec
+        # slopes (read by Cell::get_p) and gradients (read by DropEnergy) as the adapter hands them out
+        assert rec["rel_l1_slope"] <= 1e-8 and rec["rel_l1_grad"] <= 1e-8, rec
