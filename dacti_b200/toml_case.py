@@ -30,9 +30,11 @@ Reproduced quirks of the reference parser:
   fluid_1/fluid_2 are parsed after it (model/multi.hpp:491-499, :537-547);
 - `transform_like` naming no geometry gives the identity transform (std::unordered_map::operator[]).
 
-Not supported, with a clear error: STL geometry files (`path`), solid objects and objects with a
-boundary condition (object boundary tagging), airfoil and line shapes, built-in shapes in 3D, and
-refinement zones with a rotated transform.
+Objects with a boundary condition (solids) make the cells inside them inactive and give the faces
+towards them the condition, with the shape's normal (scene/scene.cpp:47-147, :249-337).
+
+Not supported, with a clear error: STL geometry files (`path`), airfoil and line shapes, built-in
+shapes in 3D, and refinement zones with a rotated transform.
 """
 from __future__ import annotations
 
@@ -329,9 +331,6 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
                                   "build does not have; use a built-in shape")
     if "shape" not in g:
         raise ConfigError("Undefined Geometry")
-    if typ == "solid" or bc is not None:
-        raise NotImplementedError(f"geometry '{name}': solid objects and objects with a boundary condition "
-                                  "(object boundary tagging) are not supported")
     if D != 2:
         raise NotImplementedError(f"geometry '{name}': built-in shapes are 2D curves (extruded in 3D by the "
                                   "reference); only 2D cases take them here")
@@ -346,10 +345,10 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
     S = t.scaling[:2]
     if shape == "ellipse":
         axes = (get_entry(g, "a", "float") * S[0], get_entry(g, "b", "float") * S[1])
-        return EllipseObject(tuple(c), axes, typ, None, float(t.rotation[2])), t
+        return EllipseObject(tuple(c), axes, typ, bc, float(t.rotation[2])), t
     if shape == "circle":
         r = get_entry(g, "radius", "float")
-        return EllipseObject(tuple(c), (r * S[0], r * S[1]), typ, None, float(t.rotation[2])), t
+        return EllipseObject(tuple(c), (r * S[0], r * S[1]), typ, bc, float(t.rotation[2])), t
     if shape in ("diamond", "quadrilateral", "triangle"):
         if shape == "diamond":
             a, b = get_entry(g, "width", "float"), get_entry(g, "height", "float")
@@ -358,7 +357,7 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
             keys = ("v1", "v2", "v3", "v4") if shape == "quadrilateral" else ("v1", "v2", "v3")
             v = np.array([get_entry(g, k, "vec", size=2) for k in keys])
         world = (v * S[None, :]) @ R.T + c[None, :]
-        return PolygonObject(world.tolist(), typ, None), t
+        return PolygonObject(world.tolist(), typ, bc), t
     if shape in ("naca_airfoil", "Joukowski_airfoil", "line"):
         raise NotImplementedError(f"geometry '{name}': shape '{shape}' is not supported")
     raise ConfigError("Unknown shape type")

@@ -20,11 +20,14 @@ pytestmark = pytest.mark.gpu
 CHECK = os.path.join(ROOT, "oracle", "_ref", "dacti_adapter_check")
 
 
-@pytest.mark.parametrize("name,steps", [("drop2d", 2), ("bubble_jump2d", 2), ("channel_ns2d", 3)])
-def test_toml_case_matches_reference_integrator(name, steps, tmp_path):
+# Steps stay short of the reference's own NaN: with surface tension at these refinement levels its
+# integrator breaks down within a few steps (the smeared drop at step 3).
+@pytest.mark.parametrize("name,steps,diffuse", [("drop2d", 2, True), ("bubble_jump2d", 3, False),
+                                                ("channel_ns2d", 3, False), ("cylinder_ns2d", 4, False)])
+def test_toml_case_matches_reference_integrator(name, steps, diffuse, tmp_path):
     if not os.path.exists(CHECK):
         pytest.fail("oracle/_ref/dacti_adapter_check is not built (make -C oracle after building the library)")
-    tc = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"))
+    tc = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"), honour_diffuse_ic=diffuse)
     case = str(tmp_path / f"{name}.case")
     write_case(tc.case, case)
     r = subprocess.run([CHECK, case, str(tmp_path / name), str(steps), "--adapter-check"], capture_output=True,
@@ -39,11 +42,12 @@ def test_toml_case_matches_reference_integrator(name, steps, tmp_path):
 
 
 def test_toml_driver_drop_energy(tmp_path):
-    tc = load_toml_case(os.path.join(GOLDEN, "toml", "drop2d.toml"))
+    tc = load_toml_case(os.path.join(GOLDEN, "toml", "drop2d.toml"), honour_diffuse_ic=True)
+    tc.run.io_interval = 0.0  # a frame after every step
     s = Solver(tc.case)
-    d = driver_for(tc, s, str(tmp_path), observers=[DropEnergy(), Totals(6)], max_steps=6)
+    d = driver_for(tc, s, str(tmp_path), observers=[DropEnergy(), Totals(6)], max_steps=2)
     res = d.run()
-    assert not res["force_break"] and res["steps"] == 6
+    assert not res["force_break"] and res["steps"] == 2 and res["frames"] == 2
     path = tmp_path / "drop2d" / "drop2d_observables.csv"
     rows = list(csv.reader(open(path)))
     assert rows[0][:6] == ["time", "frame", "step", "n_cells", "ke", "Etot"]

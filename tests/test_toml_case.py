@@ -50,6 +50,15 @@ type = "periodic"
 """
 
 
+def _write_text(text):
+    import tempfile
+
+    f = tempfile.NamedTemporaryFile("w", suffix=".toml", delete=False)
+    f.write(text)
+    f.close()
+    return f.name
+
+
 def _leaves(tc):
     t = tc.case.tree
     return t.leaf_mask()
@@ -168,7 +177,11 @@ def test_bubble_jump_zone_and_periodic():
     tc = load_toml_case(_path("bubble_jump2d"))
     prm, t = tc.case.params, tc.case.tree
     lm = _leaves(tc)
-    assert prm.sigma == 1.0 / 0.02 and prm.mu1 == 0.0  # We only
+    assert prm.sigma == 0.0 and prm.mu1 == 0.0
+    we = load_toml_case(_write_text(open(_path("bubble_jump2d")).read().replace("L = 0.1", "L = 0.1\nWe = 0.02")))
+    assert we.case.params.sigma == 1.0 / 0.02 and we.case.params.mu1 == 0.0  # We alone: tension, no viscosity
+    with pytest.raises(ConfigError, match="needs We"):
+        load_toml_case(_write_text(open(_path("bubble_jump2d")).read().replace("L = 0.1", "L = 0.1\nRe = 10.0")))
     assert list(prm.periodic) == [False, True]
     # jump: x > -1.5 takes value_pos, else value_neg, then the bubble's gas
     c, p = t.center[lm], t.p[lm]
@@ -226,9 +239,6 @@ def test_geometry_support_and_rejections(tmp_path):
     drop = open(_path("drop2d")).read()
     with pytest.raises(ConfigError, match="Must define boundary condition"):
         load_toml_case(_write(tmp_path, drop.replace('type = "droplet"', 'type = "solid"')))
-    with pytest.raises(NotImplementedError, match="solid"):
-        load_toml_case(_write(tmp_path, drop.replace('type = "droplet"', 'type = "solid"') +
-                              '\n[boundary_conditions.drop]\ntype = "noslip"\n'))
     with pytest.raises(NotImplementedError, match="STL"):
         load_toml_case(_write(tmp_path, drop.replace('shape = "ellipse"', 'path = "stl/x.stl"')))
     with pytest.raises(NotImplementedError, match="naca_airfoil"):
@@ -255,3 +265,59 @@ def test_case_file_round_trip(tmp_path):
         assert np.array_equal(back.tree.p, tc.case.tree.p) and np.array_equal(back.tree.flags, tc.case.tree.flags)
         assert np.array_equal(back.params.param_vector(), tc.case.params.param_vector())
         assert len(back.params.zones) == len(tc.case.params.zones)
+
+
+def _face_neighbours(t, nodes, act, periodic):
+    """Same-level neighbour lookup (Domain::find) for every face of `nodes`: (n, 2D) node indices."""
+    from dacti_b200.scene import _find
+
+    class G:  # the tree's arrays under the names the lookup reads
+        flags, level, center, children = t.flags, t.level, t.center, t.children
+
+    D = t.center.shape[1]
+    size = 4.0 * 0.5 ** t.level[nodes].astype(np.float64)
+    out = np.zeros((nodes.size, 2 * D), np.int64)
+    for d in range(D):
+        for side_dir in range(2):
+            ncen = t.center[nodes].copy()
+            ncen[:, d] += (2.0 * side_dir - 1.0) * size
+            out[:, 2 * d + side_dir] = _find(G, ncen, t.level[nodes], act, periodic)
+    return out
+
+
+def test_solid_cylinder_boundaries():
+    tc = load_toml_case(_path("cylinder_ns2d"))
+    t = tc.case.tree
+    leaf = (t.flags & F_LEAF) != 0
+    act = (t.flags & F_ACTIVE) != 0
+    leaf[0] = False
+    r = np.hypot(t.center[:, 0] + 0.8, t.center[:, 1])
+    inbox = np.abs(t.center[:, 1]) < 1.0
+    al, il = np.nonzero(leaf & act)[0], np.nonzero(leaf & ~act & inbox)[0]
+    # scene.cpp:76-82: cells inside the solid are inactive, all others in the box active
+    assert (r[il] < 0.2).all() and (r[al] > 0.2).all() and il.size > 0
+    # object faces carry the no-slip condition, cells next to the solid are at the geometry level
+    # and cannot coarsen (scene.cpp:118-138)
+    obj = t.bc[al] >= 4
+    walls = al[obj.any(axis=1)]
+    assert walls.size > 0 and (t.level[walls] == 6).all()
+    assert all(t.bcs[b].type == BcType.NOSLIP for b in np.unique(t.bc[al][obj]))
+    from dacti_b200.models import F_CAN_UNSPLIT, F_IS_BOUNDARY
+    assert ((t.flags[walls] & F_CAN_UNSPLIT) == 0).all() and ((t.flags[walls] & F_IS_BOUNDARY) != 0).all()
+    # every face of an active leaf either has a condition or an active neighbour; faces with a
+    # condition towards a cell of the box are paired with one on the other side (fix_boundary's last
+    # pass, scene.cpp:316-334)
+    act_box = np.array([4.0, 2.0])
+    nb = _face_neighbours(t, al, act_box, [False, False])
+    free = t.bc[al] < 0
+    assert ((t.flags[nb[free]] & F_ACTIVE) != 0).all() and (nb[free] != 0).all()
+    for f in range(4):
+        has = (t.bc[al, f] >= 0) & (nb[:, f] != 0)
+        opp = f ^ 1
+        assert (t.bc[nb[has, f], opp] >= 0).all()
+    # the wall normals are the circle's radial directions
+    for i in walls[:8]:
+        for f in np.nonzero(t.bc[i] >= 4)[0]:
+            n = np.asarray(t.bcs[t.bc[i, f]].normal)
+            radial = (t.center[i] - [-0.8, 0.0]) / r[i]
+            assert np.allclose(n, radial, atol=1e-12)
