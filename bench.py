@@ -64,7 +64,7 @@ def workload_config(args) -> dict:
     nb = 1 << args.base_level
     return {
         "workload": f"shock_drop_3d multi<3> {nb}x{nb // 2}x{nb // 2} base +{args.levels} levels, LTS, max_cfl 0.25, "
-                    f"Mach 1.5 shock on a 0.5 mm water drop, plain FP64 form",
+                    f"Mach 1.5 shock on a 0.5 mm water drop; value is the last form in --forms",
         "model": "multi<3> (five-equation, stiffened gas)",
         "base_grid": [nb, nb // 2, nb // 2],
         "levels": args.levels,
