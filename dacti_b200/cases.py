@@ -287,3 +287,35 @@ def osc_drop(base_level: int = 4, levels: int = 2, thresholds=(1e-3, 1e-2), max_
         mu1=mu1, mu2=mu1 / 10.0, lambda1=conductivity[0], lambda2=conductivity[1], sigma=sigma,
     )
     return Case(build_tree(spec), prm)
+
+
+def cylinder_ns(mach: float = 0.3, base_level: int = 5, levels: int = 3, reynolds: float = 200.0,
+                prandtl: float = 0.72, thresholds=(5e-3, 1e-2), max_cfl: float = 0.4,
+                weights=(1.0, 0.01, 0.01, 1e-5), diameter: float = 1.0, center=(-10.0, 0.0)) -> Case:
+    """2D Navier-Stokes flow past a cylinder: domain 40 x 20 (root side 40, so a 2^base_level x
+    2^(base_level-1) base grid), a solid circle of the given diameter with a no-slip wall, inflow of air
+    (rho 1.2, p 101325) at the given Mach number on x-, outflow on x+, free-slip walls on y. The
+    viscosity follows the reference's Navier-Stokes dict (model/navier_stokes.hpp:120-134) with the
+    diameter as length: mu = rho |u| D / Re, lambda = mu cp / Pr. Cells next to the cylinder sit at the
+    finest level."""
+    shape = ModelShape(ModelId.NAVIER_STOKES, 2)
+    rho, p = 1.2, 101325.0
+    u = mach * math.sqrt(1.4 * p / rho)
+    mu = rho * u * diameter / reynolds
+    ref = [rho, u, 0.0, p]
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        return np.tile(ref, (c.shape[0], 1))
+
+    out = [0.0, 0.0, 0.0, p]
+    domain_bc = [(BoundarySpec(BcType.INFLOW, ref), BoundarySpec(BcType.OUTFLOW, out)),
+                 (BoundarySpec(BcType.FREESLIP), BoundarySpec(BcType.FREESLIP))]
+    wall = SphereObject(center, 0.5 * diameter, "solid", BoundarySpec(BcType.NOSLIP))
+    top = base_level + levels
+    spec = SceneSpec(shape, (40.0, 20.0), base_level, top, x2p, domain_bc, max_level_geom=top, objects=[wall])
+    prm = SolverParams(
+        side_length=40.0, active_size=(40.0, 20.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=top, min_level=base_level, weights=weights,
+        ns_mu=mu, ns_lambda=mu * 1005.0 / prandtl,
+    )
+    return Case(build_tree(spec), prm)

@@ -127,6 +127,14 @@ int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long
 	});
 }
 
+int dg_forecast_features(dg_solver *s, double *features, long long max_cells, long long *n_out) {
+	if (!s || !features) return DG_ERR_ARG;
+	return guarded(s, [&] {
+		long long n = s->impl->forecast_features(features, max_cells);
+		if (n_out) *n_out = n;
+	});
+}
+
 int dg_get_stats(dg_solver *s, dg_stats *out) {
 	if (!s || !out) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->stats(out); });

@@ -38,6 +38,8 @@ public:
 	virtual long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) = 0;
 	virtual long long read_slopes(double *data, long long max_cells) = 0;
 	virtual long long read_gradients(double *data, long long max_cells) = 0;
+	virtual long long forecast_features(double *data, long long max_cells) = 0;
+	virtual int dims() const = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
@@ -916,6 +918,15 @@ public:
 			k_gather_slopes<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, list, cnt, base, o);
 		});
 	}
+
+	// Regrid-forecaster features, [5 + 5D] per active cell, in read_cells' order.
+	long long forecast_features(double *data, long long max_cells) override {
+		return read_per_cell(data, max_cells, 5 + 5 * D, "forecast_features",
+		                     [&](const int32_t *list, int cnt, int base, double *o) {
+			                     k_forecast_features<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, C_, list, cnt, base, o);
+		                     });
+	}
+	int dims() const override { return D; }
 
 	// Gradients of the gradient inputs, [D][G] per active cell, in read_cells' order.
 	long long read_gradients(double *data, long long max_cells) override {

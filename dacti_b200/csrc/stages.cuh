@@ -1241,6 +1241,75 @@ __global__ void k_gather_grads(Pool P, const int32_t *list, int n, int base, dou
 	}
 }
 
+// Inputs of the regrid forecaster (no reference counterpart). For leaf i with size h, from its
+// primitive state and limited slopes: a = |grad rho| h / rho, b = |grad p| h / p, w = |curl v| h / (|v| + c);
+// compressed as log(1 + 100 x).
+template<class M>
+__device__ __forceinline__ void forecast_scales(const Pool &P, const Consts &C, int i, double *abw, double *vel) {
+	constexpr int D = M::D, E = M::E;
+	double p[E];
+	load_p<M>(P, i, p);
+	const double h   = C.size[P.level[i]];
+	const double rho = M::MULTI ? p[0] + p[1] : p[0];
+	double gr = 0.0, gp = 0.0, v2 = 0.0;
+	for (int d = 0; d < D; ++d) {
+		const double sr = M::MULTI ? rec_slope<M>(P, i, d, 0) + rec_slope<M>(P, i, d, 1) : rec_slope<M>(P, i, d, 0);
+		const double sp = rec_slope<M>(P, i, d, M::IP);
+		gr += sr * sr;
+		gp += sp * sp;
+		v2 += p[M::IU + d] * p[M::IU + d];
+	}
+	double w2 = 0.0;
+	if constexpr (D == 2) {
+		const double w = rec_slope<M>(P, i, 0, M::IU + 1) - rec_slope<M>(P, i, 1, M::IU);
+		w2 = w * w;
+	} else if constexpr (D == 3) {
+		for (int a = 0; a < 3; ++a) {
+			const int b = (a + 1) % 3, c = (a + 2) % 3;
+			const double w = rec_slope<M>(P, i, b, M::IU + c) - rec_slope<M>(P, i, c, M::IU + b);
+			w2 += w * w;
+		}
+	}
+	const double cs   = sound_speed<M>(C.m, p);
+	const double vref = sqrt(v2) + cs;
+	abw[0] = log1p(100.0 * sqrt(gr) * h / fabs(rho));
+	abw[1] = log1p(100.0 * sqrt(gp) * h / fabs(p[M::IP]));
+	abw[2] = log1p(100.0 * sqrt(w2) * h / vref);
+	for (int d = 0; d < D; ++d) vel[d] = p[M::IU + d] / vref;
+}
+
+// Forecaster features of the listed leaves, FORECAST_F(D) = 5 + 5D doubles each: the cell's a, b, w,
+// level / 16 and log(1 + err / max_err), its velocity over (|v| + c) per dimension, then a and b of the
+// neighbour behind each face (the cell's own where the face is a boundary or the neighbour is refined).
+template<class M>
+__global__ void k_forecast_features(Pool P, Consts C, const int32_t *list, int n, int base, double *out) {
+	constexpr int D = M::D, NF = 2 * D, F = 5 + 5 * D;
+	const int cap = P.cap;
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		double *o   = out + (size_t) (base + tid) * F;
+		double abw[3], vel[D];
+		forecast_scales<M>(P, C, i, abw, vel);
+		o[0] = abw[0];
+		o[1] = abw[1];
+		o[2] = abw[2];
+		o[3] = P.level[i] / 16.0;
+		o[4] = log1p(fmax(P.err[i], 0.0) / C.max_err);
+		for (int d = 0; d < D; ++d) o[5 + d] = vel[d];
+		for (int f = 0; f < NF; ++f) {
+			const int j = P.nbr[(size_t) f * cap + i];
+			double a = abw[0], b = abw[1];
+			if (j > 0 && (P.flags[j] & F_LEAF)) {
+				double nabw[3], nvel[D];
+				forecast_scales<M>(P, C, j, nabw, nvel);
+				a = nabw[0], b = nabw[1];
+			}
+			o[5 + D + 2 * f]     = a;
+			o[5 + D + 2 * f + 1] = b;
+		}
+	}
+}
+
 // Gather of active-cell records for the read-back API.
 template<class M>
 __global__ void k_gather_cells(Pool P, const int32_t *list, int n, int base, double *out, int32_t *lv) {

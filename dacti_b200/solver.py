@@ -89,6 +89,19 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_read_slopes.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_longlong,
                                    ctypes.POINTER(ctypes.c_longlong)]
     lib.dg_read_gradients.argtypes = lib.dg_read_slopes.argtypes
+    lib.dg_forecast_features.argtypes = lib.dg_read_slopes.argtypes
+    fp, dp, ll = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_longlong
+    lib.dg_mlp_last_error.argtypes = []
+    lib.dg_mlp_last_error.restype = ctypes.c_char_p
+    lib.dg_mlp_create.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]
+    lib.dg_mlp_param_count.argtypes = [vp, ctypes.POINTER(ll)]
+    lib.dg_mlp_set_params.argtypes = [vp, fp]
+    lib.dg_mlp_get_params.argtypes = [vp, fp]
+    lib.dg_mlp_predict.argtypes = [vp, fp, ll, fp]
+    lib.dg_mlp_loss_grad.argtypes = [vp, fp, fp, ll, ctypes.c_float, fp, dp]
+    lib.dg_mlp_train.argtypes = [vp, fp, fp, ll, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float,
+                                 ctypes.c_ulonglong, dp]
+    lib.dg_mlp_destroy.argtypes = [vp]
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_set_form.argtypes = [vp, ctypes.c_int]
@@ -101,7 +114,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
-                    "dg_read_cells", "dg_read_slopes", "dg_read_gradients",
+                    "dg_read_cells", "dg_read_slopes", "dg_read_gradients", "dg_forecast_features",
+                    "dg_mlp_last_error", "dg_mlp_create", "dg_mlp_param_count", "dg_mlp_set_params",
+                    "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
                     "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
@@ -227,6 +242,17 @@ class Solver:
         got = ctypes.c_longlong(0)
         self._check(self._lib.dg_read_gradients(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
         return out[: got.value]
+
+    def forecast_features(self) -> np.ndarray:
+        """dg_forecast_features: the regrid forecaster's inputs, shape (n, 5 + 5D), float32, in
+        active_cells() order."""
+        sh = self.shape
+        n = self.n_active_cells()
+        F = 5 + 5 * sh.dims
+        out = np.zeros((max(n, 1), F))
+        got = ctypes.c_longlong(0)
+        self._check(self._lib.dg_forecast_features(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
+        return out[: got.value].astype(np.float32)
 
     def stats(self) -> DgStats:
         s = DgStats()

@@ -153,6 +153,41 @@ int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long 
  * whose steps skip the gradient computation. */
 int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out);
 
+/* ---- Regrid forecaster (no counterpart in the reference) -------------------------------------
+ * A small network that predicts from per-leaf features whether the refinement indicator will fire
+ * at a leaf's place a few global steps ahead. */
+
+/* Forecaster inputs of the active cells, features[n][5 + 5D], in the order of dg_read_cells: for the
+ * cell, log(1 + 100 x) of x = |grad rho| h / rho, |grad p| h / p and |curl v| h / (|v| + c), its tree
+ * level / 16, log(1 + err / max_err) of its last indicator value, its velocity / (|v| + c) per
+ * dimension; then the first two quantities of the neighbour behind each face (face order x-, x+, y-,
+ * ...; the cell's own where the face is a boundary or the neighbour is refined). */
+int dg_forecast_features(dg_solver *s, double *features, long long max_cells, long long *n_out);
+
+/* Multilayer perceptron n_in -> 64 -> 64 -> 1 (ReLU hidden layers, logistic output) on the current
+ * device, n_in <= 32. Parameters, in order: W1[64][n_in], b1[64], W2[64][64], b2[64], W3[64], b3.
+ * Training keeps FP32 master weights and Adam moments; predictions use BF16 copies of the weights.
+ * Errors: negative status, text from dg_mlp_last_error (per host thread). */
+typedef struct dg_mlp dg_mlp;
+const char *dg_mlp_last_error(void);
+/* He-uniform hidden layers and Glorot-uniform output layer from `seed`, zero biases. */
+int dg_mlp_create(int n_in, unsigned long long seed, dg_mlp **out);
+int dg_mlp_param_count(dg_mlp *m, long long *n);
+/* Replace / read the FP32 parameters; setting them also resets the Adam state. */
+int dg_mlp_set_params(dg_mlp *m, const float *params);
+int dg_mlp_get_params(dg_mlp *m, float *params);
+/* prob[n] = sigmoid(logit(x[n][n_in])) with the BF16 weights. */
+int dg_mlp_predict(dg_mlp *m, const float *x, long long n, float *prob);
+/* Sum over the n samples of the loss pw y softplus(-z) + (1 - y) softplus(z) (z the logit, FP32 master
+ * weights) and of its gradient with respect to every parameter. */
+int dg_mlp_loss_grad(dg_mlp *m, const float *x, const float *y, long long n, float pos_weight, float *grad,
+                     double *loss_sum);
+/* `epochs` passes of Adam (beta 0.9 / 0.999) over shuffled minibatches of the mean loss; mean_loss is
+ * the mean over the samples of the last pass. */
+int dg_mlp_train(dg_mlp *m, const float *x, const float *y, long long n, int epochs, int batch, float lr,
+                 float pos_weight, unsigned long long seed, double *mean_loss);
+int dg_mlp_destroy(dg_mlp *m);
+
 /* Allocation-free variant of dg_read_cells for hosts that cannot let the library call cudaMalloc
  * (a fixed device-memory budget owned by the host's allocator, or a thread that must not take the
  * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference: DACTI's

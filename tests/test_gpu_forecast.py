@@ -1,0 +1,99 @@
+"""Regrid forecaster on the GPU: the network's kernels against the CPU oracle (loss and gradient of
+the FP32 master weights, predictions with BF16 weights), training, the solver's feature kernel, and what
+the trained network gains over the method without it on a held-out cylinder-flow run."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+from dacti_b200 import cases
+from dacti_b200.forecast import Mlp, collect, scores, train_forecaster
+from dacti_b200.solver import Solver
+
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import forecast_mlp as ref  # noqa: E402
+
+pytestmark = pytest.mark.gpu
+
+
+def test_loss_gradient_matches_oracle():
+    rng = np.random.default_rng(1)
+    n_in = 15
+    net = Mlp(n_in, seed=3)
+    p = net.params
+    assert p.size == ref.n_params(n_in)
+    x = rng.normal(size=(700, n_in)).astype(np.float32)
+    y = (rng.random(700) < 0.25).astype(np.float32)
+    loss, g = net.loss_grad(x, y, pos_weight=3.0)
+    rl, rg = ref.loss_grad(p.astype(np.float64), x, y, 3.0)
+    assert abs(loss - rl) <= 1e-5 * abs(rl)
+    scale = np.abs(rg).max()
+    assert np.abs(g - rg).max() <= 1e-4 * scale, np.abs(g - rg).max() / scale
+    net.close()
+
+
+def test_predictions_use_bf16_weights():
+    rng = np.random.default_rng(2)
+    net = Mlp(20, seed=5)
+    p = rng.normal(0, 0.2, net.n_params).astype(np.float32)
+    net.params = p
+    assert np.array_equal(net.params, p)
+    x = rng.normal(size=(513, 20)).astype(np.float32)
+    got = net.predict(x)
+    want = ref.predict(ref.bf16(p), x)
+    assert np.abs(got - want).max() <= 2e-5
+    # the FP32 master weights would give a visibly different answer
+    assert np.abs(ref.predict(p.astype(np.float64), x) - want).max() > 1e-4
+    net.close()
+
+
+def test_training_separates_a_toy_problem():
+    rng = np.random.default_rng(4)
+    x = rng.normal(size=(8000, 6)).astype(np.float32)
+    y = ((x[:, 0] + 0.5 * x[:, 1] * x[:, 2]) > 0.3).astype(np.float32)
+    net = Mlp(6, seed=9)
+    first = net.loss_grad(x, y)[0] / y.size
+    last = net.train(x, y, epochs=15, batch=256, lr=3e-3)
+    assert last < 0.5 * first and last < 0.25
+    acc = ((net.predict(x) >= 0.5) == (y > 0.5)).mean()
+    assert acc > 0.93
+    net.close()
+
+
+def test_features_of_the_solver():
+    s = Solver(cases.cylinder_ns(base_level=5, levels=2))
+    for _ in range(2):
+        s.integrate()
+    f = s.forecast_features()
+    snap = s.active_cells()
+    assert f.shape == (snap.n, 15) and np.isfinite(f).all()
+    assert np.allclose(f[:, 3], snap.tree_level / 16.0)
+    max_err = s.params.error_threshold[1]
+    assert np.allclose(f[:, 4], np.log1p(np.maximum(snap.error, 0.0) / max_err), rtol=1e-6, atol=1e-7)
+    # velocity over (|v| + c): the inflow moves along +x at Mach ~0.3
+    assert np.median(f[:, 5]) > 0.15 and np.abs(f[:, 6]).max() < 1.0
+    # density-gradient features: zero-gradient regions give 0, compressed values stay moderate
+    assert (f[:, 0] >= 0).all() and f[:, 0].max() < 12
+    s.close()
+
+
+def _run(seed, steps=20, horizon=8):
+    mach = float(np.random.default_rng(seed).uniform(0.2, 0.4))
+    return collect(lambda: cases.cylinder_ns(mach=mach, base_level=5, levels=3), steps, horizon)
+
+
+def test_forecaster_beats_persistence_on_a_held_out_run():
+    train = [_run(s) for s in (11, 12, 13)]
+    test = _run(21)
+    net, cut, loss = train_forecaster(train, n_in=15, epochs=30)
+    pred = net.predict(test.x) >= cut
+    truth = test.y.astype(bool)
+    mlp, base = scores(pred, truth), scores(test.persistence, truth)
+    print("forecaster", mlp, "persistence", base, "cut", cut, "loss", loss, "samples", truth.size,
+          "positive rate", truth.mean())
+    assert truth.any() and (~truth).any()
+    assert mlp["f1"] > base["f1"] + 0.05
+    assert mlp["recall"] > base["recall"]
+    net.close()
