@@ -51,6 +51,7 @@ def parse_args():
                     help="with --profile-substep -3: the largest substep of this ACTI level instead")
     ap.add_argument("--batch-trees", type=int, default=256, help="trees of the batched 2D Riemann workload")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--forms", default="fp64,mixed", help="numerical forms to time (the last one is `value`)")
     ap.add_argument("--profile-substep", type=int, default=-1,
                     help="bracket only this substep of the first timed step of the last form with "
@@ -276,6 +277,66 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
     return out
 
 
+def learned_run(args, local_rank: int) -> dict:
+    """Regrid forecaster on 2D Navier-Stokes flow past a cylinder (cases.cylinder_ns, base 32 x 16,
+    +3 levels): three training runs with inflow Mach from U(0.2, 0.4) (seeds 11-13), one held-out run
+    (seed 21), 20 global steps each, horizon 8 steps. Reports the network's and persistence's scores
+    on the held-out run, the training time, the prediction rate, and a 16-step forecast-driven run
+    (forecast and coarsening every 8 steps) against the plain regrid."""
+    import time as _t
+
+    from dacti_b200 import cases
+    from dacti_b200.accuracy import density_rel_l1
+    from dacti_b200.forecast import collect, run_with_forecast, scores, train_forecaster
+    from dacti_b200.solver import Solver
+
+    def run(seed):
+        mach = float(np.random.default_rng(seed).uniform(0.2, 0.4))
+        return collect(lambda: cases.cylinder_ns(mach=mach, base_level=5, levels=3), 20, 8)
+
+    train = [run(s) for s in (11, 12, 13)]
+    test = run(21)
+    t0 = _t.perf_counter()
+    net, cut, loss = train_forecaster(train, n_in=15, epochs=30)
+    train_s = _t.perf_counter() - t0
+    net.predict(test.x[:1024])
+    t0 = _t.perf_counter()
+    prob = net.predict(test.x)
+    pred_s = _t.perf_counter() - t0
+    truth = test.y.astype(bool)
+    mlp, base = scores(prob >= cut, truth), scores(test.persistence, truth)
+
+    def cyl():
+        return cases.cylinder_ns(mach=0.3, base_level=5, levels=3)
+
+    plain, fc = Solver(cyl(), device=local_rank), Solver(cyl(), device=local_rank)
+    t0 = _t.perf_counter()
+    for _ in range(16):
+        plain.integrate()
+    plain_s = _t.perf_counter() - t0
+    t0 = _t.perf_counter()
+    res = run_with_forecast(fc, net, cut, steps=16, interval=8)
+    fc_s = _t.perf_counter() - t0
+    sp = plain.stats()
+    err = density_rel_l1(plain.active_cells(), fc.active_cells(), 40.0, (40.0, 20.0), 8, 1)
+    plain.close(), fc.close(), net.close()
+    keep = ("precision", "recall", "f1")
+    return {
+        "workload": "2D Navier-Stokes cylinder, 40 x 20, base 32 x 16 +3 levels, Re 200; 3 training runs, 1 held-out",
+        "network": "15 -> 64 -> 64 -> 1, BF16 inference weights, FP32 master + Adam",
+        "held_out": {"samples": int(truth.size), "positive_rate": float(truth.mean()), "cut": cut,
+                     "forecaster": {k: mlp[k] for k in keep}, "persistence": {k: base[k] for k in keep}},
+        "train_seconds": train_s, "train_samples": int(sum(r.y.size for r in train)), "last_epoch_loss": loss,
+        "predict_samples_per_s": truth.size / pred_s,
+        "regrid": {"steps": 16, "interval": 8,
+                   "plain": {"splits": sp.n_splits, "unsplits": sp.n_unsplits, "cell_updates": sp.cell_updates,
+                             "seconds": plain_s},
+                   "forecast": {"splits": res["splits"], "unsplits": res["unsplits"], "held": res["held"],
+                                "cell_updates": res["cell_updates"], "seconds": fc_s},
+                   "density_rel_l1_vs_plain": err},
+    }
+
+
 def batched_run(args, local_rank: int, world: int) -> dict:
     """Batched 2D Euler quadtree Riemann problems (seeded, see cases.riemann_batch): one global step of
     every tree per call of dg_step_many (host threads, one stream per tree), against the same trees
@@ -428,6 +489,8 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     if not args.no_batched:
         result["batched"] = batched_run(args, local_rank, world)
+    if not args.no_learned and world == 1:
+        result["learned"] = learned_run(args, local_rank)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_RUNNER):
         threads = host_threads()

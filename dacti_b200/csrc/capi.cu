@@ -135,6 +135,16 @@ int dg_forecast_features(dg_solver *s, double *features, long long max_cells, lo
 	});
 }
 
+int dg_set_hold(dg_solver *s, const unsigned char *hold, long long n) {
+	if (!s || (!hold && n > 0)) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_hold(hold, n); });
+}
+
+int dg_set_coarsen_interval(dg_solver *s, int steps) {
+	if (!s) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_coarsen_interval(steps); });
+}
+
 int dg_get_stats(dg_solver *s, dg_stats *out) {
 	if (!s || !out) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->stats(out); });

@@ -20,6 +20,7 @@ enum : uint32_t {
 	F_CAN_UNSPLIT  = 1u << 4,
 	F_SHOULD_SPLIT = 1u << 5,
 	F_IS_BOUNDARY  = 1u << 6,
+	F_HOLD         = 1u << 7,  // held by the regrid forecaster: never coarsened
 };
 
 // Refinement op codes written by the estimation kernel.
@@ -70,6 +71,7 @@ struct Consts {
 	// Active box in cells per tree level and dimension: [a0, a0 + na).
 	int a0[MAX_TREE][3], na[MAX_TREE][3];
 	int signal;  // `signal` argument of integrate (hold-droplet-still switch)
+	int coarsen; // 0 on global steps where a forecast-driven regrid skips coarsening
 };
 
 // Boundary table (one Boundary<M> value per entry).

@@ -40,6 +40,8 @@ public:
 	virtual long long read_gradients(double *data, long long max_cells) = 0;
 	virtual long long forecast_features(double *data, long long max_cells) = 0;
 	virtual int dims() const = 0;
+	virtual void set_hold(const uint8_t *hold, long long n) = 0;
+	virtual void set_coarsen_interval(int k) = 0;
 	virtual void stats(dg_stats *out) = 0;
 	virtual void set_stream(cudaStream_t s) = 0;
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
@@ -83,6 +85,7 @@ class Solver : public SolverBase {
 	int32_t *d_readlv_ = nullptr;
 	long long read_cap_ = 0;
 	int limiter_ = 0;
+	int coarsen_every_ = 1;  // global steps between coarsening passes
 	bool visc_   = false;  // viscous/heat terms present (multiphase with any non-zero mu or lambda)
 	bool mixed_  = false;  // FP32 reconstruction and flux, FP64 update and EOS recovery
 	bool sigma_  = false;  // surface tension present
@@ -241,6 +244,7 @@ public:
 		sigma_ = m.sigma != 0.0;
 		if (c.n_zones > MAX_ZONES) throw dg_error(DG_ERR_ARG, "too many refinement zones");
 		C_.n_zones = c.n_zones;
+		C_.coarsen = 1;
 		for (int z = 0; z < c.n_zones; ++z) {
 			for (int d = 0; d < 3; ++d) {
 				C_.zx0[z][d] = c.zones[7 * z + d];
@@ -683,6 +687,7 @@ public:
 	// Integrator::integrate (impl/integrate.hpp:12-87)
 	void step(int signal, int *force_break, double *global_dt, dg_substep_fn fn, void *user) override {
 		C_.signal   = signal;
+		C_.coarsen  = (n_global_ % coarsen_every_) == 0;
 		*force_break = 0;
 		const int top_seq = 1 << (MAX_ACTI - 1);
 		int seq           = 0;
@@ -927,6 +932,32 @@ public:
 		                     });
 	}
 	int dims() const override { return D; }
+
+	// Forecast-driven regrid: F_HOLD on the active cells (read_cells' order) and the interval in global
+	// steps between coarsening passes (1 = every step, the reference's behaviour).
+	void set_hold(const uint8_t *hold, long long n) override {
+		if (n != cell_count()) throw dg_error(DG_ERR_ARG, "dg_set_hold: one entry per active cell expected");
+		uint8_t *d = nullptr;
+		DG_CUDA(cudaMalloc(&d, n > 0 ? n : 1));
+		cudaError_t e = n > 0 ? cudaMemcpyAsync(d, hold, n, cudaMemcpyHostToDevice, st_) : cudaSuccess;
+		long long base = 0;
+		for (int pass = 0; e == cudaSuccess && pass < 2; ++pass) {
+			for (int l = 0; l < MAX_ACTI; ++l) {
+				const int cnt = pass == 0 ? h_cnt_->clu[l] : h_cnt_->buf[l];
+				if (cnt == 0) continue;
+				k_set_hold<M><<<grid_for(cnt), BLOCK, 0, st_>>>(P_, pass == 0 ? Ls_.clu[l] : Ls_.buf[l], cnt, (int) base, d);
+				base += cnt;
+			}
+		}
+		if (e == cudaSuccess) e = cudaGetLastError();
+		if (e == cudaSuccess) e = cudaStreamSynchronize(st_);
+		cudaFree(d);
+		if (e != cudaSuccess) throw dg_error(DG_ERR_CUDA, std::string("set_hold: ") + cudaGetErrorString(e));
+	}
+	void set_coarsen_interval(int k) override {
+		if (k < 1) throw dg_error(DG_ERR_ARG, "dg_set_coarsen_interval: interval must be >= 1");
+		coarsen_every_ = k;
+	}
 
 	// Gradients of the gradient inputs, [D][G] per active cell, in read_cells' order.
 	long long read_gradients(double *data, long long max_cells) override {

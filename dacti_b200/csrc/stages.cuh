@@ -804,7 +804,7 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 			}
 			if (ready) op |= OP_SPLIT;
 		}
-		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1) {
+		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1 && C.coarsen && !(fl & F_HOLD)) {
 			bool ok = true;
 			for (int f = 0; f < NF; ++f) {
 				const int32_t code = P.nbi[(size_t) tid * NF + f];
@@ -1307,6 +1307,15 @@ __global__ void k_forecast_features(Pool P, Consts C, const int32_t *list, int n
 			o[5 + D + 2 * f]     = a;
 			o[5 + D + 2 * f + 1] = b;
 		}
+	}
+}
+
+// Sets (hold[base + tid] != 0) or clears F_HOLD on the listed leaves.
+template<class M>
+__global__ void k_set_hold(Pool P, const int32_t *list, int n, int base, const uint8_t *hold) {
+	for (int tid = gtid(); tid < n; tid += gstride()) {
+		const int i = list[tid];
+		P.flags[i]  = hold[base + tid] ? (P.flags[i] | F_HOLD) : (P.flags[i] & ~F_HOLD);
 	}
 }
 

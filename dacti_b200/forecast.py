@@ -8,7 +8,8 @@ is positive when, at step n + horizon, its region holds a leaf whose indicator v
 threshold or has been refined past the leaf's level, or lies inside a flagged coarser leaf.
 
 The method without the network ("persistence") predicts that exactly the leaves flagged now stay
-flagged; `evaluate` scores both against the labels.
+flagged; `scores` rates either against the labels. `run_with_forecast` drives the solver's regrid
+with the network's predictions.
 """
 from __future__ import annotations
 
@@ -197,3 +198,25 @@ def train_forecaster(runs: Sequence[RunData], n_in: int, epochs: int = 30, seed:
     loss = net.train(x, y, epochs=epochs, batch=512, lr=lr, pos_weight=pw, seed=seed + 1)
     cut = best_threshold(net.predict(x), y.astype(bool))
     return net, cut, loss
+
+
+def run_with_forecast(solver: Solver, net: Mlp, cut: float, steps: int, interval: int = 8) -> dict:
+    """Advances `steps` global steps with the forecast-driven regrid: every `interval` steps the
+    network marks the cells it expects the indicator to flag within its horizon (dg_set_hold: they are
+    not coarsened), and coarsening runs on those steps only (dg_set_coarsen_interval). The plain
+    indicator still splits what it flags at every substep.
+    Returns the solver's split/unsplit counts and the number of held cells per forecast."""
+    solver.set_coarsen_interval(interval)
+    held = []
+    fb = False
+    for n in range(steps):
+        if n % interval == 0:
+            hold = net.predict(solver.forecast_features()) >= cut
+            solver.set_hold(hold)
+            held.append(int(hold.sum()))
+        _, fb = solver.integrate()
+        if fb:
+            break
+    st = solver.stats()
+    return {"splits": st.n_splits, "unsplits": st.n_unsplits, "held": held, "force_break": fb,
+            "cell_updates": st.cell_updates}

@@ -91,6 +91,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_read_gradients.argtypes = lib.dg_read_slopes.argtypes
     lib.dg_forecast_features.argtypes = lib.dg_read_slopes.argtypes
     fp, dp, ll = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_longlong
+    lib.dg_set_hold.argtypes = [vp, ctypes.POINTER(ctypes.c_ubyte), ll]
+    lib.dg_set_coarsen_interval.argtypes = [vp, ctypes.c_int]
     lib.dg_mlp_last_error.argtypes = []
     lib.dg_mlp_last_error.restype = ctypes.c_char_p
     lib.dg_mlp_create.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]
@@ -114,7 +116,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
-                    "dg_read_cells", "dg_read_slopes", "dg_read_gradients", "dg_forecast_features",
+                    "dg_read_cells", "dg_read_slopes", "dg_read_gradients", "dg_forecast_features", "dg_set_hold", "dg_set_coarsen_interval",
                     "dg_mlp_last_error", "dg_mlp_create", "dg_mlp_param_count", "dg_mlp_set_params",
                     "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
                     "dg_read_cells_noalloc", "dg_get_stats",
@@ -253,6 +255,14 @@ class Solver:
         got = ctypes.c_longlong(0)
         self._check(self._lib.dg_forecast_features(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
         return out[: got.value].astype(np.float32)
+
+    def set_hold(self, hold) -> None:
+        """dg_set_hold: one flag per active cell (active_cells() order)."""
+        h = np.ascontiguousarray(hold, np.uint8)
+        self._check(self._lib.dg_set_hold(self._h, h.ctypes.data_as(ctypes.POINTER(ctypes.c_ubyte)), h.size))
+
+    def set_coarsen_interval(self, steps: int) -> None:
+        self._check(self._lib.dg_set_coarsen_interval(self._h, steps))
 
     def stats(self) -> DgStats:
         s = DgStats()

@@ -164,6 +164,15 @@ int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long
  * ...; the cell's own where the face is a boundary or the neighbour is refined). */
 int dg_forecast_features(dg_solver *s, double *features, long long max_cells, long long *n_out);
 
+/* Forecast-driven regrid. hold[n] (one byte per active cell, dg_read_cells' order; n must equal the
+ * active cell count): a held cell is never coarsened; splitting stays with the plain indicator, which
+ * keeps splitting the cells it flags at every substep. dg_set_coarsen_interval
+ * runs the coarsening test only on global steps that are multiples of `steps` (1, the default, is the
+ * reference's every-substep behaviour). Holds stay until the next dg_set_hold; children of a split do
+ * not inherit them. */
+int dg_set_hold(dg_solver *s, const unsigned char *hold, long long n);
+int dg_set_coarsen_interval(dg_solver *s, int steps);
+
 /* Multilayer perceptron n_in -> 64 -> 64 -> 1 (ReLU hidden layers, logistic output) on the current
  * device, n_in <= 32. Parameters, in order: W1[64][n_in], b1[64], W2[64][64], b2[64], W3[64], b3.
  * Training keeps FP32 master weights and Adam moments; predictions use BF16 copies of the weights.

@@ -9,7 +9,7 @@ import pytest
 
 from conftest import ROOT
 from dacti_b200 import cases
-from dacti_b200.forecast import Mlp, collect, scores, train_forecaster
+from dacti_b200.forecast import Mlp, collect, run_with_forecast, scores, train_forecaster
 from dacti_b200.solver import Solver
 
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -96,4 +96,79 @@ def test_forecaster_beats_persistence_on_a_held_out_run():
     assert truth.any() and (~truth).any()
     assert mlp["f1"] > base["f1"] + 0.05
     assert mlp["recall"] > base["recall"]
+    net.close()
+
+
+def _cyl():
+    return cases.cylinder_ns(mach=0.3, base_level=5, levels=3)
+
+
+def test_regrid_controls_default_to_the_reference():
+    a, b = Solver(_cyl()), Solver(_cyl())
+    b.set_coarsen_interval(1)
+    b.set_hold(np.zeros(b.n_active_cells(), np.uint8))
+    for _ in range(3):
+        a.integrate()
+        b.integrate()
+    sa, sb = a.active_cells(), b.active_cells()
+    assert np.array_equal(sa.tree_level, sb.tree_level) and np.array_equal(sa.u, sb.u)
+    a.close(), b.close()
+
+
+def _coarsened(before, after, side=40.0):
+    """Leaves of `after` coarser than the leaves of `before` at their place."""
+    from dacti_b200.casefile import cell_coords
+    from dacti_b200.forecast import _keys
+
+    kb = set(_keys(before.tree_level, cell_coords(before.center, before.tree_level, side)).tolist())
+    la = after.tree_level.astype(np.int64)
+    ca = cell_coords(after.center, la, side)
+    found = np.zeros(la.size, bool)
+    for l in range(int(la.max()) + 1):
+        m = la >= l
+        anc = _keys(np.full(m.sum(), l), ca[m] >> (la[m] - l)[:, None])
+        found[np.nonzero(m)[0][np.isin(anc, np.fromiter(kb, np.uint64))]] = True
+    return int((~found).sum())
+
+
+def test_held_cells_never_coarsen():
+    free, held = Solver(_cyl()), Solver(_cyl())
+    for _ in range(6):  # the start-up transient refines around the cylinder and the wake
+        free.integrate()
+        held.integrate()
+    f6, h6 = free.active_cells(), held.active_cells()
+    held.set_hold(np.ones(held.n_active_cells(), np.uint8))
+    for _ in range(6):
+        free.integrate()
+        held.integrate()
+    # the free run coarsens some of the step-6 cells again; none of the held ones is (cells created
+    # after the hold are not held)
+    assert _coarsened(f6, free.active_cells()) > 0
+    assert _coarsened(h6, held.active_cells()) == 0
+    # coarsening skipped on global steps that are not multiples of the interval
+    free.set_coarsen_interval(8)
+    u0 = free.stats().n_unsplits
+    free.integrate()  # global step 12
+    free.integrate()  # global step 13
+    assert free.stats().n_unsplits == u0
+    free.close(), held.close()
+
+
+def test_forecast_driven_regrid_against_plain():
+    from dacti_b200.accuracy import density_rel_l1
+
+    train = [_run(s) for s in (11, 12, 13)]
+    net, cut, _ = train_forecaster(train, n_in=15, epochs=30)
+    plain, fc = Solver(_cyl()), Solver(_cyl())
+    for _ in range(16):
+        plain.integrate()
+    res = run_with_forecast(fc, net, cut, steps=16, interval=8)
+    sp = plain.stats()
+    err = density_rel_l1(plain.active_cells(), fc.active_cells(), 40.0, (40.0, 20.0), 8, 1)
+    print("plain splits", sp.n_splits, "unsplits", sp.n_unsplits, "updates", sp.cell_updates,
+          "| forecast", res, "| density rel-L1 vs plain", err)
+    assert not res["force_break"]
+    assert res["unsplits"] < sp.n_unsplits  # coarsening runs on one step in eight, never on held cells
+    assert err < 5e-3
+    plain.close(), fc.close()
     net.close()
