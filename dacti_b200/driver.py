@@ -65,6 +65,97 @@ class DropEnergy:
         return [float(ke.sum()), float((ke + vol * solver.params.sigma * norm).sum())]
 
 
+def locate(snap, side_length: float, pts: np.ndarray) -> np.ndarray:
+    """Integrator::get_cell_index (integrator/integrator.hpp:168) over the active leaves of `snap`:
+    the row of the leaf containing each point, -1 where none does."""
+    from .casefile import cell_coords
+
+    lv = snap.tree_level.astype(np.int64)
+    coords = cell_coords(snap.center, lv, side_length)
+    D = snap.dims
+
+    def key(level, c):
+        k = np.asarray(level, np.int64) << np.int64(60)
+        for d in range(D):
+            k = k | (c[:, d].astype(np.int64) << np.int64(40 - 20 * d))
+        return k
+
+    keys = key(lv, coords)
+    order = np.argsort(keys)
+    sk = keys[order]
+    out = np.full(pts.shape[0], -1, np.int64)
+    for l in np.unique(lv):
+        n_l = np.int64(1) << np.int64(l)
+        pc = np.floor((pts[:, :D] / side_length + 0.5) * n_l).astype(np.int64)
+        q = key(np.full(pts.shape[0], l), pc)
+        pos = np.clip(np.searchsorted(sk, q), 0, sk.size - 1)
+        hit = (sk[pos] == q) & (out < 0)
+        out[hit] = order[pos[hit]]
+    return out
+
+
+class AeroForce:
+    """DACTI's AeroForce observer (driver/observer/aero_force.hpp:8-131) for 2D cases with analytic
+    solid objects: pressure coefficients Cp = (p - p_ref) / (rho_ref |v_ref|^2 / 2) sampled along each
+    object's outline (segments split into max(int(10 * length), 1) samples, each moved 0.01 off the
+    surface), integrated to Cl and Cd; field variables Cp and ObjectSurface on the cells next to an
+    object. Differences from the reference: the outline is the analytic curve cut into `n_segments`
+    pieces instead of the adaptively sampled mesh, the samples move 0.01 into the fluid (the reference
+    moves them along -rotaten90 of the counter-clockwise tangent, i.e. into the body), and Cl, Cd are
+    the pressure force on the body per unit span and dynamic pressure (drag positive along +x); the
+    surface cells are those with a face neighbour centre inside an object (the signed-distance part of
+    the reference's boundary test)."""
+
+    name = "Aerodynamic Forces"
+    names = ["Cl", "Cd"]
+    field_names = ["Cp", "ObjectSurface"]
+
+    def __init__(self, objects, p_ref, vel_ref, n_segments: int = 256, sample_resolution: int = 10):
+        self.objects = list(objects)  # every object is sampled, as in the reference
+        self.walls = [o for o in self.objects if getattr(o, "bc", None) is not None]
+        self.p_ref = np.asarray(p_ref, np.float64)
+        v = np.asarray(vel_ref, np.float64)
+        self.q_inv = 2.0 / (self.p_ref[0] * float(v @ v))
+        pts, area, nrm = [], [], []
+        for o in self.objects:
+            ring = o.outline(n_segments)
+            nxt = np.roll(ring, -1, axis=0)
+            for a, b in zip(ring, nxt):
+                ab = b - a
+                length = float(np.hypot(*ab))
+                out_n = np.array([ab[1], -ab[0]]) / length  # outward for a counter-clockwise outline
+                k = max(int(sample_resolution * length), 1)
+                for j in range(k):
+                    pts.append(a + (j + 0.5) * ab / k + 0.01 * out_n)
+                    area.append(length / k)
+                    nrm.append(out_n)
+        self.pts, self.area, self.nrm = np.array(pts), np.array(area), np.array(nrm)
+
+    def observe(self, solver, snap) -> list:
+        idx = locate(snap, solver.side_length, self.pts)
+        ok = idx >= 0
+        ip = solver.shape.ip
+        cp = np.zeros(idx.size)
+        cp[ok] = (snap.p[idx[ok], ip] - self.p_ref[ip]) * self.q_inv
+        fx = -(cp * self.area * self.nrm[:, 0]).sum()
+        fy = -(cp * self.area * self.nrm[:, 1]).sum()
+        return [float(fy), float(fx)]
+
+    def fields(self, solver, snap) -> list:
+        D = snap.dims
+        size = solver.side_length * 0.5 ** snap.tree_level.astype(np.float64)
+        surf = np.zeros(snap.n, bool)
+        for d in range(D):
+            for sgn in (-1.0, 1.0):
+                c = snap.center.copy()
+                c[:, d] += sgn * size
+                for o in self.walls:
+                    surf |= o.signed_distance(c) < 0.0
+        ip = solver.shape.ip
+        cp = np.where(surf, (snap.p[:, ip] - self.p_ref[ip]) * self.q_inv, 0.0)
+        return [cp, surf.astype(np.float64)]
+
+
 class DefaultDriver:
     def __init__(self, solver: Solver, name: str, out_dir: str, end_time: Optional[float] = None,
                  io_interval: float = 0.0, observers: Sequence = (), convergence_tol: float = 0.0,
@@ -83,8 +174,14 @@ class DefaultDriver:
 
     def _frame(self, frame: int, snap) -> None:
         if self.write_frames:
+            # observers' field variables as cell data "<observer>/<field>" (driver/default_driver.hpp:45-72)
+            fields = {}
+            for ob in self.observers:
+                if hasattr(ob, "fields"):
+                    for fname, arr in zip(ob.field_names, ob.fields(self.s, snap)):
+                        fields[f"{ob.name}/{fname}"] = arr
             write_vtu(os.path.join(self.out_dir, f"{self.name}_{frame:04d}.vtu"), snap, self.s.active_slopes(),
-                      self.s.side_length)
+                      self.s.side_length, fields=fields)
 
     def run(self) -> dict:
         os.makedirs(self.out_dir, exist_ok=True)

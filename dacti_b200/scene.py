@@ -72,6 +72,12 @@ class SphereObject:
         c = np.asarray(self.center, dtype=np.float64)[: a.shape[1]]
         return _hits_unit_sphere((a - c) / self.radius, (b - c) / self.radius)
 
+    def outline(self, n: int) -> np.ndarray:
+        """n points of the 2D circle, counter-clockwise."""
+        t = 2.0 * math.pi * np.arange(n) / n
+        c = np.asarray(self.center, dtype=np.float64)[:2]
+        return c + self.radius * np.stack([np.cos(t), np.sin(t)], axis=1)
+
 
 def _unit(v: np.ndarray) -> np.ndarray:
     n = np.sqrt((v ** 2).sum(axis=1, keepdims=True))
@@ -143,6 +149,15 @@ class EllipseObject:
         yb, _, _, _ = self._frame(b_pt)
         return _hits_unit_sphere(ya / a, yb / a)
 
+    def outline(self, n: int) -> np.ndarray:
+        """n points of the 2D ellipse, counter-clockwise."""
+        t = 2.0 * math.pi * np.arange(n) / n
+        a = np.asarray(self.axes, dtype=np.float64)[:2]
+        y = np.stack([a[0] * np.cos(t), a[1] * np.sin(t)], axis=1)
+        th = self.angle_deg * math.pi / 180.0
+        R = np.array([[math.cos(th), -math.sin(th)], [math.sin(th), math.cos(th)]])
+        return np.asarray(self.center, dtype=np.float64)[:2] + y @ R.T
+
 
 @dataclass
 class PolygonObject:
@@ -187,6 +202,12 @@ class PolygonObject:
             best = np.where(closer, dist, best)
             nrm[closer] = cand[closer]
         return nrm
+
+    def outline(self, n: int = 0) -> np.ndarray:
+        """The vertices, counter-clockwise."""
+        v = np.asarray(self.vertices, np.float64)
+        area2 = (v[:, 0] * np.roll(v[:, 1], -1) - np.roll(v[:, 0], -1) * v[:, 1]).sum()
+        return v if area2 > 0 else v[::-1].copy()
 
     def segment_hits(self, p: np.ndarray, q: np.ndarray) -> np.ndarray:
         """Whether the segment p-q meets any edge (touching counts)."""

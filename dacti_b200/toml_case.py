@@ -80,6 +80,7 @@ class TomlCase:
     vel_ref: np.ndarray
     rho_ref: Optional[tuple]
     ignored: list = field(default_factory=list)  # keys present in the file that the reference ignores
+    objects: list = field(default_factory=list)  # the analytic geometry objects, for observers
 
 
 def _at_path(table: dict, path: str):
@@ -462,7 +463,7 @@ def load_toml_case(path: str, model: Optional[str] = None, limiter: int = 0, hon
         raise ConfigError("multiphase objects need reference densities")
     tree = build_tree(spec)
     run = RunSettings(name, io_interval, end_time, signal_time, steady_tol)
-    return TomlCase(Case(tree, prm), run, model, p_ref, vel_ref, rho_ref, ignored)
+    return TomlCase(Case(tree, prm), run, model, p_ref, vel_ref, rho_ref, ignored, objects)
 
 
 def driver_for(tc: TomlCase, solver, out_dir: str, observers=(), **kw):

@@ -72,3 +72,25 @@ def test_gradients_unsupported_without_viscous_terms():
     with pytest.raises(Exception, match="gradients are kept only"):
         s.active_gradients()
     s.close()
+
+
+def test_toml_cylinder_aero_force(tmp_path):
+    from dacti_b200.driver import AeroForce
+    from dacti_b200.io import read_vtu_arrays
+
+    tc = load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"))
+    tc.run.io_interval = 0.0  # a frame after every step
+    s = Solver(tc.case)
+    ob = AeroForce(tc.objects, tc.p_ref, tc.vel_ref)
+    res = driver_for(tc, s, str(tmp_path), observers=[ob], max_steps=4).run()
+    assert not res["force_break"] and res["frames"] == 4
+    rows = list(csv.reader(open(tmp_path / "cylinder_ns2d" / "cylinder_ns2d_observables.csv")))
+    assert rows[0][4:] == ["Cl", "Cd"]
+    cd = np.array([float(r[5]) for r in rows[1:]])
+    cl = np.array([float(r[4]) for r in rows[1:]])
+    # the impulsively started flow pushes the cylinder downstream; the inflow is 1 degree off axis
+    assert np.isfinite(cd).all() and cd[-1] > 0 and np.abs(cl[-1]) < cd[-1]
+    a = read_vtu_arrays(str(tmp_path / "cylinder_ns2d" / "cylinder_ns2d_0004.vtu"))
+    surf = a["Aerodynamic Forces/ObjectSurface"]
+    assert surf.sum() > 0 and (a["Aerodynamic Forces/Cp"][surf == 0] == 0).all()
+    s.close()
