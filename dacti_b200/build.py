@@ -17,7 +17,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdacti_gpu.so")
 
-UNITS = ["capi.cu", "noalloc.cu", "forecast.cu", "solver_euler.cu", "solver_ns.cu", "solver_multi.cu"]
+UNITS = ["capi.cu", "noalloc.cu", "forecast.cu", "scene_build.cu", "solver_euler.cu", "solver_ns.cu", "solver_multi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "--expt-relaxed-constexpr", "-I" + os.path.join(HERE, "..", "include")]

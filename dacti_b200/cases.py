@@ -111,10 +111,16 @@ def normal_shock(rho1: float, p1: float, mach: float, gamma: float = 1.4, P0: fl
     return r2, u2, p2
 
 
+def shock_drop_spec(*args, **kw):
+    """(SceneSpec, SolverParams) of shock_drop, for builders other than the host one."""
+    return shock_drop(*args, _spec_only=True, **kw)
+
+
 def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: float = 8e-3, aspect: int = 2,
                drop_radius: float = 0.5e-3, shock_x: float = -1.0e-3, mach: float = 1.5,
                thresholds=(0.02, 0.05), max_cfl: float = 0.25, weights: Optional[tuple] = None,
-               mu: tuple = (0.0, 0.0), conductivity: tuple = (0.0, 0.0), sigma: float = 0.0) -> Case:
+               mu: tuple = (0.0, 0.0), conductivity: tuple = (0.0, 0.0), sigma: float = 0.0,
+               _spec_only: bool = False) -> Case:
     """Config 2: five-equation air-water shock-drop.
 
     Domain ``length`` x ``length/aspect`` (x ``length/aspect``) with a ``2^base_level`` cell root
@@ -156,7 +162,7 @@ def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: floa
         shape, active, base_level, base_level + levels, x2p, dbc,
         jump=(0, shock_x),
         objects=[SphereObject((0.0, 0.0, 0.0), drop_radius, "droplet")],
-        diffuse_ic=True, rho_ref=(rho_w, rho_a),
+        diffuse_ic=True, rho_ref=(rho_w, rho_a), ic=("jump", 0, shock_x, post, pre),
     )
     if weights is None:
         weights = (1e-3, 1.0) + (0.0,) * dims + (3e-6, 1.0)
@@ -166,6 +172,8 @@ def shock_drop(dims: int = 3, base_level: int = 6, levels: int = 4, length: floa
         gamma1=4.4, gamma2=1.4, P1=6.0e8, P2=0.0, mu1=mu[0], mu2=mu[1], lambda1=conductivity[0],
         lambda2=conductivity[1], sigma=sigma,
     )
+    if _spec_only:
+        return spec, prm
     return Case(build_tree(spec), prm)
 
 

@@ -265,6 +265,9 @@ class SceneSpec:
     # init_interface sets the gas density to rho_ref[1] (scene.cpp:362); True keeps a gas density the
     # initial condition already set (a shocked gas region) instead
     keep_ic_gas_density: bool = True
+    # the initial condition as data, for the device builder: ("uniform", p) or ("jump", axis, location,
+    # p_neg, p_pos) with p_pos where x[axis] > location; must agree with x2p
+    ic: Optional[tuple] = None
 
     @property
     def side_length(self) -> float:

@@ -119,6 +119,7 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_read_cells", "dg_read_slopes", "dg_read_gradients", "dg_forecast_features", "dg_set_hold", "dg_set_coarsen_interval",
                     "dg_mlp_last_error", "dg_mlp_create", "dg_mlp_param_count", "dg_mlp_set_params",
                     "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
+                    "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
                     "dg_read_cells_noalloc", "dg_get_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 

@@ -74,6 +74,7 @@ class RunSettings:
 @dataclass
 class TomlCase:
     case: Case
+    spec: SceneSpec
     run: RunSettings
     model: str
     p_ref: np.ndarray
@@ -456,14 +457,21 @@ def load_toml_case(path: str, model: Optional[str] = None, limiter: int = 0, hon
         zones.append(RefineZone(list(x0), list(x1), level))
     prm.zones = zones
 
+    ic_data = None
+    if x2p is None:
+        if jump is None:
+            ic_data = ("uniform", np.asarray(p_ref, np.float64))
+        else:
+            ic_data = ("jump", jump[0], jump[1], get_entry(ic, "value_neg", "vec", size=shape.E),
+                       get_entry(ic, "value_pos", "vec", size=shape.E))
     spec = SceneSpec(shape, tuple(active), min_level, max_level, x2p or ic_x2p, domain_bc,
                      max_level_geom=max_level_geom, refinement_radius=radius, jump=jump, objects=objects,
-                     zones=zones, diffuse_ic=diffuse, rho_ref=rho_ref, keep_ic_gas_density=False)
+                     zones=zones, diffuse_ic=diffuse, rho_ref=rho_ref, keep_ic_gas_density=False, ic=ic_data)
     if model == "multi" and D > 1 and objects and rho_ref is None:
         raise ConfigError("multiphase objects need reference densities")
     tree = build_tree(spec)
     run = RunSettings(name, io_interval, end_time, signal_time, steady_tol)
-    return TomlCase(Case(tree, prm), run, model, p_ref, vel_ref, rho_ref, ignored, objects)
+    return TomlCase(Case(tree, prm), spec, run, model, p_ref, vel_ref, rho_ref, ignored, objects)
 
 
 def driver_for(tc: TomlCase, solver, out_dir: str, observers=(), **kw):

@@ -153,6 +153,41 @@ int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long 
  * whose steps skip the gradient computation. */
 int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out);
 
+/* ---- Initial tree on the device: Scene::init_domain (scene/scene.cpp:369-431) for analytic scenes --
+ * Droplet/bubble spheres and ellipses (no solid objects: those stay with the host builder), domain-face
+ * boundaries, refinement near objects, inflow_r faces, the initial jump and in zones, the uniform or
+ * jump initial condition and the tanh-smeared volume fraction. Produces the same nodes in the same
+ * order as the host builder; the result feeds dg_case. */
+typedef struct dg_scene {
+	int model, dims;
+	double side_length, active_size[3];
+	int min_level, max_level, max_level_geom;
+	double refinement_radius;
+	int domain_bc[3][2];  /* boundary-table id of each domain face, -1 on periodic dimensions */
+	int inflow_r[3][2];   /* 1 where that face's condition is inflow_r (refined to the maximum level) */
+	int n_objects;        /* <= 16 */
+	const double *objects; /* 10 per object: centre[3], semi-axes[3] (a sphere's radius first), cos and sin
+	                          of its rotation about z, shape (0 sphere, 1 ellipse), type (0 droplet, 1 bubble) */
+	int n_zones;          /* <= 16 */
+	const double *zones;  /* 7 per zone: x0[3], x1[3], level */
+	int refine_jump, jump_axis;
+	double jump_location;
+	int ic_kind, ic_axis; /* 0 uniform (ic_neg), 1 jump (ic_pos where x[ic_axis] > ic_location) */
+	double ic_location;
+	const double *ic_neg, *ic_pos; /* E primitive values each */
+	int diffuse_ic, keep_ic_gas_density;
+	double rho_ref[2];
+} dg_scene;
+typedef struct dg_tree dg_tree;
+const char *dg_build_last_error(void);
+int dg_build_tree(const dg_scene *scene, dg_tree **out);
+int dg_tree_nodes(const dg_tree *t, long long *n_nodes);
+/* Host copies in the layout of dg_case: parent[n], children[n][2^D], level[n], flags[n], bc[n][2D],
+ * center[n][D], p[n][E]. */
+int dg_tree_copy(const dg_tree *t, int *parent, int *children, int *level, unsigned int *flags, int *bc,
+                 double *center, double *p);
+int dg_tree_free(dg_tree *t);
+
 /* ---- Regrid forecaster (no counterpart in the reference) -------------------------------------
  * A small network that predicts from per-leaf features whether the refinement indicator will fire
  * at a leaf's place a few global steps ahead. */
