@@ -624,14 +624,23 @@ private:
 		});
 		run_k(DG_K_FLUX, 0, [&] { launch_flux_faces(grid_for((long long) n * NF / 2 + 1), dtL); });
 		run_k(DG_K_FLUX, 0, [&] { launch_flux_bfaces(grid_for(n / 4 + 1), dtL); });
-		run_k(DG_K_FLUX, 0, [&] { k_flux_walk<M><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_); });
+		run_k(DG_K_FLUX, 0, [&] {
+			if (mixed_) k_flux_walk<M, float><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_);
+			else k_flux_walk<M, double><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_);
+		});
 		run_k(DG_K_RECV, 0, [&] {
-			k_flux_receive<M><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
+			if (mixed_) k_flux_receive<M, float><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
+			else k_flux_receive<M, double><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
 			e_upd = ++epoch_;
-			if (visc_) k_gather_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
-			else k_gather_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+			if (mixed_) {
+				if (visc_) k_gather_update<M, true, float><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+				else k_gather_update<M, false, float><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+			} else {
+				if (visc_) k_gather_update<M, true, double><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+				else k_gather_update<M, false, double><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+			}
 		});
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) multiphase_aux(list, n, L, e_upd);

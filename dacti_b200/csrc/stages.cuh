@@ -290,8 +290,11 @@ __device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i
 	return (P.clu[gc] == L && ai <= P.acti[gc]) ? gc : -1;
 }
 
-__device__ __forceinline__ double *face_flux(const Pool &P, int i, int f, int nflux, int nfaces) {
-	return P.ff + ((size_t) i * nfaces + f) * nflux;
+// Face-flux slot of cell i's face f. The slots hold FP64 values in the FP64 form and FP32 values in the
+// mixed form (T = float: the same array read with a compact FP32 stride).
+template<class T = double>
+__device__ __forceinline__ T *face_flux(const Pool &P, int i, int f, int nflux, int nfaces) {
+	return reinterpret_cast<T *>(P.ff) + ((size_t) i * nfaces + f) * nflux;
 }
 
 // Face-flux source codes of plan[]: (owner * 2D + owner's face) * 2 + (1 if the cell subtracts it),
@@ -360,9 +363,9 @@ __global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const in
 		const int nb = P.nbr[(size_t) f * P.cap + i];
 		double F[M::F];
 		interior_flux<M, V, S>(P, C, i, nb, f >> 1, f & 1, dtL, F);
-		double *dst = face_flux(P, i, f, M::F, NF);
+		S *dst = face_flux<S>(P, i, f, M::F, NF);
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
+		for (int q = 0; q < M::F; ++q) dst[q] = (S) F[q];
 	}
 }
 
@@ -377,9 +380,9 @@ __global__ void k_flux_bfaces(Pool P, Consts C, BcTable B, const int32_t *tasks,
 		const int b = P.bc[(size_t) f * P.cap + i];
 		double F[M::F];
 		boundary_flux<M, V, S>(P, C, B, i, b, f >> 1, f & 1, dtL, F);
-		double *dst = face_flux(P, i, f, M::F, NF);
+		S *dst = face_flux<S>(P, i, f, M::F, NF);
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = F[q];
+		for (int q = 0; q < M::F; ++q) dst[q] = (S) F[q];
 	}
 }
 
@@ -387,7 +390,7 @@ __global__ void k_flux_bfaces(Pool P, Consts C, BcTable B, const int32_t *tasks,
 // running-cluster cells own across its faces. A group of 2D lanes (padded to 4 or 8) serves one
 // cell; lane f walks the owners across face (dim, dir) = (f / 2, f % 2) and the lane sums are
 // combined with a fixed butterfly, so the total does not depend on scheduling.
-template<class M>
+template<class M, class T = double>
 __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *list, const int *n_ptr, int L,
                                                         Counters *cnt) {
 	constexpr int NF   = 2 * M::D;
@@ -417,7 +420,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 					bool plus;
 					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, false, dn, plus);
 					if (owner < 0) continue;
-					const double *F = face_flux(P, owner, 2 * dim + dn, M::F, NF);
+					const T *F = face_flux<T>(P, owner, 2 * dim + dn, M::F, NF);
 					if (plus) {
 #pragma unroll
 						for (int q = 0; q < M::F; ++q) acc[q] += F[q];
@@ -444,7 +447,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 
 // Walk tasks: the flux sum of a running-cluster cell's face whose finer owners sit behind a non-leaf
 // neighbour, in candidate order, stored in the cell's own slot for that face.
-template<class M>
+template<class M, class T = double>
 __global__ void k_flux_walk(Pool P, const int32_t *wtasks, const int *n_ptr, int L, Counters *cnt) {
 	constexpr int NF = 2 * M::D, NSUB = 1 << (M::D - 1);
 	const int n = *n_ptr;
@@ -461,7 +464,7 @@ __global__ void k_flux_walk(Pool P, const int32_t *wtasks, const int *n_ptr, int
 			bool plus;
 			const int owner = face_owner<M>(P, &cnt->status, i, nb, f >> 1, f & 1, L, li, ai, c, true, dn, plus);
 			if (owner < 0) continue;
-			const double *F = face_flux(P, owner, (f & ~1) | dn, M::F, NF);
+			const T *F = face_flux<T>(P, owner, (f & ~1) | dn, M::F, NF);
 			if (plus) {
 #pragma unroll
 				for (int q = 0; q < M::F; ++q) acc[q] += F[q];
@@ -470,16 +473,17 @@ __global__ void k_flux_walk(Pool P, const int32_t *wtasks, const int *n_ptr, int
 				for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
 			}
 		}
-		double *dst = face_flux(P, i, f, M::F, NF);
+		T *dst = face_flux<T>(P, i, f, M::F, NF);
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = acc[q];
+		for (int q = 0; q < M::F; ++q) dst[q] = (T) acc[q];
 	}
 }
 
 // Signed contribution of a planned face source to component q, as a gather lane forms it from +0.
-__device__ __forceinline__ double face_term(const double *F, int pl, int q) {
+template<class T>
+__device__ __forceinline__ double face_term(const T *F, int pl, int q) {
 	if (pl < 0) return 0.0;
-	const double v = F[q];
+	const double v = (double) F[q];
 	return (pl & 1) ? 0.0 - v : 0.0 + v;
 }
 
@@ -488,7 +492,7 @@ __device__ __forceinline__ double face_term(const double *F, int pl, int q) {
 // terms combine in the pairing order of a butterfly over 4 (2D) or 8 (3D) lanes, the last two
 // contributing zeros in 3D. Without viscous terms (V = false) the gradient inputs are never read, so
 // t_slope is not maintained.
-template<class M, bool V>
+template<class M, bool V, class T = double>
 __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, const int32_t *list, int n, double dtL,
                                                             int epoch, Counters *cnt) {
 	constexpr int E = M::E, NF = 2 * M::D;
@@ -497,11 +501,11 @@ __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, co
 		const int i  = list[tid];
 		const int li = P.level[i];
 		int pl[NF];
-		const double *src[NF];
+		const T *src[NF];
 #pragma unroll
 		for (int f = 0; f < NF; ++f) {
 			pl[f]  = P.plan[(size_t) i * NF + f];
-			src[f] = P.ff + (size_t) (pl[f] < 0 ? 0 : pl[f] >> 1) * M::F;
+			src[f] = reinterpret_cast<const T *>(P.ff) + (size_t) (pl[f] < 0 ? 0 : pl[f] >> 1) * M::F;
 		}
 		const double vol = C.vol[li];
 		double du[M::F];

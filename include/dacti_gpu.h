@@ -31,8 +31,10 @@ enum {
 /* model ids (dacti::model::euler / navier_stokes / multi) */
 enum { DG_EULER = 0, DG_NAVIER_STOKES = 1, DG_MULTI = 2 };
 
-/* numerical forms: the reference's FP64 arithmetic, or FP32 reconstruction and HLLC flux with the
- * conservative update, the conservation totals and the pressure/temperature recovery in FP64 */
+/* numerical forms: the reference's FP64 arithmetic, or FP32 reconstruction and HLLC flux, face fluxes
+ * stored in FP32 (both sides of a face read the same value, so conservation stays exact), with the
+ * flux sums, the conservative update, the conservation totals and the pressure/temperature recovery
+ * in FP64 */
 enum { DG_FORM_FP64 = 0, DG_FORM_MIXED = 1 };
 
 /* limiter ids (dacti::integrator::slope, integrator/slope_limiters.hpp:7-57) */
