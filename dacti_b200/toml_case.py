@@ -366,11 +366,13 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
 
 
 def load_toml_case(path: str, model: Optional[str] = None, limiter: int = 0, honour_diffuse_ic: bool = False,
-                   x2p: Optional[Callable[[np.ndarray], np.ndarray]] = None) -> TomlCase:
+                   x2p: Optional[Callable[[np.ndarray], np.ndarray]] = None, builder: str = "host") -> TomlCase:
     """Reads a DACTI case file into an initial tree and solver parameters. `model` is "euler",
     "navier_stokes" or "multi" (the reference's compile-time choice; inferred from the file if None);
     `limiter` is the slope limiter id (the examples use minmod, 0); `x2p` replaces the initial condition
-    for states TOML cannot express, as code that sets Config::ic.x2p does."""
+    for states TOML cannot express, as code that sets Config::ic.x2p does. `builder` picks the tree
+    builder: "host" (numpy), "device" (dg_build_tree on the current GPU; droplet/bubble scenes only) or
+    "auto" (the device where the scene allows it, else the host)."""
     with open(path, "rb") as f:
         doc = tomllib.load(f)
     model = model or infer_model(doc)
@@ -469,7 +471,19 @@ def load_toml_case(path: str, model: Optional[str] = None, limiter: int = 0, hon
                      zones=zones, diffuse_ic=diffuse, rho_ref=rho_ref, keep_ic_gas_density=False, ic=ic_data)
     if model == "multi" and D > 1 and objects and rho_ref is None:
         raise ConfigError("multiphase objects need reference densities")
-    tree = build_tree(spec)
+    if builder not in ("host", "device", "auto"):
+        raise ValueError("builder must be 'host', 'device' or 'auto'")
+    tree = None
+    if builder in ("device", "auto"):
+        from .scene_gpu import build_tree_device
+
+        try:
+            tree = build_tree_device(spec)
+        except NotImplementedError:
+            if builder == "device":
+                raise
+    if tree is None:
+        tree = build_tree(spec)
     run = RunSettings(name, io_interval, end_time, signal_time, steady_tol)
     return TomlCase(Case(tree, prm), spec, run, model, p_ref, vel_ref, rho_ref, ignored, objects)
 

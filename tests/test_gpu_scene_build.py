@@ -56,3 +56,12 @@ def test_full_size_shock_drop_build_time():
     t_host = time.perf_counter() - t0
     print(f"shock-drop 3D tree: {dev.n_nodes} nodes, device {t_dev:.3f} s (with host copies), host {t_host:.2f} s")
     _same(host, dev)
+
+
+def test_toml_loader_device_builder():
+    for name in ("bubble_jump2d", "cylinder_ns2d"):
+        host = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"))
+        auto = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"), builder="auto")
+        _same(host.case.tree, auto.case.tree)  # the cylinder falls back to the host builder
+    with pytest.raises(NotImplementedError):
+        load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"), builder="device")
