@@ -327,3 +327,31 @@ def cylinder_ns(mach: float = 0.3, base_level: int = 5, levels: int = 3, reynold
         ns_mu=mu, ns_lambda=mu * 1005.0 / prandtl,
     )
     return Case(build_tree(spec), prm)
+
+
+def blast3d(base_level: int = 3, levels: int = 2, thresholds=(0.02, 0.05), max_cfl: float = 0.5,
+            model: ModelId = ModelId.EULER, mu: float = 0.0, prandtl: float = 0.72) -> Case:
+    """3D Euler / Navier-Stokes blast in the unit cube: rho 1.5, p 3 inside a sphere of radius 0.25 at
+    (0.1, -0.05, 0.05), rho 1, p 1 outside, uniform drift (0.2, -0.1, 0.05). Free-slip walls on x,
+    no-slip walls on y, periodic in z: the 3D neighbour search, hanging faces in three directions, both
+    wall treatments and the periodic wrap in one case."""
+    shape = ModelShape(model, 3)
+
+    def x2p(c: np.ndarray) -> np.ndarray:
+        inside = np.sqrt((c[:, 0] - 0.1) ** 2 + (c[:, 1] + 0.05) ** 2 + (c[:, 2] - 0.05) ** 2) < 0.25
+        out = np.empty((c.shape[0], 5))
+        out[:, 0] = np.where(inside, 1.5, 1.0)
+        out[:, 1] = 0.2
+        out[:, 2] = -0.1
+        out[:, 3] = 0.05
+        out[:, 4] = np.where(inside, 3.0, 1.0)
+        return out
+
+    domain_bc = [(BoundarySpec(BcType.FREESLIP),) * 2, (BoundarySpec(BcType.NOSLIP),) * 2, None]
+    spec = SceneSpec(shape, (1.0, 1.0, 1.0), base_level, base_level + levels, x2p, domain_bc)
+    prm = SolverParams(
+        side_length=1.0, active_size=(1.0, 1.0, 1.0), periodic=(False, False, True), max_cfl=max_cfl, max_dt=1.0,
+        error_threshold=thresholds, max_level=base_level + levels, min_level=base_level,
+        weights=(1.0, 0.0, 0.0, 0.0, 0.0), ns_mu=mu, ns_lambda=mu * 1005.0 / prandtl if mu else 0.0,
+    )
+    return Case(build_tree(spec), prm)

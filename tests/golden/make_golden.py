@@ -40,6 +40,9 @@ GOLDEN = {
     "multi2": (lambda: cases.shock_drop(dims=2, base_level=4, levels=2), 4, [0, 4]),
     "multi3": (lambda: cases.shock_drop(dims=3, base_level=3, levels=1), 2, [0, 2]),
     "euler2_periodic": (lambda: cases.periodic_blob(base_level=3, levels=2), 6, [6]),
+    # 3D Euler and Navier-Stokes (walls, periodic z, hanging faces in three directions)
+    "euler3": (lambda: cases.blast3d(base_level=3, levels=1), 4, [2, 4]),
+    "ns3": (lambda: cases.blast3d(base_level=3, levels=1, model=ModelId.NAVIER_STOKES, mu=2e-3), 4, [4]),
     # boundary conditions: freeslip / noslip walls, inflow with fade-in, inflow_r, Dirichlet, outflow
     "euler2_walls": (lambda: cases.box_blast(base_level=3, levels=2), 10, [5, 10]),
     "euler2_open_a": (lambda: cases.box_blast(base_level=3, levels=2, domain_bc=OPEN_A), 10, [5, 10]),

@@ -19,7 +19,7 @@ from conftest import GOLDEN, ROOT
 
 CHECK = os.path.join(ROOT, "oracle", "_ref", "dacti_adapter_check")
 
-CASES = [("euler2", 4), ("ns2", 4), ("multi2", 3), ("multi3", 2), ("euler2_periodic", 4), ("euler2_walls", 6),
+CASES = [("euler2", 4), ("ns2", 4), ("multi2", 3), ("multi3", 2), ("euler3", 4), ("ns3", 4), ("euler2_periodic", 4), ("euler2_walls", 6),
          ("euler2_open_a", 6), ("euler2_lim2", 4), ("euler2_lim5", 4), ("multi2_tension_run", 2)]
 
 
