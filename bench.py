@@ -345,7 +345,8 @@ def batched_run(args, local_rank: int, world: int) -> dict:
     from dacti_b200 import cases
     from dacti_b200.solver import Solver, step_many
 
-    threads = 8
+    # each tree's host thread mostly waits on its per-substep synchronisation, so twice the cores pays
+    threads = min(32, max(8, 2 * host_threads()))
     batch = cases.riemann_batch(args.batch_trees, seed=3)
     solvers = [Solver(c, device=local_rank) for c in batch]
     for s in solvers:
