@@ -500,11 +500,14 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
             path = os.path.join(td, "case.bin")
             write_case(case, path)
             res = run_reference_samples(path, 1, sub, threads)
+            one = run_reference_samples(path, 1, 20, 1)["samples"][0]
         s = res["samples"][0]
         result["cpu_baseline"] = {
             "value": s["updates"] / s["seconds"], "unit": UNIT, "cores": threads, "kind": "reference",
             "sample": f"first {sub} LTS substeps of the first global step ({s['updates']:.0f} updates), reference "
                       f"Integrator built from its sources (-O3 -fopenmp), {threads} threads of {cpu_model()}",
+            "single_thread": {"value": one["updates"] / one["seconds"], "cores": 1,
+                              "sample": f"first 20 LTS substeps ({one['updates']:.0f} updates), OMP_NUM_THREADS=1"},
         }
     if rank == 0:
         print(json.dumps(result), flush=True)
