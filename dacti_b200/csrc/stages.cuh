@@ -24,25 +24,14 @@ __device__ __forceinline__ void append(int32_t *list, int *count, int value, int
 }
 
 // --------------------------------------------------------------------------------------------
-// Reconstruction records. Everything a face flux needs from one side, apart from centre and time,
-// sits in one contiguous FP64 record per node: the primitive state (a copy of the pool's p), the
+// Reconstruction records (Rec, declared with the tree helpers). Everything a face flux needs from one
+// side, apart from centre and time, sits in one contiguous FP64 record per node: the primitive state (a
+// copy of the pool's p, also what neighbour gathers read), the
 // Hancock rhs, the limited slope rows (each padded to an even length so that rows start on 16-byte
 // boundaries) and, for the multiphase model, the curvature and interface normal. A neighbour's
 // face state is then a handful of 16-byte vector loads from a few cache lines instead of 3E + 2
 // scattered structure-of-arrays loads. The record is the only storage of slope and rhs.
 // --------------------------------------------------------------------------------------------
-template<class M>
-struct Rec {
-	static constexpr int E = M::E, D = M::D;
-	static constexpr int ES  = (E + 1) & ~1;  // slope row stride
-	static constexpr int P0  = 0, R0 = E;     // p and rhs, adjacent (2E doubles)
-	static constexpr int S0  = 2 * E;         // slope row d at S0 + d * ES
-	static constexpr int K0  = S0 + D * ES;   // multiphase: curvature, then the normal's D components
-	static constexpr int RAW = K0 + (M::MULTI ? 1 + D : 0);
-	static constexpr int W   = (RAW + 1) & ~1;
-};
-
-__device__ __forceinline__ double *rec_of(const Pool &P, int i, int W) { return P.rec + (size_t) i * W; }
 
 // Loads the face-dim part of node i's record, rounded to S: p, rhs, slope row `dim`, and (multiphase)
 // curvature and normal component `dim`.
@@ -566,6 +555,7 @@ __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, co
 			P.u[(size_t) q * cap + i] = u[q];
 			P.p[(size_t) q * cap + i] = p[q];
 		}
+		store_p_rec<M>(P, i, p);
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
 		P.t[i] = P.t[i] + dtL;
 		mark_up(P, P.parent[i], epoch);
@@ -606,7 +596,7 @@ __global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch
 		if (!(fl & F_LEAF)) {
 			interp_pt<M>(P, &cnt->status, nb, epoch, v);
 		} else {
-			load_p<M>(P, nb, v);
+			load_p_rec<M>(P, nb, v);
 			v[E] = P.t[nb];
 		}
 		double *o = P.nbv + t * W;
@@ -1182,6 +1172,7 @@ __global__ void k_init_cells(Pool P, Consts C, const int32_t *list, int n, Count
 		const int i = list[tid];
 		double p[E], u[E];
 		load_p<M>(P, i, p);
+		store_p_rec<M>(P, i, p);
 		cons_from_prim<M>(C.m, p, u);
 		for (int q = 0; q < E; ++q) P.u[(size_t) q * cap + i] = u[q];
 		if constexpr (M::MULTI) {

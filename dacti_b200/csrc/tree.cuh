@@ -14,6 +14,43 @@ __device__ __forceinline__ void load_p(const Pool &P, int i, double *p) {
 	for (int q = 0; q < M::E; ++q) p[q] = at(P.p, P.cap, q, i);
 }
 
+template<class M>
+struct Rec {
+	static constexpr int E = M::E, D = M::D;
+	static constexpr int ES  = (E + 1) & ~1;  // slope row stride
+	static constexpr int P0  = 0, R0 = E;     // p and rhs, adjacent (2E doubles)
+	static constexpr int S0  = 2 * E;         // slope row d at S0 + d * ES
+	static constexpr int K0  = S0 + D * ES;   // multiphase: curvature, then the normal's D components
+	static constexpr int RAW = K0 + (M::MULTI ? 1 + D : 0);
+	static constexpr int W   = (RAW + 1) & ~1;
+};
+
+__device__ __forceinline__ double *rec_of(const Pool &P, int i, int W) { return P.rec + (size_t) i * W; }
+
+// Primitive state of node i from the head of its record: one or two 32-byte sectors instead of E
+// scattered ones. The record's p equals the SoA p of every cell whenever another cell reads it
+// (the update, split, unsplit and initialisation write both).
+template<class M>
+__device__ __forceinline__ void load_p_rec(const Pool &P, int i, double *p) {
+	const double *r = P.rec + (size_t) i * Rec<M>::W;
+	const double2 *r2 = reinterpret_cast<const double2 *>(r);
+#pragma unroll
+	for (int k = 0; k < M::E / 2; ++k) {
+		const double2 v = r2[k];
+		p[2 * k] = v.x, p[2 * k + 1] = v.y;
+	}
+	if constexpr (M::E % 2) p[M::E - 1] = r[M::E - 1];
+}
+
+template<class M>
+__device__ __forceinline__ void store_p_rec(const Pool &P, int i, const double *p) {
+	double *r   = P.rec + (size_t) i * Rec<M>::W;
+	double2 *r2 = reinterpret_cast<double2 *>(r);
+#pragma unroll
+	for (int k = 0; k < M::E / 2; ++k) r2[k] = make_double2(p[2 * k], p[2 * k + 1]);
+	if constexpr (M::E % 2) r[M::E - 1] = p[M::E - 1];
+}
+
 __device__ __forceinline__ void set_status(uint32_t *status, uint32_t bit) { atomicOr(status, bit); }
 
 // Domain::find(location, node.tree_level) for the face (dim, dir) of node i, as used by
@@ -73,7 +110,7 @@ template<class M>
 __device__ void interp_pt(const Pool &P, uint32_t *status, int n, int epoch, double *out) {
 	constexpr int E = M::E, NC = 1 << M::D, AW = Avg<M>::W;
 	if (P.flags[n] & F_LEAF) {
-		load_p<M>(P, n, out);
+		load_p_rec<M>(P, n, out);
 		out[E] = P.t[n];
 		return;
 	}
@@ -99,7 +136,9 @@ __device__ void interp_pt(const Pool &P, uint32_t *status, int n, int epoch, dou
 			const uint32_t fl = P.flags[c];
 			if (!(fl & F_ACTIVE)) continue;
 			if (fl & F_LEAF) {
-				for (int q = 0; q < E; ++q) fr.f[q] = fr.f[q] + at(P.p, P.cap, q, c);
+				double pc[E];
+				load_p_rec<M>(P, c, pc);
+				for (int q = 0; q < E; ++q) fr.f[q] = fr.f[q] + pc[q];
 				fr.f[E] = fr.f[E] + P.t[c];
 				fr.cnt++;
 			} else if (memo_ok(P, c, epoch)) {
