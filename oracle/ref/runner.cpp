@@ -20,6 +20,7 @@
 #include "scene/scene.hpp"
 #ifdef DACTI_ADAPTER_CHECK
 #include "dacti_gpu/integrator.hpp"
+#include "driver/observer/drop_energy.hpp"
 #endif
 
 #include <chrono>
@@ -244,6 +245,15 @@ namespace {
 			gpu.integrate(rec(hg), true, fg);
 			compare(step, hr == hg, fr == fg);
 			if (fr || fg) break;
+		}
+		// DACTI's own DropEnergy observer (driver/observer/drop_energy.hpp), compiled unchanged, on both
+		// integrators after the last step
+		if constexpr (Model::Multiphase) {
+			observer::DropEnergy on_ref, on_gpu;
+			on_ref.observe(ref, cfg);
+			on_gpu.observe(gpu, cfg);
+			const auto a = on_ref.IntegVars(), b = on_gpu.IntegVars();
+			std::printf("DROP_ENERGY {\"ref\": [%.17g, %.17g], \"gpu\": [%.17g, %.17g]}\n", a[0], a[1], b[0], b[1]);
 		}
 		return failures ? 1 : 0;
 	}

@@ -7,7 +7,9 @@ them with the same calls a DACTI driver makes (integrate with a substep hook, n_
 for_each_active_cell, global_dt). After construction and after every global step it compares the
 hook sequence, force_break, global_dt, the active cell set with ACTI levels, the conserved state
 (relative L1 <= 1e-10), and the slopes and gradients the adapter's nodes carry (relative L1 <= 1e-8;
-gradients where the case has viscous or conduction terms), printing one JSON line per step.
+gradients where the case has viscous or conduction terms), printing one JSON line per step. For the
+multiphase cases DACTI's own DropEnergy observer (driver/observer/drop_energy.hpp), compiled unchanged
+into the same binary, runs on both integrators after the last step.
 """
 import json
 import os
@@ -39,3 +41,9 @@ def test_adapter_matches_reference_integrator(name, steps, tmp_path):
         assert rec["global_dt_equal"] and rec["n_ref"] == rec["n_gpu"] and rec["rel_l1_u"] <= 1e-10, rec
         # slopes (read by Cell::get_p) and gradients (read by DropEnergy) as the adapter hands them out
         assert rec["rel_l1_slope"] <= 1e-8 and rec["rel_l1_grad"] <= 1e-8, rec
+    # DACTI's DropEnergy observer, compiled unchanged, reads the same kinetic and total energy from both
+    de = [json.loads(x[len("DROP_ENERGY "):]) for x in r.stdout.splitlines() if x.startswith("DROP_ENERGY ")]
+    if name.startswith("multi"):
+        assert len(de) == 1
+        for a, b in zip(de[0]["ref"], de[0]["gpu"]):
+            assert abs(a - b) <= 1e-8 * max(abs(a), 1e-300), de
