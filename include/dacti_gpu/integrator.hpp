@@ -26,7 +26,9 @@
  * size() only. Refinement zones must be axis-aligned (no rotation in their Transform). Model
  * constants are read from the model's statics when the Integrator is constructed. Errors of the C
  * ABI surface as std::runtime_error, the reference's error type for configuration errors
- * (config/util.hpp:26); NaN still ends a step through force_break.
+ * (config/util.hpp:26); NaN still ends a step through force_break. Copies share one GPU solver (the
+ * reference copies its whole domain), which is what default_driver needs: it keeps and steps its own
+ * copy of the Integrator.
  */
 #pragma once
 
@@ -226,12 +228,10 @@ namespace dacti::gpu {
 			c.bc = bc.data(), c.center = center.data(), c.p = p.data();
 			dg_solver *s = nullptr;
 			detail::check(dg_create(&c, &s), nullptr, "dg_create");
-			solver_.reset(s);
+			solver_.reset(s, deleter{});
 			refresh_counters();
 		}
 
-		Integrator(const Integrator &)            = delete;
-		Integrator &operator=(const Integrator &) = delete;
 
 		/* Integrator::integrate (impl/integrate.hpp:12-87) */
 		scalar_t integrate(auto substep_hook, bool signal, bool &force_break) {
@@ -296,7 +296,9 @@ namespace dacti::gpu {
 		struct deleter {
 			void operator()(dg_solver *s) const { dg_destroy(s); }
 		};
-		std::unique_ptr<dg_solver, deleter> solver_;
+		// Copies share the GPU solver: DACTI's default_driver keeps its own copy of the Integrator
+		// (driver/default_driver.hpp:20, :34-38) and steps that copy; the tree stays on the device.
+		std::shared_ptr<dg_solver> solver_;
 		mutable std::vector<node_t> cells_;
 		mutable bool cache_valid_ = false;
 

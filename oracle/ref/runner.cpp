@@ -20,10 +20,12 @@
 #include "scene/scene.hpp"
 #ifdef DACTI_ADAPTER_CHECK
 #include "dacti_gpu/integrator.hpp"
+#include "driver/default_driver.hpp"
 #include "driver/observer/drop_energy.hpp"
 #endif
 
 #include <chrono>
+#include <iomanip>
 #include <cstdio>
 #include <set>
 #include <sstream>
@@ -42,6 +44,7 @@ namespace {
 		int sample_substeps = 0;  // >0: each integrate() call is timed up to this many substeps
 		int samples = 0;
 		bool adapter_check = false;  // side-by-side run against the GPU adapter (adapter build only)
+		bool driver_check  = false;  // DACTI's default_driver over the reference and over the adapter
 	};
 
 	template<typename Model>
@@ -259,6 +262,57 @@ namespace {
 	}
 #endif
 
+#ifdef DACTI_ADAPTER_CHECK
+	// A writer for default_driver that records what it is handed: frame times and cell counts.
+	struct RecordingWriter {
+		std::vector<std::array<double, 3>> *frames;
+		template<typename I>
+		void write_data(const I &integrator, scalar_t t, int frame, std::vector<std::vector<scalar_t>> fields,
+		                std::vector<std::string> names) {
+			frames->push_back({t, (double) frame, (double) integrator.n_active_cells()});
+		}
+	};
+
+	// DACTI's default_driver (driver/default_driver.hpp:17-217), compiled unchanged, runs the case for
+	// o.n_steps global steps once over the reference Integrator and once over the GPU adapter, with a
+	// frame after every step and (multiphase) the DropEnergy observer. Prints both observables files
+	// and the writers' records as one line: DRIVER {...}.
+	template<typename Model, typename Limiter>
+	int driver_check(const oracle::CaseData &c, const Options &o, std::shared_ptr<config::Config<Model>> cfg) {
+		constexpr int E = Model::NumEqns;
+		using Est       = integrator::error::weighted_laplacian<E>;
+		scene::Scene<Model> scene_ref(cfg), scene_gpu(cfg);
+		Runner<Model, Limiter> ref{Limiter{}, Est{cfg->error_weights}, scene_ref, cfg};
+		dacti::gpu::Integrator<Model, Limiter, Est> gpu{Limiter{}, Est{cfg->error_weights}, scene_gpu, cfg};
+		cfg->io_interval    = 0.0;
+		cfg->end_time       = (o.n_steps - 0.5) * ref.global_dt;
+		cfg->result_out_dir = o.out_prefix;
+		auto observers = [] {
+			if constexpr (Model::Multiphase) return std::tuple{observer::DropEnergy()};
+			else return std::tuple<>{};
+		};
+		std::vector<std::array<double, 3>> fr_ref, fr_gpu;
+		cfg->case_name = "driver_ref";
+		driver::default_driver d_ref{ref, RecordingWriter{&fr_ref}, cfg, observers()};
+		d_ref.run();
+		cfg->case_name = "driver_gpu";
+		driver::default_driver d_gpu{gpu, RecordingWriter{&fr_gpu}, cfg, observers()};
+		d_gpu.run();
+		auto dump = [](const std::vector<std::array<double, 3>> &v) {
+			std::ostringstream s;
+			s << "[";
+			for (size_t k = 0; k < v.size(); ++k)
+				s << (k ? ", " : "") << "[" << std::setprecision(17) << v[k][0] << ", " << v[k][1] << ", " << v[k][2] << "]";
+			s << "]";
+			return s.str();
+		};
+		std::printf("DRIVER {\"frames_ref\": %s, \"frames_gpu\": %s, \"csv_ref\": \"%s/driver_ref_observables.csv\", "
+		            "\"csv_gpu\": \"%s/driver_gpu_observables.csv\"}\n",
+		            dump(fr_ref).c_str(), dump(fr_gpu).c_str(), o.out_prefix.c_str(), o.out_prefix.c_str());
+		return 0;
+	}
+#endif
+
 	template<typename Model, typename Limiter = integrator::slope::minmod>
 	int run(const oracle::CaseData &c, const Options &o) {
 		using R = Runner<Model, Limiter>;
@@ -270,6 +324,7 @@ namespace {
 		auto cfg = make_config<Model>(c);
 #ifdef DACTI_ADAPTER_CHECK
 		if (o.adapter_check) return adapter_check<Model, Limiter>(c, o, cfg);
+		if (o.driver_check) return driver_check<Model, Limiter>(c, o, cfg);
 #endif
 
 		scene::Scene<Model> scene(cfg);
@@ -376,6 +431,8 @@ int main(int argc, char **argv) {
 			o.samples = std::atoi(argv[++i]);
 		} else if (a == "--adapter-check") {
 			o.adapter_check = true;
+		} else if (a == "--driver-check") {
+			o.driver_check = true;
 		}
 	}
 	spdlog::set_level(spdlog::level::warn);

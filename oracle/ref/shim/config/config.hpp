@@ -1,14 +1,16 @@
 // Oracle shim for DACTI's config/config.hpp (src/lib/config/config.hpp:11-117).
 //
-// Holds only the Config fields that the hot path reads: side_length, active_size, IsPeriodic,
+// Holds the Config fields that the hot path reads: side_length, active_size, IsPeriodic,
 // error_threshold, error_weights, max/min refinement level, max_dt, max_cfl
-// (integrator/integrator.hpp:80-86, impl/flux.hpp:68-74) and refine_zones (scene/scene.hpp:54-58).
+// (integrator/integrator.hpp:80-86, impl/flux.hpp:68-74) and refine_zones (scene/scene.hpp:54-58),
+// plus the run fields of the default driver loop.
 // The runner fills them from a flat case file instead of a TOML case.
 #pragma once
 
 #include "integrator/boundary.hpp"
 #include <array>
 #include <memory>
+#include <string>
 #include <vector>
 
 namespace oracle {
@@ -45,6 +47,14 @@ namespace dacti::config {
 			}
 		};
 		std::vector<RefineZone> refine_zones;
+
+		// run fields that driver/default_driver.hpp reads (config/config.hpp:28-36)
+		std::string case_name       = "case";
+		std::string result_out_dir  = ".";
+		scalar_t io_interval        = 0.0;
+		scalar_t end_time           = 0.0;
+		scalar_t signal_time        = -1.0;
+		scalar_t convergence_tol    = -1.0;
 
 		const oracle::CaseData *case_data = nullptr;
 	};

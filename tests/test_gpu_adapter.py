@@ -47,3 +47,31 @@ def test_adapter_matches_reference_integrator(name, steps, tmp_path):
         assert len(de) == 1
         for a, b in zip(de[0]["ref"], de[0]["gpu"]):
             assert abs(a - b) <= 1e-8 * max(abs(a), 1e-300), de
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name,steps", [("euler2", 4), ("ns2", 3), ("multi2", 3), ("multi2_tension_run", 2)])
+def test_reference_default_driver_runs_the_adapter(name, steps, tmp_path):
+    """DACTI's default_driver (driver/default_driver.hpp), compiled unchanged, keeps and steps its own
+    copy of the Integrator: once the reference's, once the GPU adapter. Frames, times, cell counts and
+    the observables CSV (with DropEnergy for the multiphase cases) agree."""
+    import csv
+
+    if not os.path.exists(CHECK):
+        pytest.fail("oracle/_ref/dacti_adapter_check is not built (make -C oracle after building the library)")
+    r = subprocess.run([CHECK, os.path.join(GOLDEN, f"{name}.case"), str(tmp_path), str(steps), "--driver-check"],
+                       capture_output=True, text=True, timeout=600, env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
+    rec = [json.loads(x[len("DRIVER "):]) for x in r.stdout.splitlines() if x.startswith("DRIVER ")]
+    assert len(rec) == 1
+    fr, fg = rec[0]["frames_ref"], rec[0]["frames_gpu"]
+    assert len(fr) == steps + 1 and fr == fg  # frame times, indices and cell counts, exactly
+    rows_r = list(csv.reader(open(rec[0]["csv_ref"])))
+    rows_g = list(csv.reader(open(rec[0]["csv_gpu"])))
+    assert rows_r[0] == rows_g[0] and len(rows_r) == len(rows_g) == steps + 1
+    for a, b in zip(rows_r[1:], rows_g[1:]):
+        assert a[:4] == b[:4]  # time, frame, step, n_cells
+        for x, y in zip(a[4:], b[4:]):
+            assert abs(float(x) - float(y)) <= 1e-8 * max(abs(float(x)), 1e-300), (a, b)
+    if name.startswith("multi"):
+        assert rows_r[0][4:] == ["ke", "Etot"]
