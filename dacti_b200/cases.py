@@ -297,9 +297,15 @@ def osc_drop(base_level: int = 4, levels: int = 2, thresholds=(1e-3, 1e-2), max_
     return Case(build_tree(spec), prm)
 
 
+def cylinder_ns_spec(*args, **kw):
+    """(SceneSpec, SolverParams) of cylinder_ns, for builders other than the host one."""
+    return cylinder_ns(*args, _spec_only=True, **kw)
+
+
 def cylinder_ns(mach: float = 0.3, base_level: int = 5, levels: int = 3, reynolds: float = 200.0,
                 prandtl: float = 0.72, thresholds=(5e-3, 1e-2), max_cfl: float = 0.4,
-                weights=(1.0, 0.01, 0.01, 1e-5), diameter: float = 1.0, center=(-10.0, 0.0)) -> Case:
+                weights=(1.0, 0.01, 0.01, 1e-5), diameter: float = 1.0, center=(-10.0, 0.0),
+                _spec_only: bool = False) -> Case:
     """2D Navier-Stokes flow past a cylinder: domain 40 x 20 (root side 40, so a 2^base_level x
     2^(base_level-1) base grid), a solid circle of the given diameter with a no-slip wall, inflow of air
     (rho 1.2, p 101325) at the given Mach number on x-, outflow on x+, free-slip walls on y. The
@@ -320,12 +326,15 @@ def cylinder_ns(mach: float = 0.3, base_level: int = 5, levels: int = 3, reynold
                  (BoundarySpec(BcType.FREESLIP), BoundarySpec(BcType.FREESLIP))]
     wall = SphereObject(center, 0.5 * diameter, "solid", BoundarySpec(BcType.NOSLIP))
     top = base_level + levels
-    spec = SceneSpec(shape, (40.0, 20.0), base_level, top, x2p, domain_bc, max_level_geom=top, objects=[wall])
+    spec = SceneSpec(shape, (40.0, 20.0), base_level, top, x2p, domain_bc, max_level_geom=top, objects=[wall],
+                     ic=("uniform", np.asarray(ref, np.float64)))
     prm = SolverParams(
         side_length=40.0, active_size=(40.0, 20.0), periodic=(False, False), max_cfl=max_cfl, max_dt=1.0,
         error_threshold=thresholds, max_level=top, min_level=base_level, weights=weights,
         ns_mu=mu, ns_lambda=mu * 1005.0 / prandtl,
     )
+    if _spec_only:
+        return spec, prm
     return Case(build_tree(spec), prm)
 
 

@@ -1,10 +1,12 @@
 """Initial tree built on the GPU (dg_build_tree in csrc/scene_build.cu) from a SceneSpec.
 
-Same nodes, in the same order, as scene.build_tree for the scenes it covers: droplet/bubble spheres
-and ellipses, domain-face boundaries, refinement zones, the initial jump and inflow_r faces, a uniform
-or jump initial condition given as data (`SceneSpec.ic`) and the tanh interface. Scenes with solid
-objects, polygons or a programmatic-only initial condition raise NotImplementedError; build those
-with scene.build_tree.
+Same nodes, in the same order, as scene.build_tree for the scenes it covers: spheres and ellipses
+(droplets, bubbles and solids with their object boundaries and fix_boundary), domain-face boundaries,
+refinement zones, the initial jump and inflow_r faces, a uniform or jump initial condition given as
+data (`SceneSpec.ic`) and the tanh interface. The device marks object faces; their conditions and
+normals are assigned here with the host builder's own rule, so only the numbering of the boundary
+table can differ from scene.build_tree's. Polygon objects or a programmatic-only initial condition
+raise NotImplementedError; build those with scene.build_tree.
 """
 from __future__ import annotations
 
@@ -14,7 +16,7 @@ import math
 import numpy as np
 
 from .models import BcType
-from .scene import BoundarySpec, EllipseObject, SceneSpec, SphereObject, Tree
+from .scene import BoundarySpec, EllipseObject, SceneSpec, SphereObject, Tree, _ObjectBoundaries
 from .solver import DG_OK, DgError, load_library
 
 _D = ctypes.c_double
@@ -54,6 +56,8 @@ def _bind(lib):
 
 
 def _object_row(o) -> list:
+    if not isinstance(o, (SphereObject, EllipseObject)):
+        raise NotImplementedError(f"{type(o).__name__} objects need the host builder")
     c = list(np.asarray(o.center, np.float64)) + [0.0] * 3
     if isinstance(o, SphereObject):
         axes, cs, sn, shape = [o.radius, o.radius, o.radius], 1.0, 0.0, 0
@@ -67,9 +71,10 @@ def _object_row(o) -> list:
             cs, sn = 1.0, 0.0
     else:
         raise NotImplementedError(f"{type(o).__name__} objects need the host builder")
-    if o.bc is not None or o.type not in ("droplet", "bubble"):
-        raise NotImplementedError("solid objects (object boundaries) need the host builder")
-    return c[:3] + axes + [cs, sn, float(shape), 0.0 if o.type == "droplet" else 1.0]
+    kind = {"droplet": 0.0, "bubble": 1.0}.get(o.type, 2.0)
+    has_bc = o.bc is not None
+    inflow_r = has_bc and o.bc.type == BcType.INFLOW_R
+    return c[:3] + axes + [cs, sn, float(shape), kind, 1.0 if has_bc else 0.0, 1.0 if inflow_r else 0.0]
 
 
 def build_tree_device(spec: SceneSpec) -> Tree:
@@ -105,7 +110,7 @@ def build_tree_device(spec: SceneSpec) -> Tree:
             sc.inflow_r[d][side] = 1 if b.type == BcType.INFLOW_R else 0
             bcs.append(BoundarySpec(b.type, list(b.p_in) if b.p_in is not None else [0.0] * E, normal, b.fade_in))
             k += 1
-    objs = np.array([_object_row(o) for o in spec.objects] or [[0.0] * 10], np.float64)
+    objs = np.array([_object_row(o) for o in spec.objects] or [[0.0] * 12], np.float64)
     sc.n_objects = len(spec.objects)
     sc.objects = objs.ctypes.data_as(ctypes.POINTER(_D))
     zones = np.array([list(z.x0) + list(z.x1) + [float(z.level)] for z in spec.zones] or [[0.0] * 7], np.float64)
@@ -153,5 +158,15 @@ def build_tree_device(spec: SceneSpec) -> Tree:
             raise DgError(rc, "dg_tree_copy failed")
     finally:
         lib.dg_tree_free(h)
+    marked = (bc == -2).any(axis=1)
+    if marked.any():
+        # object faces: the nearest object's condition with the surface normal there, as the host
+        # builder assigns them (scene._ObjectBoundaries)
+        walls = _ObjectBoundaries(spec, D, E)
+        nodes = np.nonzero(marked)[0]
+        ids = walls.nearest(center[nodes], bcs)
+        rows = bc[nodes]
+        rows[rows == -2] = np.repeat(ids, (rows == -2).sum(axis=1))
+        bc[nodes] = rows
     return Tree(shape=sh, parent=parent, children=children, level=level, flags=flags, bc=bc, center=center, p=p,
                 bcs=bcs)

@@ -16,14 +16,19 @@ from dacti_b200.toml_case import load_toml_case
 pytestmark = pytest.mark.gpu
 
 
+def _bc_specs(t):
+    """Each face's boundary as (type, state, normal), None without one: the boundary table's numbering
+    is free."""
+    keys = [(int(b.type), tuple(b.p_in), tuple(b.normal), float(b.fade_in)) for b in t.bcs]
+    return [[keys[k] if k >= 0 else None for k in row] for row in t.bc.tolist()]
+
+
 def _same(a, b):
-    for name in ("parent", "children", "level", "flags", "bc", "center"):
+    for name in ("parent", "children", "level", "flags", "center"):
         x, y = getattr(a, name), getattr(b, name)
         assert x.shape == y.shape and np.array_equal(x, y), name
     assert np.allclose(a.p, b.p, rtol=1e-14, atol=1e-14 * np.abs(a.p).max())
-    assert len(a.bcs) == len(b.bcs)
-    for u, v in zip(a.bcs, b.bcs):
-        assert u.type == v.type and np.array_equal(u.p_in, v.p_in) and np.array_equal(u.normal, v.normal)
+    assert _bc_specs(a) == _bc_specs(b)
 
 
 @pytest.mark.parametrize("dims,base,levels", [(2, 5, 3), (3, 4, 2)])
@@ -39,10 +44,26 @@ def test_toml_scene_tree(name, diffuse):
     _same(tc.case.tree, build_tree_device(tc.spec))
 
 
-def test_solid_objects_stay_on_the_host():
+def test_solid_objects():
+    # object faces, fix_boundary and the one-sided boundary drop on the device
     tc = load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"))
+    dev = build_tree_device(tc.spec)
+    _same(tc.case.tree, dev)
+    from dacti_b200.models import F_ACTIVE, F_IS_BOUNDARY, F_LEAF
+    assert ((dev.flags & F_IS_BOUNDARY) != 0).any() and ((dev.flags & (F_LEAF | F_ACTIVE)) == F_LEAF).any()
+    spec, _ = cases.cylinder_ns_spec(base_level=5, levels=3)
+    _same(build_tree(spec), build_tree_device(spec))
+
+
+def test_polygons_stay_on_the_host(tmp_path):
+    text = open(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml")).read().replace(
+        'shape = "circle"\nradius = 0.2', 'shape = "diamond"\nwidth = 0.4\nheight = 0.3')
+    path = tmp_path / "dia.toml"
+    path.write_text(text)
+    tc = load_toml_case(str(path))
     with pytest.raises(NotImplementedError, match="host builder"):
         build_tree_device(tc.spec)
+    _same(tc.case.tree, load_toml_case(str(path), builder="auto").case.tree)
 
 
 def test_full_size_shock_drop_build_time():
@@ -61,7 +82,5 @@ def test_full_size_shock_drop_build_time():
 def test_toml_loader_device_builder():
     for name in ("bubble_jump2d", "cylinder_ns2d"):
         host = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"))
-        auto = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"), builder="auto")
-        _same(host.case.tree, auto.case.tree)  # the cylinder falls back to the host builder
-    with pytest.raises(NotImplementedError):
-        load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"), builder="device")
+        dev = load_toml_case(os.path.join(GOLDEN, "toml", f"{name}.toml"), builder="device")
+        _same(host.case.tree, dev.case.tree)
