@@ -1,5 +1,5 @@
 // Initial tree on the device: Scene::init_domain (scene/scene.cpp:369-431) for scenes with analytic
-// spheres and ellipses, level by level as the host builder does it (dacti_b200/scene.py), so that
+// spheres, ellipses and polygons, level by level as the host builder does it (dacti_b200/scene.py), so that
 // both produce the same nodes in the same order:
 //
 //  - signed distances to the objects and the nearest object (scene.cpp:47-91), sphere |x - c| - r and
@@ -38,6 +38,8 @@ constexpr int TPB      = 256;
 constexpr int MAX_OBJ  = 16;
 constexpr int MAX_ZONE = 16;
 constexpr int BC_MARK  = -2;  // object boundary; the host assigns the condition
+constexpr int MAX_VERT = 8;   // polygon vertices per object
+constexpr int OBJ_ROW  = 13 + 2 * MAX_VERT;
 
 struct Scene {
 	int D, E, C, NF, multi, ia;
@@ -48,7 +50,9 @@ struct Scene {
 	int dbc[3][2], inflow_r[3][2];
 	int n_obj, walls;
 	double oc[MAX_OBJ][3], oa[MAX_OBJ][3], ocs[MAX_OBJ], osn[MAX_OBJ];
-	int oshape[MAX_OBJ], otype[MAX_OBJ], obc[MAX_OBJ], obc_inflow_r[MAX_OBJ];
+	int oshape[MAX_OBJ], otype[MAX_OBJ], obc[MAX_OBJ], obc_inflow_r[MAX_OBJ];  // shape 0 sphere, 1 ellipse, 2 polygon
+	int onv[MAX_OBJ];
+	double ov[MAX_OBJ][MAX_VERT][2];
 	int n_zone;
 	double zx0[MAX_ZONE][3], zx1[MAX_ZONE][3];
 	int zlevel[MAX_ZONE];
@@ -73,7 +77,52 @@ constexpr double DMAX = 1.7976931348623157e308;
 
 __device__ bool active_node(const Arrays &A, long long i) { return i != 0 && (A.flags[i] & dg::F_ACTIVE); }
 
+// Closed polygon (2D): distance to the nearest edge, negative inside (even-odd rule), in the host
+// builder's order of operations.
+__device__ double polygon_distance(const Scene &S, int o, const double *x) {
+	double dist = INFINITY;
+	bool inside = false;
+	const int nv = S.onv[o];
+	for (int k = 0; k < nv; ++k) {
+		const double a0 = S.ov[o][k][0], a1 = S.ov[o][k][1];
+		const double b0 = S.ov[o][(k + 1) % nv][0], b1 = S.ov[o][(k + 1) % nv][1];
+		const double ab0 = b0 - a0, ab1 = b1 - a1;
+		double t         = ((x[0] - a0) * ab0 + (x[1] - a1) * ab1) / (ab0 * ab0 + ab1 * ab1);
+		t                = fmin(fmax(t, 0.0), 1.0);
+		const double e0 = x[0] - (a0 + t * ab0), e1 = x[1] - (a1 + t * ab1);
+		dist            = fmin(dist, sqrt(e0 * e0 + e1 * e1));
+		const bool crosses = (a1 > x[1]) != (b1 > x[1]);
+		if (crosses) {
+			const double xc = a0 + (x[1] - a1) * ab0 / ab1;
+			if (x[0] < xc) inside = !inside;
+		}
+	}
+	return inside ? -dist : dist;
+}
+
+__device__ double sgn(double v) { return v > 0 ? 1.0 : (v < 0 ? -1.0 : 0.0); }
+
+__device__ double cross3(double o0, double o1, double a0, double a1, double b0, double b1) {
+	return (a0 - o0) * (b1 - o1) - (a1 - o1) * (b0 - o0);
+}
+
+// Segment p-q meets an edge of the polygon (touching counts).
+__device__ bool polygon_hits(const Scene &S, int o, const double *p, const double *q) {
+	const int nv = S.onv[o];
+	for (int k = 0; k < nv; ++k) {
+		const double a0 = S.ov[o][k][0], a1 = S.ov[o][k][1];
+		const double b0 = S.ov[o][(k + 1) % nv][0], b1 = S.ov[o][(k + 1) % nv][1];
+		const double d1 = cross3(a0, a1, b0, b1, p[0], p[1]), d2 = cross3(a0, a1, b0, b1, q[0], q[1]);
+		const double d3 = cross3(p[0], p[1], q[0], q[1], a0, a1), d4 = cross3(p[0], p[1], q[0], q[1], b0, b1);
+		if (sgn(d1) * sgn(d2) <= 0 && sgn(d3) * sgn(d4) <= 0 && fmin(p[0], q[0]) <= fmax(a0, b0) &&
+		    fmax(p[0], q[0]) >= fmin(a0, b0) && fmin(p[1], q[1]) <= fmax(a1, b1) && fmax(p[1], q[1]) >= fmin(a1, b1))
+			return true;
+	}
+	return false;
+}
+
 __device__ double signed_distance(const Scene &S, int o, const double *x) {
+	if (S.oshape[o] == 2) return polygon_distance(S, o, x);
 	if (S.oshape[o] == 0) {
 		double s = 0.0;
 		for (int d = 0; d < S.D; ++d) {
@@ -136,6 +185,10 @@ __device__ bool hits_unit(const double *a, const double *b, int D) {
 __device__ bool raycast(const Scene &S, const double *a, const double *b) {
 	for (int o = 0; o < S.n_obj; ++o) {
 		if (!S.obc[o]) return false;
+		if (S.oshape[o] == 2) {
+			if (polygon_hits(S, o, a, b)) return true;
+			continue;
+		}
 		double ya[3], yb[3];
 		unit_frame(S, o, a, ya);
 		unit_frame(S, o, b, yb);
@@ -620,10 +673,14 @@ int dg_build_tree(const dg_scene *in, dg_tree **out) {
 	S.n_obj = in->n_objects;
 	S.walls = 0;
 	for (int o = 0; o < S.n_obj; ++o) {
-		const double *ob = in->objects + 12 * o;
+		const double *ob = in->objects + OBJ_ROW * o;
 		for (int d = 0; d < 3; ++d) S.oc[o][d] = ob[d], S.oa[o][d] = ob[3 + d];
 		S.ocs[o] = ob[6], S.osn[o] = ob[7];
 		S.oshape[o] = (int) ob[8], S.otype[o] = (int) ob[9], S.obc[o] = (int) ob[10], S.obc_inflow_r[o] = (int) ob[11];
+		S.onv[o] = (int) ob[12];
+		if (S.oshape[o] == 2 && (S.D != 2 || S.onv[o] < 3 || S.onv[o] > MAX_VERT))
+			return fail(DG_ERR_ARG, "dg_build_tree: polygons are 2D with 3 to 8 vertices");
+		for (int k = 0; k < MAX_VERT; ++k) S.ov[o][k][0] = ob[13 + 2 * k], S.ov[o][k][1] = ob[14 + 2 * k];
 		if (S.otype[o] < 0 || S.otype[o] > 2) return fail(DG_ERR_ARG, "dg_build_tree: object type must be 0, 1 or 2");
 		if (S.obc[o]) S.walls = 1;
 	}

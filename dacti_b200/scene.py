@@ -177,8 +177,10 @@ class PolygonObject:
         inside = np.zeros(x.shape[0], bool)
         for a, b in zip(v, w):
             ab = b - a
-            t = np.clip(((x - a) @ ab) / (ab @ ab), 0.0, 1.0)
-            dist = np.minimum(dist, np.sqrt(((x - (a + t[:, None] * ab)) ** 2).sum(axis=1)))
+            # elementwise products and sums (no fused dot product): the device builder rounds the same way
+            t = np.clip(((x[:, 0] - a[0]) * ab[0] + (x[:, 1] - a[1]) * ab[1]) / (ab[0] * ab[0] + ab[1] * ab[1]), 0.0, 1.0)
+            e0, e1 = x[:, 0] - (a[0] + t * ab[0]), x[:, 1] - (a[1] + t * ab[1])
+            dist = np.minimum(dist, np.sqrt(e0 * e0 + e1 * e1))
             crosses = (a[1] > x[:, 1]) != (b[1] > x[:, 1])
             with np.errstate(divide="ignore", invalid="ignore"):
                 xc = a[0] + (x[:, 1] - a[1]) * ab[0] / ab[1]

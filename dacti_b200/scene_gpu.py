@@ -1,12 +1,12 @@
 """Initial tree built on the GPU (dg_build_tree in csrc/scene_build.cu) from a SceneSpec.
 
-Same nodes, in the same order, as scene.build_tree for the scenes it covers: spheres and ellipses
-(droplets, bubbles and solids with their object boundaries and fix_boundary), domain-face boundaries,
+Same nodes, in the same order, as scene.build_tree for the scenes it covers: spheres, ellipses and
+polygons (droplets, bubbles and solids with their object boundaries and fix_boundary), domain-face boundaries,
 refinement zones, the initial jump and inflow_r faces, a uniform or jump initial condition given as
 data (`SceneSpec.ic`) and the tanh interface. The device marks object faces; their conditions and
 normals are assigned here with the host builder's own rule, so only the numbering of the boundary
-table can differ from scene.build_tree's. Polygon objects or a programmatic-only initial condition
-raise NotImplementedError; build those with scene.build_tree.
+table can differ from scene.build_tree's. Polygons with more than 8 vertices or a programmatic-only
+initial condition raise NotImplementedError; build those with scene.build_tree.
 """
 from __future__ import annotations
 
@@ -16,7 +16,7 @@ import math
 import numpy as np
 
 from .models import BcType
-from .scene import BoundarySpec, EllipseObject, SceneSpec, SphereObject, Tree, _ObjectBoundaries
+from .scene import BoundarySpec, EllipseObject, PolygonObject, SceneSpec, SphereObject, Tree, _ObjectBoundaries
 from .solver import DG_OK, DgError, load_library
 
 _D = ctypes.c_double
@@ -55,7 +55,22 @@ def _bind(lib):
     return lib
 
 
+MAX_VERT = 8
+
+
 def _object_row(o) -> list:
+    """One row of dg_scene.objects (29 values)."""
+    kind = {"droplet": 0.0, "bubble": 1.0}.get(o.type, 2.0)
+    has_bc = o.bc is not None
+    inflow_r = has_bc and o.bc.type == BcType.INFLOW_R
+    tail = [kind, 1.0 if has_bc else 0.0, 1.0 if inflow_r else 0.0]
+    if isinstance(o, PolygonObject):
+        v = np.asarray(o.vertices, np.float64)
+        if v.shape[0] > MAX_VERT or v.shape[1] != 2:
+            raise NotImplementedError("polygons with more than 8 vertices need the host builder")
+        verts = np.zeros((MAX_VERT, 2))
+        verts[: v.shape[0]] = v
+        return [0.0] * 6 + [1.0, 0.0, 2.0] + tail + [float(v.shape[0])] + list(verts.ravel())
     if not isinstance(o, (SphereObject, EllipseObject)):
         raise NotImplementedError(f"{type(o).__name__} objects need the host builder")
     c = list(np.asarray(o.center, np.float64)) + [0.0] * 3
@@ -71,10 +86,7 @@ def _object_row(o) -> list:
             cs, sn = 1.0, 0.0
     else:
         raise NotImplementedError(f"{type(o).__name__} objects need the host builder")
-    kind = {"droplet": 0.0, "bubble": 1.0}.get(o.type, 2.0)
-    has_bc = o.bc is not None
-    inflow_r = has_bc and o.bc.type == BcType.INFLOW_R
-    return c[:3] + axes + [cs, sn, float(shape), kind, 1.0 if has_bc else 0.0, 1.0 if inflow_r else 0.0]
+    return c[:3] + axes + [cs, sn, float(shape)] + tail + [0.0] * (1 + 2 * MAX_VERT)
 
 
 def build_tree_device(spec: SceneSpec) -> Tree:
@@ -110,7 +122,7 @@ def build_tree_device(spec: SceneSpec) -> Tree:
             sc.inflow_r[d][side] = 1 if b.type == BcType.INFLOW_R else 0
             bcs.append(BoundarySpec(b.type, list(b.p_in) if b.p_in is not None else [0.0] * E, normal, b.fade_in))
             k += 1
-    objs = np.array([_object_row(o) for o in spec.objects] or [[0.0] * 12], np.float64)
+    objs = np.array([_object_row(o) for o in spec.objects] or [[0.0] * (13 + 2 * MAX_VERT)], np.float64)
     sc.n_objects = len(spec.objects)
     sc.objects = objs.ctypes.data_as(ctypes.POINTER(_D))
     zones = np.array([list(z.x0) + list(z.x1) + [float(z.level)] for z in spec.zones] or [[0.0] * 7], np.float64)

@@ -156,7 +156,7 @@ int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long 
 int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out);
 
 /* ---- Initial tree on the device: Scene::init_domain (scene/scene.cpp:369-431) for analytic scenes --
- * Spheres and ellipses (droplets, bubbles and solids with a boundary condition), domain-face
+ * Spheres, ellipses and polygons (droplets, bubbles and solids with a boundary condition), domain-face
  * boundaries, object faces and fix_boundary, refinement near objects, inflow_r faces, the initial jump
  * and in zones, the uniform or jump initial condition and the tanh-smeared volume fraction. Produces the
  * same nodes in the same order as the host builder; the result feeds dg_case. Object faces come back
@@ -170,9 +170,10 @@ typedef struct dg_scene {
 	int domain_bc[3][2];  /* boundary-table id of each domain face, -1 on periodic dimensions */
 	int inflow_r[3][2];   /* 1 where that face's condition is inflow_r (refined to the maximum level) */
 	int n_objects;        /* <= 16 */
-	const double *objects; /* 12 per object: centre[3], semi-axes[3] (a sphere's radius first), cos and sin
-	                          of its rotation about z, shape (0 sphere, 1 ellipse), type (0 droplet,
-	                          1 bubble, 2 solid), 1 if it has a boundary condition, 1 if that is inflow_r */
+	const double *objects; /* 29 per object: centre[3], semi-axes[3] (a sphere's radius first), cos and sin
+	                          of its rotation about z, shape (0 sphere, 1 ellipse, 2 polygon), type
+	                          (0 droplet, 1 bubble, 2 solid), 1 if it has a boundary condition, 1 if that
+	                          is inflow_r, the polygon's vertex count (3..8, 2D) and vertices x, y [8][2] */
 	int n_zones;          /* <= 16 */
 	const double *zones;  /* 7 per zone: x0[3], x1[3], level */
 	int refine_jump, jump_axis;

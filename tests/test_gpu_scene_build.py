@@ -55,15 +55,15 @@ def test_solid_objects():
     _same(build_tree(spec), build_tree_device(spec))
 
 
-def test_polygons_stay_on_the_host(tmp_path):
+@pytest.mark.parametrize("shape", ['shape = "diamond"\nwidth = 0.4\nheight = 0.3',
+                                   'shape = "triangle"\nv1 = [0.2, 0.0]\nv2 = [-0.15, 0.18]\nv3 = [-0.1, -0.2]'])
+def test_polygon_solids(tmp_path, shape):
     text = open(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml")).read().replace(
-        'shape = "circle"\nradius = 0.2', 'shape = "diamond"\nwidth = 0.4\nheight = 0.3')
-    path = tmp_path / "dia.toml"
+        'shape = "circle"\nradius = 0.2', shape)
+    path = tmp_path / "poly.toml"
     path.write_text(text)
     tc = load_toml_case(str(path))
-    with pytest.raises(NotImplementedError, match="host builder"):
-        build_tree_device(tc.spec)
-    _same(tc.case.tree, load_toml_case(str(path), builder="auto").case.tree)
+    _same(tc.case.tree, build_tree_device(tc.spec))
 
 
 def test_full_size_shock_drop_build_time():
