@@ -135,6 +135,20 @@ int dg_forecast_features(dg_solver *s, double *features, long long max_cells, lo
 	});
 }
 
+int dg_tree_size(dg_solver *s, long long *n) {
+	if (!s || !n) return DG_ERR_ARG;
+	return guarded(s, [&] { *n = s->impl->tree_size(); });
+}
+
+int dg_read_tree(dg_solver *s, int *parent, int *children, int *level, unsigned int *flags, double *p, double *meta,
+                 long long max_nodes, long long *n_out) {
+	if (!s || !parent || !children || !level || !flags || !p || !meta) return DG_ERR_ARG;
+	return guarded(s, [&] {
+		long long n = s->impl->read_tree(parent, children, level, flags, p, meta, max_nodes);
+		if (n_out) *n_out = n;
+	});
+}
+
 int dg_set_hold(dg_solver *s, const unsigned char *hold, long long n) {
 	if (!s || (!hold && n > 0)) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->set_hold(hold, n); });

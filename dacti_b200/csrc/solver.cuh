@@ -39,6 +39,9 @@ public:
 	virtual long long read_slopes(double *data, long long max_cells) = 0;
 	virtual long long read_gradients(double *data, long long max_cells) = 0;
 	virtual long long forecast_features(double *data, long long max_cells) = 0;
+	virtual long long tree_size() = 0;
+	virtual long long read_tree(int32_t *parent, int32_t *child, int32_t *level, uint32_t *flags, double *p, double *meta,
+	                            long long max_nodes) = 0;
 	virtual int dims() const = 0;
 	virtual void set_hold(const uint8_t *hold, long long n) = 0;
 	virtual void set_coarsen_interval(int k) = 0;
@@ -493,6 +496,12 @@ public:
 		upload_soa(P_.bc, bc.data(), n, NF);
 		upload_soa(P_.center, c.center, n, D);
 		upload_soa(P_.p, c.p, n, E);
+		// Node::error as the scene leaves it: -1 on every split child (integrator/domain.hpp:215), kept by
+		// leaves that never get an estimate (inactive ones) and summed by unsplit (domain.hpp:306-309)
+		{
+			std::vector<double> err((size_t) n, -1.0);
+			upload_soa(P_.err, err.data(), n, 1);
+		}
 		active_leaves_.clear();
 		for (int i = 1; i < n; ++i)
 			if ((c.flags[i] & DG_F_LEAF) && (c.flags[i] & DG_F_ACTIVE)) active_leaves_.push_back(i);
@@ -941,6 +950,37 @@ public:
 		                     });
 	}
 	int dims() const override { return D; }
+
+	long long tree_size() override { return h_cnt_->top; }
+
+	// The whole node pool, slots [0, top), component-major as the pool stores it: parent[n],
+	// child[C][n], level[n], flags[n], p[E][n], meta[4][n] = {acti_level, error, max_dt, cfl}. Internal,
+	// inactive and garbage slots included: what a hyper-tree writer walks from the root.
+	long long read_tree(int32_t *parent, int32_t *child, int32_t *level, uint32_t *flags, double *p, double *meta,
+	                    long long max_nodes) override {
+		const long long n = h_cnt_->top;
+		if (n > max_nodes) throw dg_error(DG_ERR_ARG, "read buffer too small");
+		const size_t cap = (size_t) P_.cap, nn = (size_t) n;
+		std::vector<int8_t> lv(nn), ac(nn);
+		auto rows = [&](void *dst, const void *src, size_t elem, int comps) {
+			DG_CUDA(cudaMemcpy2DAsync(dst, elem * nn, src, elem * cap, elem * nn, comps, cudaMemcpyDeviceToHost, st_));
+		};
+		rows(parent, P_.parent, 4, 1);
+		rows(child, P_.child, 4, NC);
+		rows(lv.data(), P_.level, 1, 1);
+		rows(ac.data(), P_.acti, 1, 1);
+		rows(flags, P_.flags, 4, 1);
+		rows(p, P_.p, 8, E);
+		rows(meta + nn, P_.err, 8, 1);
+		rows(meta + 2 * nn, P_.maxdt, 8, 1);
+		rows(meta + 3 * nn, P_.cfl, 8, 1);
+		DG_CUDA(cudaStreamSynchronize(st_));
+		for (size_t i = 0; i < nn; ++i) {
+			level[i] = lv[i];
+			meta[i]  = (double) ac[i];
+		}
+		return n;
+	}
 
 	// Forecast-driven regrid: F_HOLD on the active cells (read_cells' order) and the interval in global
 	// steps between coarsening passes (1 = every step, the reference's behaviour).

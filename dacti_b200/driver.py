@@ -4,7 +4,8 @@
 `signal = time > signal_time`; after every step it decides, as the reference does, whether to write a
 frame (simulation time advanced by at least `io_interval` since the last one, convergence, or NaN), and
 then appends a row (time, frame, step, n_cells and the observers' integral variables) to
-`<out_dir>/<name>_observables.csv` and writes `<out_dir>/<name>_<frame:04>.vtu`. Frame 0 is the initial
+`<out_dir>/<name>_observables.csv` and writes `<out_dir>/<name>_<frame:04>.vtu` (vtu_writer, the
+default) or `<out_dir>/<name>_<frame:04>.htg` (htg_writer, `writer="htg"`). Frame 0 is the initial
 state. A NaN (force_break) ends the run after its frame, as in the reference.
 """
 from __future__ import annotations
@@ -15,6 +16,7 @@ from typing import Optional, Sequence
 
 import numpy as np
 
+from .htg import write_frame
 from .io import write_vtu
 from .solver import Solver
 
@@ -159,7 +161,11 @@ class AeroForce:
 class DefaultDriver:
     def __init__(self, solver: Solver, name: str, out_dir: str, end_time: Optional[float] = None,
                  io_interval: float = 0.0, observers: Sequence = (), convergence_tol: float = 0.0,
-                 signal_time: float = 0.0, write_frames: bool = True, max_steps: Optional[int] = None):
+                 signal_time: float = 0.0, write_frames: bool = True, max_steps: Optional[int] = None,
+                 writer: str = "vtu"):
+        if writer not in ("vtu", "htg"):
+            raise ValueError("writer is 'vtu' (vtu_writer) or 'htg' (htg_writer)")
+        self.writer = writer
         self.s, self.name, self.out_dir = solver, name, out_dir
         self.end_time, self.io_interval = end_time, io_interval
         self.observers, self.convergence_tol, self.signal_time = list(observers), convergence_tol, signal_time
@@ -173,7 +179,10 @@ class DefaultDriver:
         return vals
 
     def _frame(self, frame: int, snap) -> None:
-        if self.write_frames:
+        if self.write_frames and self.writer == "htg":
+            # htg_writer takes the observers' fields and does not write them (htg_writer.hpp:27-33)
+            write_frame(self.out_dir, self.name, frame, self.s.tree_nodes(), float(self.s.params.active_size[0]))
+        elif self.write_frames:
             # observers' field variables as cell data "<observer>/<field>" (driver/default_driver.hpp:45-72)
             fields = {}
             for ob in self.observers:

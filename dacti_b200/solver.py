@@ -15,6 +15,7 @@ from typing import Callable, Optional
 import numpy as np
 
 from .casefile import Case, Snapshot
+from .htg import NodeTable
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libdacti_gpu.so")
@@ -93,6 +94,9 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     fp, dp, ll = ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_double), ctypes.c_longlong
     lib.dg_set_hold.argtypes = [vp, ctypes.POINTER(ctypes.c_ubyte), ll]
     lib.dg_set_coarsen_interval.argtypes = [vp, ctypes.c_int]
+    ip, up = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_uint)
+    lib.dg_tree_size.argtypes = [vp, ctypes.POINTER(ll)]
+    lib.dg_read_tree.argtypes = [vp, ip, ip, ip, up, dp, dp, ll, ctypes.POINTER(ll)]
     lib.dg_mlp_last_error.argtypes = []
     lib.dg_mlp_last_error.restype = ctypes.c_char_p
     lib.dg_mlp_create.argtypes = [ctypes.c_int, ctypes.c_ulonglong, ctypes.POINTER(vp)]
@@ -117,6 +121,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
 
 EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "dg_step_many", "dg_cell_count",
                     "dg_read_cells", "dg_read_slopes", "dg_read_gradients", "dg_forecast_features", "dg_set_hold", "dg_set_coarsen_interval",
+                    "dg_tree_size", "dg_read_tree",
                     "dg_mlp_last_error", "dg_mlp_create", "dg_mlp_param_count", "dg_mlp_set_params",
                     "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
                     "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
@@ -256,6 +261,33 @@ class Solver:
         got = ctypes.c_longlong(0)
         self._check(self._lib.dg_forecast_features(self._h, _ptr(out, ctypes.c_double), n, ctypes.byref(got)))
         return out[: got.value].astype(np.float32)
+
+    def tree_nodes(self) -> NodeTable:
+        """dg_read_tree: every node slot of the device pool (Integrator::get_nodes), what the HTG writer
+        walks. Slot numbers are the device's; the tree they link is the reference's."""
+        sh = self.shape
+        n = ctypes.c_longlong(0)
+        self._check(self._lib.dg_tree_size(self._h, ctypes.byref(n)))
+        n = int(n.value)
+        C = 1 << sh.dims
+        parent = np.zeros(max(n, 1), np.int32)
+        children = np.zeros((C, max(n, 1)), np.int32)
+        level = np.zeros(max(n, 1), np.int32)
+        flags = np.zeros(max(n, 1), np.uint32)
+        p = np.zeros((sh.E, max(n, 1)))
+        meta = np.zeros((4, max(n, 1)))
+        got = ctypes.c_longlong(0)
+        self._check(self._lib.dg_read_tree(self._h, _ptr(parent, ctypes.c_int), _ptr(children, ctypes.c_int),
+                                           _ptr(level, ctypes.c_int), _ptr(flags, ctypes.c_uint),
+                                           _ptr(p, ctypes.c_double), _ptr(meta, ctypes.c_double), n,
+                                           ctypes.byref(got)))
+        # the device copies component-major rows of exactly n values each
+        k = int(got.value)
+        children = children.reshape(-1)[: C * k].reshape(C, k)
+        p = p.reshape(-1)[: sh.E * k].reshape(sh.E, k)
+        meta = meta.reshape(-1)[: 4 * k].reshape(4, k)
+        return NodeTable(sh.dims, parent[:k].copy(), np.ascontiguousarray(children.T), level[:k].copy(),
+                         flags[:k].copy(), np.ascontiguousarray(p.T), np.ascontiguousarray(meta.T))
 
     def set_hold(self, hold) -> None:
         """dg_set_hold: one flag per active cell (active_cells() order)."""

@@ -155,6 +155,17 @@ int dg_read_slopes(dg_solver *s, double *slopes, long long max_cells, long long 
  * whose steps skip the gradient computation. */
 int dg_read_gradients(dg_solver *s, double *gradients, long long max_cells, long long *n_out);
 
+/* Integrator::get_nodes (integrator/integrator.hpp:165), as DACTI's HTG writer walks it
+ * (driver/io/htg_writer.hpp:112-161): every node slot [0, n) of the device pool, internal, inactive and
+ * garbage slots included, component-major: parent[n], children[2^D][n], level[n] (tree level),
+ * flags[n] (bit 0 leaf, bit 1 active, bit 2 garbage), p[E][n] (meaningful on leaves), meta[4][n] =
+ * Node::get_metadata() = {acti_level, error, max_dt, cfl} (integrator/node.hpp:56-58). Slot 0 is the
+ * null node; the root is the one non-garbage slot of level 0 (slot numbers follow the device's own
+ * re-sorts, not the reference's tree indices; child order is the reference's). dg_tree_size gives n. */
+int dg_tree_size(dg_solver *s, long long *n);
+int dg_read_tree(dg_solver *s, int *parent, int *children, int *level, unsigned int *flags, double *p, double *meta,
+                 long long max_nodes, long long *n_out);
+
 /* ---- Initial tree on the device: Scene::init_domain (scene/scene.cpp:369-431) for analytic scenes --
  * Spheres, ellipses and polygons (droplets, bubbles and solids with a boundary condition), domain-face
  * boundaries, object faces and fix_boundary, refinement near objects, inflow_r faces, the initial jump

@@ -6,6 +6,7 @@
 // Usage: dacti_ref_runner <case.bin> <out_prefix> <n_global_steps> [--check s1,s2,..]
 //                         [--t-end T] [--neighbor-audit] [--quiet]
 //                         [--sample-substeps S --samples N]   (bounded timing samples)
+//                         [--nodes]   (with each snapshot, the whole node table of get_nodes())
 // Prints one JSON line with timing (wall time of integrate() calls only), substep and
 // leaf-update counts. Leaf cell-updates are counted in the substep hook as the level's cluster
 // size, as impl/integrate.hpp:57-64 exposes it.
@@ -45,6 +46,7 @@ namespace {
 		int samples = 0;
 		bool adapter_check = false;  // side-by-side run against the GPU adapter (adapter build only)
 		bool driver_check  = false;  // DACTI's default_driver over the reference and over the adapter
+		bool nodes         = false;  // also dump Integrator::get_nodes() beside each snapshot
 	};
 
 	template<typename Model>
@@ -158,6 +160,35 @@ namespace {
 			for (int q = 0; q < NP; q++) buf[k++] = node.cell.k[q];
 			w.put(buf, k);
 		});
+	}
+
+	// Every node of Integrator::get_nodes() (integrator/integrator.hpp:165), in tree order: the input
+	// of DACTI's HTG writer (driver/io/htg_writer.hpp:112-161). "DGNODE01", int32 {D, E, n, root},
+	// then per node: int32 parent, children[2^D], tree level, flags (1 leaf, 2 active, 4 garbage),
+	// double p[E], get_metadata()[4].
+	template<typename Model, typename R>
+	void write_nodes(R &in, const std::string &path) {
+		constexpr int D = Model::NumDims;
+		constexpr int E = Model::NumEqns;
+		const auto tree = in.get_nodes();
+		oracle::SnapWriter w(path);
+		int32_t hdr[4] = {D, E, (int32_t) tree.size(), (int32_t) in.domain.root_index};
+		w.put("DGNODE01", 8);
+		w.put(hdr, 4);
+		for (const auto &node: tree) {
+			int32_t iv[3 + (1 << D)];
+			int k   = 0;
+			iv[k++] = (int32_t) node.parent_index;
+			for (int c = 0; c < (1 << D); ++c) iv[k++] = (int32_t) node.child_indices[c];
+			iv[k++] = node.tree_level;
+			iv[k++] = (node.is_leaf ? 1 : 0) | (node.is_active ? 2 : 0) | (node.is_garbage ? 4 : 0);
+			w.put(iv, k);
+			double dv[E + 4];
+			for (int q = 0; q < E; ++q) dv[q] = node.cell.get_p()[q];
+			const auto m = node.get_metadata();
+			for (int q = 0; q < 4; ++q) dv[E + q] = m[q];
+			w.put(dv, E + 4);
+		}
 	}
 
 #ifdef DACTI_ADAPTER_CHECK
@@ -338,6 +369,7 @@ namespace {
 		int steps_done   = 0;
 		bool force_break = false;
 		if (o.checks.count(0)) write_snapshot<Model>(in, o.out_prefix + "_0.snap", 0, time, updates);
+		if (o.checks.count(0) && o.nodes) write_nodes<Model>(in, o.out_prefix + "_0.nodes");
 
 		if (o.sample_substeps > 0) {
 			// Bounded timing samples: each integrate() call is timed from its start to the hook of its
@@ -389,6 +421,7 @@ namespace {
 			if (will_gc) gc_events++;
 			if (o.neighbor_audit) audit_bad += audit_neighbors(in);
 			if (o.checks.count(step)) write_snapshot<Model>(in, o.out_prefix + "_" + std::to_string(step) + ".snap", step, time, updates);
+			if (o.checks.count(step) && o.nodes) write_nodes<Model>(in, o.out_prefix + "_" + std::to_string(step) + ".nodes");
 			if (force_break) break;
 		}
 
@@ -431,6 +464,8 @@ int main(int argc, char **argv) {
 			o.samples = std::atoi(argv[++i]);
 		} else if (a == "--adapter-check") {
 			o.adapter_check = true;
+		} else if (a == "--nodes") {
+			o.nodes = true;
 		} else if (a == "--driver-check") {
 			o.driver_check = true;
 		}

@@ -82,3 +82,41 @@ def test_nan_break_writes_its_frame(tmp_path):
     assert res["force_break"] and s.calls == 3
     assert res["frames"] == 1  # the NaN step forces a frame before the loop ends
     assert (tmp_path / "n_0001.vtu").exists()
+
+
+class FakeTreeSolver(FakeSolver):
+    """FakeSolver whose four cells are the children of one root, for the HTG writer."""
+
+    class params:
+        active_size = (1.0, 1.0)
+
+    def tree_nodes(self):
+        from dacti_b200.htg import NodeTable
+        n = 6
+        children = np.zeros((n, 4), np.int32)
+        children[1] = [2, 3, 4, 5]
+        flags = np.array([0, 2, 3, 3, 3, 3], np.uint32)
+        p = np.zeros((n, 4))
+        p[2:] = self.u
+        return NodeTable(2, np.array([0, 0, 1, 1, 1, 1], np.int32), children, np.array([0, 0, 1, 1, 1, 1], np.int32),
+                         flags, p, np.zeros((n, 4)))
+
+
+def test_htg_frames(tmp_path):
+    from dacti_b200.htg import read_htg
+    s = FakeTreeSolver(dt=0.01, decay=0.5)
+    res = DefaultDriver(s, "h", str(tmp_path), end_time=0.05, io_interval=0.02, observers=[Totals(4)],
+                        writer="htg").run()
+    assert res["frames"] >= 2
+    for f in range(res["frames"] + 1):
+        a = read_htg(str(tmp_path / f"h_{f:04d}.htg"))
+        assert a["NbVerticesByLevel"].tolist() == [1, 4]
+        assert a["Descriptor"].tolist() == [True]
+    last = read_htg(str(tmp_path / f"h_{res['frames']:04d}.htg"))
+    # the leaves carry the state of a step (the decaying first cell, the other three at 1); the root
+    # vertex gets no value
+    assert 1.0 < last["p_0"][1] < 2.0 and np.all(last["p_0"][2:] == 1.0) and last["p_0"][0] == 0.0
+    assert not (tmp_path / "h_0000.vtu").exists()
+    import pytest
+    with pytest.raises(ValueError):
+        DefaultDriver(s, "h", str(tmp_path), writer="xdmf")
