@@ -21,8 +21,10 @@
  *     they are read back once per global step, on first use.
  *
  * Differences, all outside the solver step: the tree lives on the GPU, so get_domain() does not
- * exist, get_nodes() returns the active cells only, and get_node()/get_cell_index() index them
- * (1-based, 0 being the null node as in the reference); acti_clusters[l] and acti_buffers[l] expose
+ * exist and `domain` holds root_index only; get_nodes() returns the whole tree renumbered breadth
+ * first from the root (slot 1), with links, flags, p and metadata per node; get_node()/get_cell_index()
+ * index the active cells (1-based, 0 being the null node as in the reference); acti_clusters[l] and
+ * acti_buffers[l] expose
  * size() only. Refinement zones must be axis-aligned (no rotation in their Transform). Model
  * constants are read from the model's statics when the Integrator is constructed. Errors of the C
  * ABI surface as std::runtime_error, the reference's error type for configuration errors
@@ -135,6 +137,11 @@ namespace dacti::gpu {
 		std::shared_ptr<config::Config<Model>> config;
 		Limiter limiter;
 		ErrorEstimator error_estimator;
+
+		// Domain::root_index (integrator/domain.hpp:23), read by htg_writer; get_nodes() puts the root there
+		struct domain_index {
+			size_t root_index = 1;
+		} domain;
 
 		std::array<level_list, MAX_LEVEL> acti_clusters;
 		std::array<level_list, MAX_LEVEL> acti_buffers;
@@ -266,9 +273,66 @@ namespace dacti::gpu {
 			for (size_t i = 1; i < cells_.size(); ++i) action((int) (i - 1), cells_[i]);
 		}
 
+		/* The whole tree (Integrator::get_nodes, integrator/integrator.hpp:165), what DACTI's htg_writer
+		 * walks (driver/io/htg_writer.hpp:112-161): read with dg_read_tree and renumbered breadth first,
+		 * slot 0 the null node, slot 1 the root (domain.root_index), parents before children, garbage
+		 * slots left out. Each node carries its links, tree level, leaf/active flags, cell.size, cell.p
+		 * and get_metadata()'s acti_level, error, max_dt and cfl. The other cell fields are only in the
+		 * active-cell list (for_each_active_cell, get_node). */
 		std::vector<node_t> get_nodes() const {
-			load_cells();
-			return cells_;
+			constexpr int E = Model::NumEqns, C = 1 << Model::NumDims;
+			long long n = 0;
+			detail::check(dg_tree_size(solver_.get(), &n), solver_.get(), "dg_tree_size");
+			const size_t nn = (size_t) n;
+			std::vector<int> parent(nn), children((size_t) C * nn), level(nn);
+			std::vector<unsigned> flags(nn);
+			std::vector<double> p((size_t) E * nn), meta(4 * nn);
+			long long got = 0;
+			detail::check(dg_read_tree(solver_.get(), parent.data(), children.data(), level.data(), flags.data(), p.data(),
+			                           meta.data(), n, &got),
+			              solver_.get(), "dg_read_tree");
+			int root = 0;
+			for (size_t i = 1; i < nn && root == 0; ++i)
+				if (level[i] == 0 && !(flags[i] & DG_F_GARBAGE)) root = (int) i;
+			std::vector<node_t> out(1, node_t{});
+			if (root == 0) return out;
+			std::vector<int> order(1, root);
+			std::vector<size_t> renum(nn, 0);
+			renum[root] = 1;
+			for (size_t h = 0; h < order.size(); ++h) {
+				const int x = order[h];
+				if (flags[x] & DG_F_LEAF) continue;
+				for (int c = 0; c < C; ++c) {
+					const int ch = children[(size_t) c * nn + x];
+					if (ch <= 0 || (size_t) ch >= nn || renum[ch] != 0)
+						throw std::runtime_error("dg_read_tree: a subdivided node links an invalid child slot");
+					renum[ch] = order.size() + 1;
+					order.push_back(ch);
+				}
+			}
+			out.resize(order.size() + 1);
+			for (size_t k = 0; k < order.size(); ++k) {
+				const int x = order[k];
+				node_t nd{};
+				nd.parent_index = x == root ? 0 : renum[parent[x]];
+				nd.tree_level   = level[x];
+				nd.is_leaf      = (flags[x] & DG_F_LEAF) != 0;
+				nd.is_active    = (flags[x] & DG_F_ACTIVE) != 0;
+				nd.is_garbage   = false;
+				nd.child_indices.fill(0);
+				if (!nd.is_leaf)
+					for (int c = 0; c < C; ++c) nd.child_indices[c] = renum[children[(size_t) c * nn + x]];
+				scalar_t size = config->side_length;
+				for (int l = 0; l < nd.tree_level; ++l) size = 0.5 * size;
+				nd.cell.size = size;
+				for (int q = 0; q < E; ++q) nd.cell.p[q] = p[(size_t) q * nn + x];
+				nd.acti_level = (int) meta[x];
+				nd.error      = meta[nn + x];
+				nd.max_dt     = meta[2 * nn + x];
+				nd.cfl        = meta[3 * nn + x];
+				out[k + 1]    = nd;
+			}
+			return out;
 		}
 
 		node_t &get_node(size_t index) const {

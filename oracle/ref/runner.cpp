@@ -280,6 +280,11 @@ namespace {
 			compare(step, hr == hg, fr == fg);
 			if (fr || fg) break;
 		}
+		// the whole tree as DACTI's htg_writer reads it, from both integrators after the last step
+		if (o.nodes) {
+			write_nodes<Model>(ref, o.out_prefix + "_ref.nodes");
+			write_nodes<Model>(gpu, o.out_prefix + "_adapter.nodes");
+		}
 		// DACTI's own DropEnergy observer (driver/observer/drop_energy.hpp), compiled unchanged, on both
 		// integrators after the last step
 		if constexpr (Model::Multiphase) {

@@ -9,7 +9,8 @@ hook sequence, force_break, global_dt, the active cell set with ACTI levels, the
 (relative L1 <= 1e-10), and the slopes and gradients the adapter's nodes carry (relative L1 <= 1e-8;
 gradients where the case has viscous or conduction terms), printing one JSON line per step. For the
 multiphase cases DACTI's own DropEnergy observer (driver/observer/drop_energy.hpp), compiled unchanged
-into the same binary, runs on both integrators after the last step.
+into the same binary, runs on both integrators after the last step. After the last step both
+integrators' get_nodes() trees, the input of DACTI's htg_writer, are dumped and compared.
 """
 import json
 import os
@@ -31,7 +32,7 @@ def test_adapter_matches_reference_integrator(name, steps, tmp_path):
     if not os.path.exists(CHECK):
         pytest.fail("oracle/_ref/dacti_adapter_check is not built (make -C oracle after building the library)")
     r = subprocess.run([CHECK, os.path.join(GOLDEN, f"{name}.case"), str(tmp_path / name), str(steps),
-                        "--adapter-check"], capture_output=True, text=True, timeout=600,
+                        "--adapter-check", "--nodes"], capture_output=True, text=True, timeout=600,
                        env=dict(os.environ, OMP_NUM_THREADS="1"))
     lines = [json.loads(x) for x in r.stdout.splitlines() if x.startswith("{")]
     assert r.returncode == 0, r.stdout + r.stderr
@@ -47,6 +48,37 @@ def test_adapter_matches_reference_integrator(name, steps, tmp_path):
         assert len(de) == 1
         for a, b in zip(de[0]["ref"], de[0]["gpu"]):
             assert abs(a - b) <= 1e-8 * max(abs(a), 1e-300), de
+    _same_hyper_tree(str(tmp_path / f"{name}_ref.nodes"), str(tmp_path / f"{name}_adapter.nodes"))
+
+
+def _same_hyper_tree(ref_path, adapter_path):
+    """The adapter's get_nodes() (the whole device tree, renumbered from root slot 1) gives DACTI's
+    htg_writer the hyper tree that the reference integrator's get_nodes() gives it: same subdivisions,
+    mask and ACTI levels, p within the parity bar, max_dt and cfl within 1e-12, the error estimate
+    within 1e-6 of its largest value."""
+    import numpy as np
+    from oracle.htg_writer_ref import read_nodes, reference_htg
+
+    trees = []
+    for path in (ref_path, adapter_path):
+        d = read_nodes(path)
+        trees.append(reference_htg(d["dims"], d["parent"], d["children"], d["level"], d["flags"], d["p"], d["meta"],
+                                   d["root"]))
+    (desc_r, depth_r, mask_r, data_r), (desc_a, depth_a, mask_a, data_a) = trees
+    assert desc_r == desc_a and depth_r == depth_a and mask_r == mask_a
+    for nm in data_r:
+        wr = [v is not None for v in data_r[nm]]
+        assert wr == [v is not None for v in data_a[nm]], nm
+        a = np.array([v for v in data_a[nm] if v is not None])
+        b = np.array([v for v in data_r[nm] if v is not None])
+        if nm == "acti_level":
+            assert np.array_equal(a, b)
+        elif nm.startswith("p_"):
+            assert np.abs(a - b).sum() <= 1e-10 * max(np.abs(b).sum(), 1e-300), nm
+        elif nm == "error":
+            assert np.all(np.abs(a - b) <= 1e-6 * np.abs(b) + 1e-6 * np.abs(b).max()), nm
+        else:
+            assert np.all(np.abs(a - b) <= 1e-12 * np.abs(b)), nm
 
 
 @pytest.mark.gpu
