@@ -9,8 +9,9 @@ cluster sizes of the executed substeps. The plain FP64 form runs here.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
-N > 1 runs one independent replica per GPU (weak scaling; the shock-drop step has no exchange in this
-build). `--impl reference` times the reference's own CPU solver (built from its sources by
+N > 1 runs one independent replica of the shock-drop step per GPU (weak scaling; the step has no
+exchange in this build), and splits the batched section's independent trees among the GPUs (strong
+scaling of the batch, no exchange). `--impl reference` times the reference's own CPU solver (built from its sources by
 oracle/Makefile) on this box's host cores, in bounded samples of the same workload.
 """
 from __future__ import annotations
@@ -337,18 +338,22 @@ def learned_run(args, local_rank: int) -> dict:
     }
 
 
-def batched_run(args, local_rank: int, world: int) -> dict:
+def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     """Batched 2D Euler quadtree Riemann problems (seeded, see cases.riemann_batch): one global step of
     every tree per call of dg_step_many (host threads, one stream per tree), against the same trees
-    stepped one after another on one host thread. Mixed form."""
+    stepped one after another on one host thread. Mixed form. With N ranks the trees are split among
+    them (dacti_b200.batch, no exchange): the batch's total work is fixed (strong scaling)."""
     import torch
+    import torch.distributed as dist
     from dacti_b200 import cases
+    from dacti_b200.batch import my_trees, tree_work
     from dacti_b200.solver import Solver, step_many
 
     # each tree's host thread mostly waits on its per-substep synchronisation, so twice the cores pays
     threads = min(32, max(8, 2 * host_threads()))
     batch = cases.riemann_batch(args.batch_trees, seed=3)
-    solvers = [Solver(c, device=local_rank) for c in batch]
+    mine = my_trees([tree_work(c) for c in batch], rank, world)
+    solvers = [Solver(batch[i], device=local_rank) for i in mine]
     for s in solvers:
         s.set_form("mixed")
     step_many(solvers, threads=threads)  # warm-up; every solver gets its own stream here
@@ -357,11 +362,15 @@ def batched_run(args, local_rank: int, world: int) -> dict:
         return float(sum(s.stats().cell_updates for s in solvers))
 
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     u0, t0 = updates(), time.perf_counter()
     for _ in range(args.steps):
         step_many(solvers, threads=threads)
     torch.cuda.synchronize()
     b_sec, b_upd = time.perf_counter() - t0, updates() - u0
+    if world > 1:
+        dist.barrier()
     u0, t0 = updates(), time.perf_counter()
     for s in solvers:
         s.integrate()
@@ -370,15 +379,19 @@ def batched_run(args, local_rank: int, world: int) -> dict:
     cells = sum(s.n_active_cells() for s in solvers)
     for s in solvers:
         s.close()
+    _, cells = reduce_ranks(0.0, float(cells), world)
     b_ms, b_u = reduce_ranks(b_sec * 1e3, b_upd, world)
     s_ms, s_u = reduce_ranks(s_sec * 1e3, s_upd, world)
+    split = (f"; trees split across {world} ranks by estimated work (longest first to the least-loaded "
+             f"rank), no exchange" if world > 1 else "")
     return {
         "workload": f"{args.batch_trees} independent 2D Euler quadtree Riemann problems, base 2^k, k ~ U{{5..8}}, "
-                    f"+2..4 levels, seeded quadrant states (seed 3), LTS, mixed form",
+                    f"+2..4 levels, seeded quadrant states (seed 3), LTS, mixed form{split}",
+        "scaling": "strong", "trees_rank0": len(mine),
         "value": b_u / (b_ms * 1e-3), "unit": UNIT, "steps": args.steps, "threads": threads,
         "timing": "host wall clock around synchronous dg_step_many calls (each tree synchronises per substep)",
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
-        "speedup": (b_u / b_ms) / (s_u / s_ms) if s_u > 0 else None, "active_cells": cells,
+        "speedup": (b_u / b_ms) / (s_u / s_ms) if s_u > 0 else None, "active_cells": int(cells),
     }
 
 
@@ -495,7 +508,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         s2.close()
 
     if not args.no_batched:
-        result["batched"] = batched_run(args, local_rank, world)
+        result["batched"] = batched_run(args, rank, local_rank, world)
     if not args.no_learned and world == 1:
         result["learned"] = learned_run(args, local_rank)
 

@@ -337,6 +337,8 @@ def step_many(solvers, threads: int = 32, signal: bool = True) -> list:
     Returns the force_break flags; raises DgError with the first failing solver's message."""
     lib = load_library()
     n = len(solvers)
+    if n == 0:
+        return []
     hs = (ctypes.c_void_p * max(n, 1))(*[s._h for s in solvers])
     fb = (ctypes.c_int * max(n, 1))()
     gdt = (ctypes.c_double * max(n, 1))()

@@ -1,6 +1,7 @@
 """Multi-rank bench plumbing on CPU: two `gloo` ranks combine their timed regions the way
-`bench.py --gpus N` does under torchrun (maximum time over ranks, sum of leaf cell-updates), and the
-reference arm lets every rank but rank 0 exit without work."""
+`bench.py --gpus N` does under torchrun (maximum time over ranks, sum of leaf cell-updates), split a
+batch of trees between them without communicating (each computes its own share), and the reference
+arm lets every rank but rank 0 exit without work."""
 import os
 import socket
 import sys
@@ -54,3 +55,39 @@ def test_reference_arm_idles_on_nonzero_ranks(capsys):
 
     bench.bench_reference(A(), rank=1, world=2)
     assert capsys.readouterr().out == ""
+
+
+def _batch_rank(rank: int, world: int, port: int, out) -> None:
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        from dacti_b200 import cases
+        from dacti_b200.batch import my_trees, tree_work
+        batch = cases.riemann_batch(12, seed=3)
+        work = [tree_work(c) for c in batch]
+        mine = my_trees(work, rank, world)
+        got = [None] * world
+        dist.all_gather_object(got, mine)
+        out.put((rank, got, work))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_batch_split_between_two_ranks():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_batch_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=180) for _ in range(2)]
+    for p in procs:
+        p.join(120)
+        assert p.exitcode == 0
+    (_, a, work), (_, b, _) = sorted(res, key=lambda t: t[0])
+    assert a == b                                     # both ranks see the same split
+    assert sorted(a[0] + a[1]) == list(range(12)) and not set(a[0]) & set(a[1])
+    loads = [sum(work[i] for i in part) for part in a]
+    assert abs(loads[0] - loads[1]) <= max(work)
