@@ -26,7 +26,7 @@ from __future__ import annotations
 import base64
 import os
 from dataclasses import dataclass
-from typing import Dict, List, Optional
+from typing import Dict, List
 
 import numpy as np
 
@@ -118,23 +118,25 @@ def hyper_tree(nodes: NodeTable, active_size0: float) -> HyperTree:
     )
 
 
-def _values(a: np.ndarray, typ: str, fmt: str) -> str:
+def _values(a: np.ndarray, typ: str, fmt: str) -> bytes:
     if fmt == "ascii":
         if typ == "Bit" or typ == "Int64":
-            return " ".join(str(int(v)) for v in a)
-        return " ".join(repr(float(v)) for v in a)
+            return " ".join(str(int(v)) for v in a).encode("ascii")
+        return " ".join(repr(float(v)) for v in a).encode("ascii")
     if typ == "Bit":
         raw = np.packbits(a.astype(np.uint8), bitorder="big").tobytes()
     elif typ == "Int64":
         raw = np.ascontiguousarray(a, "<i8").tobytes()
     else:
         raw = np.ascontiguousarray(a, "<f8").tobytes()
-    return base64.b64encode(np.uint64(len(raw)).tobytes() + raw).decode("ascii")
+    return base64.b64encode(np.uint64(len(raw)).tobytes() + raw)
 
 
-def _array(name: str, a: np.ndarray, typ: str, fmt: str, indent: str) -> str:
-    return (f'{indent}<DataArray type="{typ}" Name="{name}" NumberOfTuples="{a.shape[0]}" format="{fmt}">'
-            f"{_values(a, typ, fmt)}</DataArray>\n")
+def _array(f, name: str, a: np.ndarray, typ: str, fmt: str, indent: str) -> None:
+    f.write(f'{indent}<DataArray type="{typ}" Name="{name}" NumberOfTuples="{a.shape[0]}" format="{fmt}">'
+            .encode("ascii"))
+    f.write(_values(a, typ, fmt))
+    f.write(b"</DataArray>\n")
 
 
 def write_htg(path: str, ht: HyperTree, fmt: str = "binary") -> None:
@@ -144,24 +146,24 @@ def write_htg(path: str, ht: HyperTree, fmt: str = "binary") -> None:
     dims = {1: "2 1 1", 2: "2 2 1", 3: "2 2 2"}[ht.dims]
     h = 0.5 * ht.extent
     base = np.array([-h, h])
-    out = ['<?xml version="1.0"?>\n',
-           '<VTKFile type="HyperTreeGrid" version="1.0" byte_order="LittleEndian" header_type="UInt64">\n',
-           f'  <HyperTreeGrid BranchFactor="2" TransposedRootIndexing="0" Dimensions="{dims}">\n',
-           "    <Grid>\n"]
-    for axis in "XYZ":
-        out.append(_array(f"{axis}Coordinates", base, "Float64", fmt, "      "))
-    out += ["    </Grid>\n", "    <Trees>\n",
-            f'      <Tree Index="0" NumberOfLevels="{ht.n_levels}" NumberOfVertices="{ht.n_vertices}">\n',
-            _array("Descriptor", ht.descriptor, "Bit", fmt, "        "),
-            _array("NbVerticesByLevel", ht.vertices_per_level, "Int64", fmt, "        "),
-            _array("Mask", ht.mask, "Bit", fmt, "        "),
-            "        <CellData>\n"]
-    for name, v in ht.cell_data.items():
-        out.append(_array(name, v, "Float64", fmt, "          "))
-    out += ["        </CellData>\n", "      </Tree>\n", "    </Trees>\n", "  </HyperTreeGrid>\n", "</VTKFile>\n"]
     os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
-    with open(path, "w") as f:
-        f.write("".join(out))
+    with open(path, "wb") as f:
+        f.write(('<?xml version="1.0"?>\n'
+                 '<VTKFile type="HyperTreeGrid" version="1.0" byte_order="LittleEndian" header_type="UInt64">\n'
+                 f'  <HyperTreeGrid BranchFactor="2" TransposedRootIndexing="0" Dimensions="{dims}">\n'
+                 "    <Grid>\n").encode("ascii"))
+        for axis in "XYZ":
+            _array(f, f"{axis}Coordinates", base, "Float64", fmt, "      ")
+        f.write(("    </Grid>\n    <Trees>\n"
+                 f'      <Tree Index="0" NumberOfLevels="{ht.n_levels}" NumberOfVertices="{ht.n_vertices}">\n')
+                .encode("ascii"))
+        _array(f, "Descriptor", ht.descriptor, "Bit", fmt, "        ")
+        _array(f, "NbVerticesByLevel", ht.vertices_per_level, "Int64", fmt, "        ")
+        _array(f, "Mask", ht.mask, "Bit", fmt, "        ")
+        f.write(b"        <CellData>\n")
+        for name, v in ht.cell_data.items():
+            _array(f, name, v, "Float64", fmt, "          ")
+        f.write(b"        </CellData>\n      </Tree>\n    </Trees>\n  </HyperTreeGrid>\n</VTKFile>\n")
 
 
 def write_frame(out_dir: str, name: str, frame: int, nodes: NodeTable, active_size0: float,
