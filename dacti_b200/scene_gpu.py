@@ -66,8 +66,9 @@ def _object_row(o) -> list:
     tail = [kind, 1.0 if has_bc else 0.0, 1.0 if inflow_r else 0.0]
     if isinstance(o, PolygonObject):
         v = np.asarray(o.vertices, np.float64)
-        if v.shape[0] > MAX_VERT or v.shape[1] != 2:
-            raise NotImplementedError("polygons with more than 8 vertices need the host builder")
+        if v.shape[0] > MAX_VERT or v.shape[0] < 3 or v.shape[1] != 2:
+            raise NotImplementedError("polygons with fewer than 3 or more than 8 vertices (lines included) need "
+                                      "the host builder")
         verts = np.zeros((MAX_VERT, 2))
         verts[: v.shape[0]] = v
         return [0.0] * 6 + [1.0, 0.0, 2.0] + tail + [float(v.shape[0])] + list(verts.ravel())

@@ -12,7 +12,7 @@ rules and error behaviour, and builds the initial tree with the analytic scene b
   fluid_1/fluid_2 constants;
 - [initial_condition] uniform (reference / fixed) and jump; [boundary_conditions.X|Y|Z] periodic or
   neg/pos of noslip, freeslip, inflow, inflow_r, outflow, zeroGradient (config.cpp:145-190);
-- [[geometry]] built-in 2D shapes ellipse, circle, diamond, quadrilateral and triangle with their
+- [[geometry]] built-in 2D shapes ellipse, circle, diamond, quadrilateral, triangle and line with their
   transform (rotation about z, scaling, translation: x = R S y + t, object_mesh.cpp:92-94) as
   analytic signed distances instead of the sampled line meshes the reference builds;
 - [[refinement_zone]] start, end, max_refinement_level, transform_like (translation and scaling).
@@ -360,7 +360,18 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
             v = np.array([get_entry(g, k, "vec", size=2) for k in keys])
         world = (v * S[None, :]) @ R.T + c[None, :]
         return PolygonObject(world.tolist(), typ, bc), t
-    if shape in ("naca_airfoil", "Joukowski_airfoil", "line"):
+    if shape == "line":
+        # geometry_data.hpp:75-93: a segment of `length` centred on the origin along x, else v1-v2; a
+        # two-vertex polygon here: no cell lies inside it, and every face whose centre-to-centre
+        # segment crosses it takes the object's condition, from both sides (a plate of no thickness)
+        length = get_entry(g, "length", "float", 0.0)
+        if length > 0.0:
+            v = np.array([[-length / 2.0, 0.0], [length / 2.0, 0.0]])
+        else:
+            v = np.array([get_entry(g, "v1", "vec", size=2), get_entry(g, "v2", "vec", size=2)])
+        world = (v * S[None, :]) @ R.T + c[None, :]
+        return PolygonObject(world.tolist(), typ, bc), t
+    if shape in ("naca_airfoil", "Joukowski_airfoil"):
         raise NotImplementedError(f"geometry '{name}': shape '{shape}' is not supported")
     raise ConfigError("Unknown shape type")
 

@@ -321,3 +321,31 @@ def test_solid_cylinder_boundaries():
             n = np.asarray(t.bcs[t.bc[i, f]].normal)
             radial = (t.center[i] - [-0.8, 0.0]) / r[i]
             assert np.allclose(n, radial, atol=1e-12)
+
+
+def test_line_geometry_is_a_plate():
+    """shape = "line" (geometry_data.hpp:75-93): a segment, here 0.8 long and turned by 10 degrees. No
+    cell lies inside it. The faces it cuts carry its free-slip condition from both sides, and the cells
+    there sit at the geometry level."""
+    tc = load_toml_case(_path("plate_line2d"))
+    t = tc.case.tree
+    leaf = (t.flags & F_LEAF) != 0
+    leaf[0] = False
+    act = (t.flags & F_ACTIVE) != 0
+    assert act[leaf].all()
+    al = np.nonzero(leaf & act)[0]
+    obj = t.bc[al] >= 4
+    walls = al[obj.any(axis=1)]
+    assert walls.size > 0
+    assert all(t.bcs[b].type == BcType.FREESLIP for b in np.unique(t.bc[al][obj]))
+    th = math.radians(10.0)
+    x = t.center[walls]
+    along = x[:, 0] * math.cos(th) + x[:, 1] * math.sin(th)
+    across = -x[:, 0] * math.sin(th) + x[:, 1] * math.cos(th)
+    size = 2.0 * 0.5 ** t.level[walls]
+    assert (np.abs(across) < size).all() and (np.abs(along) <= 0.4 + size).all()
+    assert (across > 0).any() and (across < 0).any()
+    assert (t.level[walls] == 6).all()
+    # the device builder keeps to polygons of 3 to 8 vertices; "auto" builds lines on the host
+    auto = load_toml_case(_path("plate_line2d"), builder="auto")
+    assert np.array_equal(auto.case.tree.bc, t.bc) and np.array_equal(auto.case.tree.level, t.level)
