@@ -12,7 +12,8 @@ rules and error behaviour, and builds the initial tree with the analytic scene b
   fluid_1/fluid_2 constants;
 - [initial_condition] uniform (reference / fixed) and jump; [boundary_conditions.X|Y|Z] periodic or
   neg/pos of noslip, freeslip, inflow, inflow_r, outflow, zeroGradient (config.cpp:145-190);
-- [[geometry]] built-in 2D shapes ellipse, circle, diamond, quadrilateral, triangle and line with their
+- [[geometry]] built-in 2D shapes ellipse, circle, diamond, quadrilateral, triangle, line, naca_airfoil
+  and Joukowski_airfoil (the airfoils as densely sampled polygons) with their
   transform (rotation about z, scaling, translation: x = R S y + t, object_mesh.cpp:92-94) as
   analytic signed distances instead of the sampled line meshes the reference builds;
 - [[refinement_zone]] start, end, max_refinement_level, transform_like (translation and scaling).
@@ -320,6 +321,51 @@ class _Transform:
         return (not self.rotation.any()) and bool((self.scaling == 1.0).all()) and not self.translation.any()
 
 
+def _naca4_outline(m: float, p: float, t: float, n: int = 400) -> np.ndarray:
+    """NACA4Airfoil (scene/geometry.hpp:57-100) sampled as a polygon: the parameter x in [-1, 1] runs
+    along the lower surface (x < 0) from the trailing edge to the leading edge and back along the upper
+    one. The chord runs from -0.5 to 0.5, and the closed trailing edge uses the -0.1036 x^4 thickness
+    term. Points are cosine-spaced in |x|, dense at both edges; the shared trailing-edge point appears
+    once."""
+    u = 0.5 * (1.0 - np.cos(np.linspace(0.0, math.pi, n // 2 + 1)))       # 0 .. 1
+
+    def point(x, sgn):
+        yt = 5 * t * (0.2969 * np.sqrt(x) - 0.1260 * x - 0.3516 * x * x + 0.2843 * x ** 3 - 0.1036 * x ** 4)
+        front = x < p
+        with np.errstate(divide="ignore", invalid="ignore"):
+            yc = np.where(front, m * (2 * p * x - x * x) / (p * p), m * (1 - 2 * p + 2 * p * x - x * x) / ((1 - p) ** 2))
+            dy = np.where(front, 2 * m * (p - x) / (p * p), 2 * m * (p - x) / ((1 - p) ** 2))
+        th = np.arctan(dy)
+        return np.stack([x - sgn * yt * np.sin(th) - 0.5, yc + sgn * yt * np.cos(th)], axis=1)
+
+    lower = point(u[::-1], -1.0)[:-1]        # trailing edge .. just before the leading edge
+    upper = point(u, 1.0)[:-1]               # leading edge .. just before the trailing edge
+    return np.concatenate([lower, upper])
+
+
+def _joukowski_outline(m: float, t: float, delta: float, n: int = 400) -> np.ndarray:
+    """JoukowskiAirfoil (scene/geometry.hpp:102-160) sampled as a polygon. The unit circle around
+    zeta0 = (-t/1.299, 2m) is mapped by the Karman-Trefftz transform with exponent 2 - delta/180, then
+    shifted to the mid-chord and scaled to unit chord; theta runs over [0, 2 pi)."""
+    xc, yc = -t / 1.299, 2.0 * m
+    zeta0 = complex(xc, yc)
+    beta = math.asin(yc)
+    a = math.cos(beta) + xc
+    k = 2.0 - delta / 180.0
+
+    def tr(z):
+        return 0.5 * k * a * ((z + a) ** k + (z - a) ** k) / ((z + a) ** k - (z - a) ** k)
+
+    le = tr(np.exp(1j * (beta + math.pi)) + zeta0).real
+    te = tr(np.exp(1j * (-beta)) + zeta0).real
+    chord = te - le
+    theta = np.linspace(0.0, 2.0 * math.pi, n, endpoint=False)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        z = (tr(np.exp(1j * theta) + zeta0) - 0.5 * (le + te)) / chord
+    z = z[np.isfinite(z)]
+    return np.stack([z.real, z.imag], axis=1)
+
+
 def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
     """One [[geometry]] entry: (object, transform) for the supported built-in shapes."""
     name = g.get("name")
@@ -372,7 +418,14 @@ def _geometry(g: dict, D: int, bc: Optional[BoundarySpec]):
         world = (v * S[None, :]) @ R.T + c[None, :]
         return PolygonObject(world.tolist(), typ, bc), t
     if shape in ("naca_airfoil", "Joukowski_airfoil"):
-        raise NotImplementedError(f"geometry '{name}': shape '{shape}' is not supported")
+        # geometry_data.hpp:57-73; sampled densely here, adaptively (then meshed) in the reference
+        camber, thick = get_entry(g, "camber", "float"), get_entry(g, "thickness", "float")
+        if shape == "naca_airfoil":
+            v = _naca4_outline(camber, get_entry(g, "position", "float"), thick)
+        else:
+            v = _joukowski_outline(camber, thick, get_entry(g, "trailing_edge_angle", "float", 0.0))
+        world = (v * S[None, :]) @ R.T + c[None, :]
+        return PolygonObject(world.tolist(), typ, bc), t
     raise ConfigError("Unknown shape type")
 
 

@@ -241,7 +241,7 @@ def test_geometry_support_and_rejections(tmp_path):
         load_toml_case(_write(tmp_path, drop.replace('type = "droplet"', 'type = "solid"')))
     with pytest.raises(NotImplementedError, match="STL"):
         load_toml_case(_write(tmp_path, drop.replace('shape = "ellipse"', 'path = "stl/x.stl"')))
-    with pytest.raises(NotImplementedError, match="naca_airfoil"):
+    with pytest.raises(ConfigError):   # an airfoil needs camber, position and thickness
         load_toml_case(_write(tmp_path, drop.replace('shape = "ellipse"', 'shape = "naca_airfoil"')))
     with pytest.raises(ConfigError, match="Unknown shape type"):
         load_toml_case(_write(tmp_path, drop.replace('shape = "ellipse"', 'shape = "blob"')))
@@ -349,3 +349,28 @@ def test_line_geometry_is_a_plate():
     # the device builder keeps to polygons of 3 to 8 vertices; "auto" builds lines on the host
     auto = load_toml_case(_path("plate_line2d"), builder="auto")
     assert np.array_equal(auto.case.tree.bc, t.bc) and np.array_equal(auto.case.tree.level, t.level)
+
+
+@pytest.mark.parametrize("shape,keys", [("naca_airfoil", 'camber = 0.02\nposition = 0.4\nthickness = 0.12'),
+                                        ("Joukowski_airfoil", 'camber = 0.02\nthickness = 0.12')])
+def test_airfoils_are_solid_polygons(shape, keys, tmp_path):
+    """naca_airfoil and Joukowski_airfoil (scene/geometry.hpp:57-160), unit chord centred on the
+    origin, turned by 10 degrees and made solid: the cells inside are inactive, the cells outside active,
+    and the faces between them carry the wall."""
+    text = open(_path("plate_line2d")).read().replace('shape = "line"\nlength = 0.8', f'shape = "{shape}"\n{keys}')
+    tc = load_toml_case(_write(tmp_path, text))
+    t = tc.case.tree
+    obj = tc.objects[0]
+    leaf = (t.flags & F_LEAF) != 0
+    leaf[0] = False
+    act = (t.flags & F_ACTIVE) != 0
+    sd = obj.signed_distance(t.center)
+    assert (sd[leaf & ~act] < 0).all() and (sd[leaf & act] > 0).all() and (leaf & ~act).any()
+    th = math.radians(10.0)
+    x = t.center[leaf & ~act]
+    along = x[:, 0] * math.cos(th) + x[:, 1] * math.sin(th)
+    across = -x[:, 0] * math.sin(th) + x[:, 1] * math.cos(th)
+    assert (np.abs(along) <= 0.5).all() and (np.abs(across) < 0.09).all()
+    al = np.nonzero(leaf & act)[0]
+    walls = al[(t.bc[al] >= 4).any(axis=1)]
+    assert walls.size > 0 and (t.level[walls] == 6).all()
