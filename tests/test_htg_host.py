@@ -95,7 +95,9 @@ def test_root_leaf_tree():
     assert ht.cell_data["p_0"].tolist() == [0.0] and not ht.mask[0]
 
 
-@pytest.mark.parametrize("name,steps,checks", [("euler2", 6, [2, 6]), ("multi2", 4, [0, 4]), ("euler3", 2, [2])])
+@pytest.mark.parametrize("name,steps,checks", [("euler2", 6, [2, 6]), ("multi2", 4, [0, 4]), ("euler3", 2, [2]),
+                                               ("ns2_walls", 10, [10]), ("euler2_open_a", 10, [10]),
+                                               ("euler2_periodic", 6, [6]), ("multi3", 2, [2]), ("ns3", 4, [4])])
 def test_reference_node_tables(name, steps, checks, tmp_path):
     """Node tables that DACTI's integrator dumps after steps (regrid, garbage slots) give the same hyper
     tree through both walks, its unmasked leaves are exactly the snapshot's active cells, and the file
