@@ -5,7 +5,10 @@ Workload: the five-equation model (multi<3>) on an 8 x 4 x 4 mm box, 64 x 32 x 3
 4 refinement levels, local time stepping on, Mach 1.5 shock into air hitting a water drop of radius
 0.5 mm (synthetic initial condition). A step is one global step of the LTS scheme
 (Integrator::integrate), i.e. every ACTI level substep it contains; leaf cell-updates are the
-cluster sizes of the executed substeps. The plain FP64 form runs here.
+cluster sizes of the executed substeps. `value` is the plain FP64 form (the reference's arithmetic);
+the mixed form (FP32 reconstruction and flux, FP64 update and EOS recovery) is reported beside it as
+`chosen_over_plain`, with its error against the FP64 form per conserved component and the number of
+cells whose refinement differs.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
 
@@ -53,7 +56,8 @@ def parse_args():
     ap.add_argument("--batch-trees", type=int, default=256, help="trees of the batched 2D Riemann workload")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
-    ap.add_argument("--forms", default="fp64,mixed", help="numerical forms to time (the last one is `value`)")
+    ap.add_argument("--forms", default="fp64,mixed",
+                    help="numerical forms to time; `value` is fp64 when it is among them, else the first one")
     ap.add_argument("--profile-substep", type=int, default=-1,
                     help="bracket only this substep of the first timed step of the last form with "
                          "cudaProfilerStart/Stop (for ncu --profile-from-start off); -2 brackets the whole timed "
@@ -66,7 +70,7 @@ def workload_config(args) -> dict:
     nb = 1 << args.base_level
     return {
         "workload": f"shock_drop_3d multi<3> {nb}x{nb // 2}x{nb // 2} base +{args.levels} levels, LTS, max_cfl 0.25, "
-                    f"Mach 1.5 shock on a 0.5 mm water drop; value is the last form in --forms",
+                    f"Mach 1.5 shock on a 0.5 mm water drop, plain FP64 form",
         "model": "multi<3> (five-equation, stiffened gas)",
         "base_grid": [nb, nb // 2, nb // 2],
         "levels": args.levels,
@@ -152,6 +156,18 @@ def run_reference_samples(case_path: str, samples: int, substeps: int, threads: 
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
+REF_CHUNK_SUBSTEPS = 40
+
+
+def run_reference_chunks(case_path: str, chunk: int, threads: int) -> dict:
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    r = subprocess.run([REF_RUNNER, case_path, os.path.join(tempfile.gettempdir(), "dg_ref"), "0",
+                        "--chunk-substeps", str(chunk)], capture_output=True, text=True, env=env)
+    if r.returncode != 0:
+        raise RuntimeError(f"reference runner failed: {r.stderr[-2000:]}")
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
 def host_threads() -> int:
     try:
         return len(os.sched_getaffinity(0))
@@ -172,28 +188,35 @@ def cpu_model() -> str:
 
 # ------------------------------------------------------------------------------------------------
 def bench_reference(args, rank: int, world: int) -> None:
+    """The reference's own CPU solver (oracle/_ref/dacti_ref_runner_fast, built from the reference
+    sources) on all host threads, over one complete global LTS step of the workload: the step's
+    substeps are timed in consecutive chunks; the first `warmup` chunks are warm-up and every later
+    chunk is timed (at least `steps` of them), so the timed region covers the rest of the step with its
+    real mix of fine and coarse ACTI levels."""
     if rank != 0:
         return
     from dacti_b200.casefile import write_case
     case = make_case(args)
     threads = host_threads()
-    sub = 60
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "case.bin")
         write_case(case, path)
-        res = run_reference_samples(path, args.warmup + args.steps, sub, threads)
-    timed = res["samples"][args.warmup:]
-    upd = sum(s["updates"] for s in timed)
-    sec = sum(s["seconds"] for s in timed)
+        res = run_reference_chunks(path, REF_CHUNK_SUBSTEPS, threads)
+    chunks = res["chunks"]
+    timed = chunks[min(args.warmup, max(len(chunks) - 1, 0)):]
+    upd = sum(c["updates"] for c in timed)
+    sec = sum(c["seconds"] for c in timed)
     value = upd / sec if sec > 0 else 0.0
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sec / max(len(timed), 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload_config(args),
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "reference",
-                         "sample": f"{len(timed)} samples of {sub} LTS substeps each of the first global step, "
-                                   f"reference Integrator (oracle/_ref/dacti_ref_runner_fast, -O3 -fopenmp) on "
-                                   f"{threads} threads of {cpu_model()}"},
+                         "sample": f"the first global step, {res['substeps']} LTS substeps in {len(chunks)} chunks of "
+                                   f"{REF_CHUNK_SUBSTEPS}; the first {len(chunks) - len(timed)} chunks warm-up, the other "
+                                   f"{len(timed)} timed ({upd:.0f} updates, {sec:.1f} s); reference Integrator "
+                                   f"(oracle/_ref/dacti_ref_runner_fast, -O3 -fopenmp) on {threads} threads of "
+                                   f"{cpu_model()}; ms_per_step is per chunk"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -395,6 +418,24 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     }
 
 
+def form_accuracy(snap, ref, case, level: int) -> dict:
+    """Error of one form's solution against the FP64 form's after the same steps: mixture-density and
+    per-component relative L1 on the uniform grid of `level` (conservative projection), and the cells
+    whose refinement differs (present in one solution only)."""
+    from dacti_b200.accuracy import density_rel_l1, project_uniform
+    from dacti_b200.parity import compare
+    prm = case.params
+    a = project_uniform(snap, prm.side_length, prm.active_size, level)
+    b = project_uniform(ref, prm.side_length, prm.active_size, level)
+    comp = np.abs(a - b).sum(axis=0) / np.maximum(np.abs(b).sum(axis=0), 1e-300)
+    err = density_rel_l1(snap, ref, prm.side_length, prm.active_size, level, int(case.shape.model))
+    rep = compare(ref, snap, prm.side_length)
+    return {"density_rel_l1_vs_plain_fp64": err, "bound": 1e-4, "ok": bool(err <= 1e-4),
+            "component_rel_l1": [float(x) for x in comp], "cells_only_in_plain": rep.only_ref,
+            "cells_only_in_form": rep.only_gpu, "acti_level_mismatch": rep.acti_mismatch,
+            "grid": f"uniform base level {level}"}
+
+
 def reduce_ranks(ms: float, updates: float, world: int):
     """Max of the timed region and sum of the cell updates over all ranks."""
     import torch
@@ -410,7 +451,6 @@ def reduce_ranks(ms: float, updates: float, world: int):
 
 def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     import torch
-    from dacti_b200.accuracy import density_rel_l1
     from dacti_b200.casefile import write_case
     from dacti_b200.solver import Solver
 
@@ -420,18 +460,15 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     D = case.shape.dims
 
     forms = args.forms.split(",")
+    primary = "fp64" if "fp64" in forms else forms[0]
     runs = {}
     for k, f in enumerate(forms):
         runs[f] = timed_run(case, f, args, stream, local_rank, world,
                             profile=args.profile_substep if k == len(forms) - 1 else -1)
-    chosen = runs[forms[-1]]
-    plain = runs.get("fp64", chosen)
-    err = density_rel_l1(chosen["snap"], plain["snap"], case.params.side_length, case.params.active_size,
-                         args.base_level, int(case.shape.model))
+    plain = runs[primary]
 
-    ms_max, total_updates = reduce_ranks(chosen["ms"], chosen["updates"], world)
+    ms_max, total_updates = reduce_ranks(plain["ms"], plain["updates"], world)
     value = total_updates / (ms_max * 1e-3)
-    p_ms, p_upd = reduce_ranks(plain["ms"], plain["updates"], world)
 
     # Roofline of the cell-update kernel (k_gather_update: face-flux gather fused with the conservative
     # update, EOS recovery and floors): algorithmic bytes per leaf cell-update (16 E + 8 D + 12: U read
@@ -439,7 +476,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     # CUDA-event time on the solver's stream. `traffic` is the DRAM bytes per launch from the committed
     # ncu summary of the same kernel, scaled to this run's cells per launch.
     peak, peak_kind = measured_peak()
-    kms, kl, kc = chosen["kms"], chosen["kl"], chosen["kc"]
+    kms, kl, kc = plain["kms"], plain["kl"], plain["kc"]
     dom = max(kms, key=lambda k: kms[k])
     b_per = BYTES_PER_UPDATE[D]
     upd_ms = kms["update"]
@@ -450,9 +487,9 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     if os.path.exists(tpath):
         with open(tpath) as f:
             for line in f:
-                if line.startswith("traffic_dram_bytes_per_cell"):
+                if line.startswith("fp64_dram_bytes_per_cell"):
                     traffic = float(line.split("=")[1]) * (kc["update"] / launches)
-    step_achieved = b_per * chosen["updates"] / (chosen["ms"] * 1e-3) / 1e9
+    step_achieved = b_per * plain["updates"] / (plain["ms"] * 1e-3) / 1e9
     roofline = {
         "bound": "hbm", "kernel": "k_gather_update (face-flux gather + cell update)", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
@@ -465,15 +502,25 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     result = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64 update / f32 flux", "data": "synthetic", "config": workload_config(args),
-        "form": "mixed: FP32 reconstruction + HLLC flux, FP64 update, totals and EOS recovery",
-        "gpu_launches": chosen["launches"], "roofline": roofline, "clocks": chosen["clocks"],
-        "cells": chosen["snap"].n, "substeps_timed": chosen["substeps"],
-        "plain_fp64": {"value": p_upd / (p_ms * 1e-3), "ms_per_step": p_ms / args.steps,
-                       "gpu_launches": plain["launches"], "cells": plain["snap"].n},
-        "accuracy": {"density_rel_l1_vs_plain_fp64": err, "bound": 1e-4, "ok": bool(err <= 1e-4),
-                     "grid": f"uniform base level {args.base_level}, after {args.warmup + args.steps + 1} global steps"},
+        "vs_baseline": None, "dtype": "f64" if primary == "fp64" else "f64 update / f32 flux", "data": "synthetic",
+        "config": workload_config(args),
+        "form": "plain: FP64 throughout, the reference's arithmetic" if primary == "fp64" else primary,
+        "gpu_launches": plain["launches"], "roofline": roofline, "clocks": plain["clocks"],
+        "cells": plain["snap"].n, "substeps_timed": plain["substeps"],
     }
+    for f in forms:
+        if f == primary:
+            continue
+        other = runs[f]
+        o_ms, o_upd = reduce_ranks(other["ms"], other["updates"], world)
+        acc = form_accuracy(other["snap"], plain["snap"], case, args.base_level)
+        acc["horizon"] = f"after {args.warmup + args.steps + 1} global steps from the initial state"
+        result["chosen_over_plain"] = {
+            "form": "mixed: FP32 reconstruction + HLLC flux, FP64 update, totals and EOS recovery" if f == "mixed" else f,
+            "value": o_upd / (o_ms * 1e-3), "ms_per_step": o_ms / args.steps, "gpu_launches": other["launches"],
+            "ratio_to_plain": (o_upd / o_ms) / (total_updates / ms_max), "clocks": other["clocks"],
+            "accuracy": acc,
+        }
 
     # end to end through the public API: host tree -> device, K steps with the per-step scalars read
     # back, then every active cell read back to the host
@@ -482,7 +529,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         t0 = time.perf_counter()
         s2 = Solver(case, device=local_rank)
         s2.set_stream(stream.cuda_stream)
-        s2.set_form("mixed")
+        s2.set_form(primary)
         e_upd0 = s2.stats().cell_updates
         torch.cuda.synchronize()
         t1 = time.perf_counter()

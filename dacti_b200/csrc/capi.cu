@@ -43,6 +43,15 @@ int dg_create(const dg_case *c, dg_solver **out) {
 			case DG_MULTI: impl = dg::make_solver_multi(*c); break;
 			default: throw dg::dg_error(DG_ERR_ARG, "unknown model id");
 		}
+		// the allocation-free read-back's scratch and gather kernel are placed on the device now, so
+		// that dg_read_cells_noalloc never allocates, not even on its first call
+		try {
+			dg::noalloc_prepare(g_device);
+			impl->prepare_noalloc();
+		} catch (...) {
+			delete impl;
+			throw;
+		}
 		*out = new dg_solver{impl, g_device};
 	});
 }

@@ -3,6 +3,10 @@
 
 #include "solver.cuh"
 
+namespace dg {
+void noalloc_prepare(int device);  // noalloc.cu
+}
+
 struct dg_solver {
 	dg::SolverBase *impl;
 	int device;

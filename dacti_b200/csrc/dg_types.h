@@ -21,7 +21,9 @@ enum : uint32_t {
 	F_SHOULD_SPLIT = 1u << 5,
 	F_IS_BOUNDARY  = 1u << 6,
 	F_HOLD         = 1u << 7,  // held by the regrid forecaster: never coarsened
+	F_RECV         = 1u << 8,  // the received-flux accumulator may be non-zero (set by the receive stage)
 };
+constexpr uint32_t F_PUBLIC = 0x7fu;  // the flag bits of include/dacti_gpu.h
 
 // Refinement op codes written by the estimation kernel.
 enum : uint8_t {
@@ -72,6 +74,7 @@ struct Consts {
 	int a0[MAX_TREE][3], na[MAX_TREE][3];
 	int signal;  // `signal` argument of integrate (hold-droplet-still switch)
 	int coarsen; // 0 on global steps where a forecast-driven regrid skips coarsening
+	int visc;    // viscous or heat terms present: gradients and their time slopes are stored
 };
 
 // Boundary table (one Boundary<M> value per entry).
@@ -106,8 +109,8 @@ struct Pool {
 	double *avga;     // non-leaf nodes: memo of the mean smoothed volume fraction of the subtree
 	int32_t *csta;    // epoch at which `avga` was computed
 	double *k;        // [P][cap]
-	double *tslope;   // [G][cap]
-	double *grad;     // [D][G][cap]
+	double *tslope;   // [G][cap], only with viscous or heat terms (Consts::visc)
+	double *grad;     // [D][G][cap], only with viscous or heat terms
 	double *flux;     // [F][cap]
 	double *err, *maxdt, *cfl;
 	int32_t *stamp;   // per-node dedup stamp for list building
@@ -115,8 +118,9 @@ struct Pool {
 	uint8_t *op;      // refinement op code
 	double *tmp, *tmp2;  // per-node scratch scalars (Jacobi smoothing sweeps, alternately)
 	// Per-substep scratch outside the permuted fields:
-	double *ff;       // [cap][2D][F] flux of each face a cell owns, written in the running substep
-	int32_t *plan;    // [cap][2D] source of each face's flux for the running cluster's cells
+	double *ff;       // [slot][2D][F] flux of each owned face next to a receiver (by the owner's list position)
+	double *du;       // [slot][F] face-flux sum of each running-cluster cell (by list position)
+	int32_t *pos;     // [cap] list position of each running-cluster cell, written by the face-sum stage
 	double *nbv;      // [slot][2D][NW] neighbour values of the running list's cells (p, t, centre distance)
 	int32_t *nbi;     // [slot][2D] neighbour level, leaf flag, presence and ACTI level
 };
@@ -132,9 +136,6 @@ struct Counters {
 	int n_new;        // new cluster members (children + coarsened parents)
 	int n_upd;        // neighbour-update list
 	int n_tmp;        // rebuilt cluster list
-	int n_task;       // owned interior faces of the running substep
-	int n_btask;      // owned boundary faces of the running substep
-	int n_wtask;      // faces of running-cluster cells with finer owners behind a non-leaf neighbour
 	uint32_t status;
 	unsigned long long n_split_total, n_unsplit_total;
 	double dmax;      // reduction result
@@ -150,9 +151,6 @@ struct Lists {
 	int32_t *unsplit;  // parents to coarsen
 	int32_t *fresh;    // new children and coarsened parents
 	int32_t *upd;      // neighbour-update list
-	int32_t *task;     // owned interior faces (cell * 2D + face) of the running substep
-	int32_t *btask;    // owned boundary faces
-	int32_t *wtask;    // faces whose flux sum walks finer owners
 };
 
 }  // namespace dg

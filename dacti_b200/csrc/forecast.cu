@@ -223,9 +223,7 @@ extern "C" {
 
 const char *dg_mlp_last_error(void) { return g_mlp_error.c_str(); }
 
-int dg_mlp_create(int n_in, unsigned long long seed, dg_mlp **out) {
-	if (!out || n_in < 1 || n_in > MAX_IN) return fail(DG_ERR_ARG, "dg_mlp_create: n_in must be in [1, 32]");
-	dg_mlp *h = new dg_mlp();
+static int mlp_create_steps(dg_mlp *h, int n_in, unsigned long long seed) {
 	h->L = Layout(n_in);
 	const long long n = h->L.n;
 	MLP_CUDA(cudaGetDevice(&h->device));
@@ -247,8 +245,23 @@ int dg_mlp_create(int n_in, unsigned long long seed, dg_mlp **out) {
 	fill(h->L.w1, (long long) H * n_in, std::sqrt(6.0 / n_in));
 	fill(h->L.w2, (long long) H * H, std::sqrt(6.0 / H));
 	fill(h->L.w3, H, std::sqrt(6.0 / (H + 1)));
-	*out = h;
 	return dg_mlp_set_params(h, w.data());
+}
+
+int dg_mlp_create(int n_in, unsigned long long seed, dg_mlp **out) {
+	if (!out || n_in < 1 || n_in > MAX_IN) return fail(DG_ERR_ARG, "dg_mlp_create: n_in must be in [1, 32]");
+	*out = nullptr;
+	dg_mlp *h = new dg_mlp();
+	const int rc = mlp_create_steps(h, n_in, seed);
+	if (rc != DG_OK) {
+		// release whatever the failed step left allocated; the error text of the failure is kept
+		const std::string msg = g_mlp_error;
+		dg_mlp_destroy(h);
+		g_mlp_error = msg;
+		return rc;
+	}
+	*out = h;
+	return DG_OK;
 }
 
 int dg_mlp_param_count(dg_mlp *h, long long *n) {

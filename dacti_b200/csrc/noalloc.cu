@@ -8,16 +8,19 @@
 // memory it touches besides the solver's own state.
 //
 // Limits and sharing:
-// - the scratch holds kScratchBytes (64 MiB): at most about 380 thousand cells of multi<3> and about
-//   560 thousand cells of euler<2>; larger read-backs are rejected with DG_ERR_CAPACITY and a message
-//   that states the sizes;
+// - the scratch holds kScratchBytes (64 MiB), i.e. 64 MiB / (8 (D + 2E + P + 5)) cells: about 289
+//   thousand cells of multi<3> (232 bytes each) and about 559 thousand cells of euler<2> (120 bytes);
+//   larger read-backs are rejected with DG_ERR_CAPACITY and a message that states the sizes;
 // - the array belongs to the library's module and stays resident on every GPU that loads it until
-//   the process exits;
+//   the process exits. Under CUDA's lazy module loading the module, and with it the array, is only
+//   placed on a device when something first touches it, which would be an allocation; dg_create
+//   therefore resolves the array's address (and loads the gather kernel) on the solver's device
+//   while it builds the solver, so the array is committed before the first read-back;
 // - all calls share it and it keeps the last call's contents: every record is rewritten by each
 //   call, so nothing needs clearing, but two calls whose work overlaps on the GPU (different
 //   solvers on different streams) race on it and must be serialised by the caller;
-// - the first call on a device looks up the array's device address (cudaGetSymbolAddress) with that
-//   device current; make that first call before capturing any stream.
+// - the array's device address is looked up (cudaGetSymbolAddress) once per device with that device
+//   current, by dg_create; no read-back has to come first, and none touches the lookup again.
 #include "capi_internal.h"
 
 #include <mutex>
@@ -49,6 +52,11 @@ void *scratch_address(int device) {
 }
 
 }  // namespace
+
+namespace dg {
+// Called by dg_create with the solver's device current: commits the scratch array on that device.
+void noalloc_prepare(int device) { (void) scratch_address(device); }
+}  // namespace dg
 
 extern "C" int dg_read_cells_noalloc(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out) {
 	if (!s || !levels || !data) return DG_ERR_ARG;

@@ -50,6 +50,7 @@ public:
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
 	virtual void set_profiling(bool on) = 0;
 	virtual void set_form(int form) = 0;
+	virtual void prepare_noalloc() = 0;  // loads the read-back gather kernel on the current device
 	std::string last_error;
 };
 
@@ -72,15 +73,16 @@ class Solver : public SolverBase {
 	Counters *d_cnt_ = nullptr;
 	Counters *h_cnt_ = nullptr;  // pinned
 	void *pool_mem_  = nullptr;
-	void *shadow_mem_ = nullptr;  // second pool for permutations (re-sort), allocated on first use
-	Pool S_{};
+	void *spare_mem_  = nullptr;  // one field's worth of slots: target of the re-sort and gc permutations
+	size_t spare_bytes_ = 0;
 	void *sort_mem_  = nullptr;   // keys/values/temp storage of the re-sort
 	size_t sort_bytes_ = 0;
 	bool resort_     = true;
 	void *list_mem_  = nullptr;
 	void *bc_mem_    = nullptr;
-	double *ff_mem_    = nullptr;  // face fluxes (Pool::ff)
-	int32_t *plan_mem_ = nullptr;  // face-flux sources (Pool::plan)
+	double *ff_mem_    = nullptr;  // face fluxes next to receivers (Pool::ff)
+	double *du_mem_    = nullptr;  // face-flux sums of the running cluster (Pool::du)
+	int32_t *pos_mem_  = nullptr;  // list positions of the running cluster's cells (Pool::pos)
 	double *nbv_mem_   = nullptr;  // neighbour values (Pool::nbv)
 	int32_t *nbi_mem_  = nullptr;  // neighbour facts (Pool::nbi)
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
@@ -182,14 +184,15 @@ public:
 	~Solver() override {
 		cudaStreamSynchronize(st_);
 		cudaFree(pool_mem_);
-		cudaFree(shadow_mem_);
+		cudaFree(spare_mem_);
 		cudaFree(sort_mem_);
 		cudaFree(list_mem_);
 		cudaFree(bc_mem_);
 		cudaFree(ff_mem_);
-		cudaFree(plan_mem_);
+		cudaFree(du_mem_);
 		cudaFree(nbv_mem_);
 		cudaFree(nbi_mem_);
+		cudaFree(pos_mem_);
 		cudaFree(d_cnt_);
 		cudaFreeHost(h_cnt_);
 		cudaFree(d_leaves_);
@@ -245,6 +248,7 @@ public:
 		if constexpr (M::MULTI) visc_ = m.mu1 != 0.0 || m.mu2 != 0.0 || m.lambda1 != 0.0 || m.lambda2 != 0.0;
 		else visc_ = M::VISC;
 		sigma_ = m.sigma != 0.0;
+		C_.visc = visc_ ? 1 : 0;
 		if (c.n_zones > MAX_ZONES) throw dg_error(DG_ERR_ARG, "too many refinement zones");
 		C_.n_zones = c.n_zones;
 		C_.coarsen = 1;
@@ -317,7 +321,8 @@ public:
 		    {(void **) &P.center, 8, D}, {(void **) &P.t, 8, 1}, {(void **) &P.u, 8, E},
 		    {(void **) &P.p, 8, E}, {(void **) &P.rec, 8 * Rec<M>::W, 1}, {(void **) &P.avg, 8 * Avg<M>::W, 1},
 		    {(void **) &P.mod, 4, 1}, {(void **) &P.cst, 4, 1}, {(void **) &P.avga, 8, 1}, {(void **) &P.csta, 4, 1},
-		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, M::G}, {(void **) &P.grad, 8, D * M::G},
+		    {(void **) &P.k, 8, M::P}, {(void **) &P.tslope, 8, visc_ ? M::G : -1},
+		    {(void **) &P.grad, 8, visc_ ? D * M::G : -1},
 		    {(void **) &P.flux, 8, M::F}, {(void **) &P.err, 8, 1}, {(void **) &P.maxdt, 8, 1},
 		    {(void **) &P.cfl, 8, 1}, {(void **) &P.stamp, 4, 1}, {(void **) &P.fmask, 4, 1}, {(void **) &P.op, 1, 1},
 		    {(void **) &P.tmp, 8, 1}, {(void **) &P.tmp2, 8, 1},
@@ -326,25 +331,35 @@ public:
 
 	static size_t align_up(size_t x) { return (x + 255) & ~size_t(255); }
 
-	size_t pool_bytes(int cap) {
-		Pool tmp{};
-		size_t total = 0;
-		for (auto &f: fields(tmp)) total += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
-		return total;
+	// The spare buffer holds the largest field of the pool (the reconstruction records, in practice).
+	void ensure_spare() {
+		size_t need = 0;
+		for (auto &f: fields(P_)) need = std::max(need, field_bytes(f, P_.cap));
+		if (spare_mem_ && spare_bytes_ >= need) return;
+		cudaFree(spare_mem_);
+		spare_mem_ = nullptr;
+		DG_CUDA(cudaMalloc(&spare_mem_, need));
+		spare_bytes_ = need;
+	}
+
+	// Bytes of one field: comps < 0 marks a field this case does not store (no storage, null pointer);
+	// a model without components of a field (comps 0) still gets one.
+	static size_t field_bytes(const Field &f, int cap) {
+		return f.comps < 0 ? 0 : align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
 	}
 
 	void *carve_pool(Pool &P, int cap) {
 		P.cap        = cap;
 		auto fs      = fields(P);
 		size_t total = 0;
-		for (auto &f: fs) total += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
+		for (auto &f: fs) total += field_bytes(f, cap);
 		void *mem = nullptr;
 		DG_CUDA(cudaMalloc(&mem, total));
 		DG_CUDA(cudaMemsetAsync(mem, 0, total, st_));
 		char *b = (char *) mem;
 		for (auto &f: fs) {
-			*f.ptr = b;
-			b += align_up(f.elem * (size_t) cap * (f.comps > 0 ? f.comps : 1));
+			*f.ptr = f.comps < 0 ? nullptr : b;
+			b += field_bytes(f, cap);
 		}
 		return mem;
 	}
@@ -354,33 +369,49 @@ public:
 		alloc_derived(cap);
 	}
 
-	// Per-substep scratch sized with the pool: face fluxes and face-flux sources.
+	// Per-substep scratch. By pool slot: pos (a running-cluster cell's list position). By list position,
+	// sized to the largest list a substep has run so far (grown by a quarter when a larger one comes):
+	// receiver face fluxes, face-flux sums, neighbour values and facts.
 	void alloc_derived(int cap) {
+		cudaFree(pos_mem_);
+		pos_mem_ = nullptr;
+		DG_CUDA(cudaMalloc(&pos_mem_, sizeof(int32_t) * (size_t) cap));
+		attach_derived();
+	}
+
+	long long scratch_cap_ = 0;
+	void ensure_scratch(long long n) {
+		if (n <= scratch_cap_) return;
+		const long long want = std::max(std::max(n, scratch_cap_ + scratch_cap_ / 4), 1024LL);
 		cudaFree(ff_mem_);
-		cudaFree(plan_mem_);
+		cudaFree(du_mem_);
 		cudaFree(nbv_mem_);
 		cudaFree(nbi_mem_);
-		ff_mem_   = nullptr;
-		plan_mem_ = nullptr;
-		nbv_mem_  = nullptr;
-		nbi_mem_  = nullptr;
-		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) cap));
-		DG_CUDA(cudaMalloc(&plan_mem_, sizeof(int32_t) * NF * (size_t) cap));
-		DG_CUDA(cudaMalloc(&nbv_mem_, sizeof(double) * Nbv<M>::W * NF * (size_t) cap));
-		DG_CUDA(cudaMalloc(&nbi_mem_, sizeof(int32_t) * NF * (size_t) cap));
+		ff_mem_      = nullptr;
+		du_mem_      = nullptr;
+		nbv_mem_     = nullptr;
+		nbi_mem_     = nullptr;
+		scratch_cap_ = 0;
+		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) want));
+		DG_CUDA(cudaMalloc(&du_mem_, sizeof(double) * M::F * (size_t) want));
+		DG_CUDA(cudaMalloc(&nbv_mem_, sizeof(double) * Nbv<M>::W * NF * (size_t) want));
+		DG_CUDA(cudaMalloc(&nbi_mem_, sizeof(int32_t) * NF * (size_t) want));
+		scratch_cap_ = want;
 		attach_derived();
 	}
 
 	void attach_derived() {
 		P_.ff   = ff_mem_;
-		P_.plan = plan_mem_;
+		P_.du   = du_mem_;
 		P_.nbv  = nbv_mem_;
 		P_.nbi  = nbi_mem_;
+		P_.pos  = pos_mem_;
 	}
 
 	void grow_pool(int new_cap) {
-		cudaFree(shadow_mem_);
-		shadow_mem_ = nullptr;
+		cudaFree(spare_mem_);
+		spare_mem_   = nullptr;
+		spare_bytes_ = 0;
 		Pool NP{};
 		void *mem = carve_pool(NP, new_cap);
 		auto fo = fields(P_), fn = fields(NP);
@@ -418,8 +449,7 @@ public:
 	void alloc_lists(int cap) {
 		const int nlists = 2 * MAX_ACTI + 6;
 		size_t one       = align_up(sizeof(int32_t) * (size_t) cap);
-		size_t faces     = align_up(sizeof(int32_t) * (size_t) cap * NF);
-		DG_CUDA(cudaMalloc(&list_mem_, one * nlists + 3 * faces));
+		DG_CUDA(cudaMalloc(&list_mem_, one * nlists));
 		char *b = (char *) list_mem_;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			Ls_.clu[l] = (int32_t *) b;
@@ -438,12 +468,6 @@ public:
 		Ls_.fresh   = (int32_t *) b;
 		b += one;
 		Ls_.upd     = (int32_t *) b;
-		b += one;
-		Ls_.task    = (int32_t *) b;
-		b += faces;
-		Ls_.btask   = (int32_t *) b;
-		b += faces;
-		Ls_.wtask   = (int32_t *) b;
 		list_cap_   = cap;
 	}
 
@@ -519,7 +543,9 @@ public:
 		k_nbr_init<M><<<g, BLOCK, 0, st_>>>(P_, C_, d_leaves_, n);
 		// every memo starts stale: mod = 1 > cst = 0
 		k_fill_i32<<<grid_for(P_.cap), BLOCK, 0, st_>>>(P_.mod, 1, P_.cap);
-		launch_slope(d_leaves_, n);
+		// neighbour values and slopes of every leaf, in pieces of the scratch's size
+		ensure_scratch(std::max(n / 2, 1));
+		for (int off = 0; off < n; off += (int) scratch_cap_) launch_slope(d_leaves_ + off, std::min<int>(n - off, (int) scratch_cap_));
 		if constexpr (M::MULTI) multiphase_aux(d_leaves_, n, -1, 0);
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
@@ -570,23 +596,16 @@ private:
 		}
 	}
 
-	void launch_flux_faces(int grid, double dtL) {
+	// Face-flux sums of the running cluster into du, receivers of slower clusters into Ls_.recv.
+	void launch_face_sum(const int32_t *list, int n, int L, double dtL, int stamp) {
+		constexpr int G = NF <= 4 ? 4 : 8;
+		const int g = grid_for((long long) n * G);
 		if (mixed_) {
-			if (visc_) k_flux_faces<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
-			else k_flux_faces<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
+			if (visc_) k_face_sum<M, true, float><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			else k_face_sum<M, false, float><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
 		} else {
-			if (visc_) k_flux_faces<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
-			else k_flux_faces<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, Ls_.task, &d_cnt_->n_task, dtL);
-		}
-	}
-
-	void launch_flux_bfaces(int grid, double dtL) {
-		if (mixed_) {
-			if (visc_) k_flux_bfaces<M, true, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
-			else k_flux_bfaces<M, false, float><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
-		} else {
-			if (visc_) k_flux_bfaces<M, true, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
-			else k_flux_bfaces<M, false, double><<<grid, BLOCK, 0, st_>>>(P_, C_, B_, Ls_.btask, &d_cnt_->n_btask, dtL);
+			if (visc_) k_face_sum<M, true, double><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			else k_face_sum<M, false, double><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
 		}
 	}
 
@@ -615,11 +634,12 @@ private:
 	void substep(int L) {
 		const int n      = h_cnt_->clu[L];
 		const double dtL = global_dt_ / (double) (1 << L);
+		ensure_scratch(n);
 		// A split takes 2^D new slots. When the pool cannot take a split of every cluster cell, the
 		// split requests are read back after the indicator and the pool grown to fit them.
 		const bool tight = (long long) h_cnt_->top + (long long) NC * n + 16 > P_.cap;
 		const int stamp_recv = ++stamp_;
-		// n_recv .. n_btask and status
+		// n_recv .. status
 		DG_CUDA(cudaMemsetAsync(&d_cnt_->n_recv, 0, (char *) (&d_cnt_->status + 1) - (char *) &d_cnt_->n_recv, st_));
 		const int g        = grid_for(n);
 		int32_t *list      = Ls_.clu[L];
@@ -627,29 +647,15 @@ private:
 
 		constexpr int LPC = NF <= 4 ? 4 : 8;  // receive lanes per cell
 		int e_upd = 0;                       // epoch of this substep's cell update
-		run_k(DG_K_FLUX, n, [&] {
-			k_flux_tasks<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, list, n, L, stamp_recv, Ls_.task, Ls_.btask,
-			                                                                  Ls_.wtask, Ls_.recv, d_cnt_);
-		});
-		run_k(DG_K_FLUX, 0, [&] { launch_flux_faces(grid_for((long long) n * NF / 2 + 1), dtL); });
-		run_k(DG_K_FLUX, 0, [&] { launch_flux_bfaces(grid_for(n / 4 + 1), dtL); });
-		run_k(DG_K_FLUX, 0, [&] {
-			if (mixed_) k_flux_walk<M, float><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_);
-			else k_flux_walk<M, double><<<grid_for(n / 8 + 1), BLOCK, 0, st_>>>(P_, Ls_.wtask, &d_cnt_->n_wtask, L, d_cnt_);
-		});
+		run_k(DG_K_FLUX, n, [&] { launch_face_sum(list, n, L, dtL, stamp_recv); });
 		run_k(DG_K_RECV, 0, [&] {
 			if (mixed_) k_flux_receive<M, float><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 			else k_flux_receive<M, double><<<grid_for((long long) n * LPC), BLOCK, 0, st_>>>(P_, Ls_.recv, &d_cnt_->n_recv, L, d_cnt_);
 		});
 		run_k(DG_K_UPDATE, n, [&] {
 			e_upd = ++epoch_;
-			if (mixed_) {
-				if (visc_) k_gather_update<M, true, float><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
-				else k_gather_update<M, false, float><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
-			} else {
-				if (visc_) k_gather_update<M, true, double><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
-				else k_gather_update<M, false, double><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
-			}
+			if (visc_) k_update<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
+			else k_update<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, dtL, e_upd, d_cnt_);
 		});
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) multiphase_aux(list, n, L, e_upd);
@@ -765,7 +771,7 @@ public:
 		const int top = h_cnt_->top;
 		const int n   = top - 1;
 		if (n <= 0) return;
-		if (!shadow_mem_) shadow_mem_ = carve_pool(S_, P_.cap);
+		ensure_spare();
 		size_t temp = 0;
 		DG_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, temp, (uint64_t *) nullptr, (uint64_t *) nullptr,
 		                                        (int32_t *) nullptr, (int32_t *) nullptr, n, 0, 64, st_));
@@ -792,27 +798,29 @@ public:
 		run_k(DG_K_OTHER, 0, [&] { k_sort_keys<D><<<g, BLOCK, 0, st_>>>(P_, top, k_in, v_in); });
 		DG_CUDA(cub::DeviceRadixSort::SortPairs(tmp, temp, k_in, k_out, v_in, v_out, n, 0, 64, st_));
 		run_k(DG_K_OTHER, 0, [&] { k_sort_inverse<<<g, BLOCK, 0, st_>>>(v_out, n, newidx); });
-		auto fo = fields(P_), fs = fields(S_);
+		// each field in turn: permuted into the spare buffer, then copied back over slots [1, top)
+		auto fo = fields(P_);
 		for (size_t k = 0; k < fo.size(); ++k) {
 			const int comps = fo[k].comps;
 			if (comps <= 0) continue;
+			const size_t elem = fo[k].elem;
+			void *src = *fo[k].ptr, *dst = spare_mem_;
 			run_k(DG_K_OTHER, 0, [&] {
-				switch (fo[k].elem) {
-					case 1: k_permute<int8_t><<<g, BLOCK, 0, st_>>>((const int8_t *) *fo[k].ptr, (int8_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
-					case 2: k_permute<int16_t><<<g, BLOCK, 0, st_>>>((const int16_t *) *fo[k].ptr, (int16_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
-					case 4: k_permute<int32_t><<<g, BLOCK, 0, st_>>>((const int32_t *) *fo[k].ptr, (int32_t *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
-					case 8: k_permute<double><<<g, BLOCK, 0, st_>>>((const double *) *fo[k].ptr, (double *) *fs[k].ptr, comps, P_.cap, n, v_out); break;
+				switch (elem) {
+					case 1: k_permute<int8_t><<<g, BLOCK, 0, st_>>>((const int8_t *) src, (int8_t *) dst, comps, P_.cap, n, v_out); break;
+					case 2: k_permute<int16_t><<<g, BLOCK, 0, st_>>>((const int16_t *) src, (int16_t *) dst, comps, P_.cap, n, v_out); break;
+					case 4: k_permute<int32_t><<<g, BLOCK, 0, st_>>>((const int32_t *) src, (int32_t *) dst, comps, P_.cap, n, v_out); break;
+					case 8: k_permute<double><<<g, BLOCK, 0, st_>>>((const double *) src, (double *) dst, comps, P_.cap, n, v_out); break;
 					default:  // one record of elem bytes per node
-						k_permute_words<<<grid_for((long long) n * (fo[k].elem / 8)), BLOCK, 0, st_>>>(
-						    (const double *) *fo[k].ptr, (double *) *fs[k].ptr, (int) (fo[k].elem / 8), n, v_out);
+						k_permute_words<<<grid_for((long long) n * (elem / 8)), BLOCK, 0, st_>>>(
+						    (const double *) src, (double *) dst, (int) (elem / 8), n, v_out);
 						break;
 				}
 			});
+			DG_CUDA(cudaMemcpy2DAsync((char *) src + elem, elem * (size_t) P_.cap, (const char *) dst + elem,
+			                          elem * (size_t) P_.cap, elem * (size_t) n, comps, cudaMemcpyDeviceToDevice, st_));
 		}
-		run_k(DG_K_OTHER, 0, [&] { k_remap_links<D><<<grid_for(top), BLOCK, 0, st_>>>(S_, top, newidx); });
-		std::swap(P_, S_);
-		std::swap(pool_mem_, shadow_mem_);
-		attach_derived();
+		run_k(DG_K_OTHER, 0, [&] { k_remap_links<D><<<grid_for(top), BLOCK, 0, st_>>>(P_, top, newidx); });
 		int first = 1;
 		for (int l = 0; l < MAX_ACTI; ++l) {
 			const int cnt = h_cnt_->clu[l];
@@ -843,20 +851,20 @@ private:
 		DG_CUDA(cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, keep, newidx, top + 1, st_));
 		int new_top = 0;
 		DG_CUDA(cudaMemcpyAsync(&new_top, newidx + top, sizeof(int), cudaMemcpyDeviceToHost, st_));
-		// compact into the re-sort's second pool (zeroed), which then becomes the live one
-		if (!shadow_mem_) shadow_mem_ = carve_pool(S_, P_.cap);
-		else DG_CUDA(cudaMemsetAsync(shadow_mem_, 0, pool_bytes(P_.cap), st_));
-		auto fo = fields(P_), fn = fields(S_);
+		// each field in turn: kept slots compacted into the zeroed spare buffer, which is then copied back
+		// whole (slots from new_top on end up zero)
+		ensure_spare();
+		auto fo = fields(P_);
 		for (size_t k = 0; k < fo.size(); ++k) {
 			if (fo[k].comps <= 0) continue;
-			k_gc_move<<<g, BLOCK, 0, st_>>>((const char *) *fo[k].ptr, (char *) *fn[k].ptr, (int) fo[k].elem, fo[k].comps,
+			const size_t bytes = fo[k].elem * (size_t) P_.cap * fo[k].comps;
+			DG_CUDA(cudaMemsetAsync(spare_mem_, 0, bytes, st_));
+			k_gc_move<<<g, BLOCK, 0, st_>>>((const char *) *fo[k].ptr, (char *) spare_mem_, (int) fo[k].elem, fo[k].comps,
 			                                 P_.cap, top, keep, newidx);
+			DG_CUDA(cudaMemcpyAsync(*fo[k].ptr, spare_mem_, bytes, cudaMemcpyDeviceToDevice, st_));
 		}
 		DG_CUDA(cudaStreamSynchronize(st_));
-		k_gc_remap<D><<<grid_for(new_top), BLOCK, 0, st_>>>(S_, new_top, keep, newidx);
-		std::swap(P_, S_);
-		std::swap(pool_mem_, shadow_mem_);
-		attach_derived();
+		k_gc_remap<D><<<grid_for(new_top), BLOCK, 0, st_>>>(P_, new_top, keep, newidx);
 		// full ACTI reassignment
 		Counters z{};
 		z.top    = new_top;
@@ -978,6 +986,7 @@ public:
 		for (size_t i = 0; i < nn; ++i) {
 			level[i] = lv[i];
 			meta[i]  = (double) ac[i];
+			flags[i] &= F_PUBLIC;
 		}
 		return n;
 	}
@@ -1025,6 +1034,11 @@ public:
 
 	// Same records as read_cells, gathered through caller-owned device scratch of `bytes` bytes;
 	// allocates nothing.
+	void prepare_noalloc() override {
+		cudaFuncAttributes a{};
+		DG_CUDA(cudaFuncGetAttributes(&a, k_gather_cells<M>));
+	}
+
 	long long read_cells_via(int *levels, double *data, long long max_cells, void *scratch, size_t bytes) override {
 		constexpr int W = D + 1 + 2 * E + 3 + M::P;
 		const long long n = cell_count();

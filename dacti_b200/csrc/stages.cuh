@@ -279,100 +279,12 @@ __device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i
 	return (P.clu[gc] == L && ai <= P.acti[gc]) ? gc : -1;
 }
 
-// Face-flux slot of cell i's face f. The slots hold FP64 values in the FP64 form and FP32 values in the
-// mixed form (T = float: the same array read with a compact FP32 stride).
+// Face-flux slot of face f of the cell at list position `slot`, written for owned faces next to a receiver. The slots hold FP64
+// values in the FP64 form and FP32 values in the mixed form (T = float: the same array read with a
+// compact FP32 stride).
 template<class T = double>
-__device__ __forceinline__ T *face_flux(const Pool &P, int i, int f, int nflux, int nfaces) {
-	return reinterpret_cast<T *>(P.ff) + ((size_t) i * nfaces + f) * nflux;
-}
-
-// Face-flux source codes of plan[]: (owner * 2D + owner's face) * 2 + (1 if the cell subtracts it),
-// or PLAN_NONE when no flux crosses the face in this substep. A face with finer owners behind a
-// non-leaf neighbour is queued as a walk task; the walk stores the face's signed sum in the cell's own
-// slot for that face (unused otherwise: the cell owns no face towards a non-leaf) and plans it as a
-// plain source.
-constexpr int32_t PLAN_NONE = -1;
-
-// flux_update (impl/flux.hpp:11-97), first part. One thread per (cell, face) of the running cluster
-// decides whether the cell owns the face (the finer side, or at equal levels the slower cell, or the
-// cell on the left) and queues it as a dense task, interior and boundary faces apart; it records in
-// plan[] where the face's flux will come from, and owners next to cells of slower clusters queue
-// those as receivers. Task order is scheduling dependent, task results are not.
-template<class M>
-__global__ void k_flux_tasks(Pool P, const int32_t *list, int n, int L, int stamp, int32_t *tasks, int32_t *btasks,
-                             int32_t *wtasks, int32_t *recv, Counters *cnt) {
-	constexpr int NF = 2 * M::D;
-	const int cap   = P.cap;
-	const long long total = (long long) n * NF;
-	for (long long t = gtid(); t < total; t += gstride()) {
-		const int slot = (int) (t / NF), f = (int) (t % NF);
-		const int i    = list[slot];
-		const int dir  = f & 1;
-		const int nb   = P.nbr[(size_t) f * cap + i];
-		int32_t *pl    = P.plan + (size_t) i * NF + f;
-		if (nb == 0) {
-			if (P.bc[(size_t) f * cap + i] < 0) {
-				set_status(&cnt->status, ST_MISSING_BC);
-				*pl = PLAN_NONE;
-			} else {
-				append(btasks, &cnt->n_btask, i * NF + f, cap * NF, &cnt->status);
-				*pl = (i * NF + f) * 2 + 1;
-			}
-			continue;
-		}
-		if (!(P.flags[nb] & F_LEAF)) {
-			append(wtasks, &cnt->n_wtask, i * NF + f, cap * NF, &cnt->status);
-			*pl = (i * NF + f) * 2;
-			continue;
-		}
-		const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
-		if (an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
-			if (P.clu[nb] != L) {
-				if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
-			}
-			append(tasks, &cnt->n_task, i * NF + f, cap * NF, &cnt->status);
-			*pl = (i * NF + f) * 2 + dir;
-		} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
-			*pl = (nb * NF + (f ^ 1)) * 2 + dir;
-		} else {
-			*pl = PLAN_NONE;
-		}
-	}
-}
-
-// Interior face fluxes of the queued tasks, one thread per face, into the owner's face-flux slot.
-template<class M, bool V, class S = double>
-__global__ void __launch_bounds__(BLOCK) k_flux_faces(Pool P, Consts C, const int32_t *tasks, const int *n_ptr,
-                                                      double dtL) {
-	constexpr int NF = 2 * M::D;
-	const int n = *n_ptr;
-	for (int t = gtid(); t < n; t += gstride()) {
-		const int code = tasks[t];
-		const int i = code / NF, f = code % NF;
-		const int nb = P.nbr[(size_t) f * P.cap + i];
-		double F[M::F];
-		interior_flux<M, V, S>(P, C, i, nb, f >> 1, f & 1, dtL, F);
-		S *dst = face_flux<S>(P, i, f, M::F, NF);
-#pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = (S) F[q];
-	}
-}
-
-// Boundary face fluxes of the queued tasks.
-template<class M, bool V, class S = double>
-__global__ void k_flux_bfaces(Pool P, Consts C, BcTable B, const int32_t *tasks, const int *n_ptr, double dtL) {
-	constexpr int NF = 2 * M::D;
-	const int n = *n_ptr;
-	for (int t = gtid(); t < n; t += gstride()) {
-		const int code = tasks[t];
-		const int i = code / NF, f = code % NF;
-		const int b = P.bc[(size_t) f * P.cap + i];
-		double F[M::F];
-		boundary_flux<M, V, S>(P, C, B, i, b, f >> 1, f & 1, dtL, F);
-		S *dst = face_flux<S>(P, i, f, M::F, NF);
-#pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = (S) F[q];
-	}
+__device__ __forceinline__ T *face_flux(const Pool &P, int slot, int f, int nflux, int nfaces) {
+	return reinterpret_cast<T *>(P.ff) + ((size_t) slot * nfaces + f) * nflux;
 }
 
 // flux_update, receiving side: each queued receiver sums, in a fixed face order, the fluxes that
@@ -409,7 +321,7 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 					bool plus;
 					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, false, dn, plus);
 					if (owner < 0) continue;
-					const T *F = face_flux<T>(P, owner, 2 * dim + dn, M::F, NF);
+					const T *F = face_flux<T>(P, P.pos[owner], 2 * dim + dn, M::F, NF);
 					if (plus) {
 #pragma unroll
 						for (int q = 0; q < M::F; ++q) acc[q] += F[q];
@@ -430,86 +342,135 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 #pragma unroll
 			for (int q = 0; q < M::F; ++q)
 				if ((q & (G - 1)) == sub) P.flux[(size_t) q * cap + i] += acc[q];
+			if (sub == 0) atomicOr(&P.flags[i], (uint32_t) F_RECV);
 		}
 	}
 }
 
-// Walk tasks: the flux sum of a running-cluster cell's face whose finer owners sit behind a non-leaf
-// neighbour, in candidate order, stored in the cell's own slot for that face.
-template<class M, class T = double>
-__global__ void k_flux_walk(Pool P, const int32_t *wtasks, const int *n_ptr, int L, Counters *cnt) {
-	constexpr int NF = 2 * M::D, NSUB = 1 << (M::D - 1);
-	const int n = *n_ptr;
-	for (int t = gtid(); t < n; t += gstride()) {
-		const int code = wtasks[t];
-		const int i = code / NF, f = code % NF;
-		const int li = P.level[i], ai = P.acti[i];
-		const int nb = P.nbr[(size_t) f * P.cap + i];
-		double acc[M::F];
+// flux_update (impl/flux.hpp:11-97) seen from each running-cluster cell: the signed sum of the fluxes
+// that cross its faces in this substep, one group of G lanes per cell (G = 4 in 2D, 8 in 3D; lanes past
+// 2D idle). Lane f evaluates the flux across face f: the cell's own when it owns the face (the finer
+// side, at equal levels the slower cell or the cell on the left), the same-level neighbour's when the
+// neighbour owns it, the boundary flux, or the sum over the finer owners behind a non-leaf neighbour in
+// candidate order. Every interior flux is evaluated with the owner's arguments (owner, the owner's
+// neighbour, the owner's direction), so the two cells of a face obtain identical bits and the update
+// stays conservative without a face-flux array or atomics. The lane terms combine in a fixed butterfly,
+// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0)) in 3D, into du[slot]. An owned face next to a cell of
+// a slower cluster (the coarse-time side of the LTS coupling, impl/flux.hpp:82-91) also goes to the
+// owner's face-flux slot, and that cell joins the receiver list. In the mixed form every flux is rounded
+// to FP32 once, as both sides read it; sums stay FP64.
+template<class M, bool V, class S = double>
+__global__ void __launch_bounds__(BLOCK) k_face_sum(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L,
+                                                    double dtL, int stamp, int32_t *recv, Counters *cnt) {
+	constexpr int NF = 2 * M::D, G = NF <= 4 ? 4 : 8, GW = 32 / G, NSUB = 1 << (M::D - 1), F = M::F;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot = wbase + lane / G;
+		double acc[F];
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) acc[q] = 0.0;
-		for (int c = 1; c < 1 + NSUB * (NSUB + 1); ++c) {
-			int dn;
-			bool plus;
-			const int owner = face_owner<M>(P, &cnt->status, i, nb, f >> 1, f & 1, L, li, ai, c, true, dn, plus);
-			if (owner < 0) continue;
-			const T *F = face_flux<T>(P, owner, (f & ~1) | dn, M::F, NF);
-			if (plus) {
+		for (int q = 0; q < F; ++q) acc[q] = 0.0;
+		if (slot < n && sub < NF) {
+			const int i   = list[slot];
+			if (sub == 0) P.pos[i] = slot;
+			const int f   = sub, dim = f >> 1, dir = f & 1;
+			const int nb  = P.nbr[(size_t) f * cap + i];
+			if (nb == 0) {
+				const int b = P.bc[(size_t) f * cap + i];
+				if (b < 0) {
+					set_status(&cnt->status, ST_MISSING_BC);
+				} else {
+					double Fb[F];
+					boundary_flux<M, V, S>(P, C, B, i, b, dim, dir, dtL, Fb);
 #pragma unroll
-				for (int q = 0; q < M::F; ++q) acc[q] += F[q];
+					for (int q = 0; q < F; ++q) acc[q] = 0.0 - (double) (S) Fb[q];
+				}
+			} else if (!(P.flags[nb] & F_LEAF)) {
+				const int li = P.level[i], ai = P.acti[i];
+				double w[F];
+#pragma unroll
+				for (int q = 0; q < F; ++q) w[q] = 0.0;
+				for (int c = 1; c < 1 + NSUB * (NSUB + 1); ++c) {
+					int dn;
+					bool plus;
+					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, true, dn, plus);
+					if (owner < 0) continue;
+					const int fo = 2 * dim + dn;
+					double Fw[F];
+					interior_flux<M, V, S>(P, C, owner, P.nbr[(size_t) fo * cap + owner], dim, dn, dtL, Fw);
+					if (plus) {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] += (double) (S) Fw[q];
+					} else {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] -= (double) (S) Fw[q];
+					}
+				}
+#pragma unroll
+				for (int q = 0; q < F; ++q) acc[q] = 0.0 + (double) (S) w[q];
 			} else {
+				const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
+				int own = -1, fo = f;
+				if (an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
+					own = i;
+				} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
+					own = nb;
+					fo  = f ^ 1;
+				}
+				if (own >= 0) {
+					const int other = own == i ? nb : P.nbr[(size_t) fo * cap + nb];
+					double Fi[F];
+					interior_flux<M, V, S>(P, C, own, other, dim, fo & 1, dtL, Fi);
+					if (own == i && P.clu[nb] != L) {
+						S *dst = face_flux<S>(P, slot, f, F, NF);
 #pragma unroll
-				for (int q = 0; q < M::F; ++q) acc[q] -= F[q];
+						for (int q = 0; q < F; ++q) dst[q] = (S) Fi[q];
+						if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
+					}
+#pragma unroll
+					for (int q = 0; q < F; ++q) {
+						const double v = (double) (S) Fi[q];
+						acc[q] = dir ? 0.0 - v : 0.0 + v;
+					}
+				}
 			}
 		}
-		T *dst = face_flux<T>(P, i, f, M::F, NF);
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) dst[q] = (T) acc[q];
+		for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+			for (int q = 0; q < F; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
+		if (slot < n) {
+			double *dst = P.du + (size_t) slot * F;
+#pragma unroll
+			for (int q = 0; q < F; ++q)
+				if ((q & (G - 1)) == sub) dst[q] = acc[q];
+		}
 	}
 }
 
-// Signed contribution of a planned face source to component q, as a gather lane forms it from +0.
-template<class T>
-__device__ __forceinline__ double face_term(const T *F, int pl, int q) {
-	if (pl < 0) return 0.0;
-	const double v = (double) F[q];
-	return (pl & 1) ? 0.0 - v : 0.0 + v;
-}
-
-// flux_update's gather for the running cluster fused with cell_update (impl/cell_update.hpp:10-90),
-// one thread per cell, component by component so that all face-slot loads are independent. The face
-// terms combine in the pairing order of a butterfly over 4 (2D) or 8 (3D) lanes, the last two
-// contributing zeros in 3D. Without viscous terms (V = false) the gradient inputs are never read, so
-// t_slope is not maintained.
-template<class M, bool V, class T = double>
-__global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, const int32_t *list, int n, double dtL,
-                                                            int epoch, Counters *cnt) {
-	constexpr int E = M::E, NF = 2 * M::D;
+// cell_update (impl/cell_update.hpp:10-90) of the running cluster, one thread per cell: du = (received
+// fluxes + the face sum of k_face_sum) / volume, the multiphase source from the pre-update state, the
+// EOS recovery, floors and the conservative state. The received-flux accumulator is read (and reset)
+// only when the receive stage has marked the cell. Without viscous terms (V = false) the gradient
+// inputs are never read, so t_slope is not maintained.
+template<class M, bool V>
+__global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, int epoch,
+                                                     Counters *cnt) {
+	constexpr int E = M::E;
 	const int cap = P.cap;
 	for (int tid = gtid(); tid < n; tid += gstride()) {
 		const int i  = list[tid];
 		const int li = P.level[i];
-		int pl[NF];
-		const T *src[NF];
-#pragma unroll
-		for (int f = 0; f < NF; ++f) {
-			pl[f]  = P.plan[(size_t) i * NF + f];
-			src[f] = reinterpret_cast<const T *>(P.ff) + (size_t) (pl[f] < 0 ? 0 : pl[f] >> 1) * M::F;
-		}
-		const double vol = C.vol[li];
+		const double vol  = C.vol[li];
+		const uint32_t fl0 = P.flags[i];
+		const bool rcv     = fl0 & F_RECV;
+		const double *s_in = P.du + (size_t) tid * M::F;
 		double du[M::F];
 #pragma unroll
-		for (int q = 0; q < M::F; ++q) {
-			double s;
-			if constexpr (NF <= 4) {
-				s = (face_term(src[0], pl[0], q) + face_term(src[2], pl[2], q)) +
-				    (face_term(src[1], pl[1], q) + face_term(src[3], pl[3], q));
-			} else {
-				s = ((face_term(src[0], pl[0], q) + face_term(src[4], pl[4], q)) + (face_term(src[2], pl[2], q) + 0.0)) +
-				    ((face_term(src[1], pl[1], q) + face_term(src[5], pl[5], q)) + (face_term(src[3], pl[3], q) + 0.0));
-			}
-			du[q] = (at(P.flux, cap, q, i) + s) / vol;
-		}
+		for (int q = 0; q < M::F; ++q) du[q] = ((rcv ? at(P.flux, cap, q, i) : 0.0) + s_in[q]) / vol;
 
 		double pold[E], u[E], p[E];
 		load_p<M>(P, i, pold);
@@ -556,11 +517,15 @@ __global__ void __launch_bounds__(BLOCK, 2) k_gather_update(Pool P, Consts C, co
 			P.p[(size_t) q * cap + i] = p[q];
 		}
 		store_p_rec<M>(P, i, p);
-		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
+		if (rcv) {
+			for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
+			P.flags[i] = fl0 & ~F_RECV;
+		}
 		P.t[i] = P.t[i] + dtL;
 		mark_up(P, P.parent[i], epoch);
 	}
 }
+
 
 
 // Neighbour values of a cell list: for each (cell, face) the neighbour's primitive state and time as
@@ -910,8 +875,10 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 			for (int k = 0; k < D * R::ES; ++k) rs[R::S0 + k] = rp[R::S0 + k];
 			for (int k = 0; k < M::P; ++k) P.k[(size_t) k * cap + s] = at(P.k, cap, k, par);
 			write_rec_k<M>(P, s);
-			for (int k = 0; k < M::G; ++k) P.tslope[(size_t) k * cap + s] = at(P.tslope, cap, k, par);
-			for (int k = 0; k < D * M::G; ++k) P.grad[(size_t) k * cap + s] = at(P.grad, cap, k, par);
+			if (C.visc) {
+				for (int k = 0; k < M::G; ++k) P.tslope[(size_t) k * cap + s] = at(P.tslope, cap, k, par);
+				for (int k = 0; k < D * M::G; ++k) P.grad[(size_t) k * cap + s] = at(P.grad, cap, k, par);
+			}
 			for (int k = 0; k < M::F; ++k) P.flux[(size_t) k * cap + s] = 0.0;
 			P.err[s] = -1.0;
 			for (int dim = 0; dim < D; ++dim) {
@@ -948,15 +915,17 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		for (int q = 0; q < E; ++q) u[q] = 0.0;
 		for (int q = 0; q < M::P; ++q) kk[q] = 0.0;
 		for (int q = 0; q < G; ++q) ts[q] = 0.0;
-		for (int q = 0; q < D * G; ++q) gr[q] = at(P.grad, cap, q, par);
+		for (int q = 0; q < D * G; ++q) gr[q] = C.visc ? at(P.grad, cap, q, par) : 0.0;
 		double error = 0.0;
 		for (int c = 0; c < NC; ++c) {
 			const int ch = P.child[(size_t) c * cap + par];
 			t += P.t[ch];
 			for (int q = 0; q < E; ++q) u[q] = u[q] + at(P.u, cap, q, ch);
 			for (int q = 0; q < M::P; ++q) kk[q] = kk[q] + at(P.k, cap, q, ch);
-			for (int q = 0; q < D * G; ++q) gr[q] = gr[q] + at(P.grad, cap, q, ch);
-			for (int q = 0; q < G; ++q) ts[q] = ts[q] + at(P.tslope, cap, q, ch);
+			if (C.visc) {
+				for (int q = 0; q < D * G; ++q) gr[q] = gr[q] + at(P.grad, cap, q, ch);
+				for (int q = 0; q < G; ++q) ts[q] = ts[q] + at(P.tslope, cap, q, ch);
+			}
 		}
 		for (int c = 0; c < NC; ++c) {
 			const int ch = P.child[(size_t) c * cap + par];
@@ -979,8 +948,10 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		}
 		for (int q = 0; q < M::P; ++q) P.k[(size_t) q * cap + par] = kk[q];
 		write_rec_k<M>(P, par);
-		for (int q = 0; q < G; ++q) P.tslope[(size_t) q * cap + par] = ts[q];
-		for (int q = 0; q < D * G; ++q) P.grad[(size_t) q * cap + par] = gr[q];
+		if (C.visc) {
+			for (int q = 0; q < G; ++q) P.tslope[(size_t) q * cap + par] = ts[q];
+			for (int q = 0; q < D * G; ++q) P.grad[(size_t) q * cap + par] = gr[q];
+		}
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + par] = 0.0;
 		for (int f = 0; f < 2 * D; ++f) P.nbr[(size_t) f * cap + par] = 0;
 		P.err[par]   = error;
@@ -1179,7 +1150,8 @@ __global__ void k_init_cells(Pool P, Consts C, const int32_t *list, int n, Count
 			P.k[(size_t) 0 * cap + i]         = C.m.mu1 * p[M::IA] + C.m.mu2 * (1 - p[M::IA]);
 			P.k[(size_t) M::ALPHAS * cap + i] = p[M::IA];
 		}
-		for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = 0.0;
+		if (C.visc)
+			for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = 0.0;
 		const double mdt = max_delta_time<M>(C.m, p, C.size[P.level[i]]);
 		P.maxdt[i] = mdt;
 		for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;

@@ -254,9 +254,10 @@ int dg_mlp_destroy(dg_mlp *m);
  * device-wide synchronisation of cudaMalloc/cudaFree). No counterpart in the reference: DACTI's
  * Integrator hands out host references to its nodes. Same records and order as dg_read_cells,
  * gathered through a 64 MiB scratch array that the library keeps resident on each device: read-backs
- * larger than that (about 380 thousand multi<3> cells, 560 thousand euler<2> cells) return
- * DG_ERR_CAPACITY. Calls share the scratch, so calls whose GPU work overlaps race; the first call on a
- * device looks up the scratch's device address and should come before any stream capture. */
+ * larger than that return DG_ERR_CAPACITY: a cell takes 8 (D + 2E + P + 5) bytes of it, so it holds about 289
+ * thousand multi<3> cells or 559 thousand euler<2> cells. dg_create places the scratch on the solver's
+ * device and looks up its address, so no call of this function allocates, the first one included.
+ * Calls share the scratch, so calls whose GPU work overlaps race. */
 int dg_read_cells_noalloc(dg_solver *s, int *levels, double *data, long long max_cells, long long *n_out);
 
 int dg_get_stats(dg_solver *s, dg_stats *out);

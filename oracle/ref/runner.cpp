@@ -6,6 +6,7 @@
 // Usage: dacti_ref_runner <case.bin> <out_prefix> <n_global_steps> [--check s1,s2,..]
 //                         [--t-end T] [--neighbor-audit] [--quiet]
 //                         [--sample-substeps S --samples N]   (bounded timing samples)
+//                         [--chunk-substeps S]   (one full global step timed in chunks of S substeps)
 //                         [--nodes]   (with each snapshot, the whole node table of get_nodes())
 // Prints one JSON line with timing (wall time of integrate() calls only), substep and
 // leaf-update counts. Leaf cell-updates are counted in the substep hook as the level's cluster
@@ -44,6 +45,7 @@ namespace {
 		bool quiet = false;
 		int sample_substeps = 0;  // >0: each integrate() call is timed up to this many substeps
 		int samples = 0;
+		int chunk_substeps = 0;   // >0: one whole integrate() call, timed per chunk of this many substeps
 		bool adapter_check = false;  // side-by-side run against the GPU adapter (adapter build only)
 		bool driver_check  = false;  // DACTI's default_driver over the reference and over the adapter
 		bool nodes         = false;  // also dump Integrator::get_nodes() beside each snapshot
@@ -376,6 +378,34 @@ namespace {
 		if (o.checks.count(0)) write_snapshot<Model>(in, o.out_prefix + "_0.snap", 0, time, updates);
 		if (o.checks.count(0) && o.nodes) write_nodes<Model>(in, o.out_prefix + "_0.nodes");
 
+		if (o.chunk_substeps > 0) {
+			// One complete global step; the hook closes a chunk after every chunk_substeps substeps (and
+			// after the last one), so the chunks partition the step's substeps in execution order.
+			std::printf("{\"init_s\": %.6f, \"threads\": %d, \"chunks\": [", init_s, omp_get_max_threads());
+			int seen = 0, in_chunk = 0, n_chunks = 0;
+			double upd = 0.0;
+			auto a     = clk::now();
+			auto hook  = [&](auto &itg, int level, scalar_t, int, scalar_t) {
+                upd += (double) itg.acti_clusters[level].size();
+                ++seen;
+                if (++in_chunk == o.chunk_substeps) {
+                    auto b = clk::now();
+                    std::printf("%s{\"substeps\": %d, \"updates\": %.0f, \"seconds\": %.6f}", n_chunks++ ? ", " : "",
+                                in_chunk, upd, std::chrono::duration<double>(b - a).count());
+                    std::fflush(stdout);
+                    in_chunk = 0;
+                    upd      = 0.0;
+                    a        = clk::now();
+                }
+			};
+			in.integrate(hook, true, force_break);
+			if (in_chunk > 0)
+				std::printf("%s{\"substeps\": %d, \"updates\": %.0f, \"seconds\": %.6f}", n_chunks++ ? ", " : "", in_chunk,
+				            upd, std::chrono::duration<double>(clk::now() - a).count());
+			std::printf("], \"substeps\": %d, \"force_break\": %d}\n", seen, force_break ? 1 : 0);
+			return 0;
+		}
+
 		if (o.sample_substeps > 0) {
 			// Bounded timing samples: each integrate() call is timed from its start to the hook of its
 			// sample_substeps-th substep; the hook then requests the early return the NaN path uses.
@@ -465,6 +495,8 @@ int main(int argc, char **argv) {
 			o.quiet = true;
 		} else if (a == "--sample-substeps" && i + 1 < argc) {
 			o.sample_substeps = std::atoi(argv[++i]);
+		} else if (a == "--chunk-substeps" && i + 1 < argc) {
+			o.chunk_substeps = std::atoi(argv[++i]);
 		} else if (a == "--samples" && i + 1 < argc) {
 			o.samples = std::atoi(argv[++i]);
 		} else if (a == "--adapter-check") {

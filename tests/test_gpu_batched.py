@@ -50,3 +50,26 @@ def test_batched_trees_match_reference(tree, tmp_path):
     assert rep.ok(1e-10), rep
     for s in solvers:
         s.close()
+
+
+def test_batch_extreme_trees_match_reference(tmp_path):
+    """The largest (256^2 base, +4 levels) and the smallest (32^2 base, +2 levels) trees of the
+    256-tree batch of the batched workload (cases.riemann_batch(256, seed=3)), stepped together with
+    dg_step_many for 2 global steps, against the reference solver on each tree."""
+    from dacti_b200.batch import tree_work
+    full = cases.riemann_batch(256, seed=3)
+    work = [tree_work(c) for c in full]
+    pick = [int(np.argmax(work)), int(np.argmin(work))]
+    assert full[pick[0]].params.min_level == 8 and full[pick[0]].params.max_level == 12
+    steps = 2
+    solvers = [Solver(full[k]) for k in pick]
+    for _ in range(steps):
+        assert not any(step_many(solvers, threads=2))
+    for s, k in zip(solvers, pick):
+        path = str(tmp_path / f"t{k}.case")
+        write_case(full[k], path)
+        run_reference(path, str(tmp_path / f"t{k}"), steps, [steps])
+        ref = read_snapshot(str(tmp_path / f"t{k}_{steps}.snap"))
+        rep = compare(ref, s.active_cells(), full[k].params.side_length)
+        assert rep.ok(1e-10), f"tree {k}: {rep}"
+        s.close()

@@ -100,6 +100,13 @@ def test_multi3_larger(tmp_path):
     _live(cases.shock_drop(base_level=4, levels=2), 3, [1, 3], tmp_path, "sd3")
 
 
+def test_shock_drop_config2_reduced(tmp_path):
+    """Config 2's shock-drop at a quarter of its base resolution per axis (32 x 16 x 16 base, +3 levels,
+    a 6.4e5-node initial tree) for 2 global steps against the single-thread reference."""
+    stats = _live(cases.shock_drop(base_level=5, levels=3), 2, [1, 2], tmp_path, "sd53")
+    assert stats.n_substeps > 100
+
+
 def test_periodic_without_refinement(tmp_path):
     _live(cases.periodic_blob(base_level=5, refine=False), 8, [8], tmp_path, "pnr")
 

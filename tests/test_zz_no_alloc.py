@@ -35,11 +35,32 @@ def test_noalloc_read_matches_allocating_read_twice():
     s.close()
 
 
+def test_noalloc_first_call_on_a_fresh_solver_allocates_nothing():
+    """The scratch array and the gather kernel are placed on the device by dg_create, so the first
+    read-back of a new solver leaves the device's free memory where it was."""
+    import torch
+
+    case = cases.shock_drop(base_level=3, levels=2)
+    s = Solver(case)
+    s.integrate()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    snap = s.active_cells_noalloc()
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory changed by {free0 - free1} bytes"
+    assert snap.n == s.n_active_cells() > 0
+    _same(s.active_cells(), snap)
+    s.close()
+
+
 def test_noalloc_read_rejects_more_cells_than_its_scratch_holds():
     case = cases.lax_liu3(base_level=10, levels=0)  # 2^20 euler<2> cells
     s = Solver(case)
     with pytest.raises(DgError) as e:
         s.active_cells_noalloc()
+    # euler<2>: 8 (D + 2E + P + 5) = 120 bytes per cell of the 64 MiB scratch (256 bytes of alignment slack)
     assert e.value.code == -3 and "scratch" in str(e.value)
+    assert f"about {((64 << 20) - 256) // 120} cells" in str(e.value)
     assert s.active_cells().n == 1 << 20
     s.close()
