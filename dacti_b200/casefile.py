@@ -7,6 +7,7 @@ tree level, time level, centre, time, conserved and primitive state.
 """
 from __future__ import annotations
 
+import dataclasses
 from dataclasses import dataclass, field
 from typing import Optional, Sequence
 
@@ -19,7 +20,7 @@ N_PARAMS = 32
 P = dict(
     SIDE=0, ACTIVE0=1, PERIODIC0=4, MAX_CFL=7, MAX_DT=8, MIN_ERR=9, MAX_ERR=10, MAX_LEVEL=11, MIN_LEVEL=12,
     GAMMA=13, NS_MU=14, NS_LAMBDA=15, GAMMA1=16, GAMMA2=17, P1=18, P2=19, CP1=20, CP2=21, CV1=22, CV2=23,
-    MU1=24, MU2=25, LAMBDA1=26, LAMBDA2=27, SIGMA=28,
+    MU1=24, MU2=25, LAMBDA1=26, LAMBDA2=27, SIGMA=28, PRUNED=29, POOL_CAP=30,
 )
 
 
@@ -58,6 +59,10 @@ class SolverParams:
     sigma: float = 0.0
     zones: Sequence[RefineZone] = field(default_factory=list)
     limiter: int = 0  # dacti::integrator::slope id: minmod, unlimited, van_leer, superbee, von_alba_2, koren, first_order
+    # GPU solver only (the reference runner ignores them): node slots left out of the upload by
+    # prune_inactive, which still count towards the tree size, and a node-pool capacity (0: 1.5 x nodes)
+    pruned_nodes: int = 0
+    pool_capacity: int = 0
 
     def param_vector(self) -> np.ndarray:
         v = np.zeros(N_PARAMS, np.float64)
@@ -78,6 +83,8 @@ class SolverParams:
                   "SIGMA"):
             attr = {"GAMMA1": "gamma1", "GAMMA2": "gamma2"}.get(k, k if k in ("P1", "P2") else k.lower())
             v[P[k]] = getattr(self, attr)
+        v[P["PRUNED"]] = float(self.pruned_nodes)
+        v[P["POOL_CAP"]] = float(self.pool_capacity)
         return v
 
 
@@ -89,6 +96,42 @@ class Case:
     @property
     def shape(self) -> ModelShape:
         return self.tree.shape
+
+
+def prune_inactive(case: Case, pool_capacity: int = 0) -> Case:
+    """The case without the nodes whose subtree holds no active leaf (the parts of the root box outside
+    the active box, the inside of solid objects), for the GPU solver.
+
+    Nothing the integrator computes reads those nodes: their faces towards active cells carry boundary
+    conditions, subtree means skip inactive children, and a walk that meets a removed child (slot 0)
+    treats it as the inactive leaf it stands for. Their number goes to ``pruned_nodes``, which the
+    solver adds to its tree size wherever the reference's tree.size() enters (the garbage-collection
+    trigger, impl/integrate.hpp:78-84), so results are unchanged. Node numbering changes, and the tree a
+    writer reads back (dg_read_tree) lacks the removed nodes.
+    """
+    t = case.tree
+    n = t.n_nodes
+    keep = np.zeros(n, bool)
+    keep[t.leaf_mask()] = True
+    lv = t.level.astype(np.int64)
+    order = np.argsort(-lv, kind="stable")
+    # ancestors of active leaves, deepest level first
+    for level in range(int(lv.max()), 0, -1):
+        idx = order[lv[order] == level]
+        par = t.parent[idx[keep[idx]]]
+        keep[par] = True
+    keep[0] = True
+    if n > 1:
+        keep[1] = True
+    newidx = np.cumsum(keep).astype(np.int64) - 1
+    newidx[~keep] = 0
+    ch = t.children[keep]
+    children = np.where(keep[ch], newidx[ch], 0).astype(np.int32)
+    tree = Tree(t.shape, newidx[t.parent[keep]].astype(np.int32), children, t.level[keep].copy(),
+                t.flags[keep].copy(), t.bc[keep].copy(), t.center[keep].copy(), t.p[keep].copy(), list(t.bcs))
+    prm = dataclasses.replace(case.params, pruned_nodes=int(case.params.pruned_nodes + n - int(keep.sum())),
+                              pool_capacity=int(pool_capacity))
+    return Case(tree, prm)
 
 
 def write_case(case: Case, path: str) -> None:

@@ -183,6 +183,56 @@ int dg_set_profiling(dg_solver *s, int on) {
 	return guarded(s, [&] { s->impl->set_profiling(on != 0); });
 }
 
+int dg_batch_create(dg_solver **s, int n, dg_batch **out) {
+	if (!s || n < 1 || !out) return DG_ERR_ARG;
+	*out = nullptr;
+	for (int k = 0; k < n; ++k)
+		if (!s[k] || s[k]->device != s[0]->device) return DG_ERR_ARG;
+	return guarded(s[0], [&] {
+		std::vector<dg::SolverBase *> v;
+		for (int k = 0; k < n; ++k) v.push_back(s[k]->impl);
+		const int model = v[0]->model_id(), dims = v[0]->dims();
+		for (auto *x: v)
+			if (x->model_id() != model || x->dims() != dims)
+				throw dg::dg_error(DG_ERR_ARG, "batched solvers must share one model and dimension");
+		dg::BatchBase *impl = nullptr;
+		switch (model) {
+			case DG_EULER: impl = dg::make_batch_euler(v); break;
+			case DG_NAVIER_STOKES: impl = dg::make_batch_ns(v); break;
+			default: impl = dg::make_batch_multi(v); break;
+		}
+		*out = new dg_batch{impl, s[0]->device};
+	});
+}
+
+int dg_batch_step(dg_batch *b, int signal, int *force_break, double *global_dt) {
+	if (!b || !force_break || !global_dt) return DG_ERR_ARG;
+	try {
+		cudaError_t e = cudaSetDevice(b->device);
+		if (e != cudaSuccess) throw dg::dg_error(DG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+		b->impl->step(signal, force_break, global_dt);
+		return DG_OK;
+	} catch (const dg::dg_error &e) {
+		b->impl->last_error = e.what();
+		return e.code;
+	} catch (const std::exception &e) {
+		b->impl->last_error = e.what();
+		return DG_ERR_ARG;
+	}
+}
+
+const char *dg_batch_last_error(dg_batch *b) {
+	if (!b) return g_create_error.c_str();
+	return b->impl->last_error.c_str();
+}
+
+void dg_batch_destroy(dg_batch *b) {
+	if (!b) return;
+	cudaSetDevice(b->device);
+	delete b->impl;
+	delete b;
+}
+
 const char *dg_last_error(dg_solver *s) {
 	if (!s) return g_create_error.c_str();
 	return s->impl->last_error.c_str();

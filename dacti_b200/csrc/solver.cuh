@@ -51,6 +51,7 @@ public:
 	virtual void set_profiling(bool on) = 0;
 	virtual void set_form(int form) = 0;
 	virtual void prepare_noalloc() = 0;  // loads the read-back gather kernel on the current device
+	virtual int model_id() const = 0;
 	std::string last_error;
 };
 
@@ -62,8 +63,12 @@ inline int grid_for(long long n, int max_blocks = 148 * 16) {
 }
 
 template<class M>
+class Batch;
+
+template<class M>
 class Solver : public SolverBase {
 	static constexpr int D = M::D, E = M::E, NC = 1 << D, NF = 2 * D;
+	friend class Batch<M>;
 
 	cudaStream_t st_ = 0;
 	Consts C_{};
@@ -171,8 +176,10 @@ public:
 		limiter_ = c.limiter;
 		setup_consts(c);
 		upload_bcs(c);
-		int cap = c.n_nodes + c.n_nodes / 2 + 1024;
-		alloc_pool(cap);
+		long long cap = (long long) c.n_nodes + c.n_nodes / 2 + 1024;
+		if (c.params[DG_P_POOL_CAP] > 0) cap = std::max((long long) c.params[DG_P_POOL_CAP], (long long) c.n_nodes + 1024);
+		if (cap > 2000000000LL) throw dg_error(DG_ERR_CAPACITY, "node pool capacity above 2e9 slots");
+		alloc_pool((int) cap);
 		alloc_lists(cap);
 		DG_CUDA(cudaMalloc(&d_cnt_, sizeof(Counters)));
 		DG_CUDA(cudaMallocHost(&h_cnt_, sizeof(Counters)));
@@ -228,6 +235,7 @@ public:
 		C_.max_err              = pr[DG_P_MAX_ERR];
 		C_.max_refinement_level = (int) pr[DG_P_MAX_LEVEL];
 		max_dt_cfg_             = pr[DG_P_MAX_DT];
+		pruned_                 = (long long) pr[DG_P_PRUNED];
 		for (int q = 0; q < E; ++q) C_.weights[q] = c.weights[q];
 		ModelConsts &m = C_.m;
 		m.ns_mu = pr[DG_P_NS_MU];
@@ -562,6 +570,15 @@ public:
 
 	double max_dt_cfg_ = 1.0;
 	double max_dt_cfg() const { return max_dt_cfg_; }
+	long long pruned_ = 0;  // node slots the host left out of the upload; part of the reference's tree size
+
+	// The garbage-collection trigger of impl/integrate.hpp:78-84: active leaves in clusters below a fifth
+	// of tree.size() - 1, the tree size counting the slots left out of the upload.
+	bool gc_due() const {
+		long long n_in = 0;
+		for (int l = 0; l < MAX_ACTI; ++l) n_in += h_cnt_->clu[l];
+		return (double) n_in / (double) (h_cnt_->top - 1 + pruned_) < 0.2;
+	}
 
 public:
 	void set_max_dt(double v) { max_dt_cfg_ = v; }
@@ -752,10 +769,8 @@ public:
 				if (fn) fn(user, L, acti_time_[L], (int) n_substeps_, dtL, h_cnt_->clu[L]);
 			}
 		}
-		long long n_in = 0;
-		for (int l = 0; l < MAX_ACTI; ++l) n_in += h_cnt_->clu[l];
 		n_global_++;
-		if ((double) n_in / (double) (h_cnt_->top - 1) < 0.2) gc();
+		if (gc_due()) gc();
 		if (resort_) resort();
 		*global_dt = global_dt_;
 	}
@@ -1034,6 +1049,8 @@ public:
 
 	// Same records as read_cells, gathered through caller-owned device scratch of `bytes` bytes;
 	// allocates nothing.
+	int model_id() const override { return M::ID; }
+
 	void prepare_noalloc() override {
 		cudaFuncAttributes a{};
 		DG_CUDA(cudaFuncGetAttributes(&a, k_gather_cells<M>));
@@ -1080,7 +1097,7 @@ public:
 			o->acti_time[l]    = acti_time_[l];
 			o->acti_counter[l] = acti_counter_[l];
 		}
-		o->tree_size      = h_cnt_->top;
+		o->tree_size      = h_cnt_->top + pruned_;
 		o->n_splits       = n_split_total_;
 		o->n_unsplits     = n_unsplit_total_;
 		o->n_gc           = n_gc_;
@@ -1101,5 +1118,9 @@ public:
 SolverBase *make_solver_euler(const dg_case &c);
 SolverBase *make_solver_ns(const dg_case &c);
 SolverBase *make_solver_multi(const dg_case &c);
+class BatchBase;
+BatchBase *make_batch_euler(const std::vector<SolverBase *> &s);
+BatchBase *make_batch_ns(const std::vector<SolverBase *> &s);
+BatchBase *make_batch_multi(const std::vector<SolverBase *> &s);
 
 }  // namespace dg

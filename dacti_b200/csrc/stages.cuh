@@ -17,6 +17,18 @@ constexpr int BLOCK = 256;
 __device__ __forceinline__ int gtid() { return blockIdx.x * blockDim.x + threadIdx.x; }
 __device__ __forceinline__ int gstride() { return gridDim.x * blockDim.x; }
 
+// Thread index and grid stride of the grid-stride loops of the stage bodies: the launch's own grid, or
+// (batched trees) the range of blocks a launch gives one tree.
+struct PlainGrid {
+	__device__ __forceinline__ int tid() const { return blockIdx.x * blockDim.x + threadIdx.x; }
+	__device__ __forceinline__ int stride() const { return gridDim.x * blockDim.x; }
+};
+struct BlockRange {
+	int first, count;  // blocks [first, first + count) of the launch
+	__device__ __forceinline__ int tid() const { return ((int) blockIdx.x - first) * blockDim.x + threadIdx.x; }
+	__device__ __forceinline__ int stride() const { return count * blockDim.x; }
+};
+
 __device__ __forceinline__ void append(int32_t *list, int *count, int value, int cap, uint32_t *status) {
 	int pos = atomicAdd(count, 1);
 	if (pos < cap) list[pos] = value;
@@ -78,9 +90,13 @@ __device__ __forceinline__ void write_rec_k(const Pool &P, int i) {
 	}
 }
 
+template<class M, class Grid>
+__device__ __forceinline__ void d_rec_k(const Grid &g, const Pool &P, const int32_t *list, int n) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) write_rec_k<M>(P, list[tid]);
+}
 template<class M>
 __global__ void k_rec_k(Pool P, const int32_t *list, int n) {
-	for (int tid = gtid(); tid < n; tid += gstride()) write_rec_k<M>(P, list[tid]);
+	d_rec_k<M>(PlainGrid{}, P, list, n);
 }
 
 // du[dim * G + DT] (temperature gradient along the face normal) for a run-time dim.
@@ -266,12 +282,14 @@ __device__ __forceinline__ int face_owner(const Pool &P, uint32_t *status, int i
 	const int mask = (1 << dim) - 1;
 	const int ca   = (a & mask) | (dn << dim) | ((a >> dim) << (dim + 1));
 	const int ch   = P.child[(size_t) ca * cap + nb];
+	if (ch == 0) return -1;  // left out by the host: an inactive leaf or subtree, which owns no flux
 	const bool ch_leaf = P.flags[ch] & F_LEAF;
 	if (b == 0) return (ch_leaf && P.clu[ch] == L && ai <= P.acti[ch]) ? ch : -1;
 	if (ch_leaf) return -1;
 	const int gb = b - 1;
 	const int cg = (gb & mask) | (dn << dim) | ((gb >> dim) << (dim + 1));
 	const int gc = P.child[(size_t) cg * cap + ch];
+	if (gc == 0) return -1;
 	if (!(P.flags[gc] & F_LEAF)) {
 		set_status(status, ST_DEPTH);
 		return -1;
@@ -291,9 +309,8 @@ __device__ __forceinline__ T *face_flux(const Pool &P, int slot, int f, int nflu
 // running-cluster cells own across its faces. A group of 2D lanes (padded to 4 or 8) serves one
 // cell; lane f walks the owners across face (dim, dir) = (f / 2, f % 2) and the lane sums are
 // combined with a fixed butterfly, so the total does not depend on scheduling.
-template<class M, class T = double>
-__global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *list, const int *n_ptr, int L,
-                                                        Counters *cnt) {
+template<class M, class T = double, class Grid>
+__device__ __forceinline__ void d_flux_receive(const Grid &g, const Pool &P, const int32_t *list, const int *n_ptr, int L, Counters *cnt) {
 	constexpr int NF   = 2 * M::D;
 	constexpr int G    = NF <= 4 ? 4 : 8;
 	constexpr int GW   = 32 / G;
@@ -302,8 +319,8 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
 	const int sub    = lane & (G - 1);
-	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
 		const int slot = wbase + lane / G;
 		double acc[M::F];
@@ -346,6 +363,11 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 		}
 	}
 }
+template<class M, class T = double>
+__global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *list, const int *n_ptr, int L,
+                                                        Counters *cnt) {
+	d_flux_receive<M, T>(PlainGrid{}, P, list, n_ptr, L, cnt);
+}
 
 // flux_update (impl/flux.hpp:11-97) seen from each running-cluster cell: the signed sum of the fluxes
 // that cross its faces in this substep, one group of G lanes per cell (G = 4 in 2D, 8 in 3D; lanes past
@@ -359,15 +381,14 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 // a slower cluster (the coarse-time side of the LTS coupling, impl/flux.hpp:82-91) also goes to the
 // owner's face-flux slot, and that cell joins the receiver list. In the mixed form every flux is rounded
 // to FP32 once, as both sides read it; sums stay FP64.
-template<class M, bool V, class S = double>
-__global__ void __launch_bounds__(BLOCK) k_face_sum(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L,
-                                                    double dtL, int stamp, int32_t *recv, Counters *cnt) {
+template<class M, bool V, class S = double, class Grid>
+__device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int L, double dtL, int stamp, int32_t *recv, Counters *cnt) {
 	constexpr int NF = 2 * M::D, G = NF <= 4 ? 4 : 8, GW = 32 / G, NSUB = 1 << (M::D - 1), F = M::F;
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
 	const int sub    = lane & (G - 1);
-	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
 		const int slot = wbase + lane / G;
 		double acc[F];
@@ -450,18 +471,22 @@ __global__ void __launch_bounds__(BLOCK) k_face_sum(Pool P, Consts C, BcTable B,
 		}
 	}
 }
+template<class M, bool V, class S = double>
+__global__ void __launch_bounds__(BLOCK) k_face_sum(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L,
+                                                    double dtL, int stamp, int32_t *recv, Counters *cnt) {
+	d_face_sum<M, V, S>(PlainGrid{}, P, C, B, list, n, L, dtL, stamp, recv, cnt);
+}
 
 // cell_update (impl/cell_update.hpp:10-90) of the running cluster, one thread per cell: du = (received
 // fluxes + the face sum of k_face_sum) / volume, the multiphase source from the pre-update state, the
 // EOS recovery, floors and the conservative state. The received-flux accumulator is read (and reset)
 // only when the receive stage has marked the cell. Without viscous terms (V = false) the gradient
 // inputs are never read, so t_slope is not maintained.
-template<class M, bool V>
-__global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, int epoch,
-                                                     Counters *cnt) {
+template<class M, bool V, class Grid>
+__device__ __forceinline__ void d_update(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, double dtL, int epoch, Counters *cnt) {
 	constexpr int E = M::E;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i  = list[tid];
 		const int li = P.level[i];
 		const double vol  = C.vol[li];
@@ -525,6 +550,11 @@ __global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int
 		mark_up(P, P.parent[i], epoch);
 	}
 }
+template<class M, bool V>
+__global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, int epoch,
+                                                     Counters *cnt) {
+	d_update<M, V>(PlainGrid{}, P, C, list, n, dtL, epoch, cnt);
+}
 
 
 
@@ -542,11 +572,11 @@ constexpr int32_t NB_LEAF = 1 << 8, NB_PRESENT = 1 << 9;
 __device__ __forceinline__ int nb_level(int32_t code) { return code & 0xff; }
 __device__ __forceinline__ int nb_acti(int32_t code) { return ((code >> 16) & 0xff) - 1; }
 
-template<class M>
-__global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_nbvals(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int epoch, Counters *cnt) {
 	constexpr int E = M::E, NF = 2 * M::D, W = Nbv<M>::W;
 	const long long total = (long long) n * NF;
-	for (long long t = gtid(); t < total; t += gstride()) {
+	for (long long t = g.tid(); t < total; t += g.stride()) {
 		const int slot = (int) (t / NF), f = (int) (t % NF);
 		const int i    = list[slot];
 		const int nb   = P.nbr[(size_t) f * P.cap + i];
@@ -569,6 +599,10 @@ __global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch
 		o[E + 1] = 0.5 * (C.size[P.level[i]] + C.size[ln]);
 		*oi      = NB_PRESENT | ((fl & F_LEAF) ? NB_LEAF : 0) | ln | ((P.acti[nb] + 1) << 16);
 	}
+}
+template<class M>
+__global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch, Counters *cnt) {
+	d_nbvals<M>(PlainGrid{}, P, C, list, n, epoch, cnt);
 }
 
 // compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients (only read by the viscous
@@ -642,12 +676,12 @@ __device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, co
 
 // Slope stage over a cell list, one thread per cell; each thread writes its record's [0, K0) part
 // with 16-byte stores.
-template<class M, bool V>
-__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
+template<class M, bool V, class Grid>
+__device__ __forceinline__ void d_slope(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int lim, Counters *cnt) {
 	using R = Rec<M>;
 	constexpr int K = R::K0;
 	static_assert(K % 2 == 0, "record rows are 16-byte aligned");
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = list[tid];
 		double out[K];
 		compute_slope<M, V>(P, C, B, &cnt->status, lim, i, tid, out);
@@ -655,6 +689,10 @@ __global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n,
 #pragma unroll
 		for (int k = 0; k < K / 2; ++k) dst[k] = make_double2(out[2 * k], out[2 * k + 1]);
 	}
+}
+template<class M, bool V>
+__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
+	d_slope<M, V>(PlainGrid{}, P, C, B, list, n, lim, cnt);
 }
 
 // Recompute the Hancock rhs from the stored slope (used for split parents, whose curvature may
@@ -694,12 +732,11 @@ __device__ bool can_split_at(const Pool &P, const Consts &C, int i) {
 
 // Error estimation and split/unsplit detection (impl/adaptive_refinement.hpp:16-149) with the
 // weighted_laplacian estimator (integrator/error_estimators.hpp:19-37).
-template<class M>
-__global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list,
-                           Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NF = 2 * D;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i  = list[tid];
 		const int li = P.level[i];
 		const double h = C.size[li];
@@ -775,13 +812,18 @@ __global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, 
 		if (op & OP_SPLIT) append(split_list, &cnt->n_split, i, cap, &cnt->status);
 	}
 }
+template<class M>
+__global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list,
+                           Counters *cnt) {
+	d_estimate<M>(PlainGrid{}, P, C, list, n, L, counter_L, split_list, cnt);
+}
 
 // A parent coarsens when all its children are coarsening candidates of this cluster
 // (impl/adaptive_refinement.hpp:198-209); the first child decides.
-template<class M>
-__global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int32_t *unsplit_list, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_unsplit_select(const Grid &g, const Pool &P, const int32_t *list, int n, int L, int32_t *unsplit_list, Counters *cnt) {
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = list[tid];
 		if (!(P.op[i] & OP_UCAND)) continue;
 		const int par = P.parent[i];
@@ -799,14 +841,17 @@ __global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int3
 		if (all) append(unsplit_list, &cnt->n_unsplit, par, cap, &cnt->status);
 	}
 }
+template<class M>
+__global__ void k_unsplit_select(Pool P, const int32_t *list, int n, int L, int32_t *unsplit_list, Counters *cnt) {
+	d_unsplit_select<M>(PlainGrid{}, P, list, n, L, unsplit_list, cnt);
+}
 
 // Domain::split (integrator/domain.hpp:192-247) plus the child set-up of
 // impl/adaptive_refinement.hpp:167-195. Children take the parent's primitive state extrapolated
 // with its slope, reuse the parent's old child slots when it has any, start with a zero Hancock
 // rhs, and join the running cluster.
-template<class M>
-__global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
-                        int epoch, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_split(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh, int epoch, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D, GW = 32 / NC;
 	using R = Rec<M>;
 	const int n      = *n_ptr;
@@ -814,8 +859,8 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 	const int lane   = threadIdx.x & 31;
 	const int c      = lane & (NC - 1);  // the child this lane sets up
 	const int lead   = lane & ~(NC - 1);
-	const int warp   = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-	const int nwarps = (gridDim.x * blockDim.x) >> 5;
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
 	// one group of 2^D lanes per parent: the group's first lane allocates, every lane builds one child
 	for (int base = warp * GW; base < n; base += nwarps * GW) {
 		const int slot    = base + lane / NC;
@@ -899,17 +944,21 @@ __global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split
 		}
 	}
 }
+template<class M>
+__global__ void k_split(Pool P, Consts C, const int *n_ptr, const int32_t *split_list, int L, int32_t *fresh,
+                        int epoch, Counters *cnt) {
+	d_split<M>(PlainGrid{}, P, C, n_ptr, split_list, L, fresh, epoch, cnt);
+}
 
 // Domain::unsplit with interpolated_cell (integrator/domain.hpp:150-180, 296-325): the parent takes
 // the children's mean t, u, k, t_slope and gradient (the gradient sum starts from the parent's own
 // stale gradient, as interpolated_cell does not reset it) and keeps its old slope and rhs.
-template<class M>
-__global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh,
-                          int epoch, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_unsplit(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh, int epoch, Counters *cnt) {
 	constexpr int E = M::E, D = M::D, NC = 1 << D, G = M::G;
 	const int n   = *n_ptr;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int par = unsplit_list[tid];
 		double t = 0.0, u[E], kk[M::P > 0 ? M::P : 1], ts[G > 0 ? G : 1], gr[D * G > 0 ? D * G : 1];
 		for (int q = 0; q < E; ++q) u[q] = 0.0;
@@ -962,6 +1011,11 @@ __global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *uns
 		mark_up(P, P.parent[par], epoch);
 	}
 }
+template<class M>
+__global__ void k_unsplit(Pool P, Consts C, const int *n_ptr, const int32_t *unsplit_list, int L, int32_t *fresh,
+                          int epoch, Counters *cnt) {
+	d_unsplit<M>(PlainGrid{}, P, C, n_ptr, unsplit_list, L, fresh, epoch, cnt);
+}
 
 // Domain::update_neighbors for one active leaf (integrator/domain.hpp:249-293): faces without a
 // boundary get the node found at the same level (or the coarser leaf); a neighbour more than one
@@ -996,6 +1050,7 @@ __device__ void update_face_subtree(const Pool &P, const Consts &C, uint32_t *st
 	stack[sp++] = root;
 	while (sp > 0) {
 		const int x = stack[--sp];
+		if (x == 0) continue;  // a subtree without active leaves that the host left out
 		const uint32_t fl = P.flags[x];
 		if (fl & F_LEAF) {
 			if (fl & F_ACTIVE) update_neighbor_face<M>(P, C, x, dim, dir);
@@ -1022,6 +1077,7 @@ __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_
 	stack[sp++] = root;
 	while (sp > 0) {
 		const int x = stack[--sp];
+		if (x == 0) continue;  // a subtree without active leaves that the host left out
 		const uint32_t fl = P.flags[x];
 		if (fl & F_LEAF) {
 			if (fl & F_ACTIVE) update_neighbors_leaf<M>(P, C, x);
@@ -1040,11 +1096,11 @@ __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_
 // Neighbour repair, first pass (impl/adaptive_refinement.hpp:236-249): new children and coarsened
 // parents, then queue their neighbours for the second pass.
 // Each neighbour is queued once with the mask of its faces towards new cells.
-template<class M>
-__global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *fresh, int32_t *upd, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_nbr_fresh(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *fresh, int32_t *upd, Counters *cnt) {
 	const int n   = *n_ptr;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = fresh[tid];
 		update_neighbors_subtree<M>(P, C, &cnt->status, i);
 		for (int f = 0; f < 2 * M::D; ++f) {
@@ -1055,12 +1111,16 @@ __global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *f
 		}
 	}
 }
+template<class M>
+__global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *fresh, int32_t *upd, Counters *cnt) {
+	d_nbr_fresh<M>(PlainGrid{}, P, C, n_ptr, fresh, upd, cnt);
+}
 
 // Neighbour repair, second pass: the queued neighbours' faces towards new cells.
-template<class M>
-__global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, const int32_t *list, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_nbr_list(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *list, Counters *cnt) {
 	const int n = *n_ptr;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int x       = list[tid];
 		const uint32_t m  = P.fmask[x];
 		for (int f = 0; f < 2 * M::D; ++f)
@@ -1068,16 +1128,19 @@ __global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, const int32_t *li
 		P.fmask[x] = 0;
 	}
 }
+template<class M>
+__global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, const int32_t *list, Counters *cnt) {
+	d_nbr_list<M>(PlainGrid{}, P, C, n_ptr, list, cnt);
+}
 
 // ACTI reassignment (impl/adaptive_refinement.hpp:264-322): per-cell CFL decides whether a cell
 // stays, drops one time level (into the buffer of L-1, only when level L is synchronised with L-1)
 // or rises by floor(log2(cfl/max_cfl))+1 levels.
-template<class M>
-__global__ void k_reassign(Pool P, Consts C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL,
-                           int counter_L, Lists Ls, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL, int counter_L, const Lists &Ls, Counters *cnt) {
 	const int n   = n_ptr ? *n_ptr : n_host;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = list[tid];
 		double p[M::E];
 		load_p<M>(P, i, p);
@@ -1111,17 +1174,26 @@ __global__ void k_reassign(Pool P, Consts C, const int32_t *list, const int *n_p
 		P.cfl[i] = cfl;
 	}
 }
+template<class M>
+__global__ void k_reassign(Pool P, Consts C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL,
+                           int counter_L, Lists Ls, Counters *cnt) {
+	d_reassign<M>(PlainGrid{}, P, C, list, n_ptr, n_host, L, dtL, counter_L, Ls, cnt);
+}
 
 // flush_acti_buffer (impl/acti_utils.hpp:365-372)
-static __global__ void k_flush(Pool P, const int32_t *buf, const int *n_ptr, int32_t *clu_list, int *clu_count, int L,
-                        Counters *cnt) {
+template<class Grid>
+__device__ __forceinline__ void d_flush(const Grid &g, const Pool &P, const int32_t *buf, const int *n_ptr, int32_t *clu_list, int *clu_count, int L, Counters *cnt) {
 	const int n = *n_ptr;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = buf[tid];
 		append(clu_list, clu_count, i, P.cap, &cnt->status);
 		P.acti[i] = (int8_t) L;
 		P.clu[i]  = (int8_t) L;
 	}
+}
+static __global__ void k_flush(Pool P, const int32_t *buf, const int *n_ptr, int32_t *clu_list, int *clu_count, int L,
+                        Counters *cnt) {
+	d_flush(PlainGrid{}, P, buf, n_ptr, clu_list, clu_count, L, cnt);
 }
 
 static __global__ void k_set_count(int *dst, const int *src) { *dst = *src; }
@@ -1364,10 +1436,9 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 // smooth_alpha, one Jacobi sweep (impl/smooth.hpp:10-51): reads the previous sweep's values of the
 // list's cells from `cur` (nullptr for the first sweep: everything from k[ALPHAS]) and writes `out`;
 // the sweeps alternate between two scratch arrays and only the result of the last is stored.
-template<class M>
-__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, const double *cur, double *out,
-                               int Lm, int epoch, int e_upd, Counters *cnt) {
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_smooth_alpha(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, const double *cur, double *out, int Lm, int epoch, int e_upd, Counters *cnt) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i     = list[tid];
 		const double ac = cur ? cur[i] : at(P.k, P.cap, M::ALPHAS, i);
 		double s        = 0.0;
@@ -1380,20 +1451,29 @@ __global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list,
 		out[i] = s / (double) (2 * M::D);
 	}
 }
+template<class M>
+__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, const double *cur, double *out,
+                               int Lm, int epoch, int e_upd, Counters *cnt) {
+	d_smooth_alpha<M>(PlainGrid{}, P, C, B, list, n, cur, out, Lm, epoch, e_upd, cnt);
+}
 
-static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp, const double *src) {
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+template<class Grid>
+__device__ __forceinline__ void d_store_tmp(const Grid &g, const Pool &P, const int32_t *list, int n, int comp, const double *src) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = list[tid];
 		P.k[(size_t) comp * P.cap + i] = src[i];
 	}
 }
+static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp, const double *src) {
+	d_store_tmp(PlainGrid{}, P, list, n, comp, src);
+}
 
 // compute_normal (impl/normal_curvature.hpp:7-55)
-template<class M>
-__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
 	constexpr int D = M::D;
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i = list[tid];
 		double nrm[D];
 		for (int dim = 0; dim < D; ++dim) {
@@ -1413,12 +1493,16 @@ __global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n
 		for (int d = 0; d < D; ++d) kr[1 + d] = nrm[d];
 	}
 }
+template<class M>
+__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
+	d_normal<M>(PlainGrid{}, P, C, B, list, n, epoch, e_upd, cnt);
+}
 
 // compute_curvature (impl/normal_curvature.hpp:59-102)
-template<class M>
-__global__ void k_curvature(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_curvature(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, Counters *cnt) {
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i  = list[tid];
 		double kappa = 0.0;
 		for (int dim = 0; dim < M::D; ++dim) {
@@ -1430,12 +1514,16 @@ __global__ void k_curvature(Pool P, Consts C, BcTable B, const int32_t *list, in
 		P.k[(size_t) M::KAPPA * cap + i] = kappa;
 	}
 }
+template<class M>
+__global__ void k_curvature(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	d_curvature<M>(PlainGrid{}, P, C, B, list, n, cnt);
+}
 
 // smooth_curvature, one weighted sweep into P.tmp (impl/smooth.hpp:63-133)
-template<class M>
-__global__ void k_smooth_kappa(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+template<class M, class Grid>
+__device__ __forceinline__ void d_smooth_kappa(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, Counters *cnt) {
 	const int cap = P.cap;
-	for (int tid = gtid(); tid < n; tid += gstride()) {
+	for (int tid = g.tid(); tid < n; tid += g.stride()) {
 		const int i     = list[tid];
 		const double kc = at(P.k, cap, M::KAPPA, i);
 		const double as = at(P.k, cap, M::ALPHAS, i);
@@ -1473,6 +1561,10 @@ __global__ void k_smooth_kappa(Pool P, Consts C, BcTable B, const int32_t *list,
 		}
 		P.tmp[i] = (w > 1e-6) ? ks / w : 0.0;
 	}
+}
+template<class M>
+__global__ void k_smooth_kappa(Pool P, Consts C, BcTable B, const int32_t *list, int n, Counters *cnt) {
+	d_smooth_kappa<M>(PlainGrid{}, P, C, B, list, n, cnt);
 }
 
 // --------------------------------------------------------------------------------------------

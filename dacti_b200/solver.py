@@ -115,6 +115,12 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_last_error.restype = ctypes.c_char_p
     lib.dg_destroy.argtypes = [vp]
     lib.dg_destroy.restype = None
+    lib.dg_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(vp)]
+    lib.dg_batch_step.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double)]
+    lib.dg_batch_last_error.argtypes = [vp]
+    lib.dg_batch_last_error.restype = ctypes.c_char_p
+    lib.dg_batch_destroy.argtypes = [vp]
+    lib.dg_batch_destroy.restype = None
     _lib = lib
     return lib
 
@@ -125,7 +131,8 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_mlp_last_error", "dg_mlp_create", "dg_mlp_param_count", "dg_mlp_set_params",
                     "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
                     "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
-                    "dg_read_cells_noalloc", "dg_get_stats",
+                    "dg_read_cells_noalloc", "dg_get_stats", "dg_batch_create", "dg_batch_step",
+                    "dg_batch_last_error", "dg_batch_destroy",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
@@ -350,3 +357,43 @@ def step_many(solvers, threads: int = 32, signal: bool = True) -> list:
                 raise DgError(st[k], lib.dg_last_error(solvers[k]._h).decode())
         raise DgError(rc, "dg_step_many failed")
     return [bool(fb[k]) for k in range(n)]
+
+
+class Batch:
+    """dg_batch: independent solvers of one model stepped in lockstep, one launch per stage for all trees
+    that run a level (merged ACTI schedules). Per tree the results equal Solver.integrate's bit for bit.
+    The solvers stay usable for read-backs; step them through the batch only, and close the batch before
+    closing them."""
+
+    def __init__(self, solvers):
+        self._lib = load_library()
+        self.solvers = list(solvers)
+        hs = (ctypes.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
+        h = ctypes.c_void_p()
+        rc = self._lib.dg_batch_create(hs, len(self.solvers), ctypes.byref(h))
+        if rc != DG_OK:
+            raise DgError(rc, self._lib.dg_batch_last_error(None).decode())
+        self._h = h
+
+    def step(self, signal: bool = True) -> list:
+        """One global step of every tree; returns the force_break flags."""
+        n = len(self.solvers)
+        fb = (ctypes.c_int * n)()
+        gdt = (ctypes.c_double * n)()
+        rc = self._lib.dg_batch_step(self._h, 1 if signal else 0, fb, gdt)
+        if rc != DG_OK:
+            raise DgError(rc, self._lib.dg_batch_last_error(self._h).decode())
+        for k, s in enumerate(self.solvers):
+            s.global_dt = gdt[k]
+        return [bool(fb[k]) for k in range(n)]
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dg_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

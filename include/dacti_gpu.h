@@ -46,7 +46,10 @@ enum {
 	DG_P_MAX_ERR = 10, DG_P_MAX_LEVEL = 11, DG_P_MIN_LEVEL = 12, DG_P_GAMMA = 13, DG_P_NS_MU = 14,
 	DG_P_NS_LAMBDA = 15, DG_P_GAMMA1 = 16, DG_P_GAMMA2 = 17, DG_P_P1 = 18, DG_P_P2 = 19, DG_P_CP1 = 20,
 	DG_P_CP2 = 21, DG_P_CV1 = 22, DG_P_CV2 = 23, DG_P_MU1 = 24, DG_P_MU2 = 25, DG_P_LAMBDA1 = 26,
-	DG_P_LAMBDA2 = 27, DG_P_SIGMA = 28, DG_N_PARAMS = 32
+	DG_P_LAMBDA2 = 27, DG_P_SIGMA = 28,
+	/* GPU solver only: node slots the host left out of the upload (subtrees without active leaves), counted
+	 * in the tree size as the reference counts them; node-pool capacity in slots (0: 1.5 x n_nodes) */
+	DG_P_PRUNED = 29, DG_P_POOL_CAP = 30, DG_N_PARAMS = 32
 };
 
 /* node flag bits of dg_case.flags (integrator/node.hpp:60-66) */
@@ -130,6 +133,21 @@ int dg_step(dg_solver *s, int signal, int *force_break, double *global_dt, dg_su
  * a stream of its own. No substep callback. */
 int dg_step_many(dg_solver **solvers, int n, int threads, int signal, int *force_break, double *global_dt,
                  int *status);
+
+/* A batch of independent trees of one model, numeric form and set of viscous/tension terms, stepped in
+ * lockstep by one host thread (the chosen form's batched path; no counterpart in the reference, where
+ * every tree is an Integrator stepped on its own, impl/integrate.hpp:12-87). The trees' ACTI schedules
+ * are merged; each substep of level L launches every stage once for all trees that run L, over block
+ * ranges split among them by work, with one synchronisation per merged substep. Per tree the results
+ * are dg_step's, bit for bit. While in the batch, the solvers run on the batch's stream and keep their
+ * counters in the batch's array: step them through dg_batch_step only, and destroy the batch before
+ * its solvers. */
+typedef struct dg_batch dg_batch;
+int dg_batch_create(dg_solver **solvers, int n, dg_batch **out);
+/* One global step of every tree: force_break[k] and global_dt[k] per tree, as dg_step's. */
+int dg_batch_step(dg_batch *b, int signal, int *force_break, double *global_dt);
+const char *dg_batch_last_error(dg_batch *b);
+void dg_batch_destroy(dg_batch *b);
 
 /* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */
 int dg_cell_count(dg_solver *s, long long *n);

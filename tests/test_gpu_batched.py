@@ -8,7 +8,7 @@ from conftest import run_reference
 from dacti_b200 import cases
 from dacti_b200.casefile import read_snapshot, write_case
 from dacti_b200.parity import compare
-from dacti_b200.solver import Solver, step_many
+from dacti_b200.solver import Batch, Solver, step_many
 
 pytestmark = pytest.mark.gpu
 STEPS = 3
@@ -55,7 +55,7 @@ def test_batched_trees_match_reference(tree, tmp_path):
 def test_batch_extreme_trees_match_reference(tmp_path):
     """The largest (256^2 base, +4 levels) and the smallest (32^2 base, +2 levels) trees of the
     256-tree batch of the batched workload (cases.riemann_batch(256, seed=3)), stepped together with
-    dg_step_many for 2 global steps, against the reference solver on each tree."""
+    the lockstep batch (dg_batch) for 2 global steps, against the reference solver on each tree."""
     from dacti_b200.batch import tree_work
     full = cases.riemann_batch(256, seed=3)
     work = [tree_work(c) for c in full]
@@ -63,13 +63,56 @@ def test_batch_extreme_trees_match_reference(tmp_path):
     assert full[pick[0]].params.min_level == 8 and full[pick[0]].params.max_level == 12
     steps = 2
     solvers = [Solver(full[k]) for k in pick]
+    b = Batch(solvers)
     for _ in range(steps):
-        assert not any(step_many(solvers, threads=2))
+        assert not any(b.step())
+    b.close()
     for s, k in zip(solvers, pick):
         path = str(tmp_path / f"t{k}.case")
         write_case(full[k], path)
         run_reference(path, str(tmp_path / f"t{k}"), steps, [steps])
         ref = read_snapshot(str(tmp_path / f"t{k}_{steps}.snap"))
         rep = compare(ref, s.active_cells(), full[k].params.side_length)
+        assert rep.ok(1e-10), f"tree {k}: {rep}"
+        s.close()
+
+
+def test_lockstep_batch_equals_single_tree_steps():
+    """dg_batch (merged schedules, one launch per stage for all trees) gives every tree's dg_step result
+    bit for bit: cells, ACTI levels, conserved state, counters."""
+    batch = cases.riemann_batch(12, seed=11, base_levels=(4, 6), extra_levels=(2, 3))
+    together = [Solver(c) for c in batch]
+    alone = [Solver(c) for c in batch]
+    b = Batch(together)
+    for _ in range(STEPS):
+        fb_t = b.step()
+        fb_a = [s.integrate()[1] for s in alone]
+        assert fb_t == fb_a
+    b.close()
+    for a, s, c in zip(together, alone, batch):
+        sa, sb = a.active_cells().sorted(c.params.side_length), s.active_cells().sorted(c.params.side_length)
+        assert sa.n == sb.n
+        assert np.array_equal(sa.u, sb.u, equal_nan=True) and np.array_equal(sa.acti_level, sb.acti_level)
+        ta, tb = a.stats(), s.stats()
+        assert ta.cell_updates == tb.cell_updates and ta.n_substeps == tb.n_substeps
+        assert ta.tree_size == tb.tree_size and ta.global_dt == tb.global_dt
+    for s in together + alone:
+        s.close()
+
+
+def test_lockstep_batch_multiphase_matches_reference(tmp_path):
+    """Two five-equation trees of different sizes in one dg_batch against the reference solver."""
+    trees = [cases.shock_drop(base_level=3, levels=2), cases.shock_drop(base_level=4, levels=1)]
+    solvers = [Solver(c) for c in trees]
+    b = Batch(solvers)
+    for _ in range(2):
+        assert not any(b.step())
+    b.close()
+    for k, (s, c) in enumerate(zip(solvers, trees)):
+        path = str(tmp_path / f"m{k}.case")
+        write_case(c, path)
+        run_reference(path, str(tmp_path / f"m{k}"), 2, [2])
+        ref = read_snapshot(str(tmp_path / f"m{k}_2.snap"))
+        rep = compare(ref, s.active_cells(), c.params.side_length)
         assert rep.ok(1e-10), f"tree {k}: {rep}"
         s.close()

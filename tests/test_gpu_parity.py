@@ -111,6 +111,26 @@ def test_periodic_without_refinement(tmp_path):
     _live(cases.periodic_blob(base_level=5, refine=False), 8, [8], tmp_path, "pnr")
 
 
+@pytest.mark.parametrize("which", ["shock_drop", "cylinder"])
+def test_pruned_upload_gives_the_same_results(which):
+    """A tree uploaded without its inactive subtrees (casefile.prune_inactive) steps to the same cells,
+    ACTI levels and conserved state bit for bit, with the same tree size and garbage collections."""
+    from dacti_b200.casefile import prune_inactive
+    case = (cases.shock_drop(base_level=4, levels=2) if which == "shock_drop"
+            else cases.cylinder_ns(mach=0.3, base_level=4, levels=2))
+    steps = 4 if which == "shock_drop" else 12
+    out = []
+    for c in (case, prune_inactive(case)):
+        s = Solver(c)
+        for _ in range(steps):
+            assert not s.integrate()[1]
+        out.append((s.active_cells().sorted(case.params.side_length), s.stats()))
+        s.close()
+    (a, sa), (b, sb) = out
+    assert a.n == b.n and np.array_equal(a.u, b.u) and np.array_equal(a.acti_level, b.acti_level)
+    assert sa.tree_size == sb.tree_size and sa.n_gc == sb.n_gc and sa.cell_updates == sb.cell_updates
+
+
 def test_bitwise_determinism():
     case = read_case(os.path.join(GOLDEN, "multi2.case"))
     a, _ = _run(case, 4, [4])

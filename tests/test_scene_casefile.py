@@ -71,3 +71,29 @@ def test_case_file_roundtrip(tmp_path):
         write_case(c, str(a))
         write_case(read_case(str(a)), str(b))
         assert a.read_bytes() == b.read_bytes()
+
+
+def test_prune_inactive_keeps_every_active_leaf_and_counts_the_rest():
+    """prune_inactive drops exactly the subtrees without an active leaf: the active leaves, their
+    ancestors and their states stay, links stay consistent, and the dropped slots are counted."""
+    import numpy as np
+
+    from dacti_b200 import cases
+    from dacti_b200.casefile import prune_inactive
+
+    for case in (cases.shock_drop(base_level=4, levels=2), cases.cylinder_ns(mach=0.3, base_level=4, levels=2)):
+        t, p = case.tree, prune_inactive(case)
+        q = p.tree
+        assert p.params.pruned_nodes == t.n_nodes - q.n_nodes > 0
+        a, b = t.leaf_mask(), q.leaf_mask()
+        assert a.sum() == b.sum()
+        oa, ob = np.lexsort(t.center[a].T), np.lexsort(q.center[b].T)
+        assert np.array_equal(t.center[a][oa], q.center[b][ob]) and np.array_equal(t.p[a][oa], q.p[b][ob])
+        assert np.array_equal(t.bc[a][oa], q.bc[b][ob]) and np.array_equal(t.level[a][oa], q.level[b][ob])
+        # every kept node's children point back at it; the root's parent is the null slot
+        assert q.parent[1] == 0
+        for c in range(q.children.shape[1]):
+            ch = q.children[:, c]
+            live = ch > 0
+            assert np.array_equal(q.parent[ch[live]], np.nonzero(live)[0])
+        assert p.params.param_vector()[29] == p.params.pruned_nodes
