@@ -20,6 +20,7 @@ oracle/Makefile) on this box's host cores, in bounded samples of the same worklo
 from __future__ import annotations
 
 import argparse
+import dataclasses
 import json
 import os
 import statistics
@@ -56,6 +57,9 @@ def parse_args():
     ap.add_argument("--batch-trees", type=int, default=256, help="trees of the batched 2D Riemann workload")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--scale", action="store_true",
+                    help="also run the scale workload: the shock-drop at 128 x 64 x 64 base, +5 levels (~28M leaves)")
+    ap.add_argument("--scale-steps", type=int, default=1)
     ap.add_argument("--forms", default="fp64,mixed",
                     help="numerical forms to time; `value` is fp64 when it is among them, else the first one")
     ap.add_argument("--profile-substep", type=int, default=-1,
@@ -302,11 +306,12 @@ def timed_run(case, form: str, args, stream, local_rank: int, world: int, profil
 
 
 def learned_run(args, local_rank: int) -> dict:
-    """Regrid forecaster on 2D Navier-Stokes flow past a cylinder (cases.cylinder_ns, base 32 x 16,
-    +3 levels): three training runs with inflow Mach from U(0.2, 0.4) (seeds 11-13), one held-out run
-    (seed 21), 20 global steps each, horizon 8 steps. Reports the network's and persistence's scores
-    on the held-out run, the training time, the prediction rate, and a 16-step forecast-driven run
-    (forecast and coarsening every 8 steps) against the plain regrid."""
+    """Regrid forecaster on 2D Navier-Stokes flow past a cylinder (cases.cylinder_ns: domain 40 x 20,
+    128 x 64 base (the power-of-two grid nearest the stated 80 x 40), +5 levels, Re 200): sixteen
+    training runs with inflow Mach from U(0.2, 0.4) (seeds 11-26), one held-out run (seed 41), 20 global
+    steps each, horizon 8 steps. Reports the network's and persistence's scores on the held-out run, the
+    training time, the prediction rate, and a 16-step forecast-driven run (forecast every 8 steps, the
+    held cells never coarsened, coarsening at every step otherwise) against the plain regrid."""
     import time as _t
 
     from dacti_b200 import cases
@@ -316,10 +321,11 @@ def learned_run(args, local_rank: int) -> dict:
 
     def run(seed):
         mach = float(np.random.default_rng(seed).uniform(0.2, 0.4))
-        return collect(lambda: cases.cylinder_ns(mach=mach, base_level=5, levels=3), 20, 8)
+        return collect(lambda: cases.cylinder_ns(mach=mach, base_level=BASE, levels=LEVELS), 20, 8)
 
-    train = [run(s) for s in (11, 12, 13)]
-    test = run(21)
+    BASE, LEVELS = 7, 5
+    train = [run(s) for s in range(11, 27)]
+    test = run(41)
     t0 = _t.perf_counter()
     net, cut, loss = train_forecaster(train, n_in=15, epochs=30)
     train_s = _t.perf_counter() - t0
@@ -331,7 +337,7 @@ def learned_run(args, local_rank: int) -> dict:
     mlp, base = scores(prob >= cut, truth), scores(test.persistence, truth)
 
     def cyl():
-        return cases.cylinder_ns(mach=0.3, base_level=5, levels=3)
+        return cases.cylinder_ns(mach=0.3, base_level=BASE, levels=LEVELS)
 
     plain, fc = Solver(cyl(), device=local_rank), Solver(cyl(), device=local_rank)
     t0 = _t.perf_counter()
@@ -339,20 +345,20 @@ def learned_run(args, local_rank: int) -> dict:
         plain.integrate()
     plain_s = _t.perf_counter() - t0
     t0 = _t.perf_counter()
-    res = run_with_forecast(fc, net, cut, steps=16, interval=8)
+    res = run_with_forecast(fc, net, cut, steps=16, interval=8, coarsen_every=1)
     fc_s = _t.perf_counter() - t0
     sp = plain.stats()
     err = density_rel_l1(plain.active_cells(), fc.active_cells(), 40.0, (40.0, 20.0), 8, 1)
     plain.close(), fc.close(), net.close()
     keep = ("precision", "recall", "f1")
     return {
-        "workload": "2D Navier-Stokes cylinder, 40 x 20, base 32 x 16 +3 levels, Re 200; 3 training runs, 1 held-out",
+        "workload": "2D Navier-Stokes cylinder, 40 x 20, base 128 x 64 +5 levels, Re 200; 16 training runs, 1 held-out",
         "network": "15 -> 64 -> 64 -> 1, BF16 inference weights, FP32 master + Adam",
         "held_out": {"samples": int(truth.size), "positive_rate": float(truth.mean()), "cut": cut,
                      "forecaster": {k: mlp[k] for k in keep}, "persistence": {k: base[k] for k in keep}},
         "train_seconds": train_s, "train_samples": int(sum(r.y.size for r in train)), "last_epoch_loss": loss,
         "predict_samples_per_s": truth.size / pred_s,
-        "regrid": {"steps": 16, "interval": 8,
+        "regrid": {"steps": 16, "interval": 8, "coarsen_every": 1,
                    "plain": {"splits": sp.n_splits, "unsplits": sp.n_unsplits, "cell_updates": sp.cell_updates,
                              "seconds": plain_s},
                    "forecast": {"splits": res["splits"], "unsplits": res["unsplits"], "held": res["held"],
@@ -444,6 +450,93 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     }
 
 
+def scale_run(args, local_rank: int) -> dict:
+    """The scale workload: the five-equation shock-drop of the bench at twice the base resolution per axis
+    (128 x 64 x 64) and one more level (+5; finest cells 2 um), built on the device
+    (scene_build.cu), uploaded without the subtrees that hold no active leaf (casefile.prune_inactive;
+    results unchanged), then one warm-up and `scale_steps` timed global steps of the FP64 form with CUDA
+    events. Reports cells, node slots, the device memory in use after construction and its high-water
+    mark over the steps (free memory sampled after every step)."""
+    import torch
+    from dacti_b200 import cases
+    from dacti_b200.casefile import Case, prune_inactive
+    from dacti_b200.scene_gpu import build_tree_device
+    from dacti_b200.solver import Solver
+
+    torch.cuda.synchronize()
+    free0, total = torch.cuda.mem_get_info()
+    t0 = time.perf_counter()
+    spec, prm = cases.shock_drop_spec(base_level=7, levels=5)
+    tree = build_tree_device(spec)
+    n_full = tree.n_nodes
+    case = prune_inactive(Case(tree, prm))
+    del tree
+    n_kept = case.tree.n_nodes
+    leaves = int(case.tree.leaf_mask().sum())
+    # a pool of 1.6 x the uploaded nodes; the solver grows it when splits need more
+    case.params = dataclasses.replace(case.params, pool_capacity=int(n_kept * 1.6) + 1024)
+    t1 = time.perf_counter()
+    s = Solver(case, device=local_rank)
+    del case
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    free1, _ = torch.cuda.mem_get_info()
+    low = free1
+    s.integrate()
+    torch.cuda.synchronize()
+    low = min(low, torch.cuda.mem_get_info()[0])
+    u0 = s.stats().cell_updates
+    ms = 0.0
+    for _ in range(args.scale_steps):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.integrate()
+        b.record()
+        torch.cuda.synchronize()
+        ms += a.elapsed_time(b)
+        low = min(low, torch.cuda.mem_get_info()[0])
+    st = s.stats()
+    cells = s.n_active_cells()
+    s.close()
+    upd = float(st.cell_updates - u0)
+    return {
+        "workload": "shock_drop_3d multi<3> 128x64x64 base +5 levels, LTS, FP64 (the scale configuration)",
+        "nodes_built": int(n_full), "nodes_uploaded": int(n_kept), "initial_active_leaves": leaves,
+        "active_cells": int(cells), "tree_size": int(st.tree_size), "steps": args.scale_steps,
+        "value": upd / (ms * 1e-3) if ms > 0 else None, "unit": UNIT, "ms_per_step": ms / max(args.scale_steps, 1),
+        "build_s": t1 - t0, "construct_s": t2 - t1,
+        "device_gb_after_construction": (free0 - free1) / 1e9, "device_gb_high_water": (free0 - low) / 1e9,
+        "device_gb_total": total / 1e9,
+        "bytes_per_active_leaf_high_water": (free0 - low) / max(cells, 1),
+    }
+
+
+END_TIME = 2e-6  # the shock-drop configuration runs to 2 us
+
+
+def end_time_accuracy(case, form: str, level: int, t_end: float, device: int) -> dict:
+    """The form's error against the FP64 form at the configuration's end time: both run from the initial
+    state over the same global steps until the time reaches t_end (the reference driver's last step is
+    the first at or past t_end, driver/default_driver.hpp:197-213)."""
+    from dacti_b200.solver import Solver
+    out = {}
+    for f in ("fp64", form):
+        s = Solver(case, device=device)
+        s.set_form(f)
+        t, n = 0.0, 0
+        while t < t_end:
+            gdt, fb = s.integrate()
+            t += gdt
+            n += 1
+            if fb:
+                break
+        out[f] = (s.active_cells(), t, n)
+        s.close()
+    acc = form_accuracy(out[form][0], out["fp64"][0], case, level)
+    acc["horizon"] = f"t = {out['fp64'][1]:.3e} s after {out['fp64'][2]} global steps (end time {t_end:g} s)"
+    return acc
+
+
 def form_accuracy(snap, ref, case, level: int) -> dict:
     """Error of one form's solution against the FP64 form's after the same steps: mixture-density and
     per-component relative L1 on the uniform grid of `level` (conservative projection), and the cells
@@ -496,11 +589,11 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     ms_max, total_updates = reduce_ranks(plain["ms"], plain["updates"], world)
     value = total_updates / (ms_max * 1e-3)
 
-    # Roofline of the cell-update kernel (k_gather_update: face-flux gather fused with the conservative
-    # update, EOS recovery and floors): algorithmic bytes per leaf cell-update (16 E + 8 D + 12: U read
-    # and written in FP64, 2D neighbour ids, level and time) times the cells of its launches, over its
-    # CUDA-event time on the solver's stream. `traffic` is the DRAM bytes per launch from the committed
-    # ncu summary of the same kernel, scaled to this run's cells per launch.
+    # Roofline of the cell-update kernel (k_update: the conservative update from the face-flux sums and
+    # received fluxes, source, EOS recovery and floors): algorithmic bytes per leaf cell-update (16 E +
+    # 8 D + 12: U read and written in FP64, 2D neighbour ids, level and time) times the cells of its
+    # launches, over its CUDA-event time on the solver's stream. `traffic` is the DRAM bytes per launch
+    # from the committed ncu summary of the same kernel, scaled to this run's cells per launch.
     peak, peak_kind = measured_peak()
     kms, kl, kc = plain["kms"], plain["kl"], plain["kc"]
     dom = max(kms, key=lambda k: kms[k])
@@ -509,15 +602,15 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     launches = max(kl["update"], 1)
     achieved = (b_per * kc["update"] / launches) / (upd_ms * 1e-3 / launches) / 1e9 if upd_ms > 0 else 0.0
     traffic = None
-    tpath = os.path.join(HERE, "profiles", "gather_update_shock_drop_3d_small.md")
+    tpath = os.path.join(HERE, "profiles", "stage_kernels_shock_drop_3d_small.md")
     if os.path.exists(tpath):
         with open(tpath) as f:
             for line in f:
-                if line.startswith("fp64_dram_bytes_per_cell"):
+                if line.startswith("k_update_dram_bytes_per_cell"):
                     traffic = float(line.split("=")[1]) * (kc["update"] / launches)
     step_achieved = b_per * plain["updates"] / (plain["ms"] * 1e-3) / 1e9
     roofline = {
-        "bound": "hbm", "kernel": "k_gather_update (face-flux gather + cell update)", "achieved": achieved,
+        "bound": "hbm", "kernel": "k_update (conservative cell update)", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
         "bytes_per_cell_update": b_per, "launches": kl["update"], "avg_launch_us": 1e3 * upd_ms / launches,
         "whole_step": {"achieved": step_achieved, "frac": step_achieved / peak},
@@ -540,11 +633,12 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         other = runs[f]
         o_ms, o_upd = reduce_ranks(other["ms"], other["updates"], world)
         acc = form_accuracy(other["snap"], plain["snap"], case, args.base_level)
-        acc["horizon"] = f"after {args.warmup + args.steps + 1} global steps from the initial state"
+        acc["horizon"] = f"after {args.warmup + args.steps + 1} global steps from the initial state (the timed run's end)"
         result["chosen_over_plain"] = {
             "form": "mixed: FP32 reconstruction + HLLC flux, FP64 update, totals and EOS recovery" if f == "mixed" else f,
             "value": o_upd / (o_ms * 1e-3), "ms_per_step": o_ms / args.steps, "gpu_launches": other["launches"],
             "ratio_to_plain": (o_upd / o_ms) / (total_updates / ms_max), "clocks": other["clocks"],
+            "accuracy_at_end_time": end_time_accuracy(case, f, args.base_level, END_TIME, local_rank),
             "accuracy": acc,
         }
 
@@ -584,6 +678,11 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         result["batched"] = batched_run(args, rank, local_rank, world)
     if not args.no_learned and world == 1:
         result["learned"] = learned_run(args, local_rank)
+    if args.scale and world == 1:
+        try:
+            result["scale"] = scale_run(args, local_rank)
+        except Exception as e:  # reported in the line, the other sections stand
+            result["scale"] = {"error": str(e)[:300]}
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_RUNNER):
         threads = host_threads()

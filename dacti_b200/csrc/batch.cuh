@@ -46,6 +46,7 @@ __device__ __forceinline__ int tree_of_block(const int *off, int nt) {
 }
 
 #define DG_BATCH_PROLOGUE                                     \
+	if ((int) blockIdx.x >= off[nt]) return;                  \
 	const int t_ = tree_of_block(off, nt);                    \
 	const TreeArgs &a = A[t_];                                \
 	const BlockRange g{off[t_], off[t_ + 1] - off[t_]};
@@ -60,7 +61,7 @@ static __global__ void kb_zero_counters(const TreeArgs *A, int nt) {
 }
 
 template<class M, bool V, class S>
-__global__ void __launch_bounds__(BLOCK) kb_face_sum(const TreeArgs *A, const int *off, int nt) {
+__global__ void __launch_bounds__(BLOCK, 2) kb_face_sum(const TreeArgs *A, const int *off, int nt) {
 	DG_BATCH_PROLOGUE
 	d_face_sum<M, V, S>(g, a.P, *a.C, a.B, a.list, a.n, a.L, a.dtL, a.stamp, a.Ls.recv, a.cnt);
 }
@@ -77,28 +78,24 @@ __global__ void __launch_bounds__(BLOCK, 2) kb_update(const TreeArgs *A, const i
 	d_update<M, V>(g, a.P, *a.C, a.list, a.n, a.dtL, a.epoch0 + 1, a.cnt);
 }
 
-template<class M>
-__global__ void kb_nbvals(const TreeArgs *A, const int *off, int nt) {
-	DG_BATCH_PROLOGUE
-	d_nbvals<M>(g, a.P, *a.C, a.list, a.n, a.epoch0 + 2, a.cnt);
-}
-
 template<class M, bool V>
-__global__ void kb_slope(const TreeArgs *A, const int *off, int nt) {
+__global__ void __launch_bounds__(BLOCK) kb_slope(const TreeArgs *A, const int *off, int nt) {
 	DG_BATCH_PROLOGUE
-	d_slope<M, V>(g, a.P, *a.C, a.B, a.list, a.n, a.limiter, a.cnt);
+	d_slope<M, V>(g, a.P, *a.C, a.B, a.list, a.n, a.limiter, a.epoch0 + 2, a.cnt);
 }
 
 // Multiphase auxiliary stages; `k` selects the stage in the order of Solver::multiphase_aux.
 template<class M>
-__global__ void kb_aux(const TreeArgs *A, const int *off, int nt, int k) {
+__global__ void __launch_bounds__(BLOCK) kb_aux(const TreeArgs *A, const int *off, int nt, int k) {
 	DG_BATCH_PROLOGUE
 	const int e_upd = a.epoch0 + 1;
 	switch (k) {
 		case 0: d_smooth_alpha<M>(g, a.P, *a.C, a.B, a.list, a.n, nullptr, a.P.tmp, a.L, a.epoch0 + 3, e_upd, a.cnt); break;
 		case 1: d_smooth_alpha<M>(g, a.P, *a.C, a.B, a.list, a.n, a.P.tmp, a.P.tmp2, a.L, a.epoch0 + 4, e_upd, a.cnt); break;
-		case 2: d_smooth_alpha<M>(g, a.P, *a.C, a.B, a.list, a.n, a.P.tmp2, a.P.tmp, a.L, a.epoch0 + 5, e_upd, a.cnt); break;
-		case 3: d_store_tmp(g, a.P, a.list, a.n, M::ALPHAS, a.P.tmp); break;
+		case 2:
+			d_smooth_alpha<M>(g, a.P, *a.C, a.B, a.list, a.n, a.P.tmp2, a.P.k + (size_t) M::ALPHAS * a.P.cap, a.L, a.epoch0 + 5,
+			                  e_upd, a.cnt);
+			break;
 		case 4: d_normal<M>(g, a.P, *a.C, a.B, a.list, a.n, a.epoch0 + 6, e_upd, a.cnt); break;
 		case 5: d_curvature<M>(g, a.P, *a.C, a.B, a.list, a.n, a.cnt); break;
 		case 6: d_smooth_kappa<M>(g, a.P, *a.C, a.B, a.list, a.n, a.cnt); break;
@@ -107,24 +104,26 @@ __global__ void kb_aux(const TreeArgs *A, const int *off, int nt, int k) {
 	}
 }
 
+// Epochs of one substep in the tree's own sequence (Solver::substep): update + 1, slope + 2, the four
+// multiphase sweeps + 3 .. + 6, then the estimate, the split and the unsplit.
 template<class M>
-__global__ void kb_estimate(const TreeArgs *A, const int *off, int nt) {
+constexpr int EPOCH_EST = M::MULTI ? 7 : 3;
+
+template<class M>
+__global__ void __launch_bounds__(BLOCK) kb_estimate(const TreeArgs *A, const int *off, int nt) {
 	DG_BATCH_PROLOGUE
-	d_estimate<M>(g, a.P, *a.C, a.list, a.n, a.L, a.counterL, a.Ls.split, a.cnt);
+	d_estimate<M>(g, a.P, *a.C, a.list, a.n, a.L, a.counterL, a.epoch0 + EPOCH_EST<M>, a.Ls.split, a.cnt);
 }
 
-// Regrid and reassignment stages in the order of Solver::substep; `k` selects the stage. The epochs
-// follow the tree's own sequence: the update, the neighbour values and (multiphase) four auxiliary
-// sweeps come first, so split and unsplit use epoch0 + 3 and + 4 (+ 7 and + 8 with the multiphase
-// sweeps).
+// Regrid and reassignment stages in the order of Solver::substep; `k` selects the stage.
 template<class M>
 __global__ void kb_regrid(const TreeArgs *A, const int *off, int nt, int k) {
 	DG_BATCH_PROLOGUE
-	constexpr int EX = M::MULTI ? 4 : 0;
+	constexpr int EX = EPOCH_EST<M>;
 	switch (k) {
 		case 0: d_unsplit_select<M>(g, a.P, a.list, a.n, a.L, a.Ls.unsplit, a.cnt); break;
-		case 1: d_split<M>(g, a.P, *a.C, &a.cnt->n_split, a.Ls.split, a.L, a.Ls.fresh, a.epoch0 + 3 + EX, a.cnt); break;
-		case 2: d_unsplit<M>(g, a.P, *a.C, &a.cnt->n_unsplit, a.Ls.unsplit, a.L, a.Ls.fresh, a.epoch0 + 4 + EX, a.cnt); break;
+		case 1: d_split<M>(g, a.P, *a.C, &a.cnt->n_split, a.Ls.split, a.L, a.Ls.fresh, a.epoch0 + EX + 1, a.cnt); break;
+		case 2: d_unsplit<M>(g, a.P, *a.C, &a.cnt->n_unsplit, a.Ls.unsplit, a.L, a.Ls.fresh, a.epoch0 + EX + 2, a.cnt); break;
 		case 3: d_nbr_fresh<M>(g, a.P, *a.C, &a.cnt->n_new, a.Ls.fresh, a.Ls.upd, a.cnt); break;
 		case 4: d_nbr_list<M>(g, a.P, *a.C, &a.cnt->n_upd, a.Ls.upd, a.cnt); break;
 		case 5: d_reassign<M>(g, a.P, *a.C, a.list, nullptr, a.n, a.L, a.dtL, a.counterL, a.Ls, a.cnt); break;
@@ -150,18 +149,27 @@ static __global__ void kb_flush_done(const TreeArgs *A, int nt) {
 
 #undef DG_BATCH_PROLOGUE
 
+// Stage kinds of a merged substep, each with its own launch budget (blocks per SM) and timing.
+enum BatchStage : int {
+	BS_FACE_SUM = 0, BS_RECEIVE, BS_UPDATE, BS_SLOPE, BS_AUX, BS_ESTIMATE, BS_REGRID_CELL, BS_REGRID_FRESH,
+	BS_NBR_LIST, BS_FLUSH, BS_N
+};
+
 class BatchBase {
 public:
 	virtual ~BatchBase() = default;
 	virtual void step(int signal, int *force_break, double *global_dt) = 0;
 	virtual int size() const = 0;
+	virtual void set_launch(const int *blocks_per_sm, int n) = 0;
+	virtual void set_profiling(bool on) = 0;
+	virtual void stage_times(double *ms, long long *items, int n) = 0;
 	std::string last_error;
 };
 
 template<class M>
 class Batch : public BatchBase {
 	static constexpr int D = M::D, NC = 1 << D, NF = 2 * D;
-	static constexpr int EPOCHS = M::MULTI ? 8 : 4;  // epoch numbers one substep uses per tree
+	static constexpr int EPOCHS = EPOCH_EST<M> + 2;  // epoch numbers one substep uses per tree
 	std::vector<Solver<M> *> s_;
 	cudaStream_t st_      = nullptr;
 	Counters *d_cnt_      = nullptr;  // all trees' counters
@@ -172,7 +180,19 @@ class Batch : public BatchBase {
 	int *d_off_           = nullptr, *h_off_ = nullptr;
 	int n_off_sets_       = 0;
 	int device_           = 0;
+	int sms_              = 148;
 	bool mixed_ = false, visc_ = false, sigma_ = false;
+	int bps_[BS_N];  // launch budget per stage kind: blocks per SM
+	bool prof_ = false;
+	struct Timed {
+		int stage;
+		cudaEvent_t a, b;
+		long long items;
+	};
+	std::vector<Timed> timed_;
+	std::vector<cudaEvent_t> ev_free_;
+	double stage_ms_[BS_N]       = {};
+	long long stage_items_[BS_N] = {};
 
 	static constexpr int OFF_SETS = 24;  // block-offset arrays one substep may use
 
@@ -191,7 +211,9 @@ public:
 			if (s->mixed_ != mixed_ || s->visc_ != visc_ || s->sigma_ != sigma_)
 				throw dg_error(DG_ERR_ARG, "batched solvers must share the numeric form and the viscous/tension terms");
 		const int nt = (int) s_.size();
+		for (int k = 0; k < BS_N; ++k) bps_[k] = 16;
 		DG_CUDA(cudaGetDevice(&device_));
+		DG_CUDA(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
 		DG_CUDA(cudaStreamCreateWithFlags(&st_, cudaStreamNonBlocking));
 		DG_CUDA(cudaMalloc(&d_cnt_, sizeof(Counters) * nt));
 		DG_CUDA(cudaMallocHost(&h_cnt_, sizeof(Counters) * nt));
@@ -232,15 +254,81 @@ public:
 		cudaFreeHost(h_args_);
 		cudaFree(d_off_);
 		cudaFreeHost(h_off_);
+		for (auto &t: timed_) cudaEventDestroy(t.a), cudaEventDestroy(t.b);
+		for (auto e: ev_free_) cudaEventDestroy(e);
 		cudaStreamDestroy(st_);
 	}
 
 	int size() const override { return (int) s_.size(); }
 
+	void set_launch(const int *bps, int n) override {
+		for (int k = 0; k < n && k < BS_N; ++k)
+			if (bps[k] < 1 || bps[k] > 64) throw dg_error(DG_ERR_ARG, "blocks per SM must lie in [1, 64]");
+		for (int k = 0; k < n && k < BS_N; ++k) bps_[k] = bps[k];
+	}
+
+	void set_profiling(bool on) override { prof_ = on; }
+
+	// Device time and work items per stage kind since the last call (profiling on), then reset.
+	void stage_times(double *ms, long long *items, int n) override {
+		drain();
+		for (int k = 0; k < n && k < BS_N; ++k) {
+			ms[k]           = stage_ms_[k];
+			items[k]        = stage_items_[k];
+			stage_ms_[k]    = 0.0;
+			stage_items_[k] = 0;
+		}
+	}
+
 private:
+	cudaEvent_t event() {
+		if (ev_free_.empty()) {
+			cudaEvent_t e;
+			DG_CUDA(cudaEventCreate(&e));
+			return e;
+		}
+		cudaEvent_t e = ev_free_.back();
+		ev_free_.pop_back();
+		return e;
+	}
+
+	void drain() {
+		for (auto &t: timed_) {
+			float ms = 0.f;
+			DG_CUDA(cudaEventSynchronize(t.b));
+			DG_CUDA(cudaEventElapsedTime(&ms, t.a, t.b));
+			stage_ms_[t.stage] += ms;
+			stage_items_[t.stage] += t.items;
+			ev_free_.push_back(t.a);
+			ev_free_.push_back(t.b);
+		}
+		timed_.clear();
+	}
+
 	void sync() {
 		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters) * s_.size(), cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
+		if (prof_) drain();
+	}
+
+	// One launch of a stage over the trees of `sel`: block offsets in proportion to `items` within the
+	// stage's budget; `launch(grid, offsets)` issues the kernel; timed with events when profiling.
+	template<class F>
+	void stage(int kind, const std::vector<int> &sel, const std::vector<long long> &items, F &&launch) {
+		auto o = offsets(sel, items, sms_ * bps_[kind]);
+		cudaEvent_t a = nullptr, b = nullptr;
+		if (prof_) {
+			a = event();
+			b = event();
+			DG_CUDA(cudaEventRecord(a, st_));
+		}
+		launch(o.second, o.first);
+		if (prof_) {
+			DG_CUDA(cudaEventRecord(b, st_));
+			long long tot = 0;
+			for (auto v: items) tot += v;
+			timed_.push_back({kind, a, b, tot});
+		}
 	}
 
 	// Block offsets of one stage: tree k of `sel` gets blocks in proportion to its items (at least one),
@@ -310,36 +398,38 @@ private:
 		};
 		constexpr int G = NF <= 4 ? 4 : 8;
 		kb_zero_counters<<<nt, 32, 0, st_>>>(d_args_, nt);
-		{
-			auto o = offsets(sel, scaled(G));
+		const auto lanes = scaled(G), cells = scaled(1), fresh = scaled(NC + 1), repair = scaled((NC + 1) * NF);
+		stage(BS_FACE_SUM, sel, lanes, [&](int grid, const int *off) {
 			if (mixed_) {
-				if (visc_) kb_face_sum<M, true, float><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
-				else kb_face_sum<M, false, float><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
+				if (visc_) kb_face_sum<M, true, float><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+				else kb_face_sum<M, false, float><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
 			} else {
-				if (visc_) kb_face_sum<M, true, double><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
-				else kb_face_sum<M, false, double><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
+				if (visc_) kb_face_sum<M, true, double><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+				else kb_face_sum<M, false, double><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+			}
+		});
+		stage(BS_RECEIVE, sel, lanes, [&](int grid, const int *off) {
+			if (mixed_) kb_flux_receive<M, float><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+			else kb_flux_receive<M, double><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+		});
+		stage(BS_UPDATE, sel, cells, [&](int grid, const int *off) {
+			if (visc_) kb_update<M, true><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+			else kb_update<M, false><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+		});
+		stage(BS_SLOPE, sel, lanes, [&](int grid, const int *off) {
+			if (visc_) kb_slope<M, true><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+			else kb_slope<M, false><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt);
+		});
+		if constexpr (M::MULTI) {
+			// the smoothing sweeps and the normal run a lane group per cell, the curvature stages a thread
+			for (int k = 0; k < (sigma_ ? 9 : 5); ++k) {
+				if (k == 3) continue;  // the last sweep writes k[ALPHAS] itself
+				stage(BS_AUX, sel, k <= 4 ? lanes : cells,
+				      [&](int grid, const int *off) { kb_aux<M><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt, k); });
 			}
 		}
-		{
-			auto o = offsets(sel, scaled(G));
-			if (mixed_) kb_flux_receive<M, float><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
-			else kb_flux_receive<M, double><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
-		}
-		auto per_cell = offsets(sel, scaled(1));
-		if (visc_) kb_update<M, true><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt);
-		else kb_update<M, false><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt);
-		{
-			auto o = offsets(sel, scaled(NF));
-			kb_nbvals<M><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt);
-		}
-		if (visc_) kb_slope<M, true><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt);
-		else kb_slope<M, false><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt);
-		if constexpr (M::MULTI) {
-			for (int k = 0; k < 5; ++k) kb_aux<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt, k);
-			if (sigma_)
-				for (int k = 5; k < 9; ++k) kb_aux<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt, k);
-		}
-		kb_estimate<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt);
+		stage(BS_ESTIMATE, sel, lanes,
+		      [&](int grid, const int *off) { kb_estimate<M><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt); });
 		if (any_tight) {
 			// split requests back; a tree whose pool cannot take them grows (Solver::substep)
 			sync();
@@ -360,17 +450,16 @@ private:
 			}
 			if (grown) upload_args(sel);
 		}
-		kb_regrid<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt, 0);
-		auto fresh = offsets(sel, scaled(NC + 1));
-		kb_regrid<M><<<fresh.second, BLOCK, 0, st_>>>(d_args_, fresh.first, nt, 1);
-		kb_regrid<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt, 2);
-		kb_regrid<M><<<fresh.second, BLOCK, 0, st_>>>(d_args_, fresh.first, nt, 3);
-		{
-			auto o = offsets(sel, scaled((NC + 1) * NF));
-			kb_regrid<M><<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, nt, 4);
-		}
-		kb_regrid<M><<<per_cell.second, BLOCK, 0, st_>>>(d_args_, per_cell.first, nt, 5);
-		kb_regrid<M><<<fresh.second, BLOCK, 0, st_>>>(d_args_, fresh.first, nt, 6);
+		auto regrid = [&](int kind, const std::vector<long long> &items, int k) {
+			stage(kind, sel, items, [&](int grid, const int *off) { kb_regrid<M><<<grid, BLOCK, 0, st_>>>(d_args_, off, nt, k); });
+		};
+		regrid(BS_REGRID_CELL, cells, 0);   // unsplit selection
+		regrid(BS_REGRID_FRESH, fresh, 1);  // split
+		regrid(BS_REGRID_CELL, cells, 2);   // unsplit
+		regrid(BS_REGRID_FRESH, fresh, 3);  // neighbour repair, first pass
+		regrid(BS_NBR_LIST, repair, 4);     // neighbour repair, second pass
+		regrid(BS_REGRID_CELL, cells, 5);   // reassignment of the cluster
+		regrid(BS_REGRID_FRESH, fresh, 6);  // reassignment of new cells
 		for (int k = 0; k < nt; ++k) std::swap(s_[sel[k]]->Ls_.clu[L], s_[sel[k]]->Ls_.tmp);
 		kb_set_count<<<(nt + 127) / 128, 128, 0, st_>>>(d_args_, nt);
 		DG_CUDA(cudaGetLastError());
@@ -398,8 +487,8 @@ private:
 			h[k].L       = L;
 		}
 		upload_args(fl);
-		auto o = offsets(fl, items);
-		kb_flush<<<o.second, BLOCK, 0, st_>>>(d_args_, o.first, (int) fl.size());
+		stage(BS_FLUSH, fl, items,
+		      [&](int grid, const int *off) { kb_flush<<<grid, BLOCK, 0, st_>>>(d_args_, off, (int) fl.size()); });
 		kb_flush_done<<<((int) fl.size() + 127) / 128, 128, 0, st_>>>(d_args_, (int) fl.size());
 		DG_CUDA(cudaGetLastError());
 	}

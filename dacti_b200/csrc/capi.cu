@@ -28,6 +28,23 @@ int guarded(dg_solver *s, Fn &&fn) {
 		return DG_ERR_ARG;
 	}
 }
+
+template<typename Fn>
+int batch_guarded(dg_batch *b, Fn &&fn) {
+	if (!b) return DG_ERR_ARG;
+	try {
+		cudaError_t e = cudaSetDevice(b->device);
+		if (e != cudaSuccess) throw dg::dg_error(DG_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+		fn();
+		return DG_OK;
+	} catch (const dg::dg_error &e) {
+		b->impl->last_error = e.what();
+		return e.code;
+	} catch (const std::exception &e) {
+		b->impl->last_error = e.what();
+		return DG_ERR_ARG;
+	}
+}
 }  // namespace
 
 extern "C" {
@@ -219,6 +236,20 @@ int dg_batch_step(dg_batch *b, int signal, int *force_break, double *global_dt) 
 		b->impl->last_error = e.what();
 		return DG_ERR_ARG;
 	}
+}
+
+int dg_batch_set_launch(dg_batch *b, const int *bps, int n) {
+	if (!bps || n < 0) return DG_ERR_ARG;
+	return batch_guarded(b, [&] { b->impl->set_launch(bps, n); });
+}
+
+int dg_batch_set_profiling(dg_batch *b, int on) {
+	return batch_guarded(b, [&] { b->impl->set_profiling(on != 0); });
+}
+
+int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n) {
+	if (!ms || !items || n < 0) return DG_ERR_ARG;
+	return batch_guarded(b, [&] { b->impl->stage_times(ms, items, n); });
 }
 
 const char *dg_batch_last_error(dg_batch *b) {

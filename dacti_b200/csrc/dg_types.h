@@ -121,8 +121,6 @@ struct Pool {
 	double *ff;       // [slot][2D][F] flux of each owned face next to a receiver (by the owner's list position)
 	double *du;       // [slot][F] face-flux sum of each running-cluster cell (by list position)
 	int32_t *pos;     // [cap] list position of each running-cluster cell, written by the face-sum stage
-	double *nbv;      // [slot][2D][NW] neighbour values of the running list's cells (p, t, centre distance)
-	int32_t *nbi;     // [slot][2D] neighbour level, leaf flag, presence and ACTI level
 };
 
 // Device counters, copied back to the host after each substep.

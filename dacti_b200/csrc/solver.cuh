@@ -88,8 +88,6 @@ class Solver : public SolverBase {
 	double *ff_mem_    = nullptr;  // face fluxes next to receivers (Pool::ff)
 	double *du_mem_    = nullptr;  // face-flux sums of the running cluster (Pool::du)
 	int32_t *pos_mem_  = nullptr;  // list positions of the running cluster's cells (Pool::pos)
-	double *nbv_mem_   = nullptr;  // neighbour values (Pool::nbv)
-	int32_t *nbi_mem_  = nullptr;  // neighbour facts (Pool::nbi)
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
 	double *d_read_    = nullptr;
 	int32_t *d_readlv_ = nullptr;
@@ -197,8 +195,6 @@ public:
 		cudaFree(bc_mem_);
 		cudaFree(ff_mem_);
 		cudaFree(du_mem_);
-		cudaFree(nbv_mem_);
-		cudaFree(nbi_mem_);
 		cudaFree(pos_mem_);
 		cudaFree(d_cnt_);
 		cudaFreeHost(h_cnt_);
@@ -379,7 +375,7 @@ public:
 
 	// Per-substep scratch. By pool slot: pos (a running-cluster cell's list position). By list position,
 	// sized to the largest list a substep has run so far (grown by a quarter when a larger one comes):
-	// receiver face fluxes, face-flux sums, neighbour values and facts.
+	// receiver face fluxes and face-flux sums.
 	void alloc_derived(int cap) {
 		cudaFree(pos_mem_);
 		pos_mem_ = nullptr;
@@ -393,17 +389,11 @@ public:
 		const long long want = std::max(std::max(n, scratch_cap_ + scratch_cap_ / 4), 1024LL);
 		cudaFree(ff_mem_);
 		cudaFree(du_mem_);
-		cudaFree(nbv_mem_);
-		cudaFree(nbi_mem_);
 		ff_mem_      = nullptr;
 		du_mem_      = nullptr;
-		nbv_mem_     = nullptr;
-		nbi_mem_     = nullptr;
 		scratch_cap_ = 0;
 		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) want));
 		DG_CUDA(cudaMalloc(&du_mem_, sizeof(double) * M::F * (size_t) want));
-		DG_CUDA(cudaMalloc(&nbv_mem_, sizeof(double) * Nbv<M>::W * NF * (size_t) want));
-		DG_CUDA(cudaMalloc(&nbi_mem_, sizeof(int32_t) * NF * (size_t) want));
 		scratch_cap_ = want;
 		attach_derived();
 	}
@@ -411,15 +401,27 @@ public:
 	void attach_derived() {
 		P_.ff   = ff_mem_;
 		P_.du   = du_mem_;
-		P_.nbv  = nbv_mem_;
-		P_.nbi  = nbi_mem_;
 		P_.pos  = pos_mem_;
 	}
 
+	// Grows the node pool: a new pool of new_cap slots takes every field, then the old one goes. Grows
+	// between the indicator and the split of a substep, when the stages that use the list scratch are
+	// done, so the scratch, the spare buffer and the re-sort keys are released first (they come back at
+	// their next use) and the peak holds the two pools and the lists only.
 	void grow_pool(int new_cap) {
+		DG_CUDA(cudaStreamSynchronize(st_));
 		cudaFree(spare_mem_);
 		spare_mem_   = nullptr;
 		spare_bytes_ = 0;
+		cudaFree(sort_mem_);
+		sort_mem_   = nullptr;
+		sort_bytes_ = 0;
+		cudaFree(ff_mem_);
+		cudaFree(du_mem_);
+		ff_mem_      = nullptr;
+		du_mem_      = nullptr;
+		scratch_cap_ = 0;
+		attach_derived();
 		Pool NP{};
 		void *mem = carve_pool(NP, new_cap);
 		auto fo = fields(P_), fn = fields(NP);
@@ -563,6 +565,8 @@ public:
 		DG_CUDA(cudaGetLastError());
 		sync_counters();
 		check_status();
+		cudaFree(d_leaves_);  // the constructor's list of every leaf is not used again
+		d_leaves_ = nullptr;
 		max_acti_ = 0;
 		for (int l = 0; l < MAX_ACTI; ++l)
 			if (h_cnt_->clu[l] > 0) max_acti_ = std::max(max_acti_, l);
@@ -590,18 +594,20 @@ private:
 	// e_upd: epoch of the substep's cell update (0: no memoised volume-fraction means).
 	void multiphase_aux(const int32_t *list, int n, int Lm, int e_upd) {
 		if constexpr (M::MULTI) {
-			const int g = grid_for(n);
+			constexpr int G = NF <= 4 ? 4 : 8;
+			const int g  = grid_for(n);
+			const int gl = grid_for((long long) n * G);
+			double *alphas = P_.k + (size_t) M::ALPHAS * P_.cap;
 			run_k(DG_K_AUX, n, [&] {
-				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, nullptr, P_.tmp, Lm, ++epoch_, e_upd, d_cnt_);
+				k_smooth_alpha<M><<<gl, BLOCK, 0, st_>>>(P_, C_, B_, list, n, nullptr, P_.tmp, Lm, ++epoch_, e_upd, d_cnt_);
 			});
 			run_k(DG_K_AUX, n, [&] {
-				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp, P_.tmp2, Lm, ++epoch_, e_upd, d_cnt_);
+				k_smooth_alpha<M><<<gl, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp, P_.tmp2, Lm, ++epoch_, e_upd, d_cnt_);
 			});
 			run_k(DG_K_AUX, n, [&] {
-				k_smooth_alpha<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp2, P_.tmp, Lm, ++epoch_, e_upd, d_cnt_);
+				k_smooth_alpha<M><<<gl, BLOCK, 0, st_>>>(P_, C_, B_, list, n, P_.tmp2, alphas, Lm, ++epoch_, e_upd, d_cnt_);
 			});
-			run_k(DG_K_AUX, n, [&] { k_store_tmp<<<g, BLOCK, 0, st_>>>(P_, list, n, M::ALPHAS, P_.tmp); });
-			run_k(DG_K_AUX, n, [&] { k_normal<M><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, ++epoch_, e_upd, d_cnt_); });
+			run_k(DG_K_AUX, n, [&] { k_normal<M><<<gl, BLOCK, 0, st_>>>(P_, C_, B_, list, n, ++epoch_, e_upd, d_cnt_); });
 			// The curvature only enters through sigma * kappa (model/multi.hpp:142, 216, 190-193); without
 			// surface tension those products are zeros and the curvature stages are skipped.
 			if (sigma_) {
@@ -626,11 +632,12 @@ private:
 		}
 	}
 
-	// Neighbour values of the list (kept for the estimator), then slopes.
+	// Slopes, Hancock rhs and (viscous) gradients of a cell list.
 	void launch_slope(const int32_t *list, int n) {
-		k_nbvals<M><<<grid_for((long long) n * NF), BLOCK, 0, st_>>>(P_, C_, list, n, ++epoch_, d_cnt_);
-		if (visc_) k_slope<M, true><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
-		else k_slope<M, false><<<grid_for(n), BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, d_cnt_);
+		constexpr int G = NF <= 4 ? 4 : 8;
+		const int g = grid_for((long long) n * G);
+		if (visc_) k_slope<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
+		else k_slope<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
 	}
 
 	void sync_counters() {
@@ -677,7 +684,9 @@ private:
 		run_k(DG_K_SLOPE, n, [&] { launch_slope(list, n); });
 		if constexpr (M::MULTI) multiphase_aux(list, n, L, e_upd);
 		run_k(DG_K_ESTIMATE, n, [&] {
-			k_estimate<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, Ls_.split, d_cnt_);
+			constexpr int GE = NF <= 4 ? 4 : 8;
+			k_estimate<M><<<grid_for((long long) n * GE), BLOCK, 0, st_>>>(P_, C_, list, n, L, counterL, ++epoch_, Ls_.split,
+			                                                                 d_cnt_);
 		});
 		if (tight) {
 			sync_counters();

@@ -472,7 +472,7 @@ __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const C
 	}
 }
 template<class M, bool V, class S = double>
-__global__ void __launch_bounds__(BLOCK) k_face_sum(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L,
+__global__ void __launch_bounds__(BLOCK, 2) k_face_sum(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L,
                                                     double dtL, int stamp, int32_t *recv, Counters *cnt) {
 	d_face_sum<M, V, S>(PlainGrid{}, P, C, B, list, n, L, dtL, stamp, recv, cnt);
 }
@@ -558,141 +558,147 @@ __global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int
 
 
 
-// Neighbour values of a cell list: for each (cell, face) the neighbour's primitive state and time as
-// compute_slope and the error estimator see them (the leaf's own, or the mean over a non-leaf
-// neighbour's subtree), the centre distance 0.5 (h + h_n), and packed neighbour facts. One thread per
-// (cell, face), so the dependent neighbour loads of all faces proceed in parallel; the slope and
-// estimation stages then read their cell's 2D entries contiguously.
-template<class M>
-struct Nbv {
-	static constexpr int W = (M::E + 2 + 1) & ~1;  // p[E], t, centre distance
-};
+// Neighbour facts of a face as the slope and estimation stages read them: presence, leaf flag, tree
+// level and ACTI level of the face neighbour.
 constexpr int32_t NB_LEAF = 1 << 8, NB_PRESENT = 1 << 9;
 
 __device__ __forceinline__ int nb_level(int32_t code) { return code & 0xff; }
 __device__ __forceinline__ int nb_acti(int32_t code) { return ((code >> 16) & 0xff) - 1; }
 
-template<class M, class Grid>
-__device__ __forceinline__ void d_nbvals(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int epoch, Counters *cnt) {
-	constexpr int E = M::E, NF = 2 * M::D, W = Nbv<M>::W;
-	const long long total = (long long) n * NF;
-	for (long long t = g.tid(); t < total; t += g.stride()) {
-		const int slot = (int) (t / NF), f = (int) (t % NF);
-		const int i    = list[slot];
-		const int nb   = P.nbr[(size_t) f * P.cap + i];
-		int32_t *oi    = P.nbi + t;
-		if (nb == 0) {
-			*oi = 0;
-			continue;
-		}
-		const uint32_t fl = P.flags[nb];
-		const int ln      = P.level[nb];
-		double v[E + 1];
-		if (!(fl & F_LEAF)) {
-			interp_pt<M>(P, &cnt->status, nb, epoch, v);
-		} else {
-			load_p_rec<M>(P, nb, v);
-			v[E] = P.t[nb];
-		}
-		double *o = P.nbv + t * W;
-		for (int q = 0; q <= E; ++q) o[q] = v[q];
-		o[E + 1] = 0.5 * (C.size[P.level[i]] + C.size[ln]);
-		*oi      = NB_PRESENT | ((fl & F_LEAF) ? NB_LEAF : 0) | ln | ((P.acti[nb] + 1) << 16);
-	}
-}
+// The value compute_slope and the error estimator see across face f of cell i (impl/slopes.hpp:24-58,
+// impl/adaptive_refinement.hpp:16-60): the neighbour's primitive state and time (its own, or the mean
+// over a non-leaf neighbour's subtree, integrator/domain.hpp:84-148) and the centre distance
+// 0.5 (h + h_n); returns the neighbour facts, 0 when the face has no neighbour.
 template<class M>
-__global__ void k_nbvals(Pool P, Consts C, const int32_t *list, int n, int epoch, Counters *cnt) {
-	d_nbvals<M>(PlainGrid{}, P, C, list, n, epoch, cnt);
+__device__ __forceinline__ int32_t neighbour_value(const Pool &P, const Consts &C, uint32_t *status, int i, int f, int epoch,
+                                                   double *v /*[E]*/, double &tv, double &dist) {
+	constexpr int E = M::E;
+	const int nb = P.nbr[(size_t) f * P.cap + i];
+	if (nb == 0) return 0;
+	const uint32_t fl = P.flags[nb];
+	const int ln      = P.level[nb];
+	double w[E + 1];
+	if (!(fl & F_LEAF)) {
+		interp_pt<M>(P, status, nb, epoch, w);
+	} else {
+		load_p_rec<M>(P, nb, w);
+		w[E] = P.t[nb];
+	}
+#pragma unroll
+	for (int q = 0; q < E; ++q) v[q] = w[q];
+	tv   = w[E];
+	dist = 0.5 * (C.size[P.level[i]] + C.size[ln]);
+	return NB_PRESENT | ((fl & F_LEAF) ? NB_LEAF : 0) | ln | ((P.acti[nb] + 1) << 16);
 }
 
-// compute_slope (impl/slopes.hpp:16-76): limited primitive slopes, gradients (only read by the viscous
-// terms, so computed when V) and the Hancock rhs. Writes the record values [0, K0) of cell i (p, rhs,
-// slope rows) to `out`; the gradients go to the pool.
-template<class M, bool V = M::VISC>
-__device__ __forceinline__ void compute_slope(const Pool &P, const Consts &C, const BcTable &B, uint32_t *status, int lim,
-                                              int i, int slot, double *out) {
-	constexpr int E = M::E, D = M::D, NF = 2 * D, NW = Nbv<M>::W;
+// compute_slope (impl/slopes.hpp:16-76) of a cell list: limited primitive slopes, gradients (only read
+// by the viscous terms, so computed when V) and the Hancock rhs, written to the record's [0, K0) part
+// (p, rhs, slope rows); the gradients go to the pool. A group of G lanes serves one cell (G = 4 in 2D,
+// 8 in 3D): lane f fetches the value across face f (the neighbour's, or the boundary ghost at distance
+// h), the two lanes of a dimension meet to limit that dimension's slope row, and the group's first lane
+// forms the rhs from all rows. The neighbour loads of a cell's faces thus run in parallel and nothing
+// goes through memory between the fetch and the slope.
+template<class M, bool V, class Grid>
+__device__ __forceinline__ void d_slope(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
+                                        const int32_t *list, int n, int lim, int epoch, Counters *cnt) {
 	using R = Rec<M>;
-	const int cap = P.cap;
-	double pc[E];
-	load_p<M>(P, i, pc);
-	const double h = C.size[P.level[i]];
-	double slope[D * E];
+	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	static_assert(R::K0 % 2 == 0, "record rows are 16-byte aligned");
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int base   = lane & ~(G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot    = wbase + lane / G;
+		const bool active = slot < n;
+		const int i       = active ? list[slot] : 0;
+		double pc[E];
+		if (active) load_p<M>(P, i, pc);
+		else
 #pragma unroll
-	for (int dim = 0; dim < D; ++dim) {
-		double pn[E], pp[E], xn, xp, tn, tp;
-		const double xc = 0.0;
-		// impl/slopes.hpp:24-58: a ghost at distance h for boundaries, else the neighbour value
+			for (int q = 0; q < E; ++q) pc[q] = 0.0;
+		const double h  = active ? C.size[P.level[i]] : 1.0;
+		const double ti = active ? P.t[i] : 0.0;
+		// this lane's face: the value, its distance and time
+		double pv[E], x = 0.0, tv = 0.0;
 #pragma unroll
-		for (int dir = 0; dir < 2; ++dir) {
-			const int f = 2 * dim + dir;
-			double *pv = dir == 0 ? pn : pp;
-			double &x  = dir == 0 ? xn : xp;
-			double &tv = dir == 0 ? tn : tp;
-			const int32_t code = P.nbi[(size_t) slot * NF + f];
+		for (int q = 0; q < E; ++q) pv[q] = pc[q];
+		if (active && sub < NF) {
+			const int f = sub, dir = f & 1;
+			double dist;
+			const int32_t code = neighbour_value<M>(P, C, &cnt->status, i, f, epoch, pv, tv, dist);
 			if (!(code & NB_PRESENT)) {
 				const int b = P.bc[(size_t) f * cap + i];
 				if (b < 0) {
-					set_status(status, ST_MISSING_BC);
+					set_status(&cnt->status, ST_MISSING_BC);
 					for (int q = 0; q < E; ++q) pv[q] = pc[q];
 				} else {
-					boundary_value<M>(C.m, B, b, pc, P.t[i], pv);
+					boundary_value<M>(C.m, B, b, pc, ti, pv);
 				}
 				x  = dir == 0 ? -h : h;
-				tv = P.t[i];
+				tv = ti;
 			} else {
-				const double *nv = P.nbv + ((size_t) slot * NF + f) * NW;
-				for (int q = 0; q < E; ++q) pv[q] = nv[q];
-				tv = nv[E];
-				x  = dir == 0 ? -nv[E + 1] : nv[E + 1];
+				x = dir == 0 ? -dist : dist;
 			}
 		}
-		for (int q = 0; q < E; ++q) {
-			double sn = (pc[q] - pn[q]) / (xc - xn);
-			double sp = (pp[q] - pc[q]) / (xp - xc);
-			slope[dim * E + q] = limit(lim, sn, sp);
-		}
-		if constexpr (M::G > 0 && V) {
-			double gp[M::G], gn[M::G];
-			grad_input<M>(C.m, pp, gp);
-			grad_input<M>(C.m, pn, gn);
-			for (int g = 0; g < M::G; ++g) {
-				double ts = at(P.tslope, cap, g, i);
-				P.grad[(size_t) (dim * M::G + g) * cap + i] = (gp[g] - gn[g] - ts * (tp - tn)) / (xp - xn);
+		// the + side of each dimension moves to the dimension's first lane
+		const int partner = base + (sub | 1);
+		double pp[E];
+#pragma unroll
+		for (int q = 0; q < E; ++q) pp[q] = __shfl_sync(0xffffffffu, pv[q], partner);
+		const double xp = __shfl_sync(0xffffffffu, x, partner);
+		const double tp = __shfl_sync(0xffffffffu, tv, partner);
+		double row[E];
+#pragma unroll
+		for (int q = 0; q < E; ++q) row[q] = 0.0;
+		if (active && sub < NF && !(sub & 1)) {
+			const int dim   = sub >> 1;
+			const double xc = 0.0, xn = x, tn = tv;
+			for (int q = 0; q < E; ++q) {
+				double sn = (pc[q] - pv[q]) / (xc - xn);
+				double sp = (pp[q] - pc[q]) / (xp - xc);
+				row[q]    = limit(lim, sn, sp);
 			}
+			if constexpr (M::G > 0 && V) {
+				double gp[M::G], gn[M::G];
+				grad_input<M>(C.m, pp, gp);
+				grad_input<M>(C.m, pv, gn);
+				for (int k = 0; k < M::G; ++k) {
+					double ts = at(P.tslope, cap, k, i);
+					P.grad[(size_t) (dim * M::G + k) * cap + i] = (gp[k] - gn[k] - ts * (tp - tn)) / (xp - xn);
+				}
+			}
+			// slope row `dim` of the record
+			double2 *dst = reinterpret_cast<double2 *>(rec_of(P, i, R::W) + R::S0 + dim * R::ES);
+#pragma unroll
+			for (int k = 0; k < R::ES / 2; ++k) dst[k] = make_double2(row[2 * k], 2 * k + 1 < E ? row[2 * k + 1] : 0.0);
 		}
-	}
-	double rhs[E];
-	double kap = 0.0;
-	if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
-	compute_rhs<M>(C.m, pc, slope, kap, rhs);
+		// all rows to the group's first lane, which forms the rhs
+		double slope[D * E];
 #pragma unroll
-	for (int q = 0; q < E; ++q) out[R::P0 + q] = pc[q], out[R::R0 + q] = rhs[q];
+		for (int d = 0; d < D; ++d)
 #pragma unroll
-	for (int d = 0; d < D; ++d)
+			for (int q = 0; q < E; ++q) slope[d * E + q] = __shfl_sync(0xffffffffu, row[q], base + 2 * d);
+		if (active && sub == 0) {
+			double rhs[E];
+			double kap = 0.0;
+			if constexpr (M::MULTI) kap = at(P.k, cap, M::KAPPA, i);
+			compute_rhs<M>(C.m, pc, slope, kap, rhs);
+			double out[2 * E];
 #pragma unroll
-		for (int q = 0; q < R::ES; ++q) out[R::S0 + d * R::ES + q] = q < E ? slope[d * E + q] : 0.0;
-}
-
-// Slope stage over a cell list, one thread per cell; each thread writes its record's [0, K0) part
-// with 16-byte stores.
-template<class M, bool V, class Grid>
-__device__ __forceinline__ void d_slope(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int lim, Counters *cnt) {
-	using R = Rec<M>;
-	constexpr int K = R::K0;
-	static_assert(K % 2 == 0, "record rows are 16-byte aligned");
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i = list[tid];
-		double out[K];
-		compute_slope<M, V>(P, C, B, &cnt->status, lim, i, tid, out);
-		double2 *dst = reinterpret_cast<double2 *>(rec_of(P, i, R::W));
+			for (int q = 0; q < E; ++q) out[R::P0 + q] = pc[q], out[R::R0 + q] = rhs[q];
+			double2 *dst = reinterpret_cast<double2 *>(rec_of(P, i, R::W));
 #pragma unroll
-		for (int k = 0; k < K / 2; ++k) dst[k] = make_double2(out[2 * k], out[2 * k + 1]);
+			for (int k = 0; k < E; ++k) dst[k] = make_double2(out[2 * k], out[2 * k + 1]);
+		}
 	}
 }
 template<class M, bool V>
-__global__ void k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, Counters *cnt) {
-	d_slope<M, V>(PlainGrid{}, P, C, B, list, n, lim, cnt);
+__global__ void __launch_bounds__(BLOCK) k_slope(Pool P, Consts C, BcTable B, const int32_t *list, int n, int lim, int epoch,
+                                                 Counters *cnt) {
+	d_slope<M, V>(PlainGrid{}, P, C, B, list, n, lim, epoch, cnt);
 }
 
 // Recompute the Hancock rhs from the stored slope (used for split parents, whose curvature may
@@ -731,55 +737,89 @@ __device__ bool can_split_at(const Pool &P, const Consts &C, int i) {
 }
 
 // Error estimation and split/unsplit detection (impl/adaptive_refinement.hpp:16-149) with the
-// weighted_laplacian estimator (integrator/error_estimators.hpp:19-37).
+// weighted_laplacian estimator (integrator/error_estimators.hpp:19-37). A group of G lanes per cell,
+// as in the slope stage: lane f fetches the value across face f (a coarser leaf's state extrapolated
+// to the same-level position with its slope), the two lanes of a dimension meet to form that
+// dimension's second difference, and the group's first lane sums the dimensions in order and decides.
 template<class M, class Grid>
-__device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list, Counters *cnt) {
-	constexpr int E = M::E, D = M::D, NF = 2 * D;
-	const int cap = P.cap;
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i  = list[tid];
-		const int li = P.level[i];
-		const double h = C.size[li];
+__device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int L,
+                                           int counter_L, int epoch, int32_t *split_list, Counters *cnt) {
+	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int base   = lane & ~(G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot    = wbase + lane / G;
+		const bool active = slot < n;
+		const int i       = active ? list[slot] : 0;
+		const int li      = active ? P.level[i] : 0;
 		double pc[E];
-		load_p<M>(P, i, pc);
-		double error = 0.0;
-		for (int dim = 0; dim < D; ++dim) {
+		if (active) load_p<M>(P, i, pc);
+		else
+#pragma unroll
+			for (int q = 0; q < E; ++q) pc[q] = 0.0;
+		double v[E];
+#pragma unroll
+		for (int q = 0; q < E; ++q) v[q] = 0.0;
+		int32_t code = 0;
+		if (active && sub < NF) {
+			const int f = sub, dim = f >> 1, dir = f & 1;
+			double tv, dist;
+			code = neighbour_value<M>(P, C, &cnt->status, i, f, epoch, v, tv, dist);
+			if ((code & NB_PRESENT) && (code & NB_LEAF) && nb_level(code) < li) {
+				// a coarser leaf: its state extrapolated to the same-level position
+				const int nb   = P.nbr[(size_t) f * cap + i];
+				const double h = C.size[li];
+				double x[D];
+				for (int d = 0; d < D; ++d) x[d] = at(P.center, cap, d, i) + (d == dim ? h * (2 * dir - 1.0) : 0.0 * h);
+				if (C.periodic[dim] && dir == 0 && x[dim] < -0.5 * C.active[dim]) x[dim] += C.active[dim];
+				if (C.periodic[dim] && dir == 1 && x[dim] > 0.5 * C.active[dim]) x[dim] -= C.active[dim];
+				for (int d = 0; d < D; ++d) {
+					const double off = x[d] - at(P.center, cap, d, nb);
+					for (int q = 0; q < E; ++q) v[q] = v[q] + rec_slope<M>(P, nb, d, q) * off;
+				}
+			}
+		}
+		// second difference of each dimension on the dimension's first lane
+		const int partner = base + (sub | 1);
+		double vp[E];
+#pragma unroll
+		for (int q = 0; q < E; ++q) vp[q] = __shfl_sync(0xffffffffu, v[q], partner);
+		const int32_t code_p = __shfl_sync(0xffffffffu, code, partner);
+		double sq = 0.0;
+		if (active && sub < NF && !(sub & 1)) {
 			double d2[E];
 			for (int q = 0; q < E; ++q) d2[q] = pc[q] * -2.0;
-			bool missing = false;
-			for (int dir = 0; dir < 2; ++dir) {
-				const int f = 2 * dim + dir;
-				const int32_t code = P.nbi[(size_t) tid * NF + f];
-				if (!(code & NB_PRESENT)) {
-					missing = true;
-					break;
-				}
-				const double *nv = P.nbv + ((size_t) tid * NF + f) * Nbv<M>::W;
-				double v[E];
-				for (int q = 0; q < E; ++q) v[q] = nv[q];
-				if ((code & NB_LEAF) && nb_level(code) < li) {
-					// a coarser leaf: its state extrapolated to the same-level position
-					const int nb = P.nbr[(size_t) f * cap + i];
-					double x[D];
-					for (int d = 0; d < D; ++d) x[d] = at(P.center, cap, d, i) + (d == dim ? h * (2 * dir - 1.0) : 0.0 * h);
-					if (C.periodic[dim] && dir == 0 && x[dim] < -0.5 * C.active[dim]) x[dim] += C.active[dim];
-					if (C.periodic[dim] && dir == 1 && x[dim] > 0.5 * C.active[dim]) x[dim] -= C.active[dim];
-					for (int d = 0; d < D; ++d) {
-						const double off = x[d] - at(P.center, cap, d, nb);
-						for (int q = 0; q < E; ++q) v[q] = v[q] + rec_slope<M>(P, nb, d, q) * off;
-					}
-				}
+			bool missing = !(code & NB_PRESENT);
+			if (!missing) {
 				for (int q = 0; q < E; ++q) d2[q] = d2[q] + v[q];
+				missing = !(code_p & NB_PRESENT);
+				if (!missing)
+					for (int q = 0; q < E; ++q) d2[q] = d2[q] + vp[q];
 			}
 			if (missing)
 				for (int q = 0; q < E; ++q) d2[q] = 0.0;
-			double sq = 0.0;
 			for (int q = 0; q < E; ++q) {
 				const double w = d2[q] * C.weights[q];
 				sq += w * w;
 			}
-			error += sq;
 		}
+		double sqd[D];
+#pragma unroll
+		for (int d = 0; d < D; ++d) sqd[d] = __shfl_sync(0xffffffffu, sq, base + 2 * d);
+		// neighbour facts of the whole group: a present face more than one level coarser; a present face
+		// that is not a leaf or belongs to a faster cluster
+		const bool coarse2         = (code & NB_PRESENT) && nb_level(code) < li - 1;
+		const bool busy            = (code & NB_PRESENT) && (!(code & NB_LEAF) || nb_acti(code) > L);
+		const unsigned gmask       = ((1u << G) - 1u) << base;
+		const unsigned any_coarse2 = __ballot_sync(0xffffffffu, coarse2) & gmask;
+		const unsigned any_busy    = __ballot_sync(0xffffffffu, busy) & gmask;
+		if (!active || sub != 0) continue;
+		double error = 0.0;
+		for (int d = 0; d < D; ++d) error += sqd[d];
 		error = sqrt(error);
 		P.err[i] = error;
 
@@ -792,30 +832,17 @@ __device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const C
 		}
 		uint8_t op = OP_NONE;
 		const bool want_split = (error > C.max_err && (fl & F_CAN_SPLIT)) || (fl & F_SHOULD_SPLIT);
-		if (want_split) {
-			bool ready = true;
-			for (int f = 0; f < NF; ++f) {
-				const int32_t code = P.nbi[(size_t) tid * NF + f];
-				if ((code & NB_PRESENT) && nb_level(code) < li - 1) ready = false;
-			}
-			if (ready) op |= OP_SPLIT;
-		}
-		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1 && C.coarsen && !(fl & F_HOLD)) {
-			bool ok = true;
-			for (int f = 0; f < NF; ++f) {
-				const int32_t code = P.nbi[(size_t) tid * NF + f];
-				if ((code & NB_PRESENT) && (!(code & NB_LEAF) || nb_acti(code) > L)) ok = false;
-			}
-			if (ok) op |= OP_UCAND;
-		}
+		if (want_split && !any_coarse2) op |= OP_SPLIT;
+		if (error < C.min_err && (fl & F_CAN_UNSPLIT) && li > 0 && counter_L == 1 && C.coarsen && !(fl & F_HOLD) && !any_busy)
+			op |= OP_UCAND;
 		P.op[i] = op;
 		if (op & OP_SPLIT) append(split_list, &cnt->n_split, i, cap, &cnt->status);
 	}
 }
 template<class M>
-__global__ void k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L, int32_t *split_list,
-                           Counters *cnt) {
-	d_estimate<M>(PlainGrid{}, P, C, list, n, L, counter_L, split_list, cnt);
+__global__ void __launch_bounds__(BLOCK) k_estimate(Pool P, Consts C, const int32_t *list, int n, int L, int counter_L,
+                                                    int epoch, int32_t *split_list, Counters *cnt) {
+	d_estimate<M>(PlainGrid{}, P, C, list, n, L, counter_L, epoch, split_list, cnt);
 }
 
 // A parent coarsens when all its children are coarsening candidates of this cluster
@@ -1435,25 +1462,46 @@ __device__ double k_side(const Pool &P, const Consts &C, const BcTable &B, uint3
 
 // smooth_alpha, one Jacobi sweep (impl/smooth.hpp:10-51): reads the previous sweep's values of the
 // list's cells from `cur` (nullptr for the first sweep: everything from k[ALPHAS]) and writes `out`;
-// the sweeps alternate between two scratch arrays and only the result of the last is stored.
+// the sweeps alternate between two scratch arrays and the last writes k[ALPHAS] itself (the list's own
+// values are read from `cur` throughout, so that write races with no read). A group of G lanes per cell:
+// lane f fetches the smoothed volume fraction across face f, the dimension's two lanes form its term
+// 0.5 (a_n + a_p) + a_c, and the group's first lane sums the dimensions in order.
 template<class M, class Grid>
-__device__ __forceinline__ void d_smooth_alpha(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, const double *cur, double *out, int Lm, int epoch, int e_upd, Counters *cnt) {
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i     = list[tid];
-		const double ac = cur ? cur[i] : at(P.k, P.cap, M::ALPHAS, i);
-		double s        = 0.0;
-		for (int dim = 0; dim < M::D; ++dim) {
-			double x;
-			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
-			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
-			s += 0.5 * (an + ap) + ac;
+__device__ __forceinline__ void d_smooth_alpha(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
+                                               const int32_t *list, int n, const double *cur, double *out, int Lm,
+                                               int epoch, int e_upd, Counters *cnt) {
+	constexpr int D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int base   = lane & ~(G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot    = wbase + lane / G;
+		const bool active = slot < n;
+		const int i       = active ? list[slot] : 0;
+		double v = 0.0, x = 0.0;
+		if (active && sub < NF) v = k_side<M>(P, C, B, &cnt->status, i, sub >> 1, sub & 1, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
+		const double vp = __shfl_sync(0xffffffffu, v, base + (sub | 1));
+		double term = 0.0;
+		if (active && sub < NF && !(sub & 1)) {
+			const double ac = cur ? cur[i] : at(P.k, P.cap, M::ALPHAS, i);
+			term = 0.5 * (v + vp) + ac;
 		}
-		out[i] = s / (double) (2 * M::D);
+		double terms[D];
+#pragma unroll
+		for (int d = 0; d < D; ++d) terms[d] = __shfl_sync(0xffffffffu, term, base + 2 * d);
+		if (active && sub == 0) {
+			double s = 0.0;
+			for (int d = 0; d < D; ++d) s += terms[d];
+			out[i] = s / (double) (2 * D);
+		}
 	}
 }
 template<class M>
-__global__ void k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n, const double *cur, double *out,
-                               int Lm, int epoch, int e_upd, Counters *cnt) {
+__global__ void __launch_bounds__(BLOCK) k_smooth_alpha(Pool P, Consts C, BcTable B, const int32_t *list, int n,
+                                                        const double *cur, double *out, int Lm, int epoch, int e_upd,
+                                                        Counters *cnt) {
 	d_smooth_alpha<M>(PlainGrid{}, P, C, B, list, n, cur, out, Lm, epoch, e_upd, cnt);
 }
 
@@ -1468,20 +1516,33 @@ static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp,
 	d_store_tmp(PlainGrid{}, P, list, n, comp, src);
 }
 
-// compute_normal (impl/normal_curvature.hpp:7-55)
+// compute_normal (impl/normal_curvature.hpp:7-55), a group of G lanes per cell as in smooth_alpha:
+// lane f fetches the volume fraction across face f and its centre distance, the dimension's two lanes
+// form that gradient component, the first lane normalises and writes.
 template<class M, class Grid>
-__device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
-	constexpr int D = M::D;
-	const int cap = P.cap;
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i = list[tid];
+__device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
+                                         const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
+	constexpr int D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int base   = lane & ~(G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot    = wbase + lane / G;
+		const bool active = slot < n;
+		const int i       = active ? list[slot] : 0;
+		double v = 0.0, x = 0.0;
+		if (active && sub < NF) v = k_side<M>(P, C, B, &cnt->status, i, sub >> 1, sub & 1, M::ALPHAS, false, x, nullptr, -1, epoch, e_upd);
+		const double vp = __shfl_sync(0xffffffffu, v, base + (sub | 1));
+		const double xp = __shfl_sync(0xffffffffu, x, base + (sub | 1));
+		double comp = 0.0;
+		if (active && sub < NF && !(sub & 1)) comp = (vp - v) / (xp - x);
 		double nrm[D];
-		for (int dim = 0; dim < D; ++dim) {
-			double xn, xp;
-			const double an = k_side<M>(P, C, B, &cnt->status, i, dim, 0, M::ALPHAS, false, xn, nullptr, -1, epoch, e_upd);
-			const double ap = k_side<M>(P, C, B, &cnt->status, i, dim, 1, M::ALPHAS, false, xp, nullptr, -1, epoch, e_upd);
-			nrm[dim] = (ap - an) / (xp - xn);
-		}
+#pragma unroll
+		for (int d = 0; d < D; ++d) nrm[d] = __shfl_sync(0xffffffffu, comp, base + 2 * d);
+		if (!active || sub != 0) continue;
 		double sq = 0.0;
 		for (int d = 0; d < D; ++d) sq += nrm[d] * nrm[d];
 		const double len = sqrt(sq);
@@ -1494,7 +1555,8 @@ __device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Con
 	}
 }
 template<class M>
-__global__ void k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
+__global__ void __launch_bounds__(BLOCK) k_normal(Pool P, Consts C, BcTable B, const int32_t *list, int n, int epoch,
+                                                  int e_upd, Counters *cnt) {
 	d_normal<M>(PlainGrid{}, P, C, B, list, n, epoch, e_upd, cnt);
 }
 

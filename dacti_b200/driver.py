@@ -96,23 +96,67 @@ def locate(snap, side_length: float, pts: np.ndarray) -> np.ndarray:
     return out
 
 
+def find_in_tree(nodes, side_length: float, active_size, periodic, pts: np.ndarray) -> np.ndarray:
+    """Domain::find(p, max_depth) (integrator/domain.hpp:64-80, 407-416) over a whole node table: the
+    slot of the leaf (active or not) containing each point, 0 for a point outside a non-periodic side of
+    the active box. The descent picks child bit d when the point lies strictly above the centre."""
+    D = nodes.dims
+    root = nodes.root()
+    act = np.asarray(active_size, np.float64)[:D]
+    out = np.zeros(pts.shape[0], np.int64)
+    for k in range(pts.shape[0]):
+        x = np.array(pts[k, :D], np.float64)
+        inside = True
+        for d in range(D):
+            if x[d] < -0.5 * act[d] or x[d] > 0.5 * act[d]:
+                if periodic[d]:
+                    x[d] = x[d] + act[d] if x[d] < -0.5 * act[d] else x[d] - act[d]
+                else:
+                    inside = False
+        if not inside:
+            continue
+        x = 2.0 * x / side_length
+        idx = root
+        while idx != 0 and not (nodes.flags[idx] & 1):
+            i = 0
+            for d in range(D):
+                if x[d] > 0.0:
+                    i |= 1 << d
+            q = np.array([1.0 if (i >> d) & 1 else -1.0 for d in range(D)])
+            x = (x - 0.5 * q) * 2.0
+            idx = int(nodes.children[idx, i])
+        out[k] = idx
+    return out
+
+
 class AeroForce:
     """DACTI's AeroForce observer (driver/observer/aero_force.hpp:8-131) for 2D cases with analytic
     solid objects: pressure coefficients Cp = (p - p_ref) / (rho_ref |v_ref|^2 / 2) sampled along each
-    object's outline (segments split into max(int(10 * length), 1) samples, each moved 0.01 off the
-    surface), integrated to Cl and Cd; field variables Cp and ObjectSurface on the cells next to an
-    object. Differences from the reference: the outline is the analytic curve cut into `n_segments`
-    pieces instead of the adaptively sampled mesh, the samples move 0.01 into the fluid (the reference
-    moves them along -rotaten90 of the counter-clockwise tangent, i.e. into the body), and Cl, Cd are
-    the pressure force on the body per unit span and dynamic pressure (drag positive along +x); the
-    surface cells are those with a face neighbour centre inside an object (the signed-distance part of
-    the reference's boundary test)."""
+    object's outline, integrated to Cl and Cd; field variables Cp and ObjectSurface on the cells next to an
+    object.
+
+    convention="reference" (the default) follows aero_force.hpp:37-62 and 83-100: each outline segment
+    a-b (the outline in the order its curve is sampled, counter-clockwise for circles and ellipses,
+    scene/geometry_data.cpp:103-135) is split into max(int(10 |ab|), 1) samples at a + (j + 0.5) ab / n,
+    each moved by -0.01 n_s with n_s = rotaten90(ab / |ab|) = (ab_y, -ab_x) / |ab| (into the body for a
+    counter-clockwise outline); the sample's cell is Domain::find over the whole tree, inactive leaves
+    included (Integrator::get_cell_index, integrator.hpp:168), so samples inside a body read that
+    leaf's stored state; Cl = sum Cp area n_s,y and Cd = sum Cp area n_s,x. The outline is the analytic
+    curve cut into `n_segments` pieces instead of the adaptively sampled mesh.
+
+    convention="fluid" moves the samples 0.01 into the fluid, locates them among the active cells, and
+    reports the pressure force on the body per unit span and dynamic pressure with drag positive along
+    +x: a physical reading of the same quantities, not the reference's numbers."""
 
     name = "Aerodynamic Forces"
     names = ["Cl", "Cd"]
     field_names = ["Cp", "ObjectSurface"]
 
-    def __init__(self, objects, p_ref, vel_ref, n_segments: int = 256, sample_resolution: int = 10):
+    def __init__(self, objects, p_ref, vel_ref, n_segments: int = 256, sample_resolution: int = 10,
+                 convention: str = "reference"):
+        if convention not in ("reference", "fluid"):
+            raise ValueError("convention is 'reference' or 'fluid'")
+        self.convention = convention
         self.objects = list(objects)  # every object is sampled, as in the reference
         self.walls = [o for o in self.objects if getattr(o, "bc", None) is not None]
         self.p_ref = np.asarray(p_ref, np.float64)
@@ -125,18 +169,27 @@ class AeroForce:
             for a, b in zip(ring, nxt):
                 ab = b - a
                 length = float(np.hypot(*ab))
-                out_n = np.array([ab[1], -ab[0]]) / length  # outward for a counter-clockwise outline
+                n_s = np.array([ab[1], -ab[0]]) / length  # rotaten90 of the unit tangent
                 k = max(int(sample_resolution * length), 1)
                 for j in range(k):
-                    pts.append(a + (j + 0.5) * ab / k + 0.01 * out_n)
+                    pos = a + (j + 0.5) * ab / k
+                    pts.append(pos - 0.01 * n_s if convention == "reference" else pos + 0.01 * n_s)
                     area.append(length / k)
-                    nrm.append(out_n)
+                    nrm.append(n_s)
         self.pts, self.area, self.nrm = np.array(pts), np.array(area), np.array(nrm)
 
     def observe(self, solver, snap) -> list:
+        ip = solver.shape.ip
+        if self.convention == "reference":
+            nodes = solver.tree_nodes()
+            prm = solver.params
+            idx = find_in_tree(nodes, solver.side_length, prm.active_size, prm.periodic, self.pts)
+            cp = (nodes.p[idx, ip] - self.p_ref[ip]) * self.q_inv
+            cl = float((cp * self.area * self.nrm[:, 1]).sum())
+            cd = float((cp * self.area * self.nrm[:, 0]).sum())
+            return [cl, cd]
         idx = locate(snap, solver.side_length, self.pts)
         ok = idx >= 0
-        ip = solver.shape.ip
         cp = np.zeros(idx.size)
         cp[ok] = (snap.p[idx[ok], ip] - self.p_ref[ip]) * self.q_inv
         fx = -(cp * self.area * self.nrm[:, 0]).sum()

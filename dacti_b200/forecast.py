@@ -200,13 +200,19 @@ def train_forecaster(runs: Sequence[RunData], n_in: int, epochs: int = 30, seed:
     return net, cut, loss
 
 
-def run_with_forecast(solver: Solver, net: Mlp, cut: float, steps: int, interval: int = 8) -> dict:
+def run_with_forecast(solver: Solver, net: Mlp, cut: float, steps: int, interval: int = 8,
+                      coarsen_every: int = 1) -> dict:
     """Advances `steps` global steps with the forecast-driven regrid: every `interval` steps the
     network marks the cells it expects the indicator to flag within its horizon (dg_set_hold: they are
-    not coarsened), and coarsening runs on those steps only (dg_set_coarsen_interval). The plain
-    indicator still splits what it flags at every substep.
-    Returns the solver's split/unsplit counts and the number of held cells per forecast."""
-    solver.set_coarsen_interval(interval)
+    not coarsened until the next forecast), and coarsening runs every `coarsen_every` steps
+    (dg_set_coarsen_interval; 1 = at every opportunity, as the reference). The plain indicator still
+    splits what it flags at every substep, so a miss of the network costs a late split, never a
+    missing one. With coarsening at every step only the held cells keep their level: the regrid stops
+    coarsening cells that the indicator would flag again within the horizon (the split/unsplit churn
+    behind a moving front) and leaves the rest of the grid to the plain rule.
+    Returns the solver's split/unsplit counts, the cell updates and the number of held cells per
+    forecast."""
+    solver.set_coarsen_interval(coarsen_every)
     held = []
     fb = False
     for n in range(steps):

@@ -121,6 +121,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_batch_last_error.restype = ctypes.c_char_p
     lib.dg_batch_destroy.argtypes = [vp]
     lib.dg_batch_destroy.restype = None
+    lib.dg_batch_set_launch.argtypes = [vp, ctypes.POINTER(ctypes.c_int), ctypes.c_int]
+    lib.dg_batch_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.dg_batch_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
+                                         ctypes.c_int]
     _lib = lib
     return lib
 
@@ -132,7 +136,8 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_mlp_get_params", "dg_mlp_predict", "dg_mlp_loss_grad", "dg_mlp_train", "dg_mlp_destroy",
                     "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
                     "dg_read_cells_noalloc", "dg_get_stats", "dg_batch_create", "dg_batch_step",
-                    "dg_batch_last_error", "dg_batch_destroy",
+                    "dg_batch_last_error", "dg_batch_destroy", "dg_batch_set_launch", "dg_batch_set_profiling",
+                    "dg_batch_stage_times",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
@@ -359,13 +364,18 @@ def step_many(solvers, threads: int = 32, signal: bool = True) -> list:
     return [bool(fb[k]) for k in range(n)]
 
 
+BATCH_STAGES = ("face_sum", "receive", "update", "slope", "aux", "estimate", "regrid_cell", "regrid_fresh",
+                "nbr_list", "flush")
+
+
 class Batch:
     """dg_batch: independent solvers of one model stepped in lockstep, one launch per stage for all trees
     that run a level (merged ACTI schedules). Per tree the results equal Solver.integrate's bit for bit.
     The solvers stay usable for read-backs; step them through the batch only, and close the batch before
-    closing them."""
+    closing them. `launch` (blocks per SM per stage kind) defaults to the autotuned table of the model
+    when dacti_b200/launch_table.json has one."""
 
-    def __init__(self, solvers):
+    def __init__(self, solvers, launch=None):
         self._lib = load_library()
         self.solvers = list(solvers)
         hs = (ctypes.c_void_p * len(self.solvers))(*[s._h for s in self.solvers])
@@ -374,6 +384,30 @@ class Batch:
         if rc != DG_OK:
             raise DgError(rc, self._lib.dg_batch_last_error(None).decode())
         self._h = h
+        if launch is None:
+            from .autotune import table_entry
+            launch = table_entry(self.solvers[0].shape)
+        if launch is not None:
+            self.set_launch(launch)
+
+    def _bcheck(self, rc: int) -> None:
+        if rc != DG_OK:
+            raise DgError(rc, self._lib.dg_batch_last_error(self._h).decode())
+
+    def set_launch(self, blocks_per_sm) -> None:
+        v = (ctypes.c_int * len(blocks_per_sm))(*[int(x) for x in blocks_per_sm])
+        self._bcheck(self._lib.dg_batch_set_launch(self._h, v, len(blocks_per_sm)))
+
+    def set_profiling(self, on: bool = True) -> None:
+        self._bcheck(self._lib.dg_batch_set_profiling(self._h, 1 if on else 0))
+
+    def stage_times(self) -> dict:
+        """{stage: (device ms, work items)} since the previous call (profiling on)."""
+        n = len(BATCH_STAGES)
+        ms = (ctypes.c_double * n)()
+        it = (ctypes.c_longlong * n)()
+        self._bcheck(self._lib.dg_batch_stage_times(self._h, ms, it, n))
+        return {k: (ms[i], it[i]) for i, k in enumerate(BATCH_STAGES)}
 
     def step(self, signal: bool = True) -> list:
         """One global step of every tree; returns the force_break flags."""

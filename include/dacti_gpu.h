@@ -149,6 +149,18 @@ int dg_batch_step(dg_batch *b, int signal, int *force_break, double *global_dt);
 const char *dg_batch_last_error(dg_batch *b);
 void dg_batch_destroy(dg_batch *b);
 
+/* Stage kinds of a merged batch substep, in this order: face sums, flux receive, cell update, slopes,
+ * multiphase auxiliary sweeps, indicator, per-cell regrid, regrid of new cells, neighbour repair,
+ * buffer flush. */
+enum { DG_BATCH_STAGES = 10 };
+/* Launch budget of each stage kind in blocks per SM (1..64, default 16): a launch splits that many blocks
+ * among the trees in proportion to their work. What the autotuner (dacti_b200/autotune.py) sets. */
+int dg_batch_set_launch(dg_batch *b, const int *blocks_per_sm, int n_stages);
+/* Per-stage device timing with CUDA events (off by default). */
+int dg_batch_set_profiling(dg_batch *b, int on);
+/* Device milliseconds and work items per stage kind since the previous call. */
+int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n_stages);
+
 /* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */
 int dg_cell_count(dg_solver *s, long long *n);
 

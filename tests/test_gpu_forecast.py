@@ -162,13 +162,15 @@ def test_forecast_driven_regrid_against_plain():
     plain, fc = Solver(_cyl()), Solver(_cyl())
     for _ in range(16):
         plain.integrate()
-    res = run_with_forecast(fc, net, cut, steps=16, interval=8)
+    res = run_with_forecast(fc, net, cut, steps=16, interval=8, coarsen_every=1)
     sp = plain.stats()
     err = density_rel_l1(plain.active_cells(), fc.active_cells(), 40.0, (40.0, 20.0), 8, 1)
     print("plain splits", sp.n_splits, "unsplits", sp.n_unsplits, "updates", sp.cell_updates,
           "| forecast", res, "| density rel-L1 vs plain", err)
     assert not res["force_break"]
-    assert res["unsplits"] < sp.n_unsplits  # coarsening runs on one step in eight, never on held cells
+    # held cells are never coarsened, so the regrid does less split/unsplit churn
+    assert res["unsplits"] < sp.n_unsplits
+    assert res["splits"] + res["unsplits"] < sp.n_splits + sp.n_unsplits
     assert err < 5e-3
     plain.close(), fc.close()
     net.close()

@@ -81,7 +81,7 @@ def test_toml_cylinder_aero_force(tmp_path):
     tc = load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"))
     tc.run.io_interval = 0.0  # a frame after every step
     s = Solver(tc.case)
-    ob = AeroForce(tc.objects, tc.p_ref, tc.vel_ref)
+    ob = AeroForce(tc.objects, tc.p_ref, tc.vel_ref, convention="fluid")
     res = driver_for(tc, s, str(tmp_path), observers=[ob], max_steps=4).run()
     assert not res["force_break"] and res["frames"] == 4
     rows = list(csv.reader(open(tmp_path / "cylinder_ns2d" / "cylinder_ns2d_observables.csv")))
@@ -93,4 +93,25 @@ def test_toml_cylinder_aero_force(tmp_path):
     a = read_vtu_arrays(str(tmp_path / "cylinder_ns2d" / "cylinder_ns2d_0004.vtu"))
     surf = a["Aerodynamic Forces/ObjectSurface"]
     assert surf.sum() > 0 and (a["Aerodynamic Forces/Cp"][surf == 0] == 0).all()
+    s.close()
+
+
+def test_toml_cylinder_aero_force_reference_convention():
+    """With the reference's sampling (aero_force.hpp:47-50) every sample lies 0.01 inside the solid
+    cylinder and is located in the whole tree (inactive leaves included); the coefficients are finite and
+    differ from the fluid-side reading."""
+    from dacti_b200.driver import AeroForce
+
+    tc = load_toml_case(os.path.join(GOLDEN, "toml", "cylinder_ns2d.toml"))
+    s = Solver(tc.case)
+    for _ in range(3):
+        s.integrate()
+    ref = AeroForce(tc.objects, tc.p_ref, tc.vel_ref)
+    flu = AeroForce(tc.objects, tc.p_ref, tc.vel_ref, convention="fluid")
+    inside = np.zeros(len(ref.pts), bool)
+    for o in tc.objects:
+        inside |= o.signed_distance(ref.pts) < 0.0
+    assert inside.all()
+    a, b = ref.observe(s, s.active_cells()), flu.observe(s, s.active_cells())
+    assert np.isfinite(a).all() and a != b
     s.close()
