@@ -370,8 +370,8 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 }
 
 // flux_update (impl/flux.hpp:11-97) seen from each running-cluster cell: the signed sum of the fluxes
-// that cross its faces in this substep, one group of G lanes per cell (G = 4 in 2D, 8 in 3D; lanes past
-// 2D idle). Lane f evaluates the flux across face f: the cell's own when it owns the face (the finer
+// that cross its faces in this substep, one lane per face (groups of 4 lanes in 2D, 8 cells a warp; of
+// 6 lanes in 3D, 5 cells a warp, the warp's last two lanes idle). Lane f evaluates the flux across face f: the cell's own when it owns the face (the finer
 // side, at equal levels the slower cell or the cell on the left), the same-level neighbour's when the
 // neighbour owns it, the boundary flux, or the sum over the finer owners behind a non-leaf neighbour in
 // candidate order. Every interior flux is evaluated with the owner's arguments (owner, the owner's
@@ -383,18 +383,21 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 // to FP32 once, as both sides read it; sums stay FP64.
 template<class M, bool V, class S = double, class Grid>
 __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int L, double dtL, int stamp, int32_t *recv, Counters *cnt) {
-	constexpr int NF = 2 * M::D, G = NF <= 4 ? 4 : 8, GW = 32 / G, NSUB = 1 << (M::D - 1), F = M::F;
+	constexpr int NF = 2 * M::D, G = NF, GW = 32 / G, NSUB = 1 << (M::D - 1), F = M::F;
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
-	const int sub    = lane & (G - 1);
+	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
+	const int sub    = lane - grp * G;
+	const int base   = grp * G;
 	const int warp   = g.tid() >> 5;
 	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
-		const int slot = wbase + lane / G;
+		const int slot    = wbase + grp;
+		const bool active = grp < GW && slot < n;
 		double acc[F];
 #pragma unroll
 		for (int q = 0; q < F; ++q) acc[q] = 0.0;
-		if (slot < n && sub < NF) {
+		if (active) {
 			const int i   = list[slot];
 			if (sub == 0) P.pos[i] = slot;
 			const int f   = sub, dim = f >> 1, dir = f & 1;
@@ -459,15 +462,30 @@ __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const C
 				}
 			}
 		}
+		// the group's face terms in the fixed pairing order, on every lane of the group
+		double sum[F];
+		if constexpr (NF == 4) {
+			// (f0 + f2) + (f1 + f3): a butterfly over the aligned group of four
 #pragma unroll
-		for (int off = G / 2; off > 0; off >>= 1)
+			for (int q = 0; q < F; ++q) {
+				double v = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], 2);
+				sum[q]   = v + __shfl_xor_sync(0xffffffffu, v, 1);
+			}
+		} else {
+			// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0))
 #pragma unroll
-			for (int q = 0; q < F; ++q) acc[q] += __shfl_xor_sync(0xffffffffu, acc[q], off);
-		if (slot < n) {
+			for (int q = 0; q < F; ++q) {
+				double f[6];
+#pragma unroll
+				for (int k = 0; k < 6; ++k) f[k] = __shfl_sync(0xffffffffu, acc[q], min(base + k, 31));
+				sum[q] = ((f[0] + f[4]) + (f[2] + 0.0)) + ((f[1] + f[5]) + (f[3] + 0.0));
+			}
+		}
+		if (active) {
 			double *dst = P.du + (size_t) slot * F;
 #pragma unroll
 			for (int q = 0; q < F; ++q)
-				if ((q & (G - 1)) == sub) dst[q] = acc[q];
+				if (q % G == sub) dst[q] = sum[q];
 		}
 	}
 }
@@ -593,26 +611,27 @@ __device__ __forceinline__ int32_t neighbour_value(const Pool &P, const Consts &
 
 // compute_slope (impl/slopes.hpp:16-76) of a cell list: limited primitive slopes, gradients (only read
 // by the viscous terms, so computed when V) and the Hancock rhs, written to the record's [0, K0) part
-// (p, rhs, slope rows); the gradients go to the pool. A group of G lanes serves one cell (G = 4 in 2D,
-// 8 in 3D): lane f fetches the value across face f (the neighbour's, or the boundary ghost at distance
-// h), the two lanes of a dimension meet to limit that dimension's slope row, and the group's first lane
-// forms the rhs from all rows. The neighbour loads of a cell's faces thus run in parallel and nothing
+// (p, rhs, slope rows); the gradients go to the pool. A group of G = 2D lanes serves one cell (8 cells a
+// warp in 2D, 5 in 3D with the warp's last two lanes idle): lane f fetches the value across face f (the
+// neighbour's, or the boundary ghost at distance h), the two lanes of a dimension meet to limit that
+// dimension's slope row, and the group's first lane forms the rhs from all rows. The neighbour loads of a cell's faces thus run in parallel and nothing
 // goes through memory between the fetch and the slope.
 template<class M, bool V, class Grid>
 __device__ __forceinline__ void d_slope(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
                                         const int32_t *list, int n, int lim, int epoch, Counters *cnt) {
 	using R = Rec<M>;
-	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF, GW = 32 / G;  // lanes per cell, cells per warp
 	static_assert(R::K0 % 2 == 0, "record rows are 16-byte aligned");
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
-	const int sub    = lane & (G - 1);
-	const int base   = lane & ~(G - 1);
+	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
+	const int sub    = lane - grp * G;
+	const int base   = grp * G;
 	const int warp   = g.tid() >> 5;
 	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
-		const int slot    = wbase + lane / G;
-		const bool active = slot < n;
+		const int slot    = wbase + grp;
+		const bool active = grp < GW && slot < n;
 		const int i       = active ? list[slot] : 0;
 		double pc[E];
 		if (active) load_p<M>(P, i, pc);
@@ -680,7 +699,7 @@ __device__ __forceinline__ void d_slope(const Grid &g, const Pool &P, const Cons
 #pragma unroll
 		for (int d = 0; d < D; ++d)
 #pragma unroll
-			for (int q = 0; q < E; ++q) slope[d * E + q] = __shfl_sync(0xffffffffu, row[q], base + 2 * d);
+			for (int q = 0; q < E; ++q) slope[d * E + q] = __shfl_sync(0xffffffffu, row[q], min(base + 2 * d, 31));
 		if (active && sub == 0) {
 			double rhs[E];
 			double kap = 0.0;
@@ -744,16 +763,17 @@ __device__ bool can_split_at(const Pool &P, const Consts &C, int i) {
 template<class M, class Grid>
 __device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, int L,
                                            int counter_L, int epoch, int32_t *split_list, Counters *cnt) {
-	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	constexpr int E = M::E, D = M::D, NF = 2 * D, G = NF, GW = 32 / G;  // lanes per cell, cells per warp
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
-	const int sub    = lane & (G - 1);
-	const int base   = lane & ~(G - 1);
+	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
+	const int sub    = lane - grp * G;
+	const int base   = grp * G;
 	const int warp   = g.tid() >> 5;
 	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
-		const int slot    = wbase + lane / G;
-		const bool active = slot < n;
+		const int slot    = wbase + grp;
+		const bool active = grp < GW && slot < n;
 		const int i       = active ? list[slot] : 0;
 		const int li      = active ? P.level[i] : 0;
 		double pc[E];
@@ -809,7 +829,7 @@ __device__ __forceinline__ void d_estimate(const Grid &g, const Pool &P, const C
 		}
 		double sqd[D];
 #pragma unroll
-		for (int d = 0; d < D; ++d) sqd[d] = __shfl_sync(0xffffffffu, sq, base + 2 * d);
+		for (int d = 0; d < D; ++d) sqd[d] = __shfl_sync(0xffffffffu, sq, min(base + 2 * d, 31));
 		// neighbour facts of the whole group: a present face more than one level coarser; a present face
 		// that is not a leaf or belongs to a faster cluster
 		const bool coarse2         = (code & NB_PRESENT) && nb_level(code) < li - 1;
@@ -1470,15 +1490,16 @@ template<class M, class Grid>
 __device__ __forceinline__ void d_smooth_alpha(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
                                                const int32_t *list, int n, const double *cur, double *out, int Lm,
                                                int epoch, int e_upd, Counters *cnt) {
-	constexpr int D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	constexpr int D = M::D, NF = 2 * D, G = NF, GW = 32 / G;  // lanes per cell, cells per warp
 	const int lane   = threadIdx.x & 31;
-	const int sub    = lane & (G - 1);
-	const int base   = lane & ~(G - 1);
+	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
+	const int sub    = lane - grp * G;
+	const int base   = grp * G;
 	const int warp   = g.tid() >> 5;
 	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
-		const int slot    = wbase + lane / G;
-		const bool active = slot < n;
+		const int slot    = wbase + grp;
+		const bool active = grp < GW && slot < n;
 		const int i       = active ? list[slot] : 0;
 		double v = 0.0, x = 0.0;
 		if (active && sub < NF) v = k_side<M>(P, C, B, &cnt->status, i, sub >> 1, sub & 1, M::ALPHAS, false, x, cur, Lm, epoch, e_upd);
@@ -1490,7 +1511,7 @@ __device__ __forceinline__ void d_smooth_alpha(const Grid &g, const Pool &P, con
 		}
 		double terms[D];
 #pragma unroll
-		for (int d = 0; d < D; ++d) terms[d] = __shfl_sync(0xffffffffu, term, base + 2 * d);
+		for (int d = 0; d < D; ++d) terms[d] = __shfl_sync(0xffffffffu, term, min(base + 2 * d, 31));
 		if (active && sub == 0) {
 			double s = 0.0;
 			for (int d = 0; d < D; ++d) s += terms[d];
@@ -1522,16 +1543,17 @@ static __global__ void k_store_tmp(Pool P, const int32_t *list, int n, int comp,
 template<class M, class Grid>
 __device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Consts &C, const BcTable &B,
                                          const int32_t *list, int n, int epoch, int e_upd, Counters *cnt) {
-	constexpr int D = M::D, NF = 2 * D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	constexpr int D = M::D, NF = 2 * D, G = NF, GW = 32 / G;  // lanes per cell, cells per warp
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
-	const int sub    = lane & (G - 1);
-	const int base   = lane & ~(G - 1);
+	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
+	const int sub    = lane - grp * G;
+	const int base   = grp * G;
 	const int warp   = g.tid() >> 5;
 	const int nwarps = g.stride() >> 5;
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
-		const int slot    = wbase + lane / G;
-		const bool active = slot < n;
+		const int slot    = wbase + grp;
+		const bool active = grp < GW && slot < n;
 		const int i       = active ? list[slot] : 0;
 		double v = 0.0, x = 0.0;
 		if (active && sub < NF) v = k_side<M>(P, C, B, &cnt->status, i, sub >> 1, sub & 1, M::ALPHAS, false, x, nullptr, -1, epoch, e_upd);
@@ -1541,7 +1563,7 @@ __device__ __forceinline__ void d_normal(const Grid &g, const Pool &P, const Con
 		if (active && sub < NF && !(sub & 1)) comp = (vp - v) / (xp - x);
 		double nrm[D];
 #pragma unroll
-		for (int d = 0; d < D; ++d) nrm[d] = __shfl_sync(0xffffffffu, comp, base + 2 * d);
+		for (int d = 0; d < D; ++d) nrm[d] = __shfl_sync(0xffffffffu, comp, min(base + 2 * d, 31));
 		if (!active || sub != 0) continue;
 		double sq = 0.0;
 		for (int d = 0; d < D; ++d) sq += nrm[d] * nrm[d];

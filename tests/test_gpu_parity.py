@@ -107,6 +107,13 @@ def test_shock_drop_config2_reduced(tmp_path):
     assert stats.n_substeps > 100
 
 
+def test_cylinder_config4_stated_size(tmp_path):
+    """Config 4's Navier-Stokes cylinder at its stated size (128 x 64 base, the power-of-two grid nearest
+    80 x 40, +5 levels; no-slip solid, Re 200) for 6 global steps against the single-thread reference."""
+    stats = _live(cases.cylinder_ns(mach=0.3, base_level=7, levels=5), 6, [3, 6], tmp_path, "cyl75")
+    assert stats.n_substeps > 500
+
+
 def test_periodic_without_refinement(tmp_path):
     _live(cases.periodic_blob(base_level=5, refine=False), 8, [8], tmp_path, "pnr")
 
