@@ -60,6 +60,10 @@ def parse_args():
     ap.add_argument("--scale", action="store_true",
                     help="also run the scale workload: the shock-drop at 128 x 64 x 64 base, +5 levels (~28M leaves)")
     ap.add_argument("--scale-steps", type=int, default=1)
+    ap.add_argument("--scale-only", action="store_true", help="run only the scale workload and print its section")
+    ap.add_argument("--learned-only", action="store_true", help="run only the learned sections and print them")
+    ap.add_argument("--learned-shock", action="store_true",
+                    help="also run the forecast-driven regrid on the shock-drop of the bench workload")
     ap.add_argument("--forms", default="fp64,mixed",
                     help="numerical forms to time; `value` is fp64 when it is among them, else the first one")
     ap.add_argument("--profile-substep", type=int, default=-1,
@@ -367,6 +371,58 @@ def learned_run(args, local_rank: int) -> dict:
     }
 
 
+def learned_shock_run(args, local_rank: int) -> dict:
+    """The forecast-driven regrid on the bench's shock-drop (64 x 32 x 32 base, +4 levels): a network
+    trained on four smaller shock-drops (32 x 16 x 16 base, +3 levels, Mach from U(1.3, 1.7), seeds 31-34,
+    12 global steps each, horizon 4) holds the cells it expects the indicator to flag within 4 steps;
+    coarsening runs at every step otherwise. Against the plain regrid over 8 global steps: splits,
+    unsplits, cell updates, device time, active cells at the end, density rel-L1 and the device memory
+    high-water mark."""
+    import torch
+    from dacti_b200 import cases
+    from dacti_b200.accuracy import density_rel_l1
+    from dacti_b200.forecast import collect, run_with_forecast, train_forecaster
+    from dacti_b200.solver import Solver
+
+    def run(seed):
+        mach = float(np.random.default_rng(seed).uniform(1.3, 1.7))
+        return collect(lambda: cases.shock_drop(mach=mach, base_level=5, levels=3), 12, 4)
+
+    train = [run(s) for s in (31, 32, 33, 34)]
+    net, cut, _ = train_forecaster(train, n_in=train[0].x.shape[1], epochs=20)
+    case = make_case(args)
+    out = {}
+    for name in ("plain", "forecast"):
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info()[0]
+        s = Solver(case, device=local_rank)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        if name == "plain":
+            for _ in range(8):
+                s.integrate()
+            st = s.stats()
+            res = {"splits": st.n_splits, "unsplits": st.n_unsplits, "cell_updates": st.cell_updates}
+        else:
+            res = run_with_forecast(s, net, cut, steps=8, interval=4, coarsen_every=1)
+        b.record()
+        torch.cuda.synchronize()
+        res["device_ms"] = a.elapsed_time(b)
+        res["active_cells"] = s.n_active_cells()
+        res["device_gb_used_after"] = (free0 - torch.cuda.mem_get_info()[0]) / 1e9
+        res["snap"] = s.active_cells()
+        s.close()
+        out[name] = res
+    err = density_rel_l1(out["forecast"]["snap"], out["plain"]["snap"], case.params.side_length,
+                         case.params.active_size, args.base_level, int(case.shape.model))
+    for k in out:
+        out[k].pop("snap")
+    net.close()
+    return {"workload": "shock_drop_3d 64x32x32 +4, 8 global steps; network trained on four 32x16x16 +3 runs",
+            "plain": out["plain"], "forecast": out["forecast"], "density_rel_l1_vs_plain": err,
+            "interval": 4, "coarsen_every": 1}
+
+
 def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     """Batched 2D Euler quadtree Riemann problems (seeded, see cases.riemann_batch), mixed form. The
     lockstep batch (dg_batch: merged ACTI schedules, one launch per stage for all trees of a level, one
@@ -574,6 +630,17 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     from dacti_b200.solver import Solver
 
     torch.cuda.set_device(local_rank)
+    if args.scale_only:
+        if rank == 0:
+            print(json.dumps({"scale": scale_run(args, local_rank)}), flush=True)
+        return
+    if args.learned_only:
+        if rank == 0:
+            out = {"learned": learned_run(args, local_rank)}
+            if args.learned_shock:
+                out["learned_shock"] = learned_shock_run(args, local_rank)
+            print(json.dumps(out), flush=True)
+        return
     stream = torch.cuda.Stream()
     case = make_case(args)
     D = case.shape.dims
@@ -678,6 +745,8 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         result["batched"] = batched_run(args, rank, local_rank, world)
     if not args.no_learned and world == 1:
         result["learned"] = learned_run(args, local_rank)
+    if args.learned_shock and world == 1:
+        result["learned_shock"] = learned_shock_run(args, local_rank)
     if args.scale and world == 1:
         try:
             result["scale"] = scale_run(args, local_rank)

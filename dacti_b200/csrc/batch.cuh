@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(BLOCK) kb_flux_receive(const TreeArgs *A, cons
 }
 
 template<class M, bool V>
-__global__ void __launch_bounds__(BLOCK, 2) kb_update(const TreeArgs *A, const int *off, int nt) {
+__global__ void __launch_bounds__(BLOCK, 3) kb_update(const TreeArgs *A, const int *off, int nt) {
 	DG_BATCH_PROLOGUE
 	d_update<M, V>(g, a.P, *a.C, a.list, a.n, a.dtL, a.epoch0 + 1, a.cnt);
 }

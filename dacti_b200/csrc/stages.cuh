@@ -569,7 +569,7 @@ __device__ __forceinline__ void d_update(const Grid &g, const Pool &P, const Con
 	}
 }
 template<class M, bool V>
-__global__ void __launch_bounds__(BLOCK, 2) k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, int epoch,
+__global__ void __launch_bounds__(BLOCK, 3) k_update(Pool P, Consts C, const int32_t *list, int n, double dtL, int epoch,
                                                      Counters *cnt) {
 	d_update<M, V>(PlainGrid{}, P, C, list, n, dtL, epoch, cnt);
 }
