@@ -425,11 +425,13 @@ def learned_shock_run(args, local_rank: int) -> dict:
 
 def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     """Batched 2D Euler quadtree Riemann problems (seeded, see cases.riemann_batch), mixed form. The
-    lockstep batch (dg_batch: merged ACTI schedules, one launch per stage for all trees of a level, one
-    synchronisation per merged substep) is timed with CUDA events on its stream, beside dg_step_many
-    (host threads, one stream per tree, one synchronisation per tree and substep) and the same trees
-    stepped one after another. With N ranks the trees are split among them (dacti_b200.batch, no
-    exchange): the batch's total work is fixed (strong scaling)."""
+    lockstep batch (dg_batch: merged ACTI schedules, one launch per stage for all trees of a level, the
+    global step planned on the host and issued with no synchronisation, device guards stopping a run
+    where the live counts leave the plan) is timed around its steps, beside dg_step_many (host threads,
+    one stream per tree, one synchronisation per tree and substep) and the same trees stepped one after
+    another. One more step with per-stage CUDA-event timing gives the device time per stage kind. With N
+    ranks the trees are split among them (dacti_b200.batch, no exchange): the batch's total work is fixed
+    (strong scaling)."""
     import torch
     import torch.distributed as dist
     from dacti_b200 import cases
@@ -461,6 +463,15 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         b.step()
     torch.cuda.synchronize()
     l_sec, l_upd = time.perf_counter() - t0, updates(solvers) - u0
+    runs = b.run_stats()
+    # one more step with per-stage device timing: how much of the step the stage kernels fill
+    b.set_profiling(True)
+    b.stage_times()
+    t1 = time.perf_counter()
+    b.step()
+    torch.cuda.synchronize()
+    prof_ms = (time.perf_counter() - t1) * 1e3
+    stages = {k: round(v[0], 3) for k, v in b.stage_times().items()}
     b.close()
     cells = sum(s.n_active_cells() for s in solvers)
     for s in solvers:
@@ -498,6 +509,8 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "scaling": "strong", "trees_rank0": len(mine), "unit": UNIT, "steps": args.steps,
         "value": l_u / (l_ms * 1e-3), "ms_per_step": l_ms / args.steps,
         "timing": "host wall clock around K lockstep batch steps (dg_batch_step), synchronised before and after",
+        "planned_runs": runs,
+        "profiled_step": {"wall_ms": prof_ms, "stage_ms": stages, "stage_sum_ms": round(sum(stages.values()), 3)},
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
         "speedup_vs_step_many": (l_u / l_ms) / (m_u / m_ms) if m_u > 0 else None,

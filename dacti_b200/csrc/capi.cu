@@ -252,6 +252,11 @@ int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n) {
 	return batch_guarded(b, [&] { b->impl->stage_times(ms, items, n); });
 }
 
+int dg_batch_run_stats(dg_batch *b, long long *out, int n) {
+	if (!out || n < 0) return DG_ERR_ARG;
+	return batch_guarded(b, [&] { b->impl->run_stats(out, n); });
+}
+
 const char *dg_batch_last_error(dg_batch *b) {
 	if (!b) return g_create_error.c_str();
 	return b->impl->last_error.c_str();

@@ -135,7 +135,9 @@ struct Counters {
 	int n_upd;        // neighbour-update list
 	int n_tmp;        // rebuilt cluster list
 	uint32_t status;
-	unsigned long long n_split_total, n_unsplit_total;
+	// running totals that the batched step keeps on the device (splits, coarsenings, cluster cells after
+	// each substep's flush, substeps)
+	unsigned long long n_split_total, n_unsplit_total, n_updates_total, n_substeps_total;
 	double dmax;      // reduction result
 };
 

@@ -125,6 +125,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_batch_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_batch_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.c_int]
+    lib.dg_batch_run_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     _lib = lib
     return lib
 
@@ -137,7 +138,7 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
                     "dg_read_cells_noalloc", "dg_get_stats", "dg_batch_create", "dg_batch_step",
                     "dg_batch_last_error", "dg_batch_destroy", "dg_batch_set_launch", "dg_batch_set_profiling",
-                    "dg_batch_stage_times",
+                    "dg_batch_stage_times", "dg_batch_run_stats",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
@@ -408,6 +409,13 @@ class Batch:
         it = (ctypes.c_longlong * n)()
         self._bcheck(self._lib.dg_batch_stage_times(self._h, ms, it, n))
         return {k: (ms[i], it[i]) for i, k in enumerate(BATCH_STAGES)}
+
+    def run_stats(self) -> dict:
+        """Planned runs (one per global step unless a guard stopped one), runs stopped by a guard, substeps
+        planned and substeps the host replayed after a stop, since the batch was made."""
+        v = (ctypes.c_longlong * 4)()
+        self._bcheck(self._lib.dg_batch_run_stats(self._h, v, 4))
+        return {"runs": v[0], "stops": v[1], "planned": v[2], "replayed": v[3]}
 
     def step(self, signal: bool = True) -> list:
         """One global step of every tree; returns the force_break flags."""

@@ -1,6 +1,6 @@
-"""Batched trees (dg_step_many): independent quadtree Riemann problems stepped concurrently give, tree
-by tree, exactly the results of stepping each tree alone, and those match the reference solver run on
-each tree (one Integrator per tree)."""
+"""Batched trees (dg_step_many and the lockstep dg_batch): independent quadtree Riemann problems stepped
+concurrently give, tree by tree, exactly the results of stepping each tree alone, and those match the
+reference solver run on each tree (one Integrator per tree)."""
 import numpy as np
 import pytest
 
@@ -95,7 +95,34 @@ def test_lockstep_batch_equals_single_tree_steps():
         assert np.array_equal(sa.u, sb.u, equal_nan=True) and np.array_equal(sa.acti_level, sb.acti_level)
         ta, tb = a.stats(), s.stats()
         assert ta.cell_updates == tb.cell_updates and ta.n_substeps == tb.n_substeps
+        assert ta.n_splits == tb.n_splits and ta.n_unsplits == tb.n_unsplits
         assert ta.tree_size == tb.tree_size and ta.global_dt == tb.global_dt
+    for s in together + alone:
+        s.close()
+
+
+def test_lockstep_batch_stops_and_resumes():
+    """Pools with no room to spare: the planned runs stop at the capacity guard (and wherever a tree
+    populates a finer level), the host grows the pool and resumes, and every tree still gets its dg_step
+    result bit for bit."""
+    import dataclasses
+    batch = [dataclasses.replace(c, params=dataclasses.replace(c.params, pool_capacity=1))
+             for c in cases.riemann_batch(6, seed=5, base_levels=(4, 5), extra_levels=(2, 3))]
+    together = [Solver(c) for c in batch]
+    alone = [Solver(c) for c in batch]
+    b = Batch(together)
+    for _ in range(STEPS):
+        assert b.step() == [s.integrate()[1] for s in alone]
+    st = b.run_stats()
+    b.close()
+    assert st["stops"] > 0 and st["replayed"] > 0 and STEPS <= st["runs"] <= STEPS + st["stops"]
+    for a, s, c in zip(together, alone, batch):
+        sa, sb = a.active_cells().sorted(c.params.side_length), s.active_cells().sorted(c.params.side_length)
+        assert sa.n == sb.n
+        assert np.array_equal(sa.u, sb.u, equal_nan=True) and np.array_equal(sa.acti_level, sb.acti_level)
+        ta, tb = a.stats(), s.stats()
+        assert (ta.cell_updates, ta.n_substeps, ta.n_splits, ta.n_unsplits, ta.tree_size) == \
+            (tb.cell_updates, tb.n_substeps, tb.n_splits, tb.n_unsplits, tb.tree_size)
     for s in together + alone:
         s.close()
 
