@@ -62,6 +62,7 @@ def parse_args():
     ap.add_argument("--scale-steps", type=int, default=1)
     ap.add_argument("--scale-only", action="store_true", help="run only the scale workload and print its section")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned sections and print them")
+    ap.add_argument("--batched-only", action="store_true", help="run only the batched section and print it")
     ap.add_argument("--learned-shock", action="store_true",
                     help="also run the forecast-driven regrid on the shock-drop of the bench workload")
     ap.add_argument("--forms", default="fp64,mixed",
@@ -646,6 +647,11 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
     if args.scale_only:
         if rank == 0:
             print(json.dumps({"scale": scale_run(args, local_rank)}), flush=True)
+        return
+    if args.batched_only:
+        out = batched_run(args, rank, local_rank, world)
+        if rank == 0:
+            print(json.dumps({"batched": out}), flush=True)
         return
     if args.learned_only:
         if rank == 0:
