@@ -460,8 +460,9 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     if world > 1:
         dist.barrier()
     u0, t0 = updates(solvers), time.perf_counter()
+    breaks = 0
     for _ in range(args.steps):
-        b.step()
+        breaks += sum(b.step())
     torch.cuda.synchronize()
     l_sec, l_upd = time.perf_counter() - t0, updates(solvers) - u0
     runs = b.run_stats()
@@ -511,6 +512,7 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "value": l_u / (l_ms * 1e-3), "ms_per_step": l_ms / args.steps,
         "timing": "host wall clock around K lockstep batch steps (dg_batch_step), synchronised before and after",
         "planned_runs": runs,
+        "force_breaks": int(breaks),
         "profiled_step": {"wall_ms": prof_ms, "stage_ms": stages, "stage_sum_ms": round(sum(stages.values()), 3)},
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},

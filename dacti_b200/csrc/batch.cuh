@@ -846,15 +846,20 @@ public:
 			std::vector<SubArgs> scratch_args;
 			for (int j = 0; j < i; ++j) {
 				const bool more = next(cur, halted, pred.data(), L, sel);
-				if (!more || L != plan[j].L || sel != plan[j].sel) throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan");
+				if (!more || L != plan[j].L || sel != plan[j].sel)
+					throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan at substep " + std::to_string(j) + " of " +
+					                                       std::to_string(i) + (half ? " (tail stop)" : " (head stop)"));
 				make_args(L, sel, scratch_args);
 				advance(L, sel);
 				++replayed_;
 			}
-			if (i > 0) post_checks(plan[i - 1].sel, halted, force_break, global_dt);
+			// after a stop at the head of substep i the statuses are still those of substep i - 1; after a
+			// stop at its tail they are substep i's, and kb_begin(i) found every status clear before it
+			if (i > 0 && !half) post_checks(plan[i - 1].sel, halted, force_break, global_dt);
 			if (half) {
 				const bool more = next(cur, halted, pred.data(), L, sel);
-				if (!more || L != plan[i].L || sel != plan[i].sel) throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan");
+				if (!more || L != plan[i].L || sel != plan[i].sel)
+					throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan at the stopped substep " + std::to_string(i));
 				make_args(L, sel, scratch_args);
 				finish_substep(plan[i], i);
 				advance(L, sel);
