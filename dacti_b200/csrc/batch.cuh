@@ -8,20 +8,28 @@
 // finest level is coarser simply has no substep at sequence values that only finer levels use, which
 // is the stride skip of its own schedule.
 //
-// The host plans the whole global step at once: the schedule depends on the cluster counts only through
-// "is a level above the tree's finest level populated", and the cell counts only size the launches, so
-// the plan is made on the counts at the start of the step and every substep's arguments and block
-// offsets go to the device in one copy. Then all launches are issued with no synchronisation. Each
-// substep opens with a one-block guard that checks, on the live counts, what the plan assumed: no error
-// or NaN status, no populated level above a tree's planned finest level, every running cluster within
-// its tree's scratch rows. After the indicator a second guard checks that every tree's pool takes its
-// split requests. A failed guard stops the run there: that substep's kernels and all later ones find
-// their substep closed and return. The host then sees where the run stopped, replays its own bookkeeping
-// over the substeps that ran, completes a half-run substep itself (growing the pool, as Solver::substep
+// The host plans the global step ahead: the schedule depends on the cluster counts only through "is a
+// level above the tree's finest level populated", and the cell counts only size the launches, so a run
+// of substeps is planned on the counts as it starts and every substep's arguments and block offsets go
+// to the device in one copy. Then all launches of the run are issued with no synchronisation. A run
+// takes the rest of the step, up to a window that doubles after every run that nothing stopped (so a
+// warmed-up batch plans each global step as one run) and halves after a stop.
+//
+// Each substep opens with a one-block guard. A tree whose last substep left a NaN halts there for the
+// rest of the step, as Integrator::integrate returns on force_break; its blocks return in every later
+// substep, and the other trees, which are independent, run on unchanged. Then the guard checks, on the
+// live counts, what the plan assumed: no error status, no populated level above a tree's planned finest
+// level, every running cluster within its tree's scratch rows. After the indicator a second guard checks
+// that every tree's pool takes its split requests. A failed guard stops the run there: that substep's
+// kernels and all later ones find their substep closed and return. The host then sees where the run
+// stopped, replays its own bookkeeping over the substeps that ran (and, for a halted tree, over its own
+// substeps before the halt), completes a half-run substep itself (growing the pool, as Solver::substep
 // does), and plans again from there. The stage kernels run over a block range per tree (the blocks of a
 // launch are split among the trees in proportion to their planned work); the stage bodies read the live
 // cluster length, so an approximate split costs balance, never results.
 #pragma once
+
+#include <algorithm>
 
 #include "solver.cuh"
 
@@ -37,7 +45,7 @@ struct TreeArgs {
 	Counters *cnt;
 	long long scratch;  // rows of the tree's per-substep scratch (Pool::ff, Pool::du)
 	int limiter;
-	int halted;  // the tree runs no further substep in this global step
+	int halted;  // the tree runs no further substep in this global step (set by kb_begin on a NaN)
 	int finest;  // planned finest ACTI level: a populated level above it stops the run
 };
 
@@ -66,24 +74,35 @@ __device__ __forceinline__ int tree_of_block(const int *off, int nt) {
 	return lo;
 }
 
-// `on` is the substep's head or tail flag (kb_begin, kb_split_check).
+// `on` is the substep's head or tail flag (kb_begin, kb_split_check); a halted tree's blocks return.
 #define DG_BATCH_PROLOGUE                                     \
 	if (!*on || (int) blockIdx.x >= off[nt]) return;          \
 	const int t_      = tree_of_block(off, nt);               \
 	const SubArgs &s  = SA[t_];                               \
 	const TreeArgs &a = A[s.tree];                            \
+	if (a.halted) return;                                     \
 	const BlockRange g{off[t_], off[t_ + 1] - off[t_]};
 
 #define DG_BATCH_PARAMS const TreeArgs *A, const SubArgs *SA, const int *off, int nt, const int *on
 
-// Opens merged substep `idx`. In a planned run it first checks the plan's assumptions on the live
-// counts of every tree; if one fails, or an earlier substep stopped the run, the substep stays closed
-// (both flags 0) and the first stop is recorded as 2 * idx. Otherwise each listed tree's counters
-// n_recv .. status go to zero, its cluster length goes into its arguments, and both flags open.
-static __global__ void __launch_bounds__(256) kb_begin(const TreeArgs *A, int n_trees, SubArgs *SA, int nt,
-                                                      int *flags, int *stall, int idx) {
+// Opens merged substep `idx`. A tree whose last substep left a NaN (and nothing else) halts here, as
+// Integrator::integrate returns on force_break: its blocks return in every later substep of the run and
+// halt_at[t] = idx records where. The trees are independent, so the others' substeps are unchanged. Then,
+// in a planned run, the plan's assumptions are checked on the live counts of every running tree; if one
+// fails, or an earlier substep stopped the run, the substep stays closed (both flags 0) and the first
+// stop is recorded as 2 * idx. Otherwise each listed running tree's counters n_recv .. status go to
+// zero, its cluster length goes into its arguments, and both flags open.
+static __global__ void __launch_bounds__(256) kb_begin(TreeArgs *A, int n_trees, SubArgs *SA, int nt, int *flags,
+                                                      int *stall, int *halt_at, int idx) {
 	const int stopped = *stall != STALL_NONE;
-	int bad           = 0;
+	if (!stopped)
+		for (int t = threadIdx.x; t < n_trees; t += blockDim.x)
+			if (!A[t].halted && A[t].cnt->status == ST_NAN) {
+				A[t].halted = 1;
+				halt_at[t]  = idx;
+			}
+	int bad = 0;
+	__syncthreads();
 	if (!stopped) {
 		for (int t = threadIdx.x; t < n_trees; t += blockDim.x) {
 			const TreeArgs &a = A[t];
@@ -94,7 +113,7 @@ static __global__ void __launch_bounds__(256) kb_begin(const TreeArgs *A, int n_
 		}
 		for (int k = threadIdx.x; k < nt; k += blockDim.x) {
 			const TreeArgs &a = A[SA[k].tree];
-			bad |= (long long) a.cnt->clu[SA[k].L] > a.scratch;
+			bad |= !a.halted && (long long) a.cnt->clu[SA[k].L] > a.scratch;
 		}
 	}
 	if (__syncthreads_or(bad) || stopped) {
@@ -105,7 +124,8 @@ static __global__ void __launch_bounds__(256) kb_begin(const TreeArgs *A, int n_
 		return;
 	}
 	for (int k = threadIdx.x; k < nt; k += blockDim.x) {
-		SubArgs &s  = SA[k];
+		SubArgs &s = SA[k];
+		if (A[s.tree].halted) continue;
 		Counters *c = A[s.tree].cnt;
 		s.n         = c->clu[s.L];
 		c->n_recv = c->n_split = c->n_unsplit = c->n_new = c->n_upd = c->n_tmp = 0;
@@ -124,7 +144,7 @@ static __global__ void __launch_bounds__(256) kb_split_check(const TreeArgs *A, 
 	if (flags[1])
 		for (int k = threadIdx.x; k < nt; k += blockDim.x) {
 			const TreeArgs &a = A[SA[k].tree];
-			bad |= (long long) a.cnt->top + (long long) NC * a.cnt->n_split + 16 > a.P.cap;
+			bad |= !a.halted && (long long) a.cnt->top + (long long) NC * a.cnt->n_split + 16 > a.P.cap;
 		}
 	if (__syncthreads_or(bad) && threadIdx.x == 0) {
 		*stall   = 2 * idx + 1;
@@ -212,6 +232,7 @@ static __global__ void kb_swap(TreeArgs *A, const SubArgs *SA, int nt, const int
 	if (k >= nt || !*on) return;
 	TreeArgs &a   = A[SA[k].tree];
 	const int L   = SA[k].L;
+	if (a.halted) return;
 	int32_t *x    = a.Ls.clu[L];
 	a.Ls.clu[L]   = a.Ls.tmp;
 	a.Ls.tmp      = x;
@@ -228,7 +249,7 @@ static __global__ void kb_flush(DG_BATCH_PARAMS) {
 // cells after the flush, substeps).
 static __global__ void kb_done(const TreeArgs *A, const SubArgs *SA, int nt, const int *on) {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nt || !*on) return;
+	if (k >= nt || !*on || A[SA[k].tree].halted) return;
 	Counters *c = A[SA[k].tree].cnt;
 	const int L = SA[k].L;
 	c->buf[L]   = 0;
@@ -311,6 +332,10 @@ class Batch : public BatchBase {
 	char *d_arena_ = nullptr, *h_arena_ = nullptr;  // substep slots: flags, SubArgs, offset tables
 	size_t arena_cap_ = 0;
 	int *d_stall_ = nullptr, *h_stall_ = nullptr, *h_one_ = nullptr;
+	int *d_halt_ = nullptr, *h_halt_ = nullptr;  // per tree: the planned substep whose kb_begin halted it
+	static constexpr int WINDOW_MIN = 64, WINDOW_MAX = 1 << 16;
+	int window_ = 512;  // substeps one planned run takes at most: doubles after a run that nothing stopped,
+	                    // halves after a stop
 	int device_ = 0;
 	int sms_    = 148;
 	bool mixed_ = false, visc_ = false, sigma_ = false;
@@ -358,6 +383,8 @@ public:
 		DG_CUDA(cudaMalloc(&d_stall_, sizeof(int)));
 		DG_CUDA(cudaMallocHost(&h_stall_, sizeof(int)));
 		DG_CUDA(cudaMallocHost(&h_one_, sizeof(int)));
+		DG_CUDA(cudaMalloc(&d_halt_, sizeof(int) * nt));
+		DG_CUDA(cudaMallocHost(&h_halt_, sizeof(int) * nt));
 		*h_one_ = 1;
 		// every solver moves onto the batch's stream and its counters into the batch's array
 		for (int t = 0; t < nt; ++t) {
@@ -399,6 +426,8 @@ public:
 		cudaFree(d_stall_);
 		cudaFreeHost(h_stall_);
 		cudaFreeHost(h_one_);
+		cudaFree(d_halt_);
+		cudaFreeHost(h_halt_);
 		for (auto &t: timed_) cudaEventDestroy(t.a), cudaEventDestroy(t.b);
 		for (auto e: ev_free_) cudaEventDestroy(e);
 		cudaStreamDestroy(st_);
@@ -460,6 +489,7 @@ private:
 	void sync() {
 		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters) * s_.size(), cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaMemcpyAsync(h_stall_, d_stall_, sizeof(int), cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaMemcpyAsync(h_halt_, d_halt_, sizeof(int) * s_.size(), cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
 		if (prof_) drain();
 	}
@@ -692,7 +722,7 @@ private:
 		const TreeArgs *A     = d_trees_;
 		const int *on         = flags;
 		if (head) {
-			kb_begin<<<1, 256, 0, st_>>>(A, (int) s_.size(), S, nt, flags, d_stall_, idx);
+			kb_begin<<<1, 256, 0, st_>>>(d_trees_, (int) s_.size(), S, nt, flags, d_stall_, d_halt_, idx);
 			stage(p, T_FACE, off, [&](int grid, const int *o) {
 				if (mixed_) {
 					if (visc_) kb_face_sum<M, true, float><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
@@ -746,9 +776,10 @@ private:
 
 	// Completes planned substep `idx`, whose run stopped at the capacity guard: the pools that cannot take
 	// their split requests grow (Solver::substep), then the substep's tail runs.
-	void finish_substep(const Planned &p, int idx) {
+	void finish_substep(const Planned &p, int idx, const std::vector<char> &dev_halted) {
 		bool grown = false;
 		for (int t: p.sel) {
+			if (dev_halted[t]) continue;
 			Solver<M> *s         = s_[t];
 			const long long need = (long long) s->h_cnt_->top + (long long) NC * s->h_cnt_->n_split + 16;
 			if (need > s->P_.cap) {
@@ -764,6 +795,7 @@ private:
 				a.P         = s_[t]->P_;
 				a.Ls        = s_[t]->Ls_;
 				a.scratch   = s_[t]->scratch_cap_;
+				a.halted    = a.halted || dev_halted[t];
 			}
 			upload_trees();
 		}
@@ -771,6 +803,25 @@ private:
 		DG_CUDA(cudaMemcpyAsync(flags + 1, h_one_, sizeof(int), cudaMemcpyHostToDevice, st_));
 		launch(p, idx, false, true);
 		sync();
+	}
+
+	// Tree t halted on the device at planned substep h (a NaN from its substep before h): its host state
+	// goes back to the run's start `z` and forward over its own substeps of the plan before h.
+	void replay_tree(int t, int h, const TreeState &z, const std::vector<Planned> &plan) {
+		Solver<M> *s = s_[t];
+		restore(s, z);
+		const std::vector<int> one{t};
+		std::vector<SubArgs> tmp;
+		for (int j = 0; j < h && j < (int) plan.size(); ++j) {
+			const Planned &p = plan[j];
+			if (!std::binary_search(p.sel.begin(), p.sel.end(), t)) continue;
+			if (p.L > s->max_acti_) {  // the level next() had the tree take on
+				s->max_acti_       = p.L;
+				s->acti_time_[p.L] = s->acti_time_[p.L - 1];
+			}
+			make_args(p.L, one, tmp);
+			advance(p.L, one);
+		}
 	}
 
 public:
@@ -785,6 +836,11 @@ public:
 			DG_CUDA(cudaMemcpyAsync(d_consts_ + t, &s->C_, sizeof(Consts), cudaMemcpyHostToDevice, st_));
 		}
 		std::vector<char> halted(N, 0);
+		auto halt = [&](int t) {
+			force_break[t] = 1;
+			global_dt[t]   = s_[t]->global_dt_;
+			halted[t]      = 1;
+		};
 		// a status left from before the step belongs to no substep of it
 		for (int t = 0; t < N; ++t) {
 			s_[t]->check_status();
@@ -796,20 +852,28 @@ public:
 		std::vector<Planned> plan;
 		std::vector<TreeState> saved(N);
 		std::vector<Counters> pred(N);
+		std::vector<int> all(N);
+		for (int t = 0; t < N; ++t) all[t] = t;
 		bool first = true;
 		while (true) {
-			// plan the rest of the step on the counts as they are now (the stream is idle, h_cnt_ current)
+			// plan up to window_ substeps of the rest of the step on the counts as they are now (the
+			// stream is idle, h_cnt_ current)
 			if (!first) prepare(halted);
-			first                    = false;
-			const Cursor cur0        = cur;
-			const auto halted0       = halted;
+			first              = false;
+			const Cursor cur0  = cur;
+			const auto halted0 = halted;
 			for (int t = 0; t < N; ++t) saved[t] = save(s_[t]);
 			std::copy(h_cnt_, h_cnt_ + N, pred.begin());
 			plan.clear();
-			size_t bytes = 0;
+			size_t bytes  = 0;
+			bool finished = false;
 			int L;
 			std::vector<int> sel;
-			while (next(cur, halted, pred.data(), L, sel)) {
+			while ((int) plan.size() < window_) {
+				if (!next(cur, halted, pred.data(), L, sel)) {
+					finished = true;
+					break;
+				}
 				Planned p;
 				p.L   = L;
 				p.sel = sel;
@@ -824,19 +888,33 @@ public:
 			for (auto &p: plan) write_slot(p, pred.data());
 			DG_CUDA(cudaMemcpyAsync(d_arena_, h_arena_, bytes, cudaMemcpyHostToDevice, st_));
 			DG_CUDA(cudaMemsetAsync(d_stall_, 0x7f, sizeof(int), st_));
+			DG_CUDA(cudaMemsetAsync(d_halt_, 0x7f, sizeof(int) * N, st_));
 			for (size_t i = 0; i < plan.size(); ++i) launch(plan[i], (int) i, true, true);
 			sync();
 			++runs_;
 			planned_ += (long long) plan.size();
+			// trees that a NaN halted on the device, with the substep where it was seen
+			std::vector<std::pair<int, int>> halts;
+			std::vector<char> dev_halted(N, 0);
+			for (int t = 0; t < N; ++t)
+				if (h_halt_[t] != STALL_NONE) {
+					halts.push_back({t, h_halt_[t]});
+					dev_halted[t] = 1;
+				}
 			const int stop = *h_stall_;
 			if (stop == STALL_NONE) {
-				// every planned substep ran: a NaN in a tree's last substep halts it now
-				std::vector<int> all(N);
-				for (int t = 0; t < N; ++t) all[t] = t;
+				for (auto &th: halts) {
+					replay_tree(th.first, th.second, saved[th.first], plan);
+					halt(th.first);
+				}
+				// a NaN in a tree's last substep of the run halts it now; an error throws
 				post_checks(all, halted, force_break, global_dt);
-				break;
+				if (finished) break;
+				window_ = std::min(window_ * 2, WINDOW_MAX);
+				continue;
 			}
 			++stops_;
+			window_     = std::max(window_ / 2, WINDOW_MIN);
 			const int i = stop / 2, half = stop & 1;
 			if (i == 0 && !half) throw dg_error(DG_ERR_UNSUPPORTED, "batch: a planned run stopped before its first substep");
 			// back to the state before the run, then forward over the substeps that ran
@@ -853,18 +931,24 @@ public:
 				advance(L, sel);
 				++replayed_;
 			}
-			// after a stop at the head of substep i the statuses are still those of substep i - 1; after a
-			// stop at its tail they are substep i's, and kb_begin(i) found every status clear before it
-			if (i > 0 && !half) post_checks(plan[i - 1].sel, halted, force_break, global_dt);
-			if (half) {
+			if (!half) {
+				// the statuses are still those of substep i - 1 (a NaN there has halted its tree already)
+				if (i > 0) post_checks(plan[i - 1].sel, halted, force_break, global_dt);
+			} else {
+				// substep i's head ran: its statuses are substep i's, and kb_begin(i) found every running
+				// tree's status clear before it
 				const bool more = next(cur, halted, pred.data(), L, sel);
 				if (!more || L != plan[i].L || sel != plan[i].sel)
 					throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan at the stopped substep " + std::to_string(i));
 				make_args(L, sel, scratch_args);
-				finish_substep(plan[i], i);
+				finish_substep(plan[i], i, dev_halted);
 				advance(L, sel);
 				++replayed_;
 				post_checks(sel, halted, force_break, global_dt);
+			}
+			for (auto &th: halts) {
+				replay_tree(th.first, th.second, saved[th.first], plan);
+				halt(th.first);
 			}
 		}
 		for (int t = 0; t < N; ++t) {

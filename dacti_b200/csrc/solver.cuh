@@ -61,6 +61,8 @@ inline int grid_for(long long n, int max_blocks = 148 * 16) {
 	if (b > max_blocks) b = max_blocks;
 	return (int) b;
 }
+// The same number of threads in blocks of `threads`.
+inline int grid_threads(long long n, int threads) { return grid_for(n) * (BLOCK / threads); }
 
 template<class M>
 class Batch;
@@ -621,23 +623,23 @@ private:
 
 	// Face-flux sums of the running cluster into du, receivers of slower clusters into Ls_.recv.
 	void launch_face_sum(const int32_t *list, int n, int L, double dtL, int stamp) {
-		constexpr int G = NF <= 4 ? 4 : 8;
-		const int g = grid_for((long long) n * G);
+		constexpr int G = NF <= 4 ? 4 : 8, T = FACE_THREADS;
+		const int g = grid_threads((long long) n * G, T);
 		if (mixed_) {
-			if (visc_) k_face_sum<M, true, float><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
-			else k_face_sum<M, false, float><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			if (visc_) k_face_sum<M, true, float><<<g, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			else k_face_sum<M, false, float><<<g, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
 		} else {
-			if (visc_) k_face_sum<M, true, double><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
-			else k_face_sum<M, false, double><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			if (visc_) k_face_sum<M, true, double><<<g, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			else k_face_sum<M, false, double><<<g, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
 		}
 	}
 
 	// Slopes, Hancock rhs and (viscous) gradients of a cell list.
 	void launch_slope(const int32_t *list, int n) {
-		constexpr int G = NF <= 4 ? 4 : 8;
-		const int g = grid_for((long long) n * G);
-		if (visc_) k_slope<M, true><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
-		else k_slope<M, false><<<g, BLOCK, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
+		constexpr int G = NF <= 4 ? 4 : 8, T = SLOPE_THREADS;
+		const int g = grid_threads((long long) n * G, T);
+		if (visc_) k_slope<M, true><<<g, T, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
+		else k_slope<M, false><<<g, T, 0, st_>>>(P_, C_, B_, list, n, limiter_, ++epoch_, d_cnt_);
 	}
 
 	void sync_counters() {

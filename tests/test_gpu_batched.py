@@ -127,6 +127,34 @@ def test_lockstep_batch_stops_and_resumes():
         s.close()
 
 
+def test_lockstep_batch_force_breaks_equal_single_tree_steps():
+    """Config 3's quadrant states drive some trees to a NaN pressure (force_break). A NaN tree halts on the
+    device for the rest of the global step while the other trees run on; every tree, the halted ones
+    included, still gets its dg_step result bit for bit, force_break flags and global dt too."""
+    batch = cases.riemann_batch(24, seed=3, base_levels=(4, 5), extra_levels=(2, 3))
+    together = [Solver(c) for c in batch]
+    alone = [Solver(c) for c in batch]
+    b = Batch(together)
+    breaks = 0
+    for _ in range(STEPS):
+        fb_t = b.step()
+        fb_a = [s.integrate()[1] for s in alone]
+        assert fb_t == fb_a
+        breaks += sum(fb_t)
+        assert [s.global_dt for s in together] == [s.global_dt for s in alone]
+    b.close()
+    assert breaks > 0
+    for a, s, c in zip(together, alone, batch):
+        sa, sb = a.active_cells().sorted(c.params.side_length), s.active_cells().sorted(c.params.side_length)
+        assert sa.n == sb.n
+        assert np.array_equal(sa.u, sb.u, equal_nan=True) and np.array_equal(sa.acti_level, sb.acti_level)
+        ta, tb = a.stats(), s.stats()
+        assert (ta.cell_updates, ta.n_substeps, ta.n_splits, ta.n_unsplits, ta.tree_size) == \
+            (tb.cell_updates, tb.n_substeps, tb.n_splits, tb.n_unsplits, tb.tree_size)
+    for s in together + alone:
+        s.close()
+
+
 def test_lockstep_batch_multiphase_matches_reference(tmp_path):
     """Two five-equation trees of different sizes in one dg_batch against the reference solver."""
     trees = [cases.shock_drop(base_level=3, levels=2), cases.shock_drop(base_level=4, levels=1)]
