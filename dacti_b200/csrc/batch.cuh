@@ -8,25 +8,28 @@
 // finest level is coarser simply has no substep at sequence values that only finer levels use, which
 // is the stride skip of its own schedule.
 //
-// The host plans the global step ahead: the schedule depends on the cluster counts only through "is a
-// level above the tree's finest level populated", and the cell counts only size the launches, so a run
-// of substeps is planned on the counts as it starts and every substep's arguments and block offsets go
-// to the device in one copy. Then all launches of the run are issued with no synchronisation. A run
-// takes the rest of the step, up to a window that doubles after every run that nothing stopped (so a
-// warmed-up batch plans each global step as one run) and halves after a stop.
+// The host plans the global step ahead, in runs of substeps issued with no synchronisation. The merged
+// sequence of (sequence value, level) pairs depends only on the batch's finest populated level F: the
+// stride of the sequence counter is F's. Which trees run a pair's substep, and with which stamps, epochs
+// and ACTI counters, is decided on the device: each tree's schedule state (max_acti_level, ACTI
+// counters and times, stamp and epoch counters) lives in device memory, and the substep's opening kernel
+// applies the reference's rule to the live counts, a tree taking on a newly populated level up to its
+// planned headroom as Integrator::integrate does. So the plan is the pairs of the rest of the step, each
+// with the trees that may run it, and one copy takes every substep's arguments and block offsets to the
+// device. A run takes the rest of the step, up to a window that doubles after every run nothing stopped
+// (a warmed-up batch plans each global step as one run) and halves after a stop.
 //
-// Each substep opens with a one-block guard. A tree whose last substep left a NaN halts there for the
-// rest of the step, as Integrator::integrate returns on force_break; its blocks return in every later
-// substep, and the other trees, which are independent, run on unchanged. Then the guard checks, on the
-// live counts, what the plan assumed: no error status, no populated level above a tree's planned finest
-// level, every running cluster within its tree's scratch rows. After the indicator a second guard checks
-// that every tree's pool takes its split requests. A failed guard stops the run there: that substep's
-// kernels and all later ones find their substep closed and return. The host then sees where the run
-// stopped, replays its own bookkeeping over the substeps that ran (and, for a halted tree, over its own
-// substeps before the halt), completes a half-run substep itself (growing the pool, as Solver::substep
-// does), and plans again from there. The stage kernels run over a block range per tree (the blocks of a
-// launch are split among the trees in proportion to their planned work); the stage bodies read the live
-// cluster length, so an approximate split costs balance, never results.
+// Each substep opens with a one-block kernel (kb_begin). A tree whose last substep left a NaN halts
+// there for the rest of the step, as Integrator::integrate returns on force_break; the other trees are
+// independent and run on unchanged. Then the kernel checks what the plan assumed: no error status, no
+// populated level above a tree's planned headroom (a level above F changes the sequence's stride), every
+// running cluster within its tree's scratch rows. After the indicator a second kernel checks that every
+// pool takes its split requests. A failed check stops the run there: that substep's kernels and all
+// later ones find their substep closed and return. The host reads the trees' schedule state back,
+// completes a half-run substep itself (growing the pool, as Solver::substep does), and plans again from
+// there. The stage kernels run over a block range per tree (the blocks of a launch are split among the
+// trees in proportion to their planned work); the stage bodies read the live cluster length, so an
+// approximate split costs balance, never results.
 #pragma once
 
 #include <algorithm>
@@ -35,28 +38,40 @@
 
 namespace dg {
 
-// Per-tree arguments of the batched stage kernels: fixed while a planned run executes, except the list
-// pointers of the running level, which kb_swap exchanges on the device as Solver::substep does on the host.
+// A tree's schedule state in the merged step (Integrator: max_acti_level, acti_counter, acti_time, and
+// this port's stamp and epoch counters), kept on the device while a run executes.
+struct TreeSched {
+	int max_acti, stamp, epoch, pad;
+	int counter[MAX_ACTI];
+	double time[MAX_ACTI];
+};
+
+// Per-tree arguments of the batched stage kernels: fixed while a run executes, except the list pointers
+// of the running level, which kb_swap exchanges as Solver::substep does, and the halt flag.
 struct TreeArgs {
 	Pool P;
 	const Consts *C;  // device copy of the tree's constants
 	BcTable B;
 	Lists Ls;
 	Counters *cnt;
+	TreeSched *sch;
 	long long scratch;  // rows of the tree's per-substep scratch (Pool::ff, Pool::du)
 	int limiter;
 	int halted;  // the tree runs no further substep in this global step (set by kb_begin on a NaN)
-	int finest;  // planned finest ACTI level: a populated level above it stops the run
+	int finest;  // planned headroom: the tree may run levels up to here; a populated level above stops the run
+	int epochs;  // epoch numbers one substep uses
 };
 
-// Per-tree arguments of one merged substep.
+// Per-tree arguments of one merged substep: tree, level and dtL from the plan, the rest from kb_begin.
 struct SubArgs {
 	int tree;  // index into the TreeArgs array
 	int L;
-	int n;  // cluster length as the substep starts (written by kb_begin)
+	int n;  // cluster length as the substep starts
 	int counterL;
 	int stamp;
 	int epoch0;  // the tree's epoch counter before the substep (kernels use epoch0 + k)
+	int active;  // the tree runs this substep
+	int pad;
 	double dtL;
 };
 
@@ -74,24 +89,29 @@ __device__ __forceinline__ int tree_of_block(const int *off, int nt) {
 	return lo;
 }
 
-// `on` is the substep's head or tail flag (kb_begin, kb_split_check); a halted tree's blocks return.
+// `on` is the substep's head or tail flag (kb_begin, kb_split_check); the blocks of a tree that does not
+// run the substep return.
 #define DG_BATCH_PROLOGUE                                     \
 	if (!*on || (int) blockIdx.x >= off[nt]) return;          \
-	const int t_      = tree_of_block(off, nt);               \
-	const SubArgs &s  = SA[t_];                               \
+	const int t_     = tree_of_block(off, nt);                \
+	const SubArgs &s = SA[t_];                                \
+	if (!s.active) return;                                    \
 	const TreeArgs &a = A[s.tree];                            \
-	if (a.halted) return;                                     \
 	const BlockRange g{off[t_], off[t_ + 1] - off[t_]};
 
 #define DG_BATCH_PARAMS const TreeArgs *A, const SubArgs *SA, const int *off, int nt, const int *on
 
 // Opens merged substep `idx`. A tree whose last substep left a NaN (and nothing else) halts here, as
-// Integrator::integrate returns on force_break: its blocks return in every later substep of the run and
-// halt_at[t] = idx records where. The trees are independent, so the others' substeps are unchanged. Then,
-// in a planned run, the plan's assumptions are checked on the live counts of every running tree; if one
-// fails, or an earlier substep stopped the run, the substep stays closed (both flags 0) and the first
-// stop is recorded as 2 * idx. Otherwise each listed running tree's counters n_recv .. status go to
-// zero, its cluster length goes into its arguments, and both flags open.
+// Integrator::integrate returns on force_break: it runs no later substep of the step, and halt_at[t] =
+// idx records where. The trees are independent, so the others' substeps are unchanged. Then, in order:
+// - the run's assumptions on the live counts of every running tree: no error status, no populated level
+//   above the tree's headroom, the running clusters within the scratch rows. If one fails, or an earlier
+//   substep stopped the run, the substep stays closed (both flags 0) and the first stop is recorded as
+//   2 * idx;
+// - for each listed tree, Integrator::integrate's rule for level L (impl/integrate.hpp:32-39): a populated
+//   level above max_acti_level becomes the tree's finest (its time taken from the next coarser level),
+//   and the tree runs the substep if L <= max_acti_level. A running tree's counters n_recv .. status go
+//   to zero and its arguments get the cluster length, the ACTI counter and the next stamp and epochs.
 static __global__ void __launch_bounds__(256) kb_begin(TreeArgs *A, int n_trees, SubArgs *SA, int nt, int *flags,
                                                       int *stall, int *halt_at, int idx) {
 	const int stopped = *stall != STALL_NONE;
@@ -101,8 +121,8 @@ static __global__ void __launch_bounds__(256) kb_begin(TreeArgs *A, int n_trees,
 				A[t].halted = 1;
 				halt_at[t]  = idx;
 			}
-	int bad = 0;
 	__syncthreads();
+	int bad = 0;
 	if (!stopped) {
 		for (int t = threadIdx.x; t < n_trees; t += blockDim.x) {
 			const TreeArgs &a = A[t];
@@ -113,7 +133,9 @@ static __global__ void __launch_bounds__(256) kb_begin(TreeArgs *A, int n_trees,
 		}
 		for (int k = threadIdx.x; k < nt; k += blockDim.x) {
 			const TreeArgs &a = A[SA[k].tree];
-			bad |= !a.halted && (long long) a.cnt->clu[SA[k].L] > a.scratch;
+			const int L       = SA[k].L;
+			const int n       = a.cnt->clu[L];
+			bad |= !a.halted && (L <= a.sch->max_acti || n > 0) && (long long) n > a.scratch;
 		}
 	}
 	if (__syncthreads_or(bad) || stopped) {
@@ -124,12 +146,29 @@ static __global__ void __launch_bounds__(256) kb_begin(TreeArgs *A, int n_trees,
 		return;
 	}
 	for (int k = threadIdx.x; k < nt; k += blockDim.x) {
-		SubArgs &s = SA[k];
-		if (A[s.tree].halted) continue;
-		Counters *c = A[s.tree].cnt;
-		s.n         = c->clu[s.L];
-		c->n_recv = c->n_split = c->n_unsplit = c->n_new = c->n_upd = c->n_tmp = 0;
-		c->status                                                        = 0;
+		SubArgs &s        = SA[k];
+		const TreeArgs &a = A[s.tree];
+		int run           = 0;
+		if (!a.halted) {
+			TreeSched &z = *a.sch;
+			Counters *c  = a.cnt;
+			const int L  = s.L;
+			if (c->clu[L] > 0 && L > z.max_acti) {
+				z.max_acti = L;
+				z.time[L]  = z.time[L - 1];
+			}
+			run = L <= z.max_acti;
+			if (run) {
+				s.n        = c->clu[L];
+				s.counterL = z.counter[L];
+				s.stamp    = ++z.stamp;
+				s.epoch0   = z.epoch;
+				z.epoch += a.epochs;
+				c->n_recv = c->n_split = c->n_unsplit = c->n_new = c->n_upd = c->n_tmp = 0;
+				c->status                                                        = 0;
+			}
+		}
+		s.active = run;
 	}
 	if (threadIdx.x == 0) flags[0] = flags[1] = 1;
 }
@@ -144,7 +183,7 @@ static __global__ void __launch_bounds__(256) kb_split_check(const TreeArgs *A, 
 	if (flags[1])
 		for (int k = threadIdx.x; k < nt; k += blockDim.x) {
 			const TreeArgs &a = A[SA[k].tree];
-			bad |= !a.halted && (long long) a.cnt->top + (long long) NC * a.cnt->n_split + 16 > a.P.cap;
+			bad |= SA[k].active && (long long) a.cnt->top + (long long) NC * a.cnt->n_split + 16 > a.P.cap;
 		}
 	if (__syncthreads_or(bad) && threadIdx.x == 0) {
 		*stall   = 2 * idx + 1;
@@ -153,7 +192,7 @@ static __global__ void __launch_bounds__(256) kb_split_check(const TreeArgs *A, 
 }
 
 template<class M, bool V, class R>
-__global__ void __launch_bounds__(BLOCK, 2) kb_face_sum(DG_BATCH_PARAMS) {
+__global__ void __launch_bounds__(FACE_THREADS, FACE_MIN_BLOCKS) kb_face_sum(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
 	d_face_sum<M, V, R>(g, a.P, *a.C, a.B, a.Ls.clu[s.L], s.n, s.L, s.dtL, s.stamp, a.Ls.recv, a.cnt);
 }
@@ -171,7 +210,7 @@ __global__ void __launch_bounds__(BLOCK, 3) kb_update(DG_BATCH_PARAMS) {
 }
 
 template<class M, bool V>
-__global__ void __launch_bounds__(BLOCK) kb_slope(DG_BATCH_PARAMS) {
+__global__ void __launch_bounds__(SLOPE_THREADS, SLOPE_MIN_BLOCKS) kb_slope(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
 	d_slope<M, V>(g, a.P, *a.C, a.B, a.Ls.clu[s.L], s.n, a.limiter, s.epoch0 + 2, a.cnt);
 }
@@ -229,10 +268,9 @@ __global__ void kb_regrid(DG_BATCH_PARAMS, int k) {
 // swap of Lists::clu[L] and Lists::tmp).
 static __global__ void kb_swap(TreeArgs *A, const SubArgs *SA, int nt, const int *on) {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nt || !*on) return;
+	if (k >= nt || !*on || !SA[k].active) return;
 	TreeArgs &a   = A[SA[k].tree];
 	const int L   = SA[k].L;
-	if (a.halted) return;
 	int32_t *x    = a.Ls.clu[L];
 	a.Ls.clu[L]   = a.Ls.tmp;
 	a.Ls.tmp      = x;
@@ -245,14 +283,18 @@ static __global__ void kb_flush(DG_BATCH_PARAMS) {
 	d_flush(g, a.P, a.Ls.buf[s.L], &a.cnt->buf[s.L], a.Ls.clu[s.L], &a.cnt->clu[s.L], s.L, a.cnt);
 }
 
-// Closes a substep: buffer L to zero, then the running totals (splits, coarsenings, the cluster's
-// cells after the flush, substeps).
+// Closes a substep for each tree that ran it: the ACTI counter and time of level L advance
+// (impl/integrate.hpp:56-57), buffer L goes to zero, then the running totals (splits, coarsenings, the
+// cluster's cells after the flush, substeps).
 static __global__ void kb_done(const TreeArgs *A, const SubArgs *SA, int nt, const int *on) {
 	const int k = blockIdx.x * blockDim.x + threadIdx.x;
-	if (k >= nt || !*on || A[SA[k].tree].halted) return;
-	Counters *c = A[SA[k].tree].cnt;
-	const int L = SA[k].L;
-	c->buf[L]   = 0;
+	if (k >= nt || !*on || !SA[k].active) return;
+	const TreeArgs &a = A[SA[k].tree];
+	Counters *c       = a.cnt;
+	const int L       = SA[k].L;
+	a.sch->counter[L] = (a.sch->counter[L] + 1) % 2;
+	a.sch->time[L] += SA[k].dtL;
+	c->buf[L] = 0;
 	c->n_split_total += (unsigned long long) c->n_split;
 	c->n_unsplit_total += (unsigned long long) c->n_unsplit;
 	c->n_updates_total += (unsigned long long) c->clu[L];
@@ -260,9 +302,9 @@ static __global__ void kb_done(const TreeArgs *A, const SubArgs *SA, int nt, con
 }
 
 // Status of every tree to zero as a global step starts (a tree's status holds its last substep's).
-static __global__ void kb_clear_status(const TreeArgs *A, int n_trees) {
+static __global__ void kb_clear_status(Counters *cnt, int n_trees) {
 	const int t = blockIdx.x * blockDim.x + threadIdx.x;
-	if (t < n_trees) A[t].cnt->status = 0;
+	if (t < n_trees) cnt[t].status = 0;
 }
 
 #undef DG_BATCH_PROLOGUE
@@ -291,6 +333,7 @@ class Batch : public BatchBase {
 	static constexpr int D = M::D, NC = 1 << D, NF = 2 * D;
 	static constexpr int EPOCHS = EPOCH_EST<M> + 2;  // epoch numbers one substep uses per tree
 	static constexpr int LANES  = NF <= 4 ? 4 : 8;    // lanes per cell of the lane-group stages
+	static constexpr int HEADROOM = 2;  // levels above its finest that a tree may take on within a run
 
 	// Block-offset tables of a substep: the stage kind whose budget sizes the launch, and the work items
 	// per cluster cell it is split by (lanes, cells, new cells, repair tasks, buffer cells).
@@ -298,6 +341,9 @@ class Batch : public BatchBase {
 	static constexpr int TABLE_STAGE[TABLES] = {BS_FACE_SUM, BS_RECEIVE, BS_UPDATE, BS_SLOPE, BS_AUX, BS_AUX,
 	                                            BS_ESTIMATE, BS_REGRID_CELL, BS_REGRID_FRESH, BS_NBR_LIST, BS_FLUSH};
 	static constexpr long long TABLE_ITEMS[TABLES] = {LANES, LANES, 1, LANES, LANES, 1, LANES, 1, NC + 1, (NC + 1) * NF, 0};
+	// threads per block of each table's launches (the face sums and slopes run smaller blocks)
+	static constexpr int TABLE_THREADS[TABLES] = {FACE_THREADS, BLOCK, BLOCK, SLOPE_THREADS, BLOCK, BLOCK,
+	                                              BLOCK, BLOCK, BLOCK, BLOCK, BLOCK};
 
 	// The schedule's position: sequence value and the next level index to look at in it (MAX_ACTI: the
 	// next sequence value is due).
@@ -305,18 +351,12 @@ class Batch : public BatchBase {
 		int seq = 0;
 		int l   = MAX_ACTI;
 	};
-	// A tree's host-side schedule state, saved before a planned run and restored when it stops early.
-	struct TreeState {
-		int max_acti, stamp, epoch;
-		int acti_counter[MAX_ACTI];
-		double acti_time[MAX_ACTI];
-		Lists Ls;
-	};
-	// One planned merged substep: its level, its trees, their arguments and its slot in the arena.
+	// One planned merged substep: its level, the trees that may run it, the schedule position after it
+	// and its slot in the arena.
 	struct Planned {
 		int L;
 		std::vector<int> sel;
-		std::vector<SubArgs> args;
+		Cursor after;
 		size_t at;
 		int grid[TABLES];
 		long long items[TABLES];
@@ -329,6 +369,7 @@ class Batch : public BatchBase {
 	std::vector<Counters *> own_d_, own_h_;
 	Consts *d_consts_ = nullptr;  // all trees' constants
 	TreeArgs *d_trees_ = nullptr, *h_trees_ = nullptr;
+	TreeSched *d_sched_ = nullptr, *h_sched_ = nullptr;
 	char *d_arena_ = nullptr, *h_arena_ = nullptr;  // substep slots: flags, SubArgs, offset tables
 	size_t arena_cap_ = 0;
 	int *d_stall_ = nullptr, *h_stall_ = nullptr, *h_one_ = nullptr;
@@ -354,7 +395,7 @@ class Batch : public BatchBase {
 		long long split, unsplit, updates, substeps;
 	};
 	std::vector<Base> base_;  // the solvers' statistics when they joined the batch
-	long long runs_ = 0, stops_ = 0, planned_ = 0, replayed_ = 0;
+	long long runs_ = 0, stops_ = 0, planned_ = 0, completed_ = 0;
 
 public:
 	explicit Batch(const std::vector<SolverBase *> &solvers) {
@@ -380,6 +421,8 @@ public:
 		DG_CUDA(cudaMalloc(&d_consts_, sizeof(Consts) * nt));
 		DG_CUDA(cudaMalloc(&d_trees_, sizeof(TreeArgs) * nt));
 		DG_CUDA(cudaMallocHost(&h_trees_, sizeof(TreeArgs) * nt));
+		DG_CUDA(cudaMalloc(&d_sched_, sizeof(TreeSched) * nt));
+		DG_CUDA(cudaMallocHost(&h_sched_, sizeof(TreeSched) * nt));
 		DG_CUDA(cudaMalloc(&d_stall_, sizeof(int)));
 		DG_CUDA(cudaMallocHost(&h_stall_, sizeof(int)));
 		DG_CUDA(cudaMallocHost(&h_one_, sizeof(int)));
@@ -421,6 +464,8 @@ public:
 		cudaFree(d_consts_);
 		cudaFree(d_trees_);
 		cudaFreeHost(h_trees_);
+		cudaFree(d_sched_);
+		cudaFreeHost(h_sched_);
 		cudaFree(d_arena_);
 		cudaFreeHost(h_arena_);
 		cudaFree(d_stall_);
@@ -454,10 +499,10 @@ public:
 		}
 	}
 
-	// Planned runs, runs stopped by a guard, substeps planned and substeps replayed on the host after a
-	// stop, since the batch was made.
+	// Planned runs, runs a check stopped, substeps planned and substeps the host completed after a stop,
+	// since the batch was made.
 	void run_stats(long long *out, int n) override {
-		const long long v[4] = {runs_, stops_, planned_, replayed_};
+		const long long v[4] = {runs_, stops_, planned_, completed_};
 		for (int k = 0; k < n && k < 4; ++k) out[k] = v[k];
 	}
 
@@ -486,36 +531,40 @@ private:
 		timed_.clear();
 	}
 
+	// Counters, the stop record, the halts, the trees' schedule state and list pointers back to the host;
+	// the solvers take their schedule state and lists from the device.
 	void sync() {
-		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters) * s_.size(), cudaMemcpyDeviceToHost, st_));
+		const size_t N = s_.size();
+		DG_CUDA(cudaMemcpyAsync(h_cnt_, d_cnt_, sizeof(Counters) * N, cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaMemcpyAsync(h_stall_, d_stall_, sizeof(int), cudaMemcpyDeviceToHost, st_));
-		DG_CUDA(cudaMemcpyAsync(h_halt_, d_halt_, sizeof(int) * s_.size(), cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaMemcpyAsync(h_halt_, d_halt_, sizeof(int) * N, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaMemcpyAsync(h_sched_, d_sched_, sizeof(TreeSched) * N, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaMemcpyAsync(h_trees_, d_trees_, sizeof(TreeArgs) * N, cudaMemcpyDeviceToHost, st_));
 		DG_CUDA(cudaStreamSynchronize(st_));
 		if (prof_) drain();
+		for (size_t t = 0; t < N; ++t) {
+			Solver<M> *s       = s_[t];
+			const TreeSched &z = h_sched_[t];
+			s->max_acti_       = z.max_acti;
+			s->stamp_          = z.stamp;
+			s->epoch_          = z.epoch;
+			std::copy(z.counter, z.counter + MAX_ACTI, s->acti_counter_);
+			std::copy(z.time, z.time + MAX_ACTI, s->acti_time_);
+			s->Ls_ = h_trees_[t].Ls;
+		}
 	}
 
 	// ---- the schedule --------------------------------------------------------------------------
 
-	// The next merged substep (impl/integrate.hpp:26-67 per tree, merged): its level L and the trees
-	// that run it, decided on the cluster counts `cnt`; a tree whose level above its finest level is
-	// populated takes that level on (max_acti_level and its time, as the reference does).
-	bool next(Cursor &c, const std::vector<char> &halted, const Counters *cnt, int &L, std::vector<int> &sel) {
-		const int N       = (int) s_.size();
+	// The next (sequence value, level) pair of the merged schedule (impl/integrate.hpp:25-28 per tree,
+	// merged) when the batch's finest populated level is F: the sequence counter advances with F's
+	// stride (values in between only have levels above F due, which are empty), and at each value the
+	// due levels up to F run from the finest down.
+	static bool next_pair(Cursor &c, int F, int &L) {
 		const int top_seq = 1 << (MAX_ACTI - 1);
 		while (true) {
 			if (c.l >= MAX_ACTI) {
-				int finest = 0;
-				for (int t = 0; t < N; ++t) {
-					if (halted[t]) continue;
-					int f = s_[t]->max_acti_;
-					for (int l = MAX_ACTI - 1; l > f; --l)
-						if (cnt[t].clu[l] > 0) {
-							f = l;
-							break;
-						}
-					finest = std::max(finest, f);
-				}
-				const int stride = 1 << (MAX_ACTI - 1 - finest);
+				const int stride = 1 << (MAX_ACTI - 1 - F);
 				c.seq            = (c.seq / stride + 1) * stride;
 				if (c.seq > top_seq) return false;
 				c.l = 0;
@@ -523,74 +572,25 @@ private:
 			for (; c.l < MAX_ACTI; ++c.l) {
 				if (c.seq % (1 << c.l) != 0) continue;
 				L = MAX_ACTI - c.l - 1;
-				sel.clear();
-				for (int t = 0; t < N; ++t) {
-					if (halted[t]) continue;
-					Solver<M> *s = s_[t];
-					if (cnt[t].clu[L] > 0 && L > s->max_acti_) {
-						s->max_acti_     = L;
-						s->acti_time_[L] = s->acti_time_[L - 1];
-					}
-					if (L > s->max_acti_) continue;
-					sel.push_back(t);
-				}
-				if (sel.empty()) continue;
+				if (L > F) continue;
 				++c.l;
 				return true;
 			}
 		}
 	}
 
-	// The substep's per-tree arguments; advances each tree's stamp and epoch counters.
-	void make_args(int L, const std::vector<int> &sel, std::vector<SubArgs> &out) {
-		out.resize(sel.size());
-		for (size_t k = 0; k < sel.size(); ++k) {
-			Solver<M> *s = s_[sel[k]];
-			SubArgs &a   = out[k];
-			a.tree       = sel[k];
-			a.L          = L;
-			a.n          = 0;
-			a.counterL   = s->acti_counter_[L];
-			a.stamp      = ++s->stamp_;
-			a.epoch0     = s->epoch_;
-			a.dtL        = s->global_dt_ / (double) (1 << L);
-			s->epoch_ += EPOCHS;
-		}
+	// A tree's finest level as a run starts: its max_acti_level or a populated level above it.
+	int finest_of(int t) const {
+		int f = s_[t]->max_acti_;
+		for (int l = MAX_ACTI - 1; l > f; --l)
+			if (h_cnt_[t].clu[l] > 0) return l;
+		return f;
 	}
 
-	// The host's part of a finished substep: ACTI counter and time of level L, the list swap.
-	void advance(int L, const std::vector<int> &sel) {
-		for (int t: sel) {
-			Solver<M> *s        = s_[t];
-			s->acti_counter_[L] = (s->acti_counter_[L] + 1) % 2;
-			s->acti_time_[L] += s->global_dt_ / (double) (1 << L);
-			std::swap(s->Ls_.clu[L], s->Ls_.tmp);
-		}
-	}
-
-	TreeState save(const Solver<M> *s) const {
-		TreeState z;
-		z.max_acti = s->max_acti_;
-		z.stamp    = s->stamp_;
-		z.epoch    = s->epoch_;
-		std::copy(s->acti_counter_, s->acti_counter_ + MAX_ACTI, z.acti_counter);
-		std::copy(s->acti_time_, s->acti_time_ + MAX_ACTI, z.acti_time);
-		z.Ls = s->Ls_;
-		return z;
-	}
-	void restore(Solver<M> *s, const TreeState &z) const {
-		s->max_acti_ = z.max_acti;
-		s->stamp_    = z.stamp;
-		s->epoch_    = z.epoch;
-		std::copy(z.acti_counter, z.acti_counter + MAX_ACTI, s->acti_counter_);
-		std::copy(z.acti_time, z.acti_time + MAX_ACTI, s->acti_time_);
-		s->Ls_ = z.Ls;
-	}
-
-	// After substeps with these trees ran: a capacity or structure error throws, a NaN halts the tree
-	// for the rest of the global step (force_break).
-	void post_checks(const std::vector<int> &sel, std::vector<char> &halted, int *force_break, double *global_dt) {
-		for (int t: sel) {
+	// After substeps ran: a capacity or structure error throws, a NaN halts the tree for the rest of the
+	// global step (force_break).
+	void post_checks(std::vector<char> &halted, int *force_break, double *global_dt) {
+		for (size_t t = 0; t < s_.size(); ++t) {
 			if (halted[t]) continue;
 			Solver<M> *s = s_[t];
 			s->check_status();
@@ -604,18 +604,15 @@ private:
 
 	// ---- device side of a planned run ----------------------------------------------------------
 
-	// Scratch rows for the clusters as they are now (and half as much again), then every tree's arguments.
-	void prepare(const std::vector<char> &halted) {
+	// Scratch rows for the clusters as they are now (and half as much again), then every tree's arguments
+	// and schedule state; `head[t]` is the highest level tree t may run within the run.
+	void prepare(const std::vector<char> &halted, const std::vector<int> &head) {
 		const int N = (int) s_.size();
 		for (int t = 0; t < N; ++t) {
-			Solver<M> *s   = s_[t];
+			Solver<M> *s      = s_[t];
 			const Counters &c = h_cnt_[t];
-			long long most = 0;
-			int finest     = s->max_acti_;
-			for (int l = 0; l < MAX_ACTI; ++l) {
-				most = std::max<long long>(most, c.clu[l]);
-				if (c.clu[l] > 0) finest = std::max(finest, l);
-			}
+			long long most    = 0;
+			for (int l = 0; l < MAX_ACTI; ++l) most = std::max<long long>(most, c.clu[l]);
 			if (!halted[t]) s->ensure_scratch(most + most / 2);
 			TreeArgs &a = h_trees_[t];
 			a.P         = s->P_;
@@ -623,12 +620,22 @@ private:
 			a.B         = s->B_;
 			a.Ls        = s->Ls_;
 			a.cnt       = s->d_cnt_;
+			a.sch       = d_sched_ + t;
 			a.scratch   = s->scratch_cap_;
 			a.limiter   = s->limiter_;
 			a.halted    = halted[t];
-			a.finest    = finest;
+			a.finest    = head[t];
+			a.epochs    = EPOCHS;
+			TreeSched &z = h_sched_[t];
+			z.max_acti   = s->max_acti_;
+			z.stamp      = s->stamp_;
+			z.epoch      = s->epoch_;
+			z.pad        = 0;
+			std::copy(s->acti_counter_, s->acti_counter_ + MAX_ACTI, z.counter);
+			std::copy(s->acti_time_, s->acti_time_ + MAX_ACTI, z.time);
 		}
 		upload_trees();
+		DG_CUDA(cudaMemcpyAsync(d_sched_, h_sched_, sizeof(TreeSched) * N, cudaMemcpyHostToDevice, st_));
 	}
 
 	void upload_trees() {
@@ -642,25 +649,26 @@ private:
 	void ensure_arena(size_t bytes) {
 		if (bytes <= arena_cap_) return;
 		DG_CUDA(cudaStreamSynchronize(st_));
+		const size_t want = std::max(bytes, arena_cap_ + arena_cap_ / 2);
 		cudaFree(d_arena_);
 		cudaFreeHost(h_arena_);
 		d_arena_   = nullptr;
 		h_arena_   = nullptr;
 		arena_cap_ = 0;
-		const size_t want = std::max(bytes, arena_cap_ + arena_cap_ / 2);
 		DG_CUDA(cudaMalloc(&d_arena_, want));
 		DG_CUDA(cudaMallocHost(&h_arena_, want));
 		arena_cap_ = want;
 	}
 
-	// Block offsets of one table: tree k gets blocks in proportion to its planned items (at least one),
-	// the launch at most `cap` blocks in total unless every tree needs its one. Returns the block count.
-	static int fill_offsets(int *h, const std::vector<long long> &items, int cap) {
+	// Block offsets of one table: tree k gets blocks of `threads` in proportion to its planned items (at
+	// least one), the launch at most `cap` blocks in total unless every tree needs its one. Returns the
+	// block count.
+	static int fill_offsets(int *h, const std::vector<long long> &items, int cap, int threads) {
 		const int nt   = (int) items.size();
 		long long want = 0;
 		std::vector<long long> nb(nt);
 		for (int k = 0; k < nt; ++k) {
-			nb[k] = std::max<long long>(1, (items[k] + BLOCK - 1) / BLOCK);
+			nb[k] = std::max<long long>(1, (items[k] + threads - 1) / threads);
 			want += nb[k];
 		}
 		if (want > cap) {
@@ -672,13 +680,20 @@ private:
 		return h[nt];
 	}
 
-	// The slot of a planned substep in the host arena: closed flags, arguments, offset tables sized on
-	// the planning counts `cnt`.
+	// The slot of a planned substep in the host arena: closed flags, the trees' rows (tree, level, dtL;
+	// kb_begin writes the rest), offset tables sized on the planning counts `cnt`.
 	void write_slot(Planned &p, const Counters *cnt) {
 		const int nt = (int) p.sel.size();
 		char *slot   = h_arena_ + p.at;
 		std::memset(slot, 0, 16);
-		std::memcpy(slot + 16, p.args.data(), sizeof(SubArgs) * nt);
+		SubArgs *S = (SubArgs *) (slot + 16);
+		for (int k = 0; k < nt; ++k) {
+			SubArgs a{};
+			a.tree = p.sel[k];
+			a.L    = p.L;
+			a.dtL  = s_[p.sel[k]]->global_dt_ / (double) (1 << p.L);
+			S[k]   = a;
+		}
 		int *off = (int *) (slot + 16 + sizeof(SubArgs) * nt);
 		std::vector<long long> items(nt);
 		for (int tb = 0; tb < TABLES; ++tb) {
@@ -690,7 +705,7 @@ private:
 				items[k] = tb == T_FLUSH ? (p.L + 1 < MAX_ACTI ? c.clu[p.L + 1] / 2 : 0) : n * TABLE_ITEMS[tb];
 				tot += items[k];
 			}
-			p.grid[tb]  = fill_offsets(off + (size_t) tb * (nt + 1), items, sms_ * bps_[TABLE_STAGE[tb]]);
+			p.grid[tb]  = fill_offsets(off + (size_t) tb * (nt + 1), items, sms_ * bps_[TABLE_STAGE[tb]], TABLE_THREADS[tb]);
 			p.items[tb] = tot;
 		}
 	}
@@ -711,25 +726,27 @@ private:
 		}
 	}
 
-	// The launches of planned substep `idx`: the head (guard, fluxes, update, slopes, multiphase
-	// auxiliaries, indicator, capacity guard) and the tail (regrid, reassignment, list swap, flush, totals).
+	// The launches of planned substep `idx`: the head (opening and checks, fluxes, update, slopes,
+	// multiphase auxiliaries, indicator, capacity check) and the tail (regrid, reassignment, list swap,
+	// flush, closing).
 	void launch(const Planned &p, int idx, bool head, bool tail) {
-		const int nt          = (int) p.sel.size();
-		char *slot            = d_arena_ + p.at;
-		int *flags            = (int *) slot;
-		SubArgs *S            = (SubArgs *) (slot + 16);
-		const int *off        = (const int *) (slot + 16 + sizeof(SubArgs) * nt);
-		const TreeArgs *A     = d_trees_;
-		const int *on         = flags;
+		const int nt      = (int) p.sel.size();
+		char *slot        = d_arena_ + p.at;
+		int *flags        = (int *) slot;
+		SubArgs *S        = (SubArgs *) (slot + 16);
+		const int *off    = (const int *) (slot + 16 + sizeof(SubArgs) * nt);
+		const TreeArgs *A = d_trees_;
+		const int *on     = flags;
 		if (head) {
 			kb_begin<<<1, 256, 0, st_>>>(d_trees_, (int) s_.size(), S, nt, flags, d_stall_, d_halt_, idx);
 			stage(p, T_FACE, off, [&](int grid, const int *o) {
+				constexpr int T = FACE_THREADS;
 				if (mixed_) {
-					if (visc_) kb_face_sum<M, true, float><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
-					else kb_face_sum<M, false, float><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
+					if (visc_) kb_face_sum<M, true, float><<<grid, T, 0, st_>>>(A, S, o, nt, on);
+					else kb_face_sum<M, false, float><<<grid, T, 0, st_>>>(A, S, o, nt, on);
 				} else {
-					if (visc_) kb_face_sum<M, true, double><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
-					else kb_face_sum<M, false, double><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
+					if (visc_) kb_face_sum<M, true, double><<<grid, T, 0, st_>>>(A, S, o, nt, on);
+					else kb_face_sum<M, false, double><<<grid, T, 0, st_>>>(A, S, o, nt, on);
 				}
 			});
 			stage(p, T_RECV, off, [&](int grid, const int *o) {
@@ -741,8 +758,9 @@ private:
 				else kb_update<M, false><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
 			});
 			stage(p, T_SLOPE, off, [&](int grid, const int *o) {
-				if (visc_) kb_slope<M, true><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
-				else kb_slope<M, false><<<grid, BLOCK, 0, st_>>>(A, S, o, nt, on);
+				constexpr int T = SLOPE_THREADS;
+				if (visc_) kb_slope<M, true><<<grid, T, 0, st_>>>(A, S, o, nt, on);
+				else kb_slope<M, false><<<grid, T, 0, st_>>>(A, S, o, nt, on);
 			});
 			if constexpr (M::MULTI) {
 				// the smoothing sweeps and the normal run a lane group per cell, the curvature stages a thread
@@ -774,13 +792,17 @@ private:
 		DG_CUDA(cudaGetLastError());
 	}
 
-	// Completes planned substep `idx`, whose run stopped at the capacity guard: the pools that cannot take
-	// their split requests grow (Solver::substep), then the substep's tail runs.
-	void finish_substep(const Planned &p, int idx, const std::vector<char> &dev_halted) {
+	// Completes planned substep `idx`, whose run stopped at the capacity check: the pools of the trees
+	// that ran it and cannot take their split requests grow (Solver::substep), then the substep's tail runs.
+	void finish_substep(const Planned &p, int idx) {
+		const int nt = (int) p.sel.size();
+		std::vector<SubArgs> rows(nt);
+		DG_CUDA(cudaMemcpyAsync(rows.data(), d_arena_ + p.at + 16, sizeof(SubArgs) * nt, cudaMemcpyDeviceToHost, st_));
+		DG_CUDA(cudaStreamSynchronize(st_));
 		bool grown = false;
-		for (int t: p.sel) {
-			if (dev_halted[t]) continue;
-			Solver<M> *s         = s_[t];
+		for (int k = 0; k < nt; ++k) {
+			if (!rows[k].active) continue;
+			Solver<M> *s         = s_[p.sel[k]];
 			const long long need = (long long) s->h_cnt_->top + (long long) NC * s->h_cnt_->n_split + 16;
 			if (need > s->P_.cap) {
 				const long long want = std::max(need + need / 4, (long long) s->P_.cap * 5 / 4);
@@ -789,13 +811,12 @@ private:
 			}
 		}
 		if (grown) {
-			// the host's lists mirror the device's after the replay: every tree's row is rewritten
+			// the pools and lists moved; the halt flags are the device's (read back by the last sync)
 			for (size_t t = 0; t < s_.size(); ++t) {
 				TreeArgs &a = h_trees_[t];
 				a.P         = s_[t]->P_;
 				a.Ls        = s_[t]->Ls_;
 				a.scratch   = s_[t]->scratch_cap_;
-				a.halted    = a.halted || dev_halted[t];
 			}
 			upload_trees();
 		}
@@ -803,25 +824,6 @@ private:
 		DG_CUDA(cudaMemcpyAsync(flags + 1, h_one_, sizeof(int), cudaMemcpyHostToDevice, st_));
 		launch(p, idx, false, true);
 		sync();
-	}
-
-	// Tree t halted on the device at planned substep h (a NaN from its substep before h): its host state
-	// goes back to the run's start `z` and forward over its own substeps of the plan before h.
-	void replay_tree(int t, int h, const TreeState &z, const std::vector<Planned> &plan) {
-		Solver<M> *s = s_[t];
-		restore(s, z);
-		const std::vector<int> one{t};
-		std::vector<SubArgs> tmp;
-		for (int j = 0; j < h && j < (int) plan.size(); ++j) {
-			const Planned &p = plan[j];
-			if (!std::binary_search(p.sel.begin(), p.sel.end(), t)) continue;
-			if (p.L > s->max_acti_) {  // the level next() had the tree take on
-				s->max_acti_       = p.L;
-				s->acti_time_[p.L] = s->acti_time_[p.L - 1];
-			}
-			make_args(p.L, one, tmp);
-			advance(p.L, one);
-		}
 	}
 
 public:
@@ -836,51 +838,48 @@ public:
 			DG_CUDA(cudaMemcpyAsync(d_consts_ + t, &s->C_, sizeof(Consts), cudaMemcpyHostToDevice, st_));
 		}
 		std::vector<char> halted(N, 0);
-		auto halt = [&](int t) {
-			force_break[t] = 1;
-			global_dt[t]   = s_[t]->global_dt_;
-			halted[t]      = 1;
-		};
 		// a status left from before the step belongs to no substep of it
 		for (int t = 0; t < N; ++t) {
 			s_[t]->check_status();
 			h_cnt_[t].status = 0;
 		}
-		prepare(halted);
-		kb_clear_status<<<(N + 127) / 128, 128, 0, st_>>>(d_trees_, N);
+		kb_clear_status<<<(N + 127) / 128, 128, 0, st_>>>(d_cnt_, N);
 		Cursor cur;
 		std::vector<Planned> plan;
-		std::vector<TreeState> saved(N);
 		std::vector<Counters> pred(N);
-		std::vector<int> all(N);
-		for (int t = 0; t < N; ++t) all[t] = t;
-		bool first = true;
+		std::vector<int> head(N);
 		while (true) {
-			// plan up to window_ substeps of the rest of the step on the counts as they are now (the
-			// stream is idle, h_cnt_ current)
-			if (!first) prepare(halted);
-			first              = false;
-			const Cursor cur0  = cur;
-			const auto halted0 = halted;
-			for (int t = 0; t < N; ++t) saved[t] = save(s_[t]);
+			// a run from here, planned on the counts as they are now (the stream is idle, h_cnt_ and the
+			// solvers' schedule state current): the batch's finest level F sets the pairs, a tree may run
+			// levels up to HEADROOM above its own finest
+			int F = -1;
+			for (int t = 0; t < N; ++t) {
+				head[t] = finest_of(t);
+				if (!halted[t]) F = std::max(F, head[t]);
+			}
+			if (F < 0) break;  // every tree has halted
+			for (int t = 0; t < N; ++t) head[t] = std::min(F, head[t] + HEADROOM);
+			prepare(halted, head);
 			std::copy(h_cnt_, h_cnt_ + N, pred.begin());
 			plan.clear();
 			size_t bytes  = 0;
 			bool finished = false;
-			int L;
-			std::vector<int> sel;
 			while ((int) plan.size() < window_) {
-				if (!next(cur, halted, pred.data(), L, sel)) {
+				int L;
+				if (!next_pair(cur, F, L)) {
 					finished = true;
 					break;
 				}
+				std::vector<int> sel;
+				for (int t = 0; t < N; ++t)
+					if (!halted[t] && L <= head[t]) sel.push_back(t);
+				if (sel.empty()) continue;
 				Planned p;
-				p.L   = L;
-				p.sel = sel;
-				p.at  = bytes;
-				make_args(L, sel, p.args);
-				advance(L, sel);
-				bytes += slot_bytes((int) sel.size());
+				p.L     = L;
+				p.sel   = std::move(sel);
+				p.after = cur;
+				p.at    = bytes;
+				bytes += slot_bytes((int) p.sel.size());
 				plan.push_back(std::move(p));
 			}
 			if (plan.empty()) break;
@@ -893,22 +892,16 @@ public:
 			sync();
 			++runs_;
 			planned_ += (long long) plan.size();
-			// trees that a NaN halted on the device, with the substep where it was seen
-			std::vector<std::pair<int, int>> halts;
-			std::vector<char> dev_halted(N, 0);
 			for (int t = 0; t < N; ++t)
 				if (h_halt_[t] != STALL_NONE) {
-					halts.push_back({t, h_halt_[t]});
-					dev_halted[t] = 1;
+					force_break[t] = 1;
+					global_dt[t]   = s_[t]->global_dt_;
+					halted[t]      = 1;
 				}
 			const int stop = *h_stall_;
 			if (stop == STALL_NONE) {
-				for (auto &th: halts) {
-					replay_tree(th.first, th.second, saved[th.first], plan);
-					halt(th.first);
-				}
 				// a NaN in a tree's last substep of the run halts it now; an error throws
-				post_checks(all, halted, force_break, global_dt);
+				post_checks(halted, force_break, global_dt);
 				if (finished) break;
 				window_ = std::min(window_ * 2, WINDOW_MAX);
 				continue;
@@ -917,39 +910,16 @@ public:
 			window_     = std::max(window_ / 2, WINDOW_MIN);
 			const int i = stop / 2, half = stop & 1;
 			if (i == 0 && !half) throw dg_error(DG_ERR_UNSUPPORTED, "batch: a planned run stopped before its first substep");
-			// back to the state before the run, then forward over the substeps that ran
-			cur    = cur0;
-			halted = halted0;
-			for (int t = 0; t < N; ++t) restore(s_[t], saved[t]);
-			std::vector<SubArgs> scratch_args;
-			for (int j = 0; j < i; ++j) {
-				const bool more = next(cur, halted, pred.data(), L, sel);
-				if (!more || L != plan[j].L || sel != plan[j].sel)
-					throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan at substep " + std::to_string(j) + " of " +
-					                                       std::to_string(i) + (half ? " (tail stop)" : " (head stop)"));
-				make_args(L, sel, scratch_args);
-				advance(L, sel);
-				++replayed_;
-			}
 			if (!half) {
-				// the statuses are still those of substep i - 1 (a NaN there has halted its tree already)
-				if (i > 0) post_checks(plan[i - 1].sel, halted, force_break, global_dt);
+				// substep i did not start: the schedule resumes at it
+				cur = plan[i - 1].after;
 			} else {
-				// substep i's head ran: its statuses are substep i's, and kb_begin(i) found every running
-				// tree's status clear before it
-				const bool more = next(cur, halted, pred.data(), L, sel);
-				if (!more || L != plan[i].L || sel != plan[i].sel)
-					throw dg_error(DG_ERR_UNSUPPORTED, "batch: replay left the plan at the stopped substep " + std::to_string(i));
-				make_args(L, sel, scratch_args);
-				finish_substep(plan[i], i, dev_halted);
-				advance(L, sel);
-				++replayed_;
-				post_checks(sel, halted, force_break, global_dt);
+				// substep i's head ran: complete it, then resume after it
+				finish_substep(plan[i], i);
+				++completed_;
+				cur = plan[i].after;
 			}
-			for (auto &th: halts) {
-				replay_tree(th.first, th.second, saved[th.first], plan);
-				halt(th.first);
-			}
+			post_checks(halted, force_break, global_dt);
 		}
 		for (int t = 0; t < N; ++t) {
 			Solver<M> *s       = s_[t];

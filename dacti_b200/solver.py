@@ -411,11 +411,12 @@ class Batch:
         return {k: (ms[i], it[i]) for i, k in enumerate(BATCH_STAGES)}
 
     def run_stats(self) -> dict:
-        """Planned runs (one per global step unless a guard stopped one), runs stopped by a guard, substeps
-        planned and substeps the host replayed after a stop, since the batch was made."""
+        """Planned runs (one per global step once warmed up, unless a check stopped one), runs a check
+        stopped, substeps planned, and substeps the host completed after a stop at the capacity check,
+        since the batch was made."""
         v = (ctypes.c_longlong * 4)()
         self._bcheck(self._lib.dg_batch_run_stats(self._h, v, 4))
-        return {"runs": v[0], "stops": v[1], "planned": v[2], "replayed": v[3]}
+        return {"runs": v[0], "stops": v[1], "planned": v[2], "completed": v[3]}
 
     def step(self, signal: bool = True) -> list:
         """One global step of every tree; returns the force_break flags."""

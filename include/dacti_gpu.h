@@ -138,9 +138,11 @@ int dg_step_many(dg_solver **solvers, int n, int threads, int signal, int *force
  * lockstep by one host thread (the chosen form's batched path; no counterpart in the reference, where
  * every tree is an Integrator stepped on its own, impl/integrate.hpp:12-87). The trees' ACTI schedules
  * are merged; each substep of level L launches every stage once for all trees that run L, over block
- * ranges split among them by work. The host plans the global step from the counts at its start and
- * issues it with no synchronisation; device-side guards stop the run where the live counts leave the
- * plan (a newly populated finer level, a NaN, a pool that must grow), and the host resumes from there.
+ * ranges split among them by work. The host plans the global step and issues it with no
+ * synchronisation; each tree's schedule state lives on the device, which applies the reference's level
+ * rule per tree and halts a tree with a NaN there. Device-side checks stop a run only where the live
+ * counts leave the plan (a tree populating a level beyond its headroom, a pool that must grow), and the
+ * host resumes from there.
  * Per tree the results are dg_step's, bit for bit. While in the batch, the solvers run on the batch's stream and keep their
  * counters in the batch's array: step them through dg_batch_step only, and destroy the batch before
  * its solvers. */
@@ -162,8 +164,8 @@ int dg_batch_set_launch(dg_batch *b, const int *blocks_per_sm, int n_stages);
 int dg_batch_set_profiling(dg_batch *b, int on);
 /* Device milliseconds and work items per stage kind since the previous call. */
 int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n_stages);
-/* Since the batch was made: out[0] planned runs, out[1] runs a guard stopped, out[2] substeps planned,
- * out[3] substeps the host replayed after a stop (n <= 4 values). */
+/* Since the batch was made: out[0] planned runs, out[1] runs a check stopped, out[2] substeps planned,
+ * out[3] substeps the host completed after a stop at the capacity check (n <= 4 values). */
 int dg_batch_run_stats(dg_batch *b, long long *out, int n);
 
 /* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */

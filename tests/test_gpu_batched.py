@@ -102,9 +102,8 @@ def test_lockstep_batch_equals_single_tree_steps():
 
 
 def test_lockstep_batch_stops_and_resumes():
-    """Pools with no room to spare: the planned runs stop at the capacity guard (and wherever a tree
-    populates a finer level), the host grows the pool and resumes, and every tree still gets its dg_step
-    result bit for bit."""
+    """Pools with no room to spare: the planned runs stop at the capacity check, the host grows the pool,
+    completes the substep and resumes, and every tree still gets its dg_step result bit for bit."""
     import dataclasses
     batch = [dataclasses.replace(c, params=dataclasses.replace(c.params, pool_capacity=1))
              for c in cases.riemann_batch(6, seed=5, base_levels=(4, 5), extra_levels=(2, 3))]
@@ -115,7 +114,7 @@ def test_lockstep_batch_stops_and_resumes():
         assert b.step() == [s.integrate()[1] for s in alone]
     st = b.run_stats()
     b.close()
-    assert st["stops"] > 0 and st["replayed"] > 0 and STEPS <= st["runs"] <= STEPS + st["stops"]
+    assert st["stops"] > 0 and st["completed"] > 0 and st["runs"] >= STEPS
     for a, s, c in zip(together, alone, batch):
         sa, sb = a.active_cells().sorted(c.params.side_length), s.active_cells().sorted(c.params.side_length)
         assert sa.n == sb.n
