@@ -325,6 +325,7 @@ public:
 	virtual void set_profiling(bool on) = 0;
 	virtual void stage_times(double *ms, long long *items, int n) = 0;
 	virtual void run_stats(long long *out, int n) = 0;
+	virtual void set_pregrow(bool on) = 0;
 	std::string last_error;
 };
 
@@ -381,7 +382,8 @@ class Batch : public BatchBase {
 	int sms_    = 148;
 	bool mixed_ = false, visc_ = false, sigma_ = false;
 	int bps_[BS_N];  // launch budget per stage kind: blocks per SM
-	bool prof_ = false;
+	bool prof_    = false;
+	bool pregrow_ = true;
 	struct Timed {
 		int stage;
 		cudaEvent_t a, b;
@@ -487,6 +489,9 @@ public:
 	}
 
 	void set_profiling(bool on) override { prof_ = on; }
+
+	// Pools grown ahead of a run (on by default); off, a pool grows only at the capacity check.
+	void set_pregrow(bool on) override { pregrow_ = on; }
 
 	// Device time and work items per stage kind since the last call (profiling on), then reset.
 	void stage_times(double *ms, long long *items, int n) override {
@@ -613,7 +618,17 @@ private:
 			const Counters &c = h_cnt_[t];
 			long long most    = 0;
 			for (int l = 0; l < MAX_ACTI; ++l) most = std::max<long long>(most, c.clu[l]);
-			if (!halted[t]) s->ensure_scratch(most + most / 2);
+			if (!halted[t]) {
+				// room for a split of every cell of the largest cluster, the test under which Solver::substep
+				// prepares to grow; growing early only changes the capacity, never a result, and spares the
+				// run a stop at the capacity check
+				const long long need = (long long) c.top + (long long) NC * most + 16;
+				if (pregrow_ && need > s->P_.cap) {
+					const long long want = std::max(need + need / 4, (long long) s->P_.cap * 5 / 4);
+					s->grow_pool((int) std::min<long long>(want, 2000000000LL));
+				}
+				s->ensure_scratch(most + most / 2);
+			}
 			TreeArgs &a = h_trees_[t];
 			a.P         = s->P_;
 			a.C         = d_consts_ + t;

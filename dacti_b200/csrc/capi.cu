@@ -252,6 +252,10 @@ int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n) {
 	return batch_guarded(b, [&] { b->impl->stage_times(ms, items, n); });
 }
 
+int dg_batch_set_pregrow(dg_batch *b, int on) {
+	return batch_guarded(b, [&] { b->impl->set_pregrow(on != 0); });
+}
+
 int dg_batch_run_stats(dg_batch *b, long long *out, int n) {
 	if (!out || n < 0) return DG_ERR_ARG;
 	return batch_guarded(b, [&] { b->impl->run_stats(out, n); });

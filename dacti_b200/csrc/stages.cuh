@@ -584,69 +584,76 @@ __global__ void __launch_bounds__(FACE_THREADS, FACE_MIN_BLOCKS) k_face_sum(Pool
 template<class M, bool V, class Grid>
 __device__ __forceinline__ void d_update(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, int n, double dtL, int epoch, Counters *cnt) {
 	constexpr int E = M::E;
-	const int cap = P.cap;
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i  = list[tid];
-		const int li = P.level[i];
-		const double vol  = C.vol[li];
-		const uint32_t fl0 = P.flags[i];
-		const bool rcv     = fl0 & F_RECV;
-		const double *s_in = P.du + (size_t) tid * M::F;
-		double du[M::F];
-#pragma unroll
-		for (int q = 0; q < M::F; ++q) du[q] = ((rcv ? at(P.flux, cap, q, i) : 0.0) + s_in[q]) / vol;
+	const int cap  = P.cap;
+	const int lane = threadIdx.x & 31;
+	// warp-uniform loop: the whole warp stamps the updated cells' ancestors together
+	for (int t0 = g.tid() - lane; t0 < n; t0 += g.stride()) {
+		const int tid = t0 + lane;
+		int up        = 0;
+		if (tid < n) {
+			const int i  = list[tid];
+			const int li = P.level[i];
+			const double vol  = C.vol[li];
+			const uint32_t fl0 = P.flags[i];
+			const bool rcv     = fl0 & F_RECV;
+			const double *s_in = P.du + (size_t) tid * M::F;
+			double du[M::F];
+	#pragma unroll
+			for (int q = 0; q < M::F; ++q) du[q] = ((rcv ? at(P.flux, cap, q, i) : 0.0) + s_in[q]) / vol;
 
-		double pold[E], u[E], p[E];
-		load_p<M>(P, i, pold);
-		for (int q = 0; q < E; ++q) u[q] = at(P.u, cap, q, i);
-		double gold[M::G > 0 ? M::G : 1];
-		if constexpr (V) grad_input<M>(C.m, pold, gold);
-		for (int q = 0; q < E; ++q) u[q] += du[q];
-		if constexpr (M::MULTI) {
-			if (!C.signal) {
-				if (u[M::IA] > 0.001)
-					for (int k = M::IU; k < M::IU + M::D; ++k) u[k] = 0.0;
+			double pold[E], u[E], p[E];
+			load_p<M>(P, i, pold);
+			for (int q = 0; q < E; ++q) u[q] = at(P.u, cap, q, i);
+			double gold[M::G > 0 ? M::G : 1];
+			if constexpr (V) grad_input<M>(C.m, pold, gold);
+			for (int q = 0; q < E; ++q) u[q] += du[q];
+			if constexpr (M::MULTI) {
+				if (!C.signal) {
+					if (u[M::IA] > 0.001)
+						for (int k = M::IU; k < M::IU + M::D; ++k) u[k] = 0.0;
+				}
+				// source (model/multi.hpp:186-203) from the pre-update state
+				const double kap = at(P.k, cap, M::KAPPA, i);
+				const double sg  = C.m.sigma;
+				double s[E];
+				for (int q = 0; q < E; ++q) s[q] = 0.0;
+				for (int d = 0; d < M::D; ++d) s[M::IU + d] = -sg * kap * du[M::IA + 2 + d];
+				s[M::IP] = sg * kap * (-du[M::IA] + pold[M::IA] * du[M::IA + 1]);
+				s[M::IA] = -pold[M::IA] * du[M::IA + 1];
+				for (int q = 0; q < E; ++q) u[q] = u[q] + s[q];
 			}
-			// source (model/multi.hpp:186-203) from the pre-update state
-			const double kap = at(P.k, cap, M::KAPPA, i);
-			const double sg  = C.m.sigma;
-			double s[E];
-			for (int q = 0; q < E; ++q) s[q] = 0.0;
-			for (int d = 0; d < M::D; ++d) s[M::IU + d] = -sg * kap * du[M::IA + 2 + d];
-			s[M::IP] = sg * kap * (-du[M::IA] + pold[M::IA] * du[M::IA + 1]);
-			s[M::IA] = -pold[M::IA] * du[M::IA + 1];
-			for (int q = 0; q < E; ++q) u[q] = u[q] + s[q];
+			prim_from_cons<M>(C.m, u, p);
+			if (isnan(p[M::IP]) || isnan(p[0])) set_status(&cnt->status, ST_NAN);
+			if constexpr (M::MULTI) {
+				p[0] = smax(p[0], 1e-3);
+				p[1] = smax(p[1], 1e-6);
+			} else {
+				p[0] = smax(p[0], 1e-3);
+			}
+			p[M::IP] = smax(p[M::IP], 1e-3);
+			cons_from_prim<M>(C.m, p, u);
+			if constexpr (M::G > 0 && V) {
+				double gnew[M::G];
+				grad_input<M>(C.m, p, gnew);
+				for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = (gnew[g] - gold[g]) / dtL;
+			}
+			if constexpr (M::MULTI) {
+				P.k[(size_t) 0 * cap + i]        = C.m.mu1 * p[M::IA] + C.m.mu2 * (1 - p[M::IA]);
+				P.k[(size_t) M::ALPHAS * cap + i] = p[M::IA];
+			}
+			for (int q = 0; q < E; ++q) {
+				P.u[(size_t) q * cap + i] = u[q];
+				P.p[(size_t) q * cap + i] = p[q];
+			}
+			store_p_rec<M>(P, i, p);
+			if (rcv) {
+				for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
+				P.flags[i] = fl0 & ~F_RECV;
+			}
+			P.t[i] = P.t[i] + dtL;
+			up     = P.parent[i];
 		}
-		prim_from_cons<M>(C.m, u, p);
-		if (isnan(p[M::IP]) || isnan(p[0])) set_status(&cnt->status, ST_NAN);
-		if constexpr (M::MULTI) {
-			p[0] = smax(p[0], 1e-3);
-			p[1] = smax(p[1], 1e-6);
-		} else {
-			p[0] = smax(p[0], 1e-3);
-		}
-		p[M::IP] = smax(p[M::IP], 1e-3);
-		cons_from_prim<M>(C.m, p, u);
-		if constexpr (M::G > 0 && V) {
-			double gnew[M::G];
-			grad_input<M>(C.m, p, gnew);
-			for (int g = 0; g < M::G; ++g) P.tslope[(size_t) g * cap + i] = (gnew[g] - gold[g]) / dtL;
-		}
-		if constexpr (M::MULTI) {
-			P.k[(size_t) 0 * cap + i]        = C.m.mu1 * p[M::IA] + C.m.mu2 * (1 - p[M::IA]);
-			P.k[(size_t) M::ALPHAS * cap + i] = p[M::IA];
-		}
-		for (int q = 0; q < E; ++q) {
-			P.u[(size_t) q * cap + i] = u[q];
-			P.p[(size_t) q * cap + i] = p[q];
-		}
-		store_p_rec<M>(P, i, p);
-		if (rcv) {
-			for (int q = 0; q < M::F; ++q) P.flux[(size_t) q * cap + i] = 0.0;
-			P.flags[i] = fl0 & ~F_RECV;
-		}
-		P.t[i] = P.t[i] + dtL;
-		mark_up(P, P.parent[i], epoch);
+		mark_up_warp(P, up, epoch);
 	}
 }
 template<class M, bool V>

@@ -181,6 +181,25 @@ __device__ __forceinline__ void mark_up(const Pool &P, int first, int epoch) {
 	}
 }
 
+// mark_up for a warp at once: lanes that name the same node leave it to one of them, so a node shared
+// by many cells of the warp (their parent, grandparent, ...) is read and written once per warp instead
+// of once per cell, and the cells of the first wave no longer all store to the same ancestors. The
+// stamped set is mark_up's. Every lane of the warp calls it (first = 0 for a lane with nothing to stamp).
+__device__ __forceinline__ void mark_up_warp(const Pool &P, int first, int epoch) {
+	const int lane = threadIdx.x & 31;
+	int a          = first;
+	for (int guard = 0; guard < MAX_TREE; ++guard) {
+		if (!__any_sync(0xffffffffu, a != 0)) break;
+		const unsigned same = __match_any_sync(0xffffffffu, a);
+		int next            = 0;
+		if (a != 0 && __ffs(same) - 1 == lane && __ldcg(P.mod + a) != epoch) {
+			P.mod[a] = epoch;
+			next     = P.parent[a];
+		}
+		a = next;
+	}
+}
+
 // Mean of a per-node scalar over the subtree of n (the leaf's own value for a leaf), children in slot
 // order as the recursion of interpolate_k visits them; `val(x)` gives a leaf's value.
 template<int D, class Val>

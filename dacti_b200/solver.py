@@ -126,6 +126,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_batch_stage_times.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong),
                                          ctypes.c_int]
     lib.dg_batch_run_stats.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    lib.dg_batch_set_pregrow.argtypes = [vp, ctypes.c_int]
     _lib = lib
     return lib
 
@@ -138,7 +139,7 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_build_last_error", "dg_build_tree", "dg_tree_nodes", "dg_tree_copy", "dg_tree_free",
                     "dg_read_cells_noalloc", "dg_get_stats", "dg_batch_create", "dg_batch_step",
                     "dg_batch_last_error", "dg_batch_destroy", "dg_batch_set_launch", "dg_batch_set_profiling",
-                    "dg_batch_stage_times", "dg_batch_run_stats",
+                    "dg_batch_stage_times", "dg_batch_run_stats", "dg_batch_set_pregrow",
                     "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
 
 
@@ -409,6 +410,10 @@ class Batch:
         it = (ctypes.c_longlong * n)()
         self._bcheck(self._lib.dg_batch_stage_times(self._h, ms, it, n))
         return {k: (ms[i], it[i]) for i, k in enumerate(BATCH_STAGES)}
+
+    def set_pregrow(self, on: bool = True) -> None:
+        """Grow pools ahead of each planned run (default) or only where a run stops at the capacity check."""
+        self._bcheck(self._lib.dg_batch_set_pregrow(self._h, 1 if on else 0))
 
     def run_stats(self) -> dict:
         """Planned runs (one per global step once warmed up, unless a check stopped one), runs a check

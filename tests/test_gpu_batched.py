@@ -110,6 +110,7 @@ def test_lockstep_batch_stops_and_resumes():
     together = [Solver(c) for c in batch]
     alone = [Solver(c) for c in batch]
     b = Batch(together)
+    b.set_pregrow(False)
     for _ in range(STEPS):
         assert b.step() == [s.integrate()[1] for s in alone]
     st = b.run_stats()
