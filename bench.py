@@ -63,6 +63,7 @@ def parse_args():
     ap.add_argument("--scale-only", action="store_true", help="run only the scale workload and print its section")
     ap.add_argument("--learned-only", action="store_true", help="run only the learned sections and print them")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched section and print it")
+    ap.add_argument("--no-pregrow", action="store_true", help="batched section: grow pools only at the capacity check")
     ap.add_argument("--learned-shock", action="store_true",
                     help="also run the forecast-driven regrid on the shock-drop of the bench workload")
     ap.add_argument("--forms", default="fp64,mixed",
@@ -454,6 +455,7 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     # lockstep batch: W warm-up steps, K timed steps between events on the batch's stream
     solvers = make()
     b = Batch(solvers)
+    b.set_pregrow(not args.no_pregrow)
     for _ in range(args.warmup):
         b.step()
     torch.cuda.synchronize()
@@ -512,6 +514,7 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "value": l_u / (l_ms * 1e-3), "ms_per_step": l_ms / args.steps,
         "timing": "host wall clock around K lockstep batch steps (dg_batch_step), synchronised before and after",
         "planned_runs": runs,
+        "pregrow": not args.no_pregrow,
         "force_breaks": int(breaks),
         "profiled_step": {"wall_ms": prof_ms, "stage_ms": stages, "stage_sum_ms": round(sum(stages.values()), 3)},
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},

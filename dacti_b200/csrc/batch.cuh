@@ -619,12 +619,12 @@ private:
 			long long most    = 0;
 			for (int l = 0; l < MAX_ACTI; ++l) most = std::max<long long>(most, c.clu[l]);
 			if (!halted[t]) {
-				// room for a split of every cell of the largest cluster, the test under which Solver::substep
-				// prepares to grow; growing early only changes the capacity, never a result, and spares the
-				// run a stop at the capacity check
-				const long long need = (long long) c.top + (long long) NC * most + 16;
-				if (pregrow_ && need > s->P_.cap) {
-					const long long want = std::max(need + need / 4, (long long) s->P_.cap * 5 / 4);
+				// at least a fifth of the tree free as a run starts, else room for half the tree again: growing
+				// early only changes the capacity, never a result, and spares most runs a stop at the
+				// capacity check
+				const long long top = c.top;
+				if (pregrow_ && top + top / 5 + 16 * NC > s->P_.cap) {
+					const long long want = std::max(top + top / 2 + 16 * NC, (long long) s->P_.cap * 5 / 4);
 					s->grow_pool((int) std::min<long long>(want, 2000000000LL));
 				}
 				s->ensure_scratch(most + most / 2);

@@ -376,42 +376,21 @@ __global__ void __launch_bounds__(BLOCK) k_flux_receive(Pool P, const int32_t *l
 
 // flux_update (impl/flux.hpp:11-97) seen from each running-cluster cell: the signed sum of the fluxes
 // that cross its faces in this substep, one lane per face (groups of 4 lanes in 2D, 8 cells a warp; of
-// 6 lanes in 3D, 5 cells a warp, the warp's last two lanes idle). Face f of a cell needs:
-// - nothing when the neighbour's own substep carries the face;
-// - the boundary flux;
-// - the flux of the face's owner (the finer side; at equal levels the slower cell or the cell on the
-//   left), which may be the cell or its same-level neighbour;
-// - or, behind a non-leaf neighbour, the fluxes of the finer owners in candidate order.
-// Every interior flux is evaluated with the owner's arguments (owner, the owner's neighbour, the owner's
-// direction), so the two cells of a face obtain identical bits and the update stays conservative
-// without a face-flux array or atomics.
-//
-// The evaluations are spread over the warp instead of run by the lane that needs them: each lane lists
-// its tasks (up to FACE_QUEUE of them) in shared memory, the warp evaluates the packed list 32 tasks at a
-// time, and each lane takes its results back in its own order. A lane behind a non-leaf neighbour thus
-// no longer holds the warp for one evaluation per finer owner, and lanes without a flux do not idle
-// through the others' evaluations. A lane with more tasks than the queue holds evaluates the rest
-// itself, in order. The lane terms combine in a fixed pairing order, ((f0 + f4) + (f2 + 0)) + ((f1 +
-// f5) + (f3 + 0)) in 3D, into du[slot]. An owned face next to a cell of a slower cluster (the coarse-time
-// side of the LTS coupling, impl/flux.hpp:82-91) also goes to the owner's face-flux slot, and that cell
-// joins the receiver list. In the mixed form every flux is rounded to FP32 once, as both sides read it;
-// sums stay FP64.
-constexpr int FACE_QUEUE = 4;  // queued flux tasks per lane
-
-// A queued flux task: x = owner (the cell for a boundary task), y = the owner's neighbour (the boundary
-// index), z = dim | dir << 2 | plus << 3 | kind << 4.
-enum : int { FT_NONE = 0, FT_BOUNDARY = 1, FT_LEAF = 2, FT_HANGING = 3 };
-
+// 6 lanes in 3D, 5 cells a warp, the warp's last two lanes idle). Lane f evaluates the flux across face f: the cell's own when it owns the face (the finer
+// side, at equal levels the slower cell or the cell on the left), the same-level neighbour's when the
+// neighbour owns it, the boundary flux, or the sum over the finer owners behind a non-leaf neighbour in
+// candidate order. Every interior flux is evaluated with the owner's arguments (owner, the owner's
+// neighbour, the owner's direction), so the two cells of a face obtain identical bits and the update
+// stays conservative without a face-flux array or atomics. The lane terms combine in a fixed butterfly,
+// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0)) in 3D, into du[slot]. An owned face next to a cell of
+// a slower cluster (the coarse-time side of the LTS coupling, impl/flux.hpp:82-91) also goes to the
+// owner's face-flux slot, and that cell joins the receiver list. In the mixed form every flux is rounded
+// to FP32 once, as both sides read it; sums stay FP64.
 template<class M, bool V, class S = double, class Grid>
 __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const Consts &C, const BcTable &B, const int32_t *list, int n, int L, double dtL, int stamp, int32_t *recv, Counters *cnt) {
 	constexpr int NF = 2 * M::D, G = NF, GW = 32 / G, NSUB = 1 << (M::D - 1), F = M::F;
-	constexpr int NCAND = 1 + NSUB * (NSUB + 1), WARPS = FACE_THREADS / 32, QT = FACE_QUEUE;
-	__shared__ int4 tq[WARPS][32 * QT];  // the warp's tasks, lane-major
-	__shared__ int ts[WARPS][32];        // first packed task index of each lane
-	__shared__ double tr[WARPS][32][F];  // results of one round of 32 tasks
 	const int cap    = P.cap;
 	const int lane   = threadIdx.x & 31;
-	const int wib    = threadIdx.x >> 5;
 	const int grp    = lane / G;  // the lane's cell within the warp; lanes past GW * G idle
 	const int sub    = lane - grp * G;
 	const int base   = grp * G;
@@ -420,42 +399,49 @@ __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const C
 	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
 		const int slot    = wbase + grp;
 		const bool active = grp < GW && slot < n;
-		const int f = sub, dim = f >> 1, dir = f & 1;
-		int i = 0, nb = 0, li = 0, ai = 0;
-		int kind  = FT_NONE;
-		int nq    = 0;      // queued tasks
-		int cnext = NCAND;  // a hanging face's first candidate past the queue
-		int4 *q   = &tq[wib][lane * QT];
+		double acc[F];
+#pragma unroll
+		for (int q = 0; q < F; ++q) acc[q] = 0.0;
 		if (active) {
-			i = list[slot];
+			const int i   = list[slot];
 			if (sub == 0) P.pos[i] = slot;
-			nb = P.nbr[(size_t) f * cap + i];
+			const int f   = sub, dim = f >> 1, dir = f & 1;
+			const int nb  = P.nbr[(size_t) f * cap + i];
 			if (nb == 0) {
 				const int b = P.bc[(size_t) f * cap + i];
 				if (b < 0) {
 					set_status(&cnt->status, ST_MISSING_BC);
 				} else {
-					kind  = FT_BOUNDARY;
-					q[nq++] = make_int4(i, b, dim | dir << 2 | FT_BOUNDARY << 4, 0);
+					double Fb[F];
+					boundary_flux<M, V, S>(P, C, B, i, b, dim, dir, dtL, Fb);
+#pragma unroll
+					for (int q = 0; q < F; ++q) acc[q] = 0.0 - (double) (S) Fb[q];
 				}
 			} else if (!(P.flags[nb] & F_LEAF)) {
-				kind = FT_HANGING;
-				li = P.level[i], ai = P.acti[i];
-				for (int c = 1; c < NCAND; ++c) {
+				const int li = P.level[i], ai = P.acti[i];
+				double w[F];
+#pragma unroll
+				for (int q = 0; q < F; ++q) w[q] = 0.0;
+				for (int c = 1; c < 1 + NSUB * (NSUB + 1); ++c) {
 					int dn;
 					bool plus;
 					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, true, dn, plus);
 					if (owner < 0) continue;
-					if (nq == QT) {
-						cnext = c;
-						break;
-					}
 					const int fo = 2 * dim + dn;
-					q[nq++]      = make_int4(owner, P.nbr[(size_t) fo * cap + owner], dim | dn << 2 | (plus ? 8 : 0) | FT_HANGING << 4, 0);
+					double Fw[F];
+					interior_flux<M, V, S>(P, C, owner, P.nbr[(size_t) fo * cap + owner], dim, dn, dtL, Fw);
+					if (plus) {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] += (double) (S) Fw[q];
+					} else {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] -= (double) (S) Fw[q];
+					}
 				}
+#pragma unroll
+				for (int q = 0; q < F; ++q) acc[q] = 0.0 + (double) (S) w[q];
 			} else {
-				li = P.level[i], ai = P.acti[i];
-				const int ln = P.level[nb], an = P.acti[nb];
+				const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
 				int own = -1, fo = f;
 				if (an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
 					own = i;
@@ -464,109 +450,47 @@ __device__ __forceinline__ void d_face_sum(const Grid &g, const Pool &P, const C
 					fo  = f ^ 1;
 				}
 				if (own >= 0) {
-					kind          = FT_LEAF;
-					const int oth = own == i ? nb : P.nbr[(size_t) fo * cap + nb];
-					q[nq++]       = make_int4(own, oth, dim | (fo & 1) << 2 | (own == i ? 8 : 0) | FT_LEAF << 4, 0);
-				}
-			}
-		}
-		// packed task indices: an exclusive scan of the queue lengths over the warp
-		int incl = nq;
-#pragma unroll
-		for (int o = 1; o < 32; o <<= 1) {
-			const int v = __shfl_up_sync(0xffffffffu, incl, o);
-			if (lane >= o) incl += v;
-		}
-		const int first = incl - nq;
-		const int total = __shfl_sync(0xffffffffu, incl, 31);
-		ts[wib][lane]   = first;
-		__syncwarp();
-		double w[F];
-#pragma unroll
-		for (int k = 0; k < F; ++k) w[k] = 0.0;
-		for (int r = 0; r < total; r += 32) {
-			const int t = r + lane;
-			if (t < total) {
-				// the lane whose tasks hold t: the last with first index <= t
-				int lo = 0, hi = 31;
-				while (lo < hi) {
-					const int mid = (lo + hi + 1) >> 1;
-					if (ts[wib][mid] <= t) lo = mid;
-					else hi = mid - 1;
-				}
-				const int4 d   = tq[wib][lo * QT + (t - ts[wib][lo])];
-				const int tdim = d.z & 3, tdir = (d.z >> 2) & 1;
-				double Fx[F];
-				if ((d.z >> 4) == FT_BOUNDARY) boundary_flux<M, V, S>(P, C, B, d.x, d.y, tdim, tdir, dtL, Fx);
-				else interior_flux<M, V, S>(P, C, d.x, d.y, tdim, tdir, dtL, Fx);
-#pragma unroll
-				for (int k = 0; k < F; ++k) tr[wib][lane][k] = (double) (S) Fx[k];
-			}
-			__syncwarp();
-			// this lane's results of the round, in its own order
-			for (int t2 = max(first, r); t2 < min(first + nq, r + 32); ++t2) {
-				const double *res = tr[wib][t2 - r];
-				if (kind == FT_HANGING) {
-					const bool plus = (q[t2 - first].z >> 3) & 1;
-#pragma unroll
-					for (int k = 0; k < F; ++k) w[k] = plus ? w[k] + res[k] : w[k] - res[k];
-				} else if (kind == FT_BOUNDARY) {
-#pragma unroll
-					for (int k = 0; k < F; ++k) w[k] = 0.0 - res[k];
-				} else {
-					if (((q[0].z >> 3) & 1) && P.clu[nb] != L) {
-						// an owned face next to a slower cell: its flux to the slot, the cell to the receivers
+					const int other = own == i ? nb : P.nbr[(size_t) fo * cap + nb];
+					double Fi[F];
+					interior_flux<M, V, S>(P, C, own, other, dim, fo & 1, dtL, Fi);
+					if (own == i && P.clu[nb] != L) {
 						S *dst = face_flux<S>(P, slot, f, F, NF);
 #pragma unroll
-						for (int k = 0; k < F; ++k) dst[k] = (S) res[k];
+						for (int q = 0; q < F; ++q) dst[q] = (S) Fi[q];
 						if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 					}
 #pragma unroll
-					for (int k = 0; k < F; ++k) w[k] = dir ? 0.0 - res[k] : 0.0 + res[k];
+					for (int q = 0; q < F; ++q) {
+						const double v = (double) (S) Fi[q];
+						acc[q] = dir ? 0.0 - v : 0.0 + v;
+					}
 				}
 			}
-			__syncwarp();
-		}
-		if (kind == FT_HANGING) {
-			// owners past the queue, in candidate order, by this lane
-			for (int c = cnext; c < NCAND; ++c) {
-				int dn;
-				bool plus;
-				const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, c, true, dn, plus);
-				if (owner < 0) continue;
-				const int fo = 2 * dim + dn;
-				double Fw[F];
-				interior_flux<M, V, S>(P, C, owner, P.nbr[(size_t) fo * cap + owner], dim, dn, dtL, Fw);
-#pragma unroll
-				for (int k = 0; k < F; ++k) w[k] = plus ? w[k] + (double) (S) Fw[k] : w[k] - (double) (S) Fw[k];
-			}
-#pragma unroll
-			for (int k = 0; k < F; ++k) w[k] = 0.0 + (double) (S) w[k];
 		}
 		// the group's face terms in the fixed pairing order, on every lane of the group
 		double sum[F];
 		if constexpr (NF == 4) {
 			// (f0 + f2) + (f1 + f3): a butterfly over the aligned group of four
 #pragma unroll
-			for (int k = 0; k < F; ++k) {
-				double v = w[k] + __shfl_xor_sync(0xffffffffu, w[k], 2);
-				sum[k]   = v + __shfl_xor_sync(0xffffffffu, v, 1);
+			for (int q = 0; q < F; ++q) {
+				double v = acc[q] + __shfl_xor_sync(0xffffffffu, acc[q], 2);
+				sum[q]   = v + __shfl_xor_sync(0xffffffffu, v, 1);
 			}
 		} else {
 			// ((f0 + f4) + (f2 + 0)) + ((f1 + f5) + (f3 + 0))
 #pragma unroll
-			for (int k = 0; k < F; ++k) {
-				double fv[6];
+			for (int q = 0; q < F; ++q) {
+				double f[6];
 #pragma unroll
-				for (int m = 0; m < 6; ++m) fv[m] = __shfl_sync(0xffffffffu, w[k], min(base + m, 31));
-				sum[k] = ((fv[0] + fv[4]) + (fv[2] + 0.0)) + ((fv[1] + fv[5]) + (fv[3] + 0.0));
+				for (int k = 0; k < 6; ++k) f[k] = __shfl_sync(0xffffffffu, acc[q], min(base + k, 31));
+				sum[q] = ((f[0] + f[4]) + (f[2] + 0.0)) + ((f[1] + f[5]) + (f[3] + 0.0));
 			}
 		}
 		if (active) {
 			double *dst = P.du + (size_t) slot * F;
 #pragma unroll
-			for (int k = 0; k < F; ++k)
-				if (k % G == sub) dst[k] = sum[k];
+			for (int q = 0; q < F; ++q)
+				if (q % G == sub) dst[q] = sum[q];
 		}
 	}
 }

@@ -167,9 +167,9 @@ int dg_batch_stage_times(dg_batch *b, double *ms, long long *items, int n_stages
 /* Since the batch was made: out[0] planned runs, out[1] runs a check stopped, out[2] substeps planned,
  * out[3] substeps the host completed after a stop at the capacity check (n <= 4 values). */
 int dg_batch_run_stats(dg_batch *b, long long *out, int n);
-/* Pools grown ahead of each planned run to room for a split of every cell of the tree's largest cluster
- * (on by default; capacity never changes a result). Off, a pool grows only where a run stops at the
- * capacity check. */
+/* Pools grown ahead of each planned run when less than a fifth of the tree is free, to half the tree
+ * again (on by default; capacity never changes a result). Off, a pool grows only where a run stops at
+ * the capacity check. */
 int dg_batch_set_pregrow(dg_batch *b, int on);
 
 /* Integrator::n_active_cells (integrator/integrator.hpp:193-202) */
