@@ -64,6 +64,7 @@ def parse_args():
     ap.add_argument("--learned-only", action="store_true", help="run only the learned sections and print them")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched section and print it")
     ap.add_argument("--no-pregrow", action="store_true", help="batched section: grow pools only at the capacity check")
+    ap.add_argument("--batch-groups", type=int, default=8, help="batched section: lockstep groups stepped concurrently")
     ap.add_argument("--learned-shock", action="store_true",
                     help="also run the forecast-driven regrid on the shock-drop of the bench workload")
     ap.add_argument("--forms", default="fp64,mixed",
@@ -481,6 +482,31 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     for s in solvers:
         s.close()
 
+    # the trees in work-balanced groups, one lockstep batch and host thread each: merged launches within a
+    # group, concurrent streams across groups
+    from dacti_b200.batch import partition
+    from dacti_b200.solver import step_batches
+    groups = args.batch_groups
+    solvers = make()
+    parts = partition([tree_work(batch[i]) for i in mine], groups)
+    gb = [Batch([solvers[k] for k in part]) for part in parts if part]
+    for x in gb:
+        x.set_pregrow(not args.no_pregrow)
+    for _ in range(args.warmup):
+        step_batches(gb)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    u0, t0 = updates(solvers), time.perf_counter()
+    for _ in range(args.steps):
+        step_batches(gb)
+    torch.cuda.synchronize()
+    g_sec, g_upd = time.perf_counter() - t0, updates(solvers) - u0
+    for x in gb:
+        x.close()
+    for s in solvers:
+        s.close()
+
     # host-threaded dg_step_many over fresh copies of the same trees
     threads = min(32, max(8, 2 * host_threads()))
     solvers = make()
@@ -504,6 +530,7 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     _, cells = reduce_ranks(0.0, float(cells), world)
     l_ms, l_u = reduce_ranks(l_sec * 1e3, l_upd, world)
     m_ms, m_u = reduce_ranks(m_sec * 1e3, m_upd, world)
+    g_ms, g_u = reduce_ranks(g_sec * 1e3, g_upd, world)
     s_ms, s_u = reduce_ranks(s_sec * 1e3, s_upd, world)
     split = (f"; trees split across {world} ranks by estimated work (longest first to the least-loaded "
              f"rank), no exchange" if world > 1 else "")
@@ -517,12 +544,41 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "pregrow": not args.no_pregrow,
         "force_breaks": int(breaks),
         "profiled_step": {"wall_ms": prof_ms, "stage_ms": stages, "stage_sum_ms": round(sum(stages.values()), 3)},
+        "grouped": {"value": g_u / (g_ms * 1e-3), "groups": groups, "ms_per_step": g_ms / args.steps,
+                    "speedup_vs_step_many": (g_u / g_ms) / (m_u / m_ms) if m_u > 0 else None,
+                    "timing": "host wall clock around K steps of every group (dacti_b200.solver.step_batches)"},
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
         "speedup_vs_step_many": (l_u / l_ms) / (m_u / m_ms) if m_u > 0 else None,
         "speedup_vs_one_at_a_time": (l_u / l_ms) / (s_u / s_ms) if s_u > 0 else None,
         "active_cells": int(cells),
     }
+
+
+def host_memory_available_gb():
+    """Host memory this process may still use: the smaller of MemAvailable and the cgroup limit's room,
+    in GB (None when neither can be read)."""
+    vals = []
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    vals.append(int(line.split()[1]) * 1024 / 1e9)
+    except OSError:
+        pass
+    for lim, cur in (("/sys/fs/cgroup/memory.max", "/sys/fs/cgroup/memory.current"),
+                     ("/sys/fs/cgroup/memory/memory.limit_in_bytes", "/sys/fs/cgroup/memory/memory.usage_in_bytes")):
+        try:
+            with open(lim) as f:
+                raw = f.read().strip()
+            with open(cur) as f:
+                used = int(f.read().strip())
+            if raw != "max" and int(raw) < (1 << 60):
+                vals.append((int(raw) - used) / 1e9)
+            break
+        except (OSError, ValueError):
+            continue
+    return min(vals) if vals else None
 
 
 def scale_run(args, local_rank: int) -> dict:
@@ -538,6 +594,13 @@ def scale_run(args, local_rank: int) -> dict:
     from dacti_b200.scene_gpu import build_tree_device
     from dacti_b200.solver import Solver
 
+    # the host holds the built tree (about 150 B per node, ~100 M nodes) and its pruned copy at once;
+    # run only with room for that on the host, so a short box fails this section instead of its host
+    need_gb = 48.0
+    avail_gb = host_memory_available_gb()
+    if avail_gb is not None and avail_gb < need_gb:
+        return {"workload": "shock_drop_3d multi<3> 128x64x64 base +5 levels (the scale configuration)",
+                "skipped": f"host memory available {avail_gb:.0f} GB < {need_gb:.0f} GB for the host-side build"}
     torch.cuda.synchronize()
     free0, total = torch.cuda.mem_get_info()
     t0 = time.perf_counter()

@@ -370,6 +370,17 @@ BATCH_STAGES = ("face_sum", "receive", "update", "slope", "aux", "estimate", "re
                 "nbr_list", "flush")
 
 
+def step_batches(batches) -> list:
+    """One global step of several lockstep batches at once, one host thread each (every batch has its own
+    stream, and ctypes releases the GIL during the call), so the batches' kernels overlap on the GPU.
+    Returns the force_break flags of every batch's trees, batch by batch."""
+    from concurrent.futures import ThreadPoolExecutor
+    if len(batches) == 1:
+        return [batches[0].step()]
+    with ThreadPoolExecutor(max_workers=len(batches)) as ex:
+        return list(ex.map(lambda b: b.step(), batches))
+
+
 class Batch:
     """dg_batch: independent solvers of one model stepped in lockstep, one launch per stage for all trees
     that run a level (merged ACTI schedules). Per tree the results equal Solver.integrate's bit for bit.
