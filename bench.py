@@ -611,8 +611,9 @@ def scale_run(args, local_rank: int) -> dict:
     del tree
     n_kept = case.tree.n_nodes
     leaves = int(case.tree.leaf_mask().sum())
-    # a pool of 1.6 x the uploaded nodes; the solver grows it when splits need more
-    case.params = dataclasses.replace(case.params, pool_capacity=int(n_kept * 1.6) + 1024)
+    # a pool of 3.3 x the uploaded nodes (the first steps refine the shock and the interface): growing a
+    # pool holds the old and the new one at once, which at this size leaves little room to grow
+    case.params = dataclasses.replace(case.params, pool_capacity=int(n_kept * 3.3) + 1024)
     t1 = time.perf_counter()
     s = Solver(case, device=local_rank)
     del case
@@ -620,27 +621,38 @@ def scale_run(args, local_rank: int) -> dict:
     t2 = time.perf_counter()
     free1, _ = torch.cuda.mem_get_info()
     low = free1
-    s.integrate()
-    torch.cuda.synchronize()
-    low = min(low, torch.cuda.mem_get_info()[0])
-    u0 = s.stats().cell_updates
-    ms = 0.0
-    for _ in range(args.scale_steps):
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
+    error = None
+    ms, u0, done = 0.0, 0, 0
+    try:
         s.integrate()
-        b.record()
         torch.cuda.synchronize()
-        ms += a.elapsed_time(b)
         low = min(low, torch.cuda.mem_get_info()[0])
+        u0 = s.stats().cell_updates
+        for _ in range(args.scale_steps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            s.integrate()
+            b.record()
+            torch.cuda.synchronize()
+            ms += a.elapsed_time(b)
+            done += 1
+            low = min(low, torch.cuda.mem_get_info()[0])
+    except Exception as e:  # a device allocation that did not fit: report what was reached
+        error = f"{type(e).__name__}: {e}"
     st = s.stats()
-    cells = s.n_active_cells()
+    cells = s.n_active_cells() if error is None else None
     s.close()
     upd = float(st.cell_updates - u0)
+    if error is not None:
+        return {"workload": "shock_drop_3d multi<3> 128x64x64 base +5 levels, LTS, FP64 (the scale configuration)",
+                "error": error, "nodes_built": int(n_full), "nodes_uploaded": int(n_kept),
+                "initial_active_leaves": leaves, "tree_size_reached": int(st.tree_size),
+                "substeps_reached": int(st.n_substeps), "device_gb_after_construction": (free0 - free1) / 1e9,
+                "device_gb_total": total / 1e9}
     return {
         "workload": "shock_drop_3d multi<3> 128x64x64 base +5 levels, LTS, FP64 (the scale configuration)",
         "nodes_built": int(n_full), "nodes_uploaded": int(n_kept), "initial_active_leaves": leaves,
-        "active_cells": int(cells), "tree_size": int(st.tree_size), "steps": args.scale_steps,
+        "active_cells": int(cells), "tree_size": int(st.tree_size), "steps": done,
         "value": upd / (ms * 1e-3) if ms > 0 else None, "unit": UNIT, "ms_per_step": ms / max(args.scale_steps, 1),
         "build_s": t1 - t0, "construct_s": t2 - t1,
         "device_gb_after_construction": (free0 - free1) / 1e9, "device_gb_high_water": (free0 - low) / 1e9,

@@ -624,8 +624,8 @@ private:
 				// capacity check
 				const long long top = c.top;
 				if (pregrow_ && top + top / 5 + 16 * NC > s->P_.cap) {
-					const long long want = std::max(top + top / 2 + 16 * NC, (long long) s->P_.cap * 5 / 4);
-					s->grow_pool((int) std::min<long long>(want, 2000000000LL));
+					const long long want = s->growth_target(s->P_.cap, std::max(top + top / 2 + 16 * NC, (long long) s->P_.cap * 5 / 4));
+					if (want > s->P_.cap) s->grow_pool((int) std::min<long long>(want, 2000000000LL));
 				}
 				s->ensure_scratch(most + most / 2);
 			}
@@ -820,7 +820,7 @@ private:
 			Solver<M> *s         = s_[p.sel[k]];
 			const long long need = (long long) s->h_cnt_->top + (long long) NC * s->h_cnt_->n_split + 16;
 			if (need > s->P_.cap) {
-				const long long want = std::max(need + need / 4, (long long) s->P_.cap * 5 / 4);
+				const long long want = s->growth_target(need, std::max(need + need / 4, (long long) s->P_.cap * 5 / 4));
 				s->grow_pool((int) std::min<long long>(want, 2000000000LL));
 				grown = true;
 			}

@@ -406,6 +406,21 @@ public:
 		P_.pos  = pos_mem_;
 	}
 
+	// The capacity a pool grows to when `need` slots must fit and `want` would be chosen: `want` when the
+	// new pool and lists fit in the free device memory (counting the scratch, spare buffer and sort keys
+	// that grow_pool releases first, less 1 GiB), else as many slots as fit, and never fewer than `need`.
+	long long growth_target(long long need, long long want) {
+		size_t free_b = 0, total_b = 0;
+		DG_CUDA(cudaMemGetInfo(&free_b, &total_b));
+		const size_t released = sizeof(double) * M::F * (NF + 1) * (size_t) scratch_cap_ + spare_bytes_ + sort_bytes_;
+		size_t per_slot = sizeof(int32_t) * (2 * MAX_ACTI + 6);
+		for (auto &f: fields(P_))
+			if (f.comps >= 0) per_slot += f.elem * (size_t) (f.comps > 0 ? f.comps : 1);
+		const long long avail = (long long) (free_b + released) - (1LL << 30);
+		const long long fit   = avail > 0 ? avail / (long long) per_slot : 0;
+		return std::max(need, std::min(want, fit));
+	}
+
 	// Grows the node pool: a new pool of new_cap slots takes every field, then the old one goes. Grows
 	// between the indicator and the split of a substep, when the stages that use the list scratch are
 	// done, so the scratch, the spare buffer and the re-sort keys are released first (they come back at
@@ -695,7 +710,7 @@ private:
 			check_status();
 			const long long need = (long long) h_cnt_->top + (long long) NC * h_cnt_->n_split + 16;
 			if (need > P_.cap) {
-				const long long want = std::max(need + need / 4, (long long) P_.cap * 5 / 4);
+				const long long want = growth_target(need, std::max(need + need / 4, (long long) P_.cap * 5 / 4));
 				grow_pool((int) std::min<long long>(want, 2000000000LL));
 				list = Ls_.clu[L];
 			}
