@@ -56,7 +56,9 @@ def parse_args():
                     help="with --profile-substep -3: the largest substep of this ACTI level instead")
     ap.add_argument("--batch-trees", type=int, default=256, help="trees of the batched 2D Riemann workload")
     ap.add_argument("--no-batched", action="store_true")
-    ap.add_argument("--no-learned", action="store_true")
+    ap.add_argument("--learned", action="store_true",
+                    help="also run the learned-forecaster section at config 4's size (about 15 minutes)")
+    ap.add_argument("--no-learned", action="store_true", help="kept for older command lines; the section is opt-in")
     ap.add_argument("--scale", action="store_true",
                     help="also run the scale workload: the shock-drop at 128 x 64 x 64 base, +5 levels (~28M leaves)")
     ap.add_argument("--scale-steps", type=int, default=1)
@@ -64,7 +66,8 @@ def parse_args():
     ap.add_argument("--learned-only", action="store_true", help="run only the learned sections and print them")
     ap.add_argument("--batched-only", action="store_true", help="run only the batched section and print it")
     ap.add_argument("--no-pregrow", action="store_true", help="batched section: grow pools only at the capacity check")
-    ap.add_argument("--batch-groups", type=int, default=8, help="batched section: lockstep groups stepped concurrently")
+    ap.add_argument("--batch-groups", type=int, default=0,
+                    help="batched section: also time this many lockstep groups stepped concurrently (0: not)")
     ap.add_argument("--learned-shock", action="store_true",
                     help="also run the forecast-driven regrid on the shock-drop of the bench workload")
     ap.add_argument("--forms", default="fp64,mixed",
@@ -487,25 +490,27 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     from dacti_b200.batch import partition
     from dacti_b200.solver import step_batches
     groups = args.batch_groups
-    solvers = make()
-    parts = partition([tree_work(batch[i]) for i in mine], groups)
-    gb = [Batch([solvers[k] for k in part]) for part in parts if part]
-    for x in gb:
-        x.set_pregrow(not args.no_pregrow)
-    for _ in range(args.warmup):
-        step_batches(gb)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    u0, t0 = updates(solvers), time.perf_counter()
-    for _ in range(args.steps):
-        step_batches(gb)
-    torch.cuda.synchronize()
-    g_sec, g_upd = time.perf_counter() - t0, updates(solvers) - u0
-    for x in gb:
-        x.close()
-    for s in solvers:
-        s.close()
+    g_sec, g_upd = 0.0, 0.0
+    if groups > 1:
+        solvers = make()
+        parts = partition([tree_work(batch[i]) for i in mine], groups)
+        gb = [Batch([solvers[k] for k in part]) for part in parts if part]
+        for x in gb:
+            x.set_pregrow(not args.no_pregrow)
+        for _ in range(args.warmup):
+            step_batches(gb)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        u0, t0 = updates(solvers), time.perf_counter()
+        for _ in range(args.steps):
+            step_batches(gb)
+        torch.cuda.synchronize()
+        g_sec, g_upd = time.perf_counter() - t0, updates(solvers) - u0
+        for x in gb:
+            x.close()
+        for s in solvers:
+            s.close()
 
     # host-threaded dg_step_many over fresh copies of the same trees
     threads = min(32, max(8, 2 * host_threads()))
@@ -546,7 +551,8 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "profiled_step": {"wall_ms": prof_ms, "stage_ms": stages, "stage_sum_ms": round(sum(stages.values()), 3)},
         "grouped": {"value": g_u / (g_ms * 1e-3), "groups": groups, "ms_per_step": g_ms / args.steps,
                     "speedup_vs_step_many": (g_u / g_ms) / (m_u / m_ms) if m_u > 0 else None,
-                    "timing": "host wall clock around K steps of every group (dacti_b200.solver.step_batches)"},
+                    "timing": "host wall clock around K steps of every group (dacti_b200.solver.step_batches)"}
+        if groups > 1 else None,
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
         "speedup_vs_step_many": (l_u / l_ms) / (m_u / m_ms) if m_u > 0 else None,
@@ -842,7 +848,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
 
     if not args.no_batched:
         result["batched"] = batched_run(args, rank, local_rank, world)
-    if not args.no_learned and world == 1:
+    if args.learned and not args.no_learned and world == 1:
         result["learned"] = learned_run(args, local_rank)
     if args.learned_shock and world == 1:
         result["learned_shock"] = learned_shock_run(args, local_rank)
