@@ -89,15 +89,40 @@ __device__ __forceinline__ int tree_of_block(const int *off, int nt) {
 	return lo;
 }
 
+// Every block of a batched launch works for one tree: its argument row (and, where the stage reads them,
+// its constants) goes to shared memory once, so the stage body finds the pool's pointers and the
+// constants there instead of reloading them from global memory after its stores.
+__device__ __forceinline__ void stage_tree(const TreeArgs &src, TreeArgs &a, Consts *c) {
+	const long long *sa = reinterpret_cast<const long long *>(&src);
+	long long *da       = reinterpret_cast<long long *>(&a);
+	for (int w = threadIdx.x; w < (int) (sizeof(TreeArgs) / 8); w += blockDim.x) da[w] = sa[w];
+	if (c) {
+		const long long *sc = reinterpret_cast<const long long *>(src.C);
+		long long *dc       = reinterpret_cast<long long *>(c);
+		for (int w = threadIdx.x; w < (int) (sizeof(Consts) / 8); w += blockDim.x) dc[w] = sc[w];
+	}
+	__syncthreads();
+}
+static_assert(sizeof(TreeArgs) % 8 == 0 && sizeof(Consts) % 8 == 0, "argument rows copy as 8-byte words");
+
 // `on` is the substep's head or tail flag (kb_begin, kb_split_check); the blocks of a tree that does not
-// run the substep return.
-#define DG_BATCH_PROLOGUE                                     \
+// run the substep return (the whole block: the tree is the block's).
+#define DG_BATCH_HEAD                                         \
 	if (!*on || (int) blockIdx.x >= off[nt]) return;          \
 	const int t_     = tree_of_block(off, nt);                \
 	const SubArgs &s = SA[t_];                                \
 	if (!s.active) return;                                    \
-	const TreeArgs &a = A[s.tree];                            \
+	__shared__ TreeArgs a_sh_;                                \
+	const TreeArgs &a = a_sh_;                                \
 	const BlockRange g{off[t_], off[t_ + 1] - off[t_]};
+#define DG_BATCH_PROLOGUE                                     \
+	DG_BATCH_HEAD                                             \
+	__shared__ Consts c_sh_;                                  \
+	stage_tree(A[s.tree], a_sh_, &c_sh_);                     \
+	const Consts &cst = c_sh_;
+#define DG_BATCH_PROLOGUE_NC                                  \
+	DG_BATCH_HEAD                                             \
+	stage_tree(A[s.tree], a_sh_, nullptr);
 
 #define DG_BATCH_PARAMS const TreeArgs *A, const SubArgs *SA, const int *off, int nt, const int *on
 
@@ -194,25 +219,25 @@ static __global__ void __launch_bounds__(256) kb_split_check(const TreeArgs *A, 
 template<class M, bool V, class R>
 __global__ void __launch_bounds__(FACE_THREADS, FACE_MIN_BLOCKS) kb_face_sum(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
-	d_face_sum<M, V, R>(g, a.P, *a.C, a.B, a.Ls.clu[s.L], s.n, s.L, s.dtL, s.stamp, a.Ls.recv, a.cnt);
+	d_face_sum<M, V, R>(g, a.P, cst, a.B, a.Ls.clu[s.L], s.n, s.L, s.dtL, s.stamp, a.Ls.recv, a.cnt);
 }
 
 template<class M, class R>
 __global__ void __launch_bounds__(BLOCK) kb_flux_receive(DG_BATCH_PARAMS) {
-	DG_BATCH_PROLOGUE
+	DG_BATCH_PROLOGUE_NC
 	d_flux_receive<M, R>(g, a.P, a.Ls.recv, &a.cnt->n_recv, s.L, a.cnt);
 }
 
 template<class M, bool V>
 __global__ void __launch_bounds__(BLOCK, 3) kb_update(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
-	d_update<M, V>(g, a.P, *a.C, a.Ls.clu[s.L], s.n, s.dtL, s.epoch0 + 1, a.cnt);
+	d_update<M, V>(g, a.P, cst, a.Ls.clu[s.L], s.n, s.dtL, s.epoch0 + 1, a.cnt);
 }
 
 template<class M, bool V>
 __global__ void __launch_bounds__(SLOPE_THREADS, SLOPE_MIN_BLOCKS) kb_slope(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
-	d_slope<M, V>(g, a.P, *a.C, a.B, a.Ls.clu[s.L], s.n, a.limiter, s.epoch0 + 2, a.cnt);
+	d_slope<M, V>(g, a.P, cst, a.B, a.Ls.clu[s.L], s.n, a.limiter, s.epoch0 + 2, a.cnt);
 }
 
 // Multiphase auxiliary stages; `k` selects the stage in the order of Solver::multiphase_aux.
@@ -222,15 +247,15 @@ __global__ void __launch_bounds__(BLOCK) kb_aux(DG_BATCH_PARAMS, int k) {
 	const int e_upd      = s.epoch0 + 1;
 	const int32_t *list = a.Ls.clu[s.L];
 	switch (k) {
-		case 0: d_smooth_alpha<M>(g, a.P, *a.C, a.B, list, s.n, nullptr, a.P.tmp, s.L, s.epoch0 + 3, e_upd, a.cnt); break;
-		case 1: d_smooth_alpha<M>(g, a.P, *a.C, a.B, list, s.n, a.P.tmp, a.P.tmp2, s.L, s.epoch0 + 4, e_upd, a.cnt); break;
+		case 0: d_smooth_alpha<M>(g, a.P, cst, a.B, list, s.n, nullptr, a.P.tmp, s.L, s.epoch0 + 3, e_upd, a.cnt); break;
+		case 1: d_smooth_alpha<M>(g, a.P, cst, a.B, list, s.n, a.P.tmp, a.P.tmp2, s.L, s.epoch0 + 4, e_upd, a.cnt); break;
 		case 2:
-			d_smooth_alpha<M>(g, a.P, *a.C, a.B, list, s.n, a.P.tmp2, a.P.k + (size_t) M::ALPHAS * a.P.cap, s.L, s.epoch0 + 5,
+			d_smooth_alpha<M>(g, a.P, cst, a.B, list, s.n, a.P.tmp2, a.P.k + (size_t) M::ALPHAS * a.P.cap, s.L, s.epoch0 + 5,
 			                  e_upd, a.cnt);
 			break;
-		case 4: d_normal<M>(g, a.P, *a.C, a.B, list, s.n, s.epoch0 + 6, e_upd, a.cnt); break;
-		case 5: d_curvature<M>(g, a.P, *a.C, a.B, list, s.n, a.cnt); break;
-		case 6: d_smooth_kappa<M>(g, a.P, *a.C, a.B, list, s.n, a.cnt); break;
+		case 4: d_normal<M>(g, a.P, cst, a.B, list, s.n, s.epoch0 + 6, e_upd, a.cnt); break;
+		case 5: d_curvature<M>(g, a.P, cst, a.B, list, s.n, a.cnt); break;
+		case 6: d_smooth_kappa<M>(g, a.P, cst, a.B, list, s.n, a.cnt); break;
 		case 7: d_store_tmp(g, a.P, list, s.n, M::KAPPA, a.P.tmp); break;
 		default: d_rec_k<M>(g, a.P, list, s.n); break;
 	}
@@ -244,7 +269,7 @@ constexpr int EPOCH_EST = M::MULTI ? 7 : 3;
 template<class M>
 __global__ void __launch_bounds__(BLOCK) kb_estimate(DG_BATCH_PARAMS) {
 	DG_BATCH_PROLOGUE
-	d_estimate<M>(g, a.P, *a.C, a.Ls.clu[s.L], s.n, s.L, s.counterL, s.epoch0 + EPOCH_EST<M>, a.Ls.split, a.cnt);
+	d_estimate<M>(g, a.P, cst, a.Ls.clu[s.L], s.n, s.L, s.counterL, s.epoch0 + EPOCH_EST<M>, a.Ls.split, a.cnt);
 }
 
 // Regrid and reassignment stages in the order of Solver::substep; `k` selects the stage.
@@ -255,12 +280,12 @@ __global__ void kb_regrid(DG_BATCH_PARAMS, int k) {
 	const int L      = s.L;
 	switch (k) {
 		case 0: d_unsplit_select<M>(g, a.P, a.Ls.clu[L], s.n, L, a.Ls.unsplit, a.cnt); break;
-		case 1: d_split<M>(g, a.P, *a.C, &a.cnt->n_split, a.Ls.split, L, a.Ls.fresh, s.epoch0 + EX + 1, a.cnt); break;
-		case 2: d_unsplit<M>(g, a.P, *a.C, &a.cnt->n_unsplit, a.Ls.unsplit, L, a.Ls.fresh, s.epoch0 + EX + 2, a.cnt); break;
-		case 3: d_nbr_fresh<M>(g, a.P, *a.C, &a.cnt->n_new, a.Ls.fresh, a.Ls.upd, a.cnt); break;
-		case 4: d_nbr_list<M>(g, a.P, *a.C, &a.cnt->n_upd, a.Ls.upd, a.cnt); break;
-		case 5: d_reassign<M>(g, a.P, *a.C, a.Ls.clu[L], nullptr, s.n, L, s.dtL, s.counterL, a.Ls, a.cnt); break;
-		default: d_reassign<M>(g, a.P, *a.C, a.Ls.fresh, &a.cnt->n_new, 0, L, s.dtL, s.counterL, a.Ls, a.cnt); break;
+		case 1: d_split<M>(g, a.P, cst, &a.cnt->n_split, a.Ls.split, L, a.Ls.fresh, s.epoch0 + EX + 1, a.cnt); break;
+		case 2: d_unsplit<M>(g, a.P, cst, &a.cnt->n_unsplit, a.Ls.unsplit, L, a.Ls.fresh, s.epoch0 + EX + 2, a.cnt); break;
+		case 3: d_nbr_fresh<M>(g, a.P, cst, &a.cnt->n_new, a.Ls.fresh, a.Ls.upd, a.cnt); break;
+		case 4: d_nbr_list<M>(g, a.P, cst, &a.cnt->n_upd, a.Ls.upd, a.cnt); break;
+		case 5: d_reassign<M>(g, a.P, cst, a.Ls.clu[L], nullptr, s.n, L, s.dtL, s.counterL, a.Ls, a.cnt); break;
+		default: d_reassign<M>(g, a.P, cst, a.Ls.fresh, &a.cnt->n_new, 0, L, s.dtL, s.counterL, a.Ls, a.cnt); break;
 	}
 }
 
@@ -279,7 +304,7 @@ static __global__ void kb_swap(TreeArgs *A, const SubArgs *SA, int nt, const int
 
 // flush_acti_buffer of level L for the listed trees (impl/acti_utils.hpp:365-372).
 static __global__ void kb_flush(DG_BATCH_PARAMS) {
-	DG_BATCH_PROLOGUE
+	DG_BATCH_PROLOGUE_NC
 	d_flush(g, a.P, a.Ls.buf[s.L], &a.cnt->buf[s.L], a.Ls.clu[s.L], &a.cnt->clu[s.L], s.L, a.cnt);
 }
 
@@ -308,6 +333,8 @@ static __global__ void kb_clear_status(Counters *cnt, int n_trees) {
 }
 
 #undef DG_BATCH_PROLOGUE
+#undef DG_BATCH_PROLOGUE_NC
+#undef DG_BATCH_HEAD
 #undef DG_BATCH_PARAMS
 
 // Stage kinds of a merged substep, each with its own launch budget (blocks per SM) and timing.
