@@ -472,6 +472,8 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
     torch.cuda.synchronize()
     l_sec, l_upd = time.perf_counter() - t0, updates(solvers) - u0
     runs = b.run_stats()
+    l_tree = [s.stats().cell_updates for s in solvers]
+    l_broke = [s.stats().n_global_steps < args.warmup + args.steps for s in solvers]
     # one more step with per-stage device timing: how much of the step the stage kernels fill
     b.set_profiling(True)
     b.stage_times()
@@ -525,6 +527,11 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         step_many(solvers, threads=threads)
     torch.cuda.synchronize()
     m_sec, m_upd = time.perf_counter() - t0, updates(solvers) - u0
+    m_tree = [s.stats().cell_updates for s in solvers]
+    m_broke = [s.stats().n_global_steps < args.warmup + args.steps for s in solvers]
+    # trees that never reached a NaN in either arm: their work is defined, and equal between the arms
+    clean = [k for k in range(len(solvers)) if not l_broke[k] and not m_broke[k]]
+    clean_mismatch = sum(1 for k in clean if l_tree[k] != m_tree[k])
     u0, t0 = updates(solvers), time.perf_counter()
     for s in solvers:
         s.integrate()
@@ -556,6 +563,11 @@ def batched_run(args, rank: int, local_rank: int, world: int) -> dict:
         "step_many": {"value": m_u / (m_ms * 1e-3), "threads": threads, "ms_per_step": m_ms / args.steps},
         "one_tree_at_a_time": {"value": s_u / (s_ms * 1e-3), "steps": 1},
         "speedup_vs_step_many": (l_u / l_ms) / (m_u / m_ms) if m_u > 0 else None,
+        "step_time_ratio_step_many_over_lockstep": m_ms / l_ms if l_ms > 0 else None,
+        "trees_that_broke": {"lockstep": int(sum(l_broke)), "step_many": int(sum(m_broke))},
+        "clean_trees": {"count": len(clean), "cell_update_mismatches": int(clean_mismatch),
+                        "note": "trees with no force_break in either arm; the cell updates of a tree after a NaN "
+                                "are not defined, so arm totals differ by them"},
         "speedup_vs_one_at_a_time": (l_u / l_ms) / (s_u / s_ms) if s_u > 0 else None,
         "active_cells": int(cells),
     }
