@@ -195,6 +195,11 @@ int dg_set_form(dg_solver *s, int form) {
 	return guarded(s, [&] { s->impl->set_form(form); });
 }
 
+int dg_set_options(dg_solver *s, int options) {
+	if (!s || (options & ~(DG_OPT_ORDERED_LISTS | DG_OPT_FACE_TILES))) return DG_ERR_ARG;
+	return guarded(s, [&] { s->impl->set_options(options); });
+}
+
 int dg_set_profiling(dg_solver *s, int on) {
 	if (!s) return DG_ERR_ARG;
 	return guarded(s, [&] { s->impl->set_profiling(on != 0); });

@@ -50,6 +50,7 @@ public:
 	virtual void own_stream() = 0;  // give the solver a stream of its own if it runs on the legacy default
 	virtual void set_profiling(bool on) = 0;
 	virtual void set_form(int form) = 0;
+	virtual void set_options(int opts) = 0;
 	virtual void prepare_noalloc() = 0;  // loads the read-back gather kernel on the current device
 	virtual int model_id() const = 0;
 	std::string last_error;
@@ -90,6 +91,9 @@ class Solver : public SolverBase {
 	double *ff_mem_    = nullptr;  // face fluxes next to receivers (Pool::ff)
 	double *du_mem_    = nullptr;  // face-flux sums of the running cluster (Pool::du)
 	int32_t *pos_mem_  = nullptr;  // list positions of the running cluster's cells (Pool::pos)
+	void *sel_mem_     = nullptr;  // stay marks of the running list and the ordered compaction's temp storage
+	size_t sel_tmp_bytes_ = 0;
+	int opts_          = DG_OPT_DEFAULT;  // stage implementation choices (DG_OPT_*)
 	int32_t *d_leaves_ = nullptr;  // scratch list used at construction
 	double *d_read_    = nullptr;
 	int32_t *d_readlv_ = nullptr;
@@ -167,6 +171,7 @@ class Solver : public SolverBase {
 
 public:
 	void set_profiling(bool on) override { prof_ = on; }
+	void set_options(int opts) override { opts_ = opts; }
 	void set_form(int form) override {
 		if (form != DG_FORM_FP64 && form != DG_FORM_MIXED) throw dg_error(DG_ERR_ARG, "unknown form");
 		mixed_ = form == DG_FORM_MIXED;
@@ -197,6 +202,7 @@ public:
 		cudaFree(bc_mem_);
 		cudaFree(ff_mem_);
 		cudaFree(du_mem_);
+		cudaFree(sel_mem_);
 		cudaFree(pos_mem_);
 		cudaFree(d_cnt_);
 		cudaFreeHost(h_cnt_);
@@ -391,14 +397,25 @@ public:
 		const long long want = std::max(std::max(n, scratch_cap_ + scratch_cap_ / 4), 1024LL);
 		cudaFree(ff_mem_);
 		cudaFree(du_mem_);
+		cudaFree(sel_mem_);
 		ff_mem_      = nullptr;
 		du_mem_      = nullptr;
+		sel_mem_     = nullptr;
 		scratch_cap_ = 0;
 		DG_CUDA(cudaMalloc(&ff_mem_, sizeof(double) * M::F * NF * (size_t) want));
 		DG_CUDA(cudaMalloc(&du_mem_, sizeof(double) * M::F * (size_t) want));
+		// stay marks (one byte per list position, rounded to 256) followed by the temp storage of the
+		// order-keeping compaction of `want` items
+		sel_tmp_bytes_ = 0;
+		DG_CUDA(cub::DeviceSelect::Flagged(nullptr, sel_tmp_bytes_, (const int32_t *) nullptr, (const uint8_t *) nullptr,
+		                                   (int32_t *) nullptr, (int *) nullptr, (int) want, st_));
+		DG_CUDA(cudaMalloc(&sel_mem_, stay_bytes(want) + sel_tmp_bytes_));
 		scratch_cap_ = want;
 		attach_derived();
 	}
+
+	static size_t stay_bytes(long long want) { return ((size_t) want + 255) / 256 * 256; }
+	uint8_t *stay_marks() const { return static_cast<uint8_t *>(sel_mem_); }
 
 	void attach_derived() {
 		P_.ff   = ff_mem_;
@@ -435,8 +452,10 @@ public:
 		sort_bytes_ = 0;
 		cudaFree(ff_mem_);
 		cudaFree(du_mem_);
+		cudaFree(sel_mem_);
 		ff_mem_      = nullptr;
 		du_mem_      = nullptr;
+		sel_mem_     = nullptr;
 		scratch_cap_ = 0;
 		attach_derived();
 		Pool NP{};
@@ -639,6 +658,18 @@ private:
 	// Face-flux sums of the running cluster into du, receivers of slower clusters into Ls_.recv.
 	void launch_face_sum(const int32_t *list, int n, int L, double dtL, int stamp) {
 		constexpr int G = NF <= 4 ? 4 : 8, T = FACE_THREADS;
+		if (opts_ & DG_OPT_FACE_TILES) {
+			constexpr int TC = FaceTile<M>::TC;
+			const int gt = (int) std::max<long long>(1, ((long long) n + TC - 1) / TC);
+			if (mixed_) {
+				if (visc_) k_face_tile<M, true, float><<<gt, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+				else k_face_tile<M, false, float><<<gt, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			} else {
+				if (visc_) k_face_tile<M, true, double><<<gt, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+				else k_face_tile<M, false, double><<<gt, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
+			}
+			return;
+		}
 		const int g = grid_threads((long long) n * G, T);
 		if (mixed_) {
 			if (visc_) k_face_sum<M, true, float><<<g, T, 0, st_>>>(P_, C_, B_, list, n, L, dtL, stamp, Ls_.recv, d_cnt_);
@@ -713,6 +744,7 @@ private:
 				const long long want = growth_target(need, std::max(need + need / 4, (long long) P_.cap * 5 / 4));
 				grow_pool((int) std::min<long long>(want, 2000000000LL));
 				list = Ls_.clu[L];
+				ensure_scratch(n);  // the growth released the list scratch; the reassignment uses its marks
 			}
 		}
 		const int gf = grid_for((long long) n * (NC + 1));
@@ -729,11 +761,21 @@ private:
 		run_k(DG_K_REGRID, 0, [&] {
 			k_nbr_list<M><<<grid_for((long long) n * (NC + 1) * NF), BLOCK, 0, st_>>>(P_, C_, &d_cnt_->n_upd, Ls_.upd, d_cnt_);
 		});
+		const bool ordered = opts_ & DG_OPT_ORDERED_LISTS;
 		run_k(DG_K_REASSIGN, n, [&] {
-			k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_);
+			k_reassign<M><<<g, BLOCK, 0, st_>>>(P_, C_, list, nullptr, n, L, dtL, counterL, Ls_, d_cnt_,
+			                                    ordered ? stay_marks() : nullptr);
+			// the cells that stay at level L, in their list order (the count goes to n_tmp, which the
+			// reassignment of the new cells then appends to)
+			if (ordered) {
+				size_t bytes = sel_tmp_bytes_;
+				DG_CUDA(cub::DeviceSelect::Flagged(stay_marks() + stay_bytes(scratch_cap_), bytes, list, stay_marks(),
+				                                   Ls_.tmp, &d_cnt_->n_tmp, n, st_));
+			}
 		});
 		run_k(DG_K_REASSIGN, 0, [&] {
-			k_reassign<M><<<gf, BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, &d_cnt_->n_new, 0, L, dtL, counterL, Ls_, d_cnt_);
+			k_reassign<M><<<gf, BLOCK, 0, st_>>>(P_, C_, Ls_.fresh, &d_cnt_->n_new, 0, L, dtL, counterL, Ls_, d_cnt_,
+			                                     nullptr);
 		});
 		std::swap(Ls_.clu[L], Ls_.tmp);
 		run_k(DG_K_OTHER, 0, [&] { k_set_count<<<1, 1, 0, st_>>>(&d_cnt_->clu[L], &d_cnt_->n_tmp); });

@@ -500,6 +500,179 @@ __global__ void __launch_bounds__(FACE_THREADS, FACE_MIN_BLOCKS) k_face_sum(Pool
 	d_face_sum<M, V, S>(PlainGrid{}, P, C, B, list, n, L, dtL, stamp, recv, cnt);
 }
 
+// The same face sums over tiles of TC consecutive list positions, one 128-thread block per tile. After
+// the Morton re-sort (and with the order-keeping list rebuild) a tile is a compact patch of cells, and
+// most faces have both cells in it; such a face is evaluated once, by the task of its owner, instead of
+// once by each of its cells. Per tile:
+//   1. every (cell, face) incidence is classified as d_face_sum classifies its lane: boundary, non-leaf
+//      neighbour (the sum over the finer owners), a flux owned by the cell, a flux owned by the
+//      same-level neighbour, or none. A flux owned by the neighbour becomes a reference to the
+//      neighbour's own incidence when the neighbour is in the tile (it then evaluates that face as its
+//      own), else a task of this cell; every other flux is a task;
+//   2. the block's threads run the tasks, interior fluxes first (compacted at the low end of the task
+//      list, boundary and non-leaf sums at the high end, so that warps diverge less), into shared memory;
+//   3. each (cell, component) thread combines the cell's face terms in d_face_sum's fixed pairing order
+//      and writes du.
+// Every flux is the same call with the same arguments as in d_face_sum (the owner's), and the terms are
+// combined in the same order with the same signs, so du is the same bit for bit.
+template<class M>
+struct FaceTile {
+	static constexpr int NF = 2 * M::D, F = M::F;
+	static constexpr int TC0 = 40960 / (NF * F * 8);  // the tile's face results within 40 KB
+	static constexpr int TC  = TC0 >= 128 ? 128 : TC0 >= 64 ? 64 : 32;
+	static constexpr int NI  = TC * NF;  // (cell, face) incidences of a tile
+	static_assert(NI < 32768, "task indices are 16-bit");
+};
+enum : uint8_t { FT_NONE = 0, FT_BND = 1, FT_HANG = 2, FT_INT = 3, FT_INT_FF = 4, FT_REF = 5 };
+
+template<class M, bool V, class S>
+__global__ void __launch_bounds__(FACE_THREADS, FACE_MIN_BLOCKS)
+k_face_tile(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L, double dtL, int stamp, int32_t *recv,
+            Counters *cnt) {
+	using T = FaceTile<M>;
+	constexpr int NF = T::NF, F = T::F, TC = T::TC, NI = T::NI, NSUB = 1 << (M::D - 1);
+	__shared__ double s_res[NI * F];  // face results by incidence
+	__shared__ int32_t s_a[NI];       // owner of a task, or the partner incidence of a reference
+	__shared__ int32_t s_b[NI];       // the task's other cell, boundary id or non-leaf neighbour
+	__shared__ int16_t s_task[NI];
+	__shared__ int32_t s_cell[TC];
+	__shared__ uint8_t s_kind[NI];
+	__shared__ int s_lo, s_hi;
+	const int cap = P.cap;
+	for (int t0 = blockIdx.x * TC; t0 < n; t0 += gridDim.x * TC) {
+		for (int c = threadIdx.x; c < TC; c += blockDim.x) {
+			const int slot = t0 + c;
+			int i          = -1;
+			if (slot < n) {
+				i        = list[slot];
+				P.pos[i] = slot;
+			}
+			s_cell[c] = i;
+		}
+		if (threadIdx.x == 0) s_lo = 0, s_hi = 0;
+		__syncthreads();
+		// 1. classification
+		for (int inc = threadIdx.x; inc < NI; inc += blockDim.x) {
+			const int c = inc / NF, f = inc - c * NF, dir = f & 1;
+			const int i = s_cell[c];
+			uint8_t kind = FT_NONE;
+			int a = 0, b = 0;
+			bool low = true;
+			if (i >= 0) {
+				const int nb = P.nbr[(size_t) f * cap + i];
+				if (nb == 0) {
+					b = P.bc[(size_t) f * cap + i];
+					if (b < 0) set_status(&cnt->status, ST_MISSING_BC);
+					else kind = FT_BND, low = false;
+				} else if (!(P.flags[nb] & F_LEAF)) {
+					kind = FT_HANG, b = nb, low = false;
+				} else {
+					const int li = P.level[i], ai = P.acti[i], ln = P.level[nb], an = P.acti[nb];
+					if (an <= ai && (ln < li || (ln == li && (dir == 1 || an < ai)))) {
+						kind = FT_INT, a = i, b = nb;
+						if (P.clu[nb] != L) {
+							kind = FT_INT_FF;
+							if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
+						}
+					} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
+						const int other = P.nbr[(size_t) (f ^ 1) * cap + nb];
+						const int cn    = __ldcg(P.pos + nb) - t0;
+						if (other == i && cn >= 0 && cn < TC && s_cell[cn] == nb) {
+							kind = FT_REF, a = cn * NF + (f ^ 1);
+						} else {
+							kind = FT_INT, a = nb, b = other;
+						}
+					}
+				}
+			}
+			s_kind[inc] = kind;
+			s_a[inc]    = a;
+			s_b[inc]    = b;
+			if (kind != FT_NONE && kind != FT_REF) {
+				if (low) s_task[atomicAdd(&s_lo, 1)] = (int16_t) inc;
+				else s_task[NI - 1 - atomicAdd(&s_hi, 1)] = (int16_t) inc;
+			}
+		}
+		__syncthreads();
+		// 2. the tasks
+		const int nlo = s_lo, ntask = s_lo + s_hi;
+		for (int k = threadIdx.x; k < ntask; k += blockDim.x) {
+			const int inc = k < nlo ? s_task[k] : s_task[NI - 1 - (k - nlo)];
+			const int c = inc / NF, f = inc - c * NF, dim = f >> 1, dir = f & 1;
+			const int i = s_cell[c];
+			const uint8_t kind = s_kind[inc];
+			double *res = s_res + (size_t) inc * F;
+			if (kind == FT_BND) {
+				double Fb[F];
+				boundary_flux<M, V, S>(P, C, B, i, s_b[inc], dim, dir, dtL, Fb);
+#pragma unroll
+				for (int q = 0; q < F; ++q) res[q] = 0.0 - (double) (S) Fb[q];
+			} else if (kind == FT_HANG) {
+				const int nb = s_b[inc];
+				const int li = P.level[i], ai = P.acti[i];
+				double w[F];
+#pragma unroll
+				for (int q = 0; q < F; ++q) w[q] = 0.0;
+				for (int cc = 1; cc < 1 + NSUB * (NSUB + 1); ++cc) {
+					int dn;
+					bool plus;
+					const int owner = face_owner<M>(P, &cnt->status, i, nb, dim, dir, L, li, ai, cc, true, dn, plus);
+					if (owner < 0) continue;
+					const int fo = 2 * dim + dn;
+					double Fw[F];
+					interior_flux<M, V, S>(P, C, owner, P.nbr[(size_t) fo * cap + owner], dim, dn, dtL, Fw);
+					if (plus) {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] += (double) (S) Fw[q];
+					} else {
+#pragma unroll
+						for (int q = 0; q < F; ++q) w[q] -= (double) (S) Fw[q];
+					}
+				}
+#pragma unroll
+				for (int q = 0; q < F; ++q) res[q] = 0.0 + (double) (S) w[q];
+			} else {
+				const int own = s_a[inc];
+				const int dir_o = own == i ? dir : 1 - dir;
+				double Fi[F];
+				interior_flux<M, V, S>(P, C, own, s_b[inc], dim, dir_o, dtL, Fi);
+#pragma unroll
+				for (int q = 0; q < F; ++q) res[q] = (double) (S) Fi[q];
+				if (kind == FT_INT_FF) {
+					S *dst = face_flux<S>(P, t0 + c, f, F, NF);
+#pragma unroll
+					for (int q = 0; q < F; ++q) dst[q] = (S) Fi[q];
+				}
+			}
+		}
+		__syncthreads();
+		// 3. each cell's face terms in d_face_sum's pairing order
+		for (int idx = threadIdx.x; idx < TC * F; idx += blockDim.x) {
+			const int c = idx / F, q = idx - c * F;
+			if (t0 + c >= n) continue;
+			double fv[NF];
+#pragma unroll
+			for (int k = 0; k < NF; ++k) {
+				const int inc = c * NF + k;
+				const uint8_t kind = s_kind[inc];
+				double v = 0.0;
+				if (kind == FT_BND || kind == FT_HANG) {
+					v = s_res[inc * F + q];
+				} else if (kind != FT_NONE) {
+					const double raw = s_res[(kind == FT_REF ? s_a[inc] : inc) * F + q];
+					v = (k & 1) ? 0.0 - raw : 0.0 + raw;
+				}
+				fv[k] = v;
+			}
+			double sum;
+			if constexpr (NF == 4) sum = (fv[0] + fv[2]) + (fv[1] + fv[3]);
+			else sum = ((fv[0] + fv[4]) + (fv[2] + 0.0)) + ((fv[1] + fv[5]) + (fv[3] + 0.0));
+			P.du[(size_t) (t0 + c) * F + q] = sum;
+		}
+		__syncthreads();
+	}
+}
+
 // cell_update (impl/cell_update.hpp:10-90) of the running cluster, one thread per cell: du = (received
 // fluxes + the face sum of k_face_sum) / volume, the multiphase source from the pre-update state, the
 // EOS recovery, floors and the conservative state. The received-flux accumulator is read (and reset)
@@ -1195,8 +1368,13 @@ __global__ void k_nbr_list(Pool P, Consts C, const int *n_ptr, const int32_t *li
 // ACTI reassignment (impl/adaptive_refinement.hpp:264-322): per-cell CFL decides whether a cell
 // stays, drops one time level (into the buffer of L-1, only when level L is synchronised with L-1)
 // or rises by floor(log2(cfl/max_cfl))+1 levels.
+//
+// `stay` (optional, one byte per list position): instead of appending the cells that stay at level L to
+// the rebuilt list with an atomic counter (which leaves them in the order the warps reach the counter),
+// mark them, so that an order-keeping compaction can rebuild the list in the old list's order. After the
+// Morton re-sort that keeps each cluster list in Morton order through the whole global step.
 template<class M, class Grid>
-__device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL, int counter_L, const Lists &Ls, Counters *cnt) {
+__device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const Consts &C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL, int counter_L, const Lists &Ls, Counters *cnt, uint8_t *stay = nullptr) {
 	const int n   = n_ptr ? *n_ptr : n_host;
 	const int cap = P.cap;
 	for (int tid = g.tid(); tid < n; tid += g.stride()) {
@@ -1207,6 +1385,7 @@ __device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const C
 		P.maxdt[i]       = mdt;
 		double cfl       = dtL / mdt;
 		const uint32_t fl = P.flags[i];
+		if (stay) stay[tid] = 0;
 		if (!(fl & F_LEAF) || (fl & F_GARBAGE)) {
 			P.cfl[i] = cfl;
 			P.clu[i] = CLU_NONE;
@@ -1227,7 +1406,8 @@ __device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const C
 				P.clu[i] = CLU_NONE;
 			}
 		} else {
-			append(Ls.tmp, &cnt->n_tmp, i, cap, &cnt->status);
+			if (stay) stay[tid] = 1;
+			else append(Ls.tmp, &cnt->n_tmp, i, cap, &cnt->status);
 			P.clu[i] = (int8_t) L;
 		}
 		P.cfl[i] = cfl;
@@ -1235,8 +1415,8 @@ __device__ __forceinline__ void d_reassign(const Grid &g, const Pool &P, const C
 }
 template<class M>
 __global__ void k_reassign(Pool P, Consts C, const int32_t *list, const int *n_ptr, int n_host, int L, double dtL,
-                           int counter_L, Lists Ls, Counters *cnt) {
-	d_reassign<M>(PlainGrid{}, P, C, list, n_ptr, n_host, L, dtL, counter_L, Ls, cnt);
+                           int counter_L, Lists Ls, Counters *cnt, uint8_t *stay) {
+	d_reassign<M>(PlainGrid{}, P, C, list, n_ptr, n_host, L, dtL, counter_L, Ls, cnt, stay);
 }
 
 // flush_acti_buffer (impl/acti_utils.hpp:365-372)

@@ -111,6 +111,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     lib.dg_get_stats.argtypes = [vp, ctypes.POINTER(DgStats)]
     lib.dg_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.dg_set_form.argtypes = [vp, ctypes.c_int]
+    lib.dg_set_options.argtypes = [vp, ctypes.c_int]
     lib.dg_last_error.argtypes = [vp]
     lib.dg_last_error.restype = ctypes.c_char_p
     lib.dg_destroy.argtypes = [vp]
@@ -140,7 +141,12 @@ EXPORTED_SYMBOLS = ("dg_set_device", "dg_create", "dg_set_stream", "dg_step", "d
                     "dg_read_cells_noalloc", "dg_get_stats", "dg_batch_create", "dg_batch_step",
                     "dg_batch_last_error", "dg_batch_destroy", "dg_batch_set_launch", "dg_batch_set_profiling",
                     "dg_batch_stage_times", "dg_batch_run_stats", "dg_batch_set_pregrow",
-                    "dg_set_form", "dg_set_profiling", "dg_last_error", "dg_destroy")
+                    "dg_set_form", "dg_set_options", "dg_set_profiling", "dg_last_error", "dg_destroy")
+
+# Stage implementation choices (DG_OPT_* in dacti_gpu.h); every combination gives the same bits.
+OPT_ORDERED_LISTS = 1
+OPT_FACE_TILES = 2
+OPT_DEFAULT = OPT_ORDERED_LISTS | OPT_FACE_TILES
 
 
 class DgError(RuntimeError):
@@ -319,6 +325,10 @@ class Solver:
     def set_form(self, form: str) -> None:
         """'fp64' (the reference's arithmetic) or 'mixed' (FP32 reconstruction and flux, FP64 update)."""
         self._check(self._lib.dg_set_form(self._h, {"fp64": 0, "mixed": 1}[form]))
+
+    def set_options(self, options: int) -> None:
+        """Stage implementation choices: OPT_ORDERED_LISTS, OPT_FACE_TILES (OPT_DEFAULT at creation)."""
+        self._check(self._lib.dg_set_options(self._h, int(options)))
 
     def set_profiling(self, on: bool = True) -> None:
         self._check(self._lib.dg_set_profiling(self._h, 1 if on else 0))

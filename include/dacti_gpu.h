@@ -36,6 +36,14 @@ enum { DG_EULER = 0, DG_NAVIER_STOKES = 1, DG_MULTI = 2 };
  * flux sums, the conservative update, the conservation totals and the pressure/temperature recovery
  * in FP64 */
 enum { DG_FORM_FP64 = 0, DG_FORM_MIXED = 1 };
+/* Stage implementation choices of the single-tree step (dg_set_options). Every combination gives the
+ * same results bit for bit; they differ only in speed.
+ *   DG_OPT_ORDERED_LISTS: the reassignment rebuilds the running cluster's list in its old order (an
+ *     order-keeping compaction), so lists keep the Morton order of the last re-sort through the step;
+ *     without it the cells that stay are appended in the order the GPU reaches them.
+ *   DG_OPT_FACE_TILES: the face sums run over tiles of consecutive list positions and evaluate a face
+ *     whose two cells are both in the tile once instead of once per cell. */
+enum { DG_OPT_ORDERED_LISTS = 1, DG_OPT_FACE_TILES = 2, DG_OPT_DEFAULT = DG_OPT_ORDERED_LISTS | DG_OPT_FACE_TILES };
 
 /* limiter ids (dacti::integrator::slope, integrator/slope_limiters.hpp:7-57) */
 enum { DG_MINMOD = 0, DG_UNLIMITED, DG_VAN_LEER, DG_SUPERBEE, DG_VON_ALBA_2, DG_KOREN, DG_FIRST_ORDER };
@@ -306,6 +314,10 @@ int dg_get_stats(dg_solver *s, dg_stats *out);
 /* Numerical form of the following steps (DG_FORM_FP64 by default). No counterpart in the reference,
  * which computes everything in FP64. */
 int dg_set_form(dg_solver *s, int form);
+
+/* Stage implementation choices (DG_OPT_* bits, DG_OPT_DEFAULT at creation). No counterpart in the
+ * reference. */
+int dg_set_options(dg_solver *s, int options);
 
 /* Per-kernel device timing with CUDA events on the solver's stream (off by default). */
 int dg_set_profiling(dg_solver *s, int on);
