@@ -952,6 +952,12 @@ private:
 		Counters z{};
 		z.top    = new_top;
 		z.status = 0;
+		// the running totals that a batched step keeps on the device carry over (the host copy is current:
+		// gc runs after the step's last read-back)
+		z.n_split_total    = h_cnt_->n_split_total;
+		z.n_unsplit_total  = h_cnt_->n_unsplit_total;
+		z.n_updates_total  = h_cnt_->n_updates_total;
+		z.n_substeps_total = h_cnt_->n_substeps_total;
 		DG_CUDA(cudaMemcpyAsync(d_cnt_, &z, sizeof(Counters), cudaMemcpyHostToDevice, st_));
 		k_collect_active_leaves<<<grid_for(new_top), BLOCK, 0, st_>>>(P_, new_top, Ls_.fresh, &d_cnt_->n_new);
 		DG_CUDA(cudaStreamSynchronize(st_));

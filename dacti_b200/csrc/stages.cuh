@@ -1327,19 +1327,37 @@ __device__ void update_neighbors_subtree(const Pool &P, const Consts &C, uint32_
 
 // Neighbour repair, first pass (impl/adaptive_refinement.hpp:236-249): new children and coarsened
 // parents, then queue their neighbours for the second pass.
-// Each neighbour is queued once with the mask of its faces towards new cells.
+// Each neighbour is queued once with the mask of its faces towards new cells. A group of lanes serves one
+// new cell (4 in 2D, 8 in 3D with 6 busy), lane f repairing face f and queueing the neighbour across it,
+// so the tree walks of a cell's faces run side by side instead of one after another in one thread. New
+// cells are leaves; a non-leaf (which the stages do not produce) is repaired whole by its group's first
+// lane, as Domain::update_neighbors repairs a subtree.
 template<class M, class Grid>
 __device__ __forceinline__ void d_nbr_fresh(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *fresh, int32_t *upd, Counters *cnt) {
-	const int n   = *n_ptr;
-	const int cap = P.cap;
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int i = fresh[tid];
-		update_neighbors_subtree<M>(P, C, &cnt->status, i);
-		for (int f = 0; f < 2 * M::D; ++f) {
-			const int nb = P.nbr[(size_t) f * cap + i];
-			if (nb != 0 && ((P.flags[nb] & F_ACTIVE) || !(P.flags[nb] & F_LEAF))) {
-				if (atomicOr(&P.fmask[nb], 1u << (f ^ 1)) == 0) append(upd, &cnt->n_upd, nb, cap, &cnt->status);
-			}
+	constexpr int NF = 2 * M::D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	const int n      = *n_ptr;
+	const int cap    = P.cap;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	auto queue = [&](int i, int f) {
+		const int nb = P.nbr[(size_t) f * cap + i];
+		if (nb != 0 && ((P.flags[nb] & F_ACTIVE) || !(P.flags[nb] & F_LEAF))) {
+			if (atomicOr(&P.fmask[nb], 1u << (f ^ 1)) == 0) append(upd, &cnt->n_upd, nb, cap, &cnt->status);
+		}
+	};
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot = wbase + lane / G;
+		if (slot >= n || sub >= NF) continue;
+		const int i       = fresh[slot];
+		const uint32_t fl = P.flags[i];
+		if (fl & F_LEAF) {
+			if (fl & F_ACTIVE) update_neighbor_face<M>(P, C, i, sub >> 1, sub & 1);
+			queue(i, sub);
+		} else if (sub == 0) {
+			update_neighbors_subtree<M>(P, C, &cnt->status, i);
+			for (int f = 0; f < NF; ++f) queue(i, f);
 		}
 	}
 }
@@ -1348,16 +1366,24 @@ __global__ void k_nbr_fresh(Pool P, Consts C, const int *n_ptr, const int32_t *f
 	d_nbr_fresh<M>(PlainGrid{}, P, C, n_ptr, fresh, upd, cnt);
 }
 
-// Neighbour repair, second pass: the queued neighbours' faces towards new cells.
+// Neighbour repair, second pass: the queued neighbours' faces towards new cells, one lane per face (the
+// lane groups of the first pass). The group reads the face mask before its first lane clears it.
 template<class M, class Grid>
 __device__ __forceinline__ void d_nbr_list(const Grid &g, const Pool &P, const Consts &C, const int *n_ptr, const int32_t *list, Counters *cnt) {
-	const int n = *n_ptr;
-	for (int tid = g.tid(); tid < n; tid += g.stride()) {
-		const int x       = list[tid];
-		const uint32_t m  = P.fmask[x];
-		for (int f = 0; f < 2 * M::D; ++f)
-			if (m & (1u << f)) update_face_subtree<M>(P, C, &cnt->status, x, f >> 1, f & 1);
-		P.fmask[x] = 0;
+	constexpr int NF = 2 * M::D, G = NF <= 4 ? 4 : 8, GW = 32 / G;
+	const int n      = *n_ptr;
+	const int lane   = threadIdx.x & 31;
+	const int sub    = lane & (G - 1);
+	const int warp   = g.tid() >> 5;
+	const int nwarps = g.stride() >> 5;
+	for (int wbase = warp * GW; wbase < n; wbase += nwarps * GW) {
+		const int slot = wbase + lane / G;
+		const bool act = slot < n && sub < NF;
+		const int x      = act ? list[slot] : 0;
+		const uint32_t m = act ? P.fmask[x] : 0u;
+		__syncwarp();
+		if (act && (m & (1u << sub))) update_face_subtree<M>(P, C, &cnt->status, x, sub >> 1, sub & 1);
+		if (act && sub == 0) P.fmask[x] = 0;
 	}
 }
 template<class M>
