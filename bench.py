@@ -38,6 +38,7 @@ sys.path.insert(0, HERE)
 METRIC = "leaf cell-updates/s at fixed L1 err vs FP64: mixed+batched+learned vs plain GPU"
 UNIT = "cell-updates/s"
 BYTES_PER_UPDATE = {2: 148, 3: 148}  # multi<3>: 16 E + 8 D + 12 with E = 7, D = 3
+NOMINAL_HBM_GBS = 8000.0  # B200 HBM3e datasheet figure, for context beside the measured copy bandwidth
 REF_RUNNER = os.path.join(HERE, "oracle", "_ref", "dacti_ref_runner_fast")
 FALLBACK_HBM_GBS = 6650.0
 
@@ -797,6 +798,7 @@ def bench_gpu(args, rank: int, world: int, local_rank: int) -> None:
         "bound": "hbm", "kernel": "k_update (conservative cell update)", "achieved": achieved,
         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
         "bytes_per_cell_update": b_per, "launches": kl["update"], "avg_launch_us": 1e3 * upd_ms / launches,
+        "frac_of_nominal": achieved / NOMINAL_HBM_GBS, "nominal_gbs": NOMINAL_HBM_GBS,
         "whole_step": {"achieved": step_achieved, "frac": step_achieved / peak},
         "kernel_share": {k: round(v / max(sum(kms.values()), 1e-9), 4) for k, v in kms.items() if v > 0},
         "dominant_kernel_kind_by_time": dom,
