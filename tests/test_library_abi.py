@@ -30,3 +30,12 @@ def test_invalid_arguments_are_rejected_without_a_gpu():
     assert lib.dg_create(None, ctypes.byref(h)) == -1
     assert lib.dg_set_device(-1) == -1
     assert isinstance(lib.dg_last_error(None), bytes)
+
+
+def test_stage_option_constants_mirror_the_header():
+    src = open(os.path.join(ROOT, "include", "dacti_gpu.h")).read()
+    vals = dict((k, int(v)) for k, v in re.findall(r"(DG_OPT_(?:ORDERED_LISTS|FACE_TILES))\s*=\s*(\d+)", src))
+    assert vals == {"DG_OPT_ORDERED_LISTS": solver.OPT_ORDERED_LISTS, "DG_OPT_FACE_TILES": solver.OPT_FACE_TILES}
+    assert solver.OPT_DEFAULT == solver.OPT_ORDERED_LISTS | solver.OPT_FACE_TILES
+    lib = solver.load_library()
+    assert lib.dg_set_options(None, solver.OPT_DEFAULT) == -1
