@@ -575,6 +575,9 @@ k_face_tile(Pool P, Consts C, BcTable B, const int32_t *list, int n, int L, doub
 							if (atomicExch(&P.stamp[nb], stamp) != stamp) append(recv, &cnt->n_recv, nb, cap, &cnt->status);
 						}
 					} else if (ln == li && P.clu[nb] == L && ai <= an && (dir == 0 || ai < an)) {
+						// pos of a cell of this tile was written above, before the barrier; pos of any
+						// other cell may be stale or being written by another block, so only the
+						// s_cell check decides membership
 						const int other = P.nbr[(size_t) (f ^ 1) * cap + nb];
 						const int cn    = __ldcg(P.pos + nb) - t0;
 						if (other == i && cn >= 0 && cn < TC && s_cell[cn] == nb) {
