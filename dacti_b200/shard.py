@@ -18,6 +18,11 @@ Exchange of a level substep, the coupling across rank boundaries of flux_update
 Both transfers are point to point between ranks that share a boundary (torch.distributed send/recv:
 NCCL over NVLink between GPUs, gloo between CPU processes), no collective.
 
+With local time stepping the plans are per ACTI level (build_lts_plans): in the substep of level L only
+the faces owned by level-L leaves carry a flux, under the reference's ownership rule with ACTI levels
+(owns_lts), and a slower leaf across the boundary collects the returned fluxes over several substeps
+before its own update.
+
 This module is the host side of that design: the partition, the plan of which leaves and faces cross
 which rank boundary, and the packing and unpacking of the transfers. The device kernels of the solver
 do not read ghost buffers yet; one tree runs on one GPU.
@@ -192,3 +197,82 @@ def exchange_returns(plan: Plan, fluxes: Dict[int, np.ndarray], width: int) -> D
     sends = {s: fluxes[s] for s, lst in plan.returns_to.items() if lst}
     shapes = {s: (len(lst), width) for s, lst in plan.returns_from.items() if lst}
     return _exchange(sends, shapes, torch.float64)
+
+
+# ------------------------------------------------------------------------------------------------
+# Local time stepping across rank boundaries. With ACTI levels a face is evaluated in the substeps of
+# its owner's level, and the owner is not always the finer or left cell: impl/flux.hpp:52-59 lets cell
+# i evaluate its face towards leaf j when j is not faster (acti_j <= acti_i) and j is coarser, or at the
+# same tree level the face is i's + face or j is slower. A slower cell therefore collects the fluxes
+# of its faster neighbours over several of their substeps before its own update; across a rank
+# boundary those fluxes come back to its rank substep by substep and go into its accumulator in the
+# cell's fixed face order, as on one rank. The exchange plans are per ACTI level: at the substep of
+# level L only the faces owned by level-L cells carry a flux, so only their other cells' records are
+# fetched and only their fluxes are returned.
+# ------------------------------------------------------------------------------------------------
+
+def owns_lts(level: np.ndarray, acti: np.ndarray, i: int, j: int, dir_i: int) -> bool:
+    """Whether leaf i evaluates the flux of its face (direction dir_i) towards leaf j in its own
+    substeps (impl/flux.hpp:52-59). A finer j is never owned from the coarse side."""
+    li, lj, ai, aj = int(level[i]), int(level[j]), int(acti[i]), int(acti[j])
+    return aj <= ai and (lj < li or (lj == li and (dir_i == 1 or aj < ai)))
+
+
+def face_owner_lts(level: np.ndarray, acti: np.ndarray, f: Face, k: int):
+    """(owner, other, dim, owner's direction) of the flux between f.cell and its neighbour k across
+    face f, or None when neither side evaluates it (a quirk of the rule: a coarse cell faster than
+    its finer neighbours leaves their common face without a flux, as the reference does)."""
+    i = f.cell
+    if owns_lts(level, acti, i, k, f.dir):
+        return (i, k, f.dim, f.dir)
+    if owns_lts(level, acti, k, i, 1 - f.dir):
+        return (k, i, f.dim, 1 - f.dir)
+    return None
+
+
+def build_lts_plans(rank_of: np.ndarray, faces: List[List[Face]], level: np.ndarray, acti: np.ndarray,
+                    world: int) -> List[Dict[int, Plan]]:
+    """Per rank, per ACTI level L: the Plan of the substep of level L. ghosts_from[s] lists the leaves
+    of rank s that are the other cell of a face owned by one of this rank's level-L leaves;
+    returns_to[s] lists (owner, dim, owner's dir, receiving leaf) of those faces whose other cell is
+    on rank s. Every rank builds all plans from the same inputs."""
+    levels = sorted(set(int(a) for a in acti))
+    need = {L: [[set() for _ in range(world)] for _ in range(world)] for L in levels}
+    ret = {L: [[[] for _ in range(world)] for _ in range(world)] for L in levels}
+    for fl in faces:
+        for f in fl:
+            for k in f.others:
+                o = face_owner_lts(level, acti, f, k)
+                if o is None or o[0] != f.cell:
+                    continue  # each evaluated face once, from its owner's face list
+                owner, other, dim, d = o
+                L = int(acti[owner])
+                r, s = int(rank_of[owner]), int(rank_of[other])
+                if r != s:
+                    need[L][r][s].add(other)
+                    ret[L][r][s].append((owner, dim, d, other))
+    plans: List[Dict[int, Plan]] = []
+    for r in range(world):
+        per: Dict[int, Plan] = {}
+        for L in levels:
+            per[L] = Plan(
+                r,
+                {s: np.array(sorted(need[L][r][s]), np.int64) for s in range(world) if s != r},
+                {s: np.array(sorted(need[L][s][r]), np.int64) for s in range(world) if s != r},
+                {s: sorted(ret[L][r][s]) for s in range(world) if s != r},
+                {s: sorted(ret[L][s][r]) for s in range(world) if s != r},
+            )
+        plans.append(per)
+    return plans
+
+
+def lts_schedule(max_level: int) -> List[int]:
+    """ACTI levels of the substeps of one global step in the order impl/integrate.hpp:26-67 runs them:
+    the sequence counter steps through 1 .. 2^max_level, and at each value every level L whose period
+    2^(max_level - L) divides it runs, finest first."""
+    out = []
+    for seq in range(1, (1 << max_level) + 1):
+        for L in range(max_level, -1, -1):
+            if seq % (1 << (max_level - L)) == 0:
+                out.append(L)
+    return out
