@@ -276,3 +276,36 @@ def lts_schedule(max_level: int) -> List[int]:
             if seq % (1 << (max_level - L)) == 0:
                 out.append(L)
     return out
+
+
+# ------------------------------------------------------------------------------------------------
+# Reductions over ranks. The step itself needs none (global_dt is fixed at construction); the
+# construction and the diagnostics do.
+# ------------------------------------------------------------------------------------------------
+
+def initial_global_dt(local_max_dt: float, max_dt_cfg: float) -> float:
+    """integrator/integrator.hpp:100-150 over ranks: the largest max_delta_time of any active leaf (a MAX
+    all-reduce, exact in any order), then min(0.9 x that, the configured max_dt)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(local_max_dt)], dtype=torch.float64)
+    if dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return min(0.9 * float(t[0]), float(max_dt_cfg))
+
+
+def rank_ordered_sum(local: np.ndarray) -> np.ndarray:
+    """Sum over ranks of per-rank partial sums (conservation totals, regrid counts): the parts are
+    gathered and added in rank order on every rank, so every rank and every run gets the same bits,
+    which an all-reduce in an order of the library's choosing does not promise."""
+    import torch
+    import torch.distributed as dist
+    x = torch.from_numpy(np.ascontiguousarray(local, dtype=np.float64))
+    if not (dist.is_available() and dist.is_initialized()) or dist.get_world_size() == 1:
+        return x.numpy().copy()
+    parts = [torch.empty_like(x) for _ in range(dist.get_world_size())]
+    dist.all_gather(parts, x)
+    s = np.zeros_like(local, dtype=np.float64)
+    for p in parts:
+        s = s + p.numpy()
+    return s

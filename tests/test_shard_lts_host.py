@@ -27,7 +27,30 @@ def _with_prim_cons(lb):
     dp = ctypes.POINTER(ctypes.c_double)
     lb.ro_prim_from_cons.argtypes = [ctypes.c_void_p, dp, dp]
     lb.ro_cons_from_prim.argtypes = [ctypes.c_void_p, dp, dp]
+    lb.ro_max_delta_time.argtypes = [ctypes.c_void_p, dp]
+    lb.ro_max_delta_time.restype = ctypes.c_double
     return lb
+
+
+MAX_DT_CFG = 1.0
+
+
+def _local_max_dt(lb, m, rec, cells):
+    """The largest Model::max_delta_time over `cells` (integrator/integrator.hpp:113-114)."""
+    dp = ctypes.POINTER(ctypes.c_double)
+    g = -np.inf
+    for j in cells:
+        row = np.ascontiguousarray(rec[j])
+        g = max(g, lb.ro_max_delta_time(ctypes.byref(m), row.ctypes.data_as(dp)))
+    return g
+
+
+def _totals(rec, cells):
+    """Conserved totals sum(u volume) over `cells` in ascending order."""
+    s = np.zeros(4)
+    for j in sorted(cells):
+        s = s + rec[j, 5:9] * (rec[j, 0] * rec[j, 0])
+    return s
 
 
 def _start(lb, m):
@@ -126,6 +149,7 @@ def _rank(rank, world, port, q):
         mine_set = set(mine)
         rec = np.full_like(full, np.nan)
         rec[mine] = full[mine]
+        gdt = shard.initial_global_dt(_local_max_dt(lb, m, rec, mine), MAX_DT_CFG)
         acc = {j: np.zeros(4) for j in mine}
         returned_total, slower_receivers = 0, 0
         for L in shard.lts_schedule(int(acti.max())):
@@ -161,7 +185,8 @@ def _rank(rank, world, port, q):
             for j in mine:
                 acc[j] = acc[j] + terms[j]
             _update(lb, m, rec, acc, [j for j in mine if acti[j] == L], dtL)
-        q.put((rank, {j: rec[j].tobytes() for j in mine}, returned_total, slower_receivers))
+        totals = shard.rank_ordered_sum(_totals(rec, mine))
+        q.put((rank, {j: rec[j].tobytes() for j in mine}, returned_total, slower_receivers, gdt, totals.tobytes()))
     finally:
         dist.destroy_process_group()
 
@@ -190,6 +215,7 @@ def test_two_ranks_reproduce_one_rank_lts_step_bitwise():
     coords, lv, rec, acti = _start(lb, m)
     faces = shard.face_neighbours(coords, lv, 2, (1, 1))
     ref = _one_rank(lb, m, coords, lv, rec.copy(), acti, faces)
+    assert np.isfinite(_local_max_dt(lb, m, rec, range(lv.size)))
     assert np.allclose(ref[:, 1], GLOBAL_DT, rtol=1e-12, atol=0.0)  # every leaf reached the step's end
     assert np.isfinite(ref[:, 5:9]).all() and not np.array_equal(ref[:, 5:9], rec[:, 5:9])
     ctx = mp.get_context("spawn")
@@ -202,9 +228,21 @@ def test_two_ranks_reproduce_one_rank_lts_step_bitwise():
     for p in procs:
         p.join(60)
         assert p.exitcode == 0
+    # the reductions: the initial global dt over ranks equals one rank's; the totals are the per-rank
+    # sums added in rank order, the same bits on both ranks
+    keys = shard.morton_keys(coords, lv, int(lv.max()))
+    rank_of = shard.partition(keys, 2.0 ** acti, 2)
+    one_dt = min(0.9 * _local_max_dt(lb, m, rec, range(lv.size)), MAX_DT_CFG)
+    assert all(r[4] == one_dt for r in res)
+    parts = [_totals(ref, [j for j in range(lv.size) if rank_of[j] == r]) for r in range(2)]
+    want = np.zeros(4)
+    for p in parts:
+        want = want + p
+    assert all(r[5] == want.tobytes() for r in res)
+    assert np.allclose(want, _totals(ref, range(lv.size)), rtol=1e-12, atol=0.0)
     got = {}
-    for _, rows, _, _ in res:
-        got.update(rows)
+    for r in res:
+        got.update(r[1])
     assert sorted(got) == list(range(lv.size))
     assert sum(r[2] for r in res) > 0  # fluxes crossed the rank boundary
     assert sum(r[3] for r in res) > 0  # some went to slower cells, to be summed over several substeps
